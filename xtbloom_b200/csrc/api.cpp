@@ -1,0 +1,635 @@
+// The extern "C" boundary: struct initialisation, validation before any
+// output is touched, context/request/plan lifecycles, thread-local error
+// text, and dispatch into the CUDA engine.  Semantics follow the reference
+// ABI implementation (src/api.cpp:45-1169, runtime/validation.cpp:368-1447):
+// call-level failures modify no output; a SUCCESS return means every
+// per-system diagnostic was committed, failed systems carrying quiet-NaN
+// slices.  Exceptions never cross the boundary.
+#include <cmath>
+#include <cstdlib>
+#include <cstring>
+#include <memory>
+#include <mutex>
+#include <new>
+#include <string>
+
+#include <cuda_runtime.h>
+
+#include "engine.h"
+#include "xtbloom.h"
+
+namespace {
+
+thread_local std::string g_last_error;
+
+xtbloom_status_t fail(xtbloom_status_t st, const std::string& msg) {
+  g_last_error = msg;
+  return st;
+}
+
+template <class T>
+xtbloom_status_t init_struct(T* p, size_t size, size_t v1) {
+  if (p == nullptr) return fail(XTBLOOM_STATUS_INVALID_ARGUMENT, "structure pointer is NULL");
+  if (size < v1) return fail(XTBLOOM_STATUS_INVALID_ARGUMENT, "structure size is smaller than its ABI-v1 prefix");
+  const size_t n = size < sizeof(T) ? size : sizeof(T);
+  std::memset(static_cast<void*>(p), 0, n);
+  p->struct_size = static_cast<uint32_t>(n);
+  p->api_version = XTBLOOM_API_VERSION;
+  return XTBLOOM_STATUS_SUCCESS;
+}
+
+template <class T>
+bool valid_header(const T* p, size_t v1) {
+  return p != nullptr && p->struct_size >= v1 && p->api_version == XTBLOOM_API_VERSION;
+}
+
+bool has_field(uint32_t struct_size, size_t end) { return struct_size >= end; }
+
+bool buffer_active(const xtbloom_const_buffer_t& b) { return b.data != nullptr || b.size_bytes != 0; }
+
+bool check_in(const xtbloom_const_buffer_t& b, size_t need, const char* name, std::string& err) {
+  if (need == 0) return true;
+  if (b.data == nullptr) {
+    err = std::string(name) + " must not be NULL";
+    return false;
+  }
+  if (b.size_bytes < need) {
+    err = std::string(name) + " is smaller than the batch requires";
+    return false;
+  }
+  if (b.memory_space != XTBLOOM_MEMORY_HOST && b.memory_space != XTBLOOM_MEMORY_CUDA_DEVICE) {
+    err = std::string(name) + " uses an unsupported memory space";
+    return false;
+  }
+  if (b.reserved != 0) {
+    err = std::string(name) + " reserved field must be zero";
+    return false;
+  }
+  return true;
+}
+
+bool check_out(const xtbloom_buffer_t& b, size_t need, bool required, const char* name, std::string& err) {
+  if (!required) return true;
+  if (b.data == nullptr) {
+    err = std::string(name) + " output must not be NULL when requested";
+    return false;
+  }
+  if (b.size_bytes < need) {
+    err = std::string(name) + " output is smaller than the batch requires";
+    return false;
+  }
+  if (b.memory_space != XTBLOOM_MEMORY_HOST && b.memory_space != XTBLOOM_MEMORY_CUDA_DEVICE) {
+    err = std::string(name) + " output uses an unsupported memory space";
+    return false;
+  }
+  return true;
+}
+
+}  // namespace
+
+struct xtbloom_context {
+  std::mutex mutex;
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  bool own_stream = false;
+  std::unique_ptr<xtb::Engine> engine;
+};
+
+struct xtbloom_request {
+  xtbloom_context_t* context = nullptr;
+  xtbloom_request_state_t state = XTBLOOM_REQUEST_IDLE;
+  xtbloom_status_t completion = XTBLOOM_STATUS_SUCCESS;
+  uint32_t result_flags = 0;
+  std::string error;
+};
+
+struct xtbloom_plan {
+  xtbloom_context_t* context = nullptr;
+  int64_t batch_size = 0;
+  int64_t total_atoms = 0;
+  uint32_t flags = 0;
+};
+
+struct xtbloom_result_owner {
+  int refs = 1;
+  xtbloom_memory_space_t space = XTBLOOM_MEMORY_HOST;
+  int device = -1;
+  void* data = nullptr;
+  uint64_t bytes = 0;
+};
+
+namespace {
+
+xtbloom_status_t validate_and_normalise(const xtbloom_batch_t* batch,
+                                        const xtbloom_compute_options_t* options,
+                                        const xtbloom_batch_result_t* result, xtb::ComputeRequest& req,
+                                        std::string& err) {
+  if (!valid_header(batch, XTBLOOM_BATCH_V1_SIZE)) {
+    err = "batch is NULL, too small, or uses an unsupported API version";
+    return XTBLOOM_STATUS_INVALID_ARGUMENT;
+  }
+  if (!valid_header(options, XTBLOOM_COMPUTE_OPTIONS_V1_SIZE)) {
+    err = "compute options are NULL, too small, or use an unsupported API version";
+    return XTBLOOM_STATUS_INVALID_ARGUMENT;
+  }
+  if (!valid_header(result, XTBLOOM_BATCH_RESULT_V1_SIZE)) {
+    err = "batch result is NULL, too small, or uses an unsupported API version";
+    return XTBLOOM_STATUS_INVALID_ARGUMENT;
+  }
+  if (batch->batch_size <= 0) {
+    err = "batch_size must be positive";
+    return XTBLOOM_STATUS_INVALID_ARGUMENT;
+  }
+  if (batch->total_atoms < batch->batch_size) {
+    err = "total_atoms must permit at least one atom in every batch item";
+    return XTBLOOM_STATUS_INVALID_ARGUMENT;
+  }
+  if (batch->total_point_charges < 0 || batch->total_charge_response_elements < 0) {
+    err = "point-charge and response counts must be nonnegative";
+    return XTBLOOM_STATUS_INVALID_ARGUMENT;
+  }
+  const size_t B = static_cast<size_t>(batch->batch_size);
+  const size_t N = static_cast<size_t>(batch->total_atoms);
+  if (!check_in(batch->atom_offsets, (B + 1) * 8, "atom_offsets", err) ||
+      !check_in(batch->atomic_numbers, N * 4, "atomic_numbers", err) ||
+      !check_in(batch->positions, N * 24, "positions", err) ||
+      !check_in(batch->molecular_charges, B * 8, "molecular_charges", err)) {
+    return XTBLOOM_STATUS_INVALID_ARGUMENT;
+  }
+  if (buffer_active(batch->unpaired_electrons) &&
+      !check_in(batch->unpaired_electrons, B * 4, "unpaired_electrons", err)) {
+    return XTBLOOM_STATUS_INVALID_ARGUMENT;
+  }
+  if (has_field(batch->struct_size, XTBLOOM_BATCH_V2_SIZE) && buffer_active(batch->spin_channels)) {
+    if (!check_in(batch->spin_channels, B * 4, "spin_channels", err)) return XTBLOOM_STATUS_INVALID_ARGUMENT;
+    std::unique_ptr<int32_t[]> sc(new int32_t[B]);
+    if (batch->spin_channels.memory_space == XTBLOOM_MEMORY_HOST) {
+      std::memcpy(sc.get(), batch->spin_channels.data, B * 4);
+    } else if (cudaMemcpy(sc.get(), batch->spin_channels.data, B * 4, cudaMemcpyDeviceToHost) != cudaSuccess) {
+      err = "failed to read spin_channels";
+      return XTBLOOM_STATUS_INVALID_ARGUMENT;
+    }
+    for (size_t i = 0; i < B; ++i) {
+      if (sc[i] != 1 && sc[i] != 2) {
+        err = "spin_channels values must be one or two";
+        return XTBLOOM_STATUS_INVALID_ARGUMENT;
+      }
+      if (sc[i] == 2) {
+        err = "unrestricted (two-channel) systems are not supported by this CUDA path";
+        return XTBLOOM_STATUS_NOT_SUPPORTED;
+      }
+    }
+  }
+  if (batch->total_point_charges != 0 || buffer_active(batch->point_charge_offsets)) {
+    err = "external point charges are not implemented in this CUDA path";
+    return XTBLOOM_STATUS_NOT_IMPLEMENTED;
+  }
+  if (batch->total_charge_response_elements != 0 || buffer_active(batch->atomic_potential_shifts) ||
+      buffer_active(batch->charge_response_offsets) || buffer_active(batch->charge_response_matrix)) {
+    err = "periodic charge-response embedding is not implemented in this CUDA path";
+    return XTBLOOM_STATUS_NOT_IMPLEMENTED;
+  }
+  if (has_field(batch->struct_size, XTBLOOM_BATCH_V3_SIZE) &&
+      (batch->total_interactions != 0 || buffer_active(batch->interaction_descriptors))) {
+    err = "external interaction attachments are not implemented in this CUDA path";
+    return XTBLOOM_STATUS_NOT_IMPLEMENTED;
+  }
+  if (has_field(batch->struct_size, XTBLOOM_BATCH_V4_SIZE) &&
+      (buffer_active(batch->cell_matrices) || buffer_active(batch->periodic_axes))) {
+    err = "native periodic cells are not implemented";
+    return XTBLOOM_STATUS_NOT_IMPLEMENTED;
+  }
+  // options
+  if (options->model != XTBLOOM_MODEL_GFN2_XTB && options->model != XTBLOOM_MODEL_GFN1_XTB) {
+    err = "unknown model";
+    return XTBLOOM_STATUS_INVALID_ARGUMENT;
+  }
+  if (options->model == XTBLOOM_MODEL_GFN1_XTB) {
+    err = "GFN1-xTB is not implemented in this CUDA path";
+    return XTBLOOM_STATUS_NOT_IMPLEMENTED;
+  }
+  const uint32_t known = XTBLOOM_COMPUTE_ENERGY | XTBLOOM_COMPUTE_FORCES |
+                         XTBLOOM_COMPUTE_ATOMIC_CHARGES | XTBLOOM_COMPUTE_POINT_CHARGE_FORCES |
+                         XTBLOOM_COMPUTE_DIPOLE_MOMENTS;
+  if ((options->flags & ~known) != 0 || options->reserved != 0) {
+    err = "compute flags contain reserved bits";
+    return XTBLOOM_STATUS_INVALID_ARGUMENT;
+  }
+  if (options->flags & XTBLOOM_COMPUTE_POINT_CHARGE_FORCES) {
+    err = "point-charge forces were requested without point charges";
+    return XTBLOOM_STATUS_INVALID_ARGUMENT;
+  }
+  if (options->flags & XTBLOOM_COMPUTE_DIPOLE_MOMENTS) {
+    err = "dipole moments are not implemented in this CUDA path";
+    return XTBLOOM_STATUS_NOT_IMPLEMENTED;
+  }
+  if (options->max_scc_iterations <= 0) {
+    err = "max_scc_iterations must be positive";
+    return XTBLOOM_STATUS_INVALID_ARGUMENT;
+  }
+  if (!(options->charge_tolerance > 0.0) || !std::isfinite(options->charge_tolerance) ||
+      !(options->energy_tolerance > 0.0) || !std::isfinite(options->energy_tolerance) ||
+      !(options->electronic_temperature >= 0.0) || !std::isfinite(options->electronic_temperature)) {
+    err = "tolerances must be finite and positive and the electronic temperature finite and nonnegative";
+    return XTBLOOM_STATUS_INVALID_ARGUMENT;
+  }
+  req.flags = options->flags;
+  req.max_iter = options->max_scc_iterations;
+  req.ctol = options->charge_tolerance;
+  req.etol = options->energy_tolerance;
+  req.kt = options->electronic_temperature;
+  req.memory = 8;
+  req.damping = 0.4;
+  if (has_field(options->struct_size, XTBLOOM_COMPUTE_OPTIONS_V2_SIZE)) {
+    if (options->scc_start_mode == XTBLOOM_SCC_START_WARM) {
+      err = "WARM start requires a converged compatible checkpoint; none is retained";
+      return XTBLOOM_STATUS_INVALID_ARGUMENT;
+    }
+    if (options->scc_start_mode != XTBLOOM_SCC_START_FRESH && options->scc_start_mode != 0) {
+      err = "unknown SCC start mode";
+      return XTBLOOM_STATUS_INVALID_ARGUMENT;
+    }
+  }
+  if (has_field(options->struct_size, XTBLOOM_COMPUTE_OPTIONS_V3_SIZE)) {
+    if (options->scc_mixer != XTBLOOM_SCC_MIXER_MODIFIED_BROYDEN || options->scc_mixer_history < 1 ||
+        options->scc_mixer_history > 64 || !(options->scc_mixer_damping > 0.0) ||
+        !(options->scc_mixer_damping <= 1.0) ||
+        (options->determinism != XTBLOOM_DETERMINISM_DEFAULT &&
+         options->determinism != XTBLOOM_DETERMINISM_REPRODUCIBLE)) {
+      err = "invalid SCC mixer or determinism settings";
+      return XTBLOOM_STATUS_INVALID_ARGUMENT;
+    }
+    if (options->scc_mixer_history > 8) {
+      err = "Broyden history deeper than 8 is not supported by this CUDA path";
+      return XTBLOOM_STATUS_NOT_SUPPORTED;
+    }
+    req.memory = options->scc_mixer_history;
+    req.damping = options->scc_mixer_damping;
+  }
+  // result buffers
+  const uint32_t f = options->flags;
+  if (!check_out(result->energies, B * 8, (f & XTBLOOM_COMPUTE_ENERGY) != 0, "energies", err) ||
+      !check_out(result->forces, N * 24, (f & XTBLOOM_COMPUTE_FORCES) != 0, "forces", err) ||
+      !check_out(result->atomic_charges, N * 8, (f & XTBLOOM_COMPUTE_ATOMIC_CHARGES) != 0,
+                 "atomic_charges", err) ||
+      !check_out(result->scc_iterations, B * 4, true, "scc_iterations", err) ||
+      !check_out(result->scc_converged, B, true, "scc_converged", err) ||
+      !check_out(result->per_system_status, B * 4, true, "per_system_status", err)) {
+    return XTBLOOM_STATUS_INVALID_ARGUMENT;
+  }
+  // positions must be finite (host check; device inputs are checked after staging)
+  if (batch->positions.memory_space == XTBLOOM_MEMORY_HOST) {
+    const double* x = static_cast<const double*>(batch->positions.data);
+    for (size_t i = 0; i < 3 * N; ++i) {
+      if (!std::isfinite(x[i])) {
+        err = "positions contain NaN or infinity";
+        return XTBLOOM_STATUS_INVALID_ARGUMENT;
+      }
+    }
+  }
+  req.batch = batch;
+  req.options = options;
+  req.result = result;
+  return XTBLOOM_STATUS_SUCCESS;
+}
+
+xtbloom_status_t run(xtbloom_context_t* ctx, const xtbloom_batch_t* batch,
+                     const xtbloom_compute_options_t* options, const xtbloom_batch_result_t* result,
+                     uint32_t* result_flags) {
+  if (ctx == nullptr) return fail(XTBLOOM_STATUS_INVALID_ARGUMENT, "context is NULL");
+  xtb::ComputeRequest req;
+  std::string err;
+  xtbloom_status_t st = validate_and_normalise(batch, options, result, req, err);
+  if (st != XTBLOOM_STATUS_SUCCESS) return fail(st, err);
+  std::lock_guard<std::mutex> lock(ctx->mutex);
+  int prev = 0;
+  cudaGetDevice(&prev);
+  try {
+    st = ctx->engine->compute(req, err);
+  } catch (const std::bad_alloc&) {
+    st = XTBLOOM_STATUS_ALLOCATION_FAILED;
+    err = "host allocation failed";
+  } catch (...) {
+    st = XTBLOOM_STATUS_INTERNAL_ERROR;
+    err = "unexpected exception in the CUDA engine";
+  }
+  cudaSetDevice(prev);
+  if (result_flags) *result_flags = 0;
+  if (st != XTBLOOM_STATUS_SUCCESS) return fail(st, err);
+  g_last_error.clear();
+  return XTBLOOM_STATUS_SUCCESS;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* xtbloom_version_string(void) { return "0.1.0+b200"; }
+
+const char* xtbloom_status_string(xtbloom_status_t status) {
+  switch (status) {
+    case XTBLOOM_STATUS_SUCCESS: return "success";
+    case XTBLOOM_STATUS_INVALID_ARGUMENT: return "invalid argument";
+    case XTBLOOM_STATUS_BACKEND_UNAVAILABLE: return "backend unavailable";
+    case XTBLOOM_STATUS_NOT_SUPPORTED: return "not supported";
+    case XTBLOOM_STATUS_ALLOCATION_FAILED: return "allocation failed";
+    case XTBLOOM_STATUS_NOT_IMPLEMENTED: return "not implemented";
+    case XTBLOOM_STATUS_INTERNAL_ERROR: return "internal error";
+    case XTBLOOM_STATUS_SCC_NOT_CONVERGED: return "SCC not converged";
+    case XTBLOOM_STATUS_EIGENSOLVER_FAILED: return "eigensolver failed";
+  }
+  return "unknown status";
+}
+
+const char* xtbloom_get_last_error(void) { return g_last_error.c_str(); }
+
+xtbloom_status_t xtbloom_context_options_init(xtbloom_context_options_t* o, size_t size) {
+  const xtbloom_status_t st = init_struct(o, size, XTBLOOM_CONTEXT_OPTIONS_V1_SIZE);
+  if (st != XTBLOOM_STATUS_SUCCESS) return st;
+  o->backend = XTBLOOM_BACKEND_AUTO;
+  o->device_id = -1;
+  return XTBLOOM_STATUS_SUCCESS;
+}
+
+xtbloom_status_t xtbloom_batch_init(xtbloom_batch_t* b, size_t size) {
+  return init_struct(b, size, XTBLOOM_BATCH_V1_SIZE);
+}
+
+xtbloom_status_t xtbloom_compute_options_init(xtbloom_compute_options_t* o, size_t size) {
+  const xtbloom_status_t st = init_struct(o, size, XTBLOOM_COMPUTE_OPTIONS_V1_SIZE);
+  if (st != XTBLOOM_STATUS_SUCCESS) return st;
+  o->model = XTBLOOM_MODEL_GFN2_XTB;
+  o->flags = XTBLOOM_COMPUTE_ENERGY | XTBLOOM_COMPUTE_FORCES;
+  o->max_scc_iterations = 250;
+  o->charge_tolerance = 1.0e-6;
+  o->energy_tolerance = 1.0e-8;
+  o->electronic_temperature = XTBLOOM_DEFAULT_ELECTRONIC_TEMPERATURE;
+  if (size >= XTBLOOM_COMPUTE_OPTIONS_V2_SIZE) o->scc_start_mode = XTBLOOM_SCC_START_FRESH;
+  if (size >= XTBLOOM_COMPUTE_OPTIONS_V3_SIZE) {
+    o->scc_mixer = XTBLOOM_SCC_MIXER_MODIFIED_BROYDEN;
+    o->scc_mixer_history = 8;
+    o->scc_mixer_damping = 0.4;
+    o->determinism = XTBLOOM_DETERMINISM_DEFAULT;
+  }
+  return XTBLOOM_STATUS_SUCCESS;
+}
+
+xtbloom_status_t xtbloom_batch_result_init(xtbloom_batch_result_t* r, size_t size) {
+  return init_struct(r, size, XTBLOOM_BATCH_RESULT_V1_SIZE);
+}
+
+xtbloom_status_t xtbloom_workspace_query_init(xtbloom_workspace_query_t* q, size_t size) {
+  return init_struct(q, size, offsetof(xtbloom_workspace_query_t, reserved_v2) + sizeof(uint32_t));
+}
+
+xtbloom_status_t xtbloom_request_info_init(xtbloom_request_info_t* i, size_t size) {
+  return init_struct(i, size, offsetof(xtbloom_request_info_t, reserved) + sizeof(uint32_t));
+}
+
+xtbloom_status_t xtbloom_context_create(const xtbloom_context_options_t* options,
+                                        xtbloom_context_t** context) {
+  if (context == nullptr) return fail(XTBLOOM_STATUS_INVALID_ARGUMENT, "context output pointer is NULL");
+  *context = nullptr;
+  if (!valid_header(options, XTBLOOM_CONTEXT_OPTIONS_V1_SIZE))
+    return fail(XTBLOOM_STATUS_INVALID_ARGUMENT,
+                "context options are NULL, too small, or use an unsupported API version");
+  if (options->reserved != 0) return fail(XTBLOOM_STATUS_INVALID_ARGUMENT, "context options reserved field must be zero");
+  if (options->backend == XTBLOOM_BACKEND_CPU || options->backend == XTBLOOM_BACKEND_ROCM)
+    return fail(XTBLOOM_STATUS_BACKEND_UNAVAILABLE, "this library implements the CUDA backend only");
+  if (options->backend != XTBLOOM_BACKEND_AUTO && options->backend != XTBLOOM_BACKEND_CUDA)
+    return fail(XTBLOOM_STATUS_INVALID_ARGUMENT, "unknown backend");
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev <= 0) {
+    cudaGetLastError();
+    return fail(XTBLOOM_STATUS_BACKEND_UNAVAILABLE, "no CUDA device is available");
+  }
+  int dev = options->device_id;
+  if (dev < 0) {
+    if (cudaGetDevice(&dev) != cudaSuccess) dev = 0;
+  }
+  if (dev >= ndev) return fail(XTBLOOM_STATUS_INVALID_ARGUMENT, "device_id is out of range");
+  cudaDeviceProp prop{};
+  cudaGetDeviceProperties(&prop, dev);
+  if (prop.major != 10) return fail(XTBLOOM_STATUS_BACKEND_UNAVAILABLE, "this library is built for sm_100a (B200) devices only");
+  try {
+    auto* ctx = new xtbloom_context;
+    int prev = 0;
+    cudaGetDevice(&prev);
+    cudaSetDevice(dev);
+    ctx->device = dev;
+    if (options->stream != nullptr) {
+      ctx->stream = static_cast<cudaStream_t>(options->stream);
+    } else {
+      cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking);
+      ctx->own_stream = true;
+    }
+    ctx->engine.reset(new xtb::Engine(dev, ctx->stream));
+    cudaSetDevice(prev);
+    *context = ctx;
+    g_last_error.clear();
+    return XTBLOOM_STATUS_SUCCESS;
+  } catch (...) {
+    return fail(XTBLOOM_STATUS_ALLOCATION_FAILED, "failed to create the context");
+  }
+}
+
+void xtbloom_context_destroy(xtbloom_context_t* context) {
+  if (context == nullptr) return;
+  int prev = 0;
+  cudaGetDevice(&prev);
+  cudaSetDevice(context->device);
+  context->engine.reset();
+  if (context->own_stream && context->stream) cudaStreamDestroy(context->stream);
+  cudaSetDevice(prev);
+  delete context;
+}
+
+xtbloom_backend_t xtbloom_context_get_backend(const xtbloom_context_t* context) {
+  return context == nullptr ? XTBLOOM_BACKEND_AUTO : XTBLOOM_BACKEND_CUDA;
+}
+
+int32_t xtbloom_context_get_device_id(const xtbloom_context_t* context) {
+  return context == nullptr ? -1 : context->device;
+}
+
+xtbloom_status_t xtbloom_compute(xtbloom_context_t* context, const xtbloom_batch_t* batch,
+                                 const xtbloom_compute_options_t* options,
+                                 xtbloom_batch_result_t* result) {
+  uint32_t flags = 0;
+  const xtbloom_status_t st = run(context, batch, options, result, &flags);
+  if (st == XTBLOOM_STATUS_SUCCESS && result != nullptr) result->flags = flags;
+  return st;
+}
+
+xtbloom_status_t xtbloom_request_create(xtbloom_context_t* context, xtbloom_request_t** request) {
+  if (context == nullptr || request == nullptr) return fail(XTBLOOM_STATUS_INVALID_ARGUMENT, "NULL argument");
+  auto* r = new (std::nothrow) xtbloom_request;
+  if (r == nullptr) return fail(XTBLOOM_STATUS_ALLOCATION_FAILED, "failed to allocate a request");
+  r->context = context;
+  *request = r;
+  return XTBLOOM_STATUS_SUCCESS;
+}
+
+// The submission completes before enqueue returns; the request records the
+// outcome exactly as an asynchronous completion would.
+xtbloom_status_t xtbloom_compute_enqueue(xtbloom_context_t* context, const xtbloom_batch_t* batch,
+                                         const xtbloom_compute_options_t* options,
+                                         const xtbloom_batch_result_t* result,
+                                         xtbloom_request_t* request) {
+  if (request == nullptr || request->context != context)
+    return fail(XTBLOOM_STATUS_INVALID_ARGUMENT, "request is NULL or bound to another context");
+  if (request->state == XTBLOOM_REQUEST_PENDING)
+    return fail(XTBLOOM_STATUS_INVALID_ARGUMENT, "request already has pending work");
+  uint32_t flags = 0;
+  const xtbloom_status_t st = run(context, batch, options, result, &flags);
+  if (st == XTBLOOM_STATUS_INVALID_ARGUMENT || st == XTBLOOM_STATUS_NOT_IMPLEMENTED ||
+      st == XTBLOOM_STATUS_NOT_SUPPORTED) {
+    return st;   // rejected before acceptance
+  }
+  request->state = XTBLOOM_REQUEST_COMPLETE;
+  request->completion = st;
+  request->result_flags = flags;
+  request->error = st == XTBLOOM_STATUS_SUCCESS ? std::string() : g_last_error;
+  return XTBLOOM_STATUS_SUCCESS;
+}
+
+xtbloom_status_t xtbloom_request_query(xtbloom_request_t* request, xtbloom_request_info_t* info) {
+  if (request == nullptr || !valid_header(info, offsetof(xtbloom_request_info_t, reserved) + sizeof(uint32_t)))
+    return fail(XTBLOOM_STATUS_INVALID_ARGUMENT, "invalid request or info");
+  info->state = request->state;
+  info->completion_status = request->completion;
+  info->result_flags = request->result_flags;
+  return XTBLOOM_STATUS_SUCCESS;
+}
+
+xtbloom_status_t xtbloom_request_wait(xtbloom_request_t* request, xtbloom_request_info_t* info) {
+  return xtbloom_request_query(request, info);
+}
+
+const char* xtbloom_request_get_error(const xtbloom_request_t* request) {
+  return request == nullptr ? "" : request->error.c_str();
+}
+
+void xtbloom_request_destroy(xtbloom_request_t* request) { delete request; }
+
+xtbloom_status_t xtbloom_plan_create(xtbloom_context_t* context, const xtbloom_batch_t* batch,
+                                     const xtbloom_compute_options_t* options, xtbloom_plan_t** plan) {
+  if (context == nullptr || plan == nullptr) return fail(XTBLOOM_STATUS_INVALID_ARGUMENT, "NULL argument");
+  if (!valid_header(batch, XTBLOOM_BATCH_V1_SIZE) || !valid_header(options, XTBLOOM_COMPUTE_OPTIONS_V1_SIZE))
+    return fail(XTBLOOM_STATUS_INVALID_ARGUMENT, "invalid batch or options");
+  auto* p = new (std::nothrow) xtbloom_plan;
+  if (p == nullptr) return fail(XTBLOOM_STATUS_ALLOCATION_FAILED, "failed to allocate a plan");
+  p->context = context;
+  p->batch_size = batch->batch_size;
+  p->total_atoms = batch->total_atoms;
+  p->flags = options->flags;
+  *plan = p;
+  return XTBLOOM_STATUS_SUCCESS;
+}
+
+void xtbloom_plan_destroy(xtbloom_plan_t* plan) { delete plan; }
+
+xtbloom_status_t xtbloom_plan_query_workspace(const xtbloom_plan_t* plan, xtbloom_workspace_query_t* q) {
+  if (plan == nullptr || q == nullptr) return fail(XTBLOOM_STATUS_INVALID_ARGUMENT, "NULL argument");
+  if (q->compute_flags != plan->flags)
+    return fail(XTBLOOM_STATUS_INVALID_ARGUMENT, "compute_flags must equal the plan's flags");
+  // device workspace is dominated by about 20 packed n x n FP64 matrices
+  q->host_required_bytes = 0;
+  q->host_required_alignment = 1;
+  q->device_required_bytes = 0;
+  q->device_required_alignment = 256;
+  return XTBLOOM_STATUS_SUCCESS;
+}
+
+xtbloom_status_t xtbloom_plan_compute(xtbloom_plan_t* plan, const xtbloom_batch_t* batch,
+                                      const xtbloom_compute_options_t* options,
+                                      xtbloom_batch_result_t* result) {
+  if (plan == nullptr) return fail(XTBLOOM_STATUS_INVALID_ARGUMENT, "plan is NULL");
+  if (batch == nullptr || batch->batch_size != plan->batch_size || batch->total_atoms != plan->total_atoms)
+    return fail(XTBLOOM_STATUS_INVALID_ARGUMENT, "batch topology differs from the plan");
+  return xtbloom_compute(plan->context, batch, options, result);
+}
+
+xtbloom_status_t xtbloom_plan_compute_enqueue(xtbloom_plan_t* plan, const xtbloom_batch_t* batch,
+                                              const xtbloom_compute_options_t* options,
+                                              const xtbloom_batch_result_t* result,
+                                              xtbloom_request_t* request) {
+  if (plan == nullptr) return fail(XTBLOOM_STATUS_INVALID_ARGUMENT, "plan is NULL");
+  if (batch == nullptr || batch->batch_size != plan->batch_size || batch->total_atoms != plan->total_atoms)
+    return fail(XTBLOOM_STATUS_INVALID_ARGUMENT, "batch topology differs from the plan");
+  return xtbloom_compute_enqueue(plan->context, batch, options, result, request);
+}
+
+xtbloom_status_t xtbloom_result_owner_options_init(xtbloom_result_owner_options_t* o, size_t size) {
+  const xtbloom_status_t st = init_struct(o, size, offsetof(xtbloom_result_owner_options_t, reserved) + 4);
+  if (st == XTBLOOM_STATUS_SUCCESS) o->device_id = -1;
+  return st;
+}
+
+xtbloom_status_t xtbloom_result_owner_create(const xtbloom_result_owner_options_t* o,
+                                             xtbloom_result_owner_t** owner) {
+  if (owner == nullptr || !valid_header(o, offsetof(xtbloom_result_owner_options_t, reserved) + 4) ||
+      o->size_bytes == 0 || o->reserved != 0)
+    return fail(XTBLOOM_STATUS_INVALID_ARGUMENT, "invalid result owner options");
+  auto* r = new (std::nothrow) xtbloom_result_owner;
+  if (r == nullptr) return fail(XTBLOOM_STATUS_ALLOCATION_FAILED, "allocation failed");
+  r->space = o->memory_space;
+  r->bytes = o->size_bytes;
+  if (o->memory_space == XTBLOOM_MEMORY_HOST) {
+    r->data = std::malloc(o->size_bytes);
+  } else if (o->memory_space == XTBLOOM_MEMORY_CUDA_DEVICE) {
+    int prev = 0;
+    cudaGetDevice(&prev);
+    cudaSetDevice(o->device_id < 0 ? 0 : o->device_id);
+    if (cudaMalloc(&r->data, o->size_bytes) != cudaSuccess) r->data = nullptr;
+    cudaSetDevice(prev);
+    r->device = o->device_id;
+  } else {
+    delete r;
+    return fail(XTBLOOM_STATUS_INVALID_ARGUMENT, "unsupported memory space");
+  }
+  if (r->data == nullptr) {
+    delete r;
+    return fail(XTBLOOM_STATUS_ALLOCATION_FAILED, "arena allocation failed");
+  }
+  *owner = r;
+  return XTBLOOM_STATUS_SUCCESS;
+}
+
+xtbloom_status_t xtbloom_result_owner_buffer(const xtbloom_result_owner_t* owner, xtbloom_buffer_t* b) {
+  if (owner == nullptr || b == nullptr) return fail(XTBLOOM_STATUS_INVALID_ARGUMENT, "NULL argument");
+  b->data = owner->data;
+  b->size_bytes = owner->bytes;
+  b->memory_space = owner->space;
+  b->reserved = 0;
+  return XTBLOOM_STATUS_SUCCESS;
+}
+
+void xtbloom_result_owner_retain(xtbloom_result_owner_t* owner) {
+  if (owner) ++owner->refs;
+}
+
+void xtbloom_result_owner_release(xtbloom_result_owner_t* owner) {
+  if (owner == nullptr || --owner->refs > 0) return;
+  if (owner->space == XTBLOOM_MEMORY_HOST) std::free(owner->data);
+  else cudaFree(owner->data);
+  delete owner;
+}
+
+xtbloom_status_t xtbloom_result_owner_export_dltensor(const xtbloom_result_owner_t*,
+                                                      const xtbloom_dlpack_view_t*, int, void**) {
+  return fail(XTBLOOM_STATUS_NOT_IMPLEMENTED, "DLPack export is not implemented in this release");
+}
+
+xtbloom_status_t xtbloom_b200_debug_fetch(xtbloom_context_t* context, const char* name, int64_t system,
+                                          double* out, size_t capacity, size_t* count) {
+  if (context == nullptr || name == nullptr || out == nullptr || count == nullptr)
+    return fail(XTBLOOM_STATUS_INVALID_ARGUMENT, "NULL argument");
+  std::lock_guard<std::mutex> lock(context->mutex);
+  std::string err;
+  const xtbloom_status_t st = context->engine->debug_fetch(name, system, out, capacity, count, err);
+  if (st != XTBLOOM_STATUS_SUCCESS) return fail(st, err);
+  return st;
+}
+
+}  // extern "C"

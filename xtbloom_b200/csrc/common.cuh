@@ -1,0 +1,149 @@
+// Shared device-side definitions of the xtbloom_b200 CUDA path.
+//
+// Data layout in HBM (all FP64 unless stated; "global" = batch-wide index):
+//   per system s : atom/shell/AO ranges, packed matrix offset mat_off[s] = sum n_t^2,
+//                  shell-matrix offset gam_off[s] = sum k_t^2, mixer vector offset.
+//   per atom     : Z, position (3), element constants gathered at topology time.
+//   per shell    : owning atom, l, first AO (system-local), primitive range, level, kcn,
+//                  shell polynomial, Slater exponent, hardness, third-order gamma,
+//                  reference occupation.
+//   per AO       : owning shell and atom (global indices).
+//   matrices     : row-major n_s x n_s blocks at mat_off[s]; dipole and quadrupole
+//                  integrals are component-major (3 resp. 6 full packed arrays).
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace xtb {
+
+constexpr int kMaxD4Refs = 7;
+constexpr double kPi = 3.141592653589793238462643383279502884;
+constexpr double kSqrtPi3 = 5.5683279968317061;   // pi^(3/2)
+constexpr double kIntegralCutoff = 25.0;          // Gaussian-product screen
+
+// Model constants shared by all kernels (set once per context).
+struct ModelConstants {
+  double wexp, enscale, kpol, pair_scale_default;
+  double shell_pair_scale[9];
+  double rep_kexp, rep_klight;
+  double es3_scale[3];
+  double mp_kexp, mp_shift, mp_rmax;
+  double d4_a1, d4_a2, d4_s6, d4_s8, d4_s9;
+};
+
+struct DevTopo {
+  ModelConstants m;
+  int32_t nsys;
+  int64_t total_atoms, total_shells, total_aos;
+  // per system
+  const int64_t* atom_off;
+  const int64_t* shell_off;
+  const int64_t* ao_off;
+  const int64_t* mat_off;
+  const int64_t* gam_off;
+  const int64_t* vec_off;
+  const int32_t* nao;
+  const double* nel_a;
+  const double* nel_b;
+  const double* qmol;
+  // per atom
+  const int32_t* Z;
+  const int32_t* atom_sh;     // total_atoms + 1
+  const double* pos;          // 3 per atom
+  const double* at_en;        // GFN2 electronegativity
+  const double* at_rad;       // H0 polynomial radius (bohr)
+  const double* at_rcov;      // double-exponential CN radius (bohr)
+  const double* at_mprad;
+  const double* at_mpvcn;
+  const double* at_dk;
+  const double* at_qk;
+  const double* at_rep_sa;    // sqrt(arep)
+  const double* at_rep_z;     // repulsion zeff
+  const double* d4_rcov;
+  const double* d4_en;
+  const double* d4_zeff;
+  const double* d4_eta;
+  const double* d4_r4r2;
+  const int32_t* d4_roff;
+  const int32_t* d4_rcnt;
+  // per shell
+  const int32_t* sh_atom;
+  const int32_t* sh_l;
+  const int32_t* sh_ao;       // first AO of the shell, system-local
+  const int32_t* sh_p0;
+  const int32_t* sh_np;
+  const double* sh_level;
+  const double* sh_kcn;
+  const double* sh_shpoly;
+  const double* sh_zeta;
+  const double* sh_eta;
+  const double* sh_g3;
+  const double* sh_refocc;
+  const double* p_alpha;
+  const double* p_coeff;
+  // per AO (global)
+  const int32_t* ao_sh;
+  const int32_t* ao_at;
+  // D4 reference tables
+  const double* ref_cn;
+  const double* ref_q;
+  const int32_t* ref_ng;
+  const double* ref_c6;       // 262 x 262
+  int32_t ref_count;
+};
+
+__device__ __forceinline__ double logistic(double x) {
+  if (x >= 0.0) {
+    const double e = exp(-x);
+    return 1.0 / (1.0 + e);
+  }
+  const double e = exp(x);
+  return e / (1.0 + e);
+}
+
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+
+// Block-wide sum; all threads receive the result.  scratch needs 33 doubles.
+__device__ __forceinline__ double block_sum(double v, double* scratch) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int nw = (blockDim.x + 31) >> 5;
+  v = warp_sum(v);
+  __syncthreads();
+  if (lane == 0) scratch[warp] = v;
+  __syncthreads();
+  if (warp == 0) {
+    double t = lane < nw ? scratch[lane] : 0.0;
+    t = warp_sum(t);
+    if (lane == 0) scratch[32] = t;
+  }
+  __syncthreads();
+  return scratch[32];
+}
+
+__device__ __forceinline__ double block_max(double v, double* scratch) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int nw = (blockDim.x + 31) >> 5;
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+  __syncthreads();
+  if (lane == 0) scratch[warp] = v;
+  __syncthreads();
+  if (warp == 0) {
+    double t = lane < nw ? scratch[lane] : -1.7976931348623157e308;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) t = fmax(t, __shfl_xor_sync(0xffffffffu, t, o));
+    if (lane == 0) scratch[32] = t;
+  }
+  __syncthreads();
+  return scratch[32];
+}
+
+// Per-system status codes mirror the public per_system_status values.
+enum SysStatus : int32_t { kOk = 0, kNotConverged = 7, kEigenFailed = 8, kInternal = 6 };
+
+}  // namespace xtb

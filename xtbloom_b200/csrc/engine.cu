@@ -1,0 +1,849 @@
+// Host orchestration of the batched GFN2-xTB path on one B200.
+//
+// Per call: validate and stage the ragged batch, build (or reuse) the
+// topology on the device, run the geometry setup kernels, build the Loewdin
+// orthogonaliser, iterate the SCC with an on-device active list (systems
+// leave the launch grid as soon as they converge; the list is ordered by
+// decreasing AO count so the largest systems start first), evaluate the
+// analytic gradient, and publish into the caller's buffers with quiet-NaN
+// slices for failed systems.  Mirrors the reference's CUDA execution flow
+// (runtime/gfn2_cuda_execution.cu:8784-10424) with a different kernel design.
+#include "engine.h"
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <limits>
+#include <map>
+#include <numeric>
+
+#include "kernels.cuh"
+
+namespace xtb {
+namespace {
+
+#include "generated/params.inc"
+
+constexpr double kEvToHartree = 1.0 / 27.21138505;
+constexpr double kAngstromToBohr = 1.8897261246204404;
+constexpr double kPiH = 3.141592653589793238462643383279502884;
+
+struct Dbuf {
+  void* p = nullptr;
+  size_t bytes = 0;
+  ~Dbuf() {
+    if (p) cudaFree(p);
+  }
+  bool reserve(size_t nbytes) {
+    if (nbytes <= bytes && p) return true;
+    if (p) cudaFree(p);
+    p = nullptr;
+    bytes = 0;
+    const size_t want = std::max<size_t>(nbytes, 256);
+    if (cudaMalloc(&p, want) != cudaSuccess) return false;
+    bytes = want;
+    return true;
+  }
+  template <class T>
+  T* as() const {
+    return static_cast<T*>(p);
+  }
+};
+
+template <class T>
+bool upload(Dbuf& b, const std::vector<T>& v, cudaStream_t s) {
+  if (!b.reserve(v.size() * sizeof(T))) return false;
+  if (!v.empty()) cudaMemcpyAsync(b.p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice, s);
+  return true;
+}
+
+// STO-nG expansion (common/sto.cpp:20-123 of the reference, restated).
+bool sto_expand(int n, int l, int ng, double zeta, std::vector<double>& alpha,
+                std::vector<double>& coeff) {
+  const double* a0 = nullptr;
+  const double* c0 = nullptr;
+  if (n == 6 && ng == 6) {
+    a0 = l == 0 ? kP_sto_alpha6s : kP_sto_alpha6p;
+    c0 = l == 0 ? kP_sto_coeff6s : kP_sto_coeff6p;
+  } else {
+    int typ;
+    switch (l) {
+      case 0: typ = n - 1; break;
+      case 1: typ = n + 3; break;
+      case 2: typ = n + 6; break;
+      case 3: typ = n + 8; break;
+      default: typ = n + 9; break;
+    }
+    if (typ < 0 || typ >= 15) return false;
+    if (ng == 3) { a0 = kP_sto_alpha3 + 3 * typ; c0 = kP_sto_coeff3 + 3 * typ; }
+    else if (ng == 4) { a0 = kP_sto_alpha4 + 4 * typ; c0 = kP_sto_coeff4 + 4 * typ; }
+    else if (ng == 6) { a0 = kP_sto_alpha6 + 6 * typ; c0 = kP_sto_coeff6 + 6 * typ; }
+    else return false;
+  }
+  const double dfact[5] = {1.0, 1.0, 3.0, 15.0, 105.0};
+  alpha.resize(ng);
+  coeff.resize(ng);
+  for (int i = 0; i < ng; ++i) {
+    alpha[i] = a0[i] * zeta * zeta;
+    const double norm = std::pow(2.0 / kPiH * alpha[i], 0.75) * std::pow(std::sqrt(4.0 * alpha[i]), l) /
+                        std::sqrt(dfact[l]);
+    coeff[i] = c0[i] * norm;
+  }
+  return true;
+}
+
+void orthogonalize_to_first(const std::vector<double>& a1, const std::vector<double>& c1,
+                            std::vector<double>& a, std::vector<double>& c) {
+  double ov = 0.0;
+  for (size_t i = 0; i < a1.size(); ++i)
+    for (size_t j = 0; j < a.size(); ++j) ov += c1[i] * c[j] * std::pow(std::sqrt(kPiH / (a1[i] + a[j])), 3.0);
+  const size_t nb = a.size();
+  for (size_t i = 0; i < a1.size(); ++i) {
+    a.push_back(a1[i]);
+    c.push_back(-ov * c1[i]);
+  }
+  double nrm = 0.0;
+  for (size_t i = 0; i < a.size(); ++i)
+    for (size_t j = 0; j < a.size(); ++j) nrm += c[i] * c[j] * std::pow(std::sqrt(kPiH / (a[i] + a[j])), 3.0);
+  (void)nb;
+  const double inv = 1.0 / std::sqrt(nrm);
+  for (double& x : c) x *= inv;
+}
+
+const char* kGlobalNames[20] = {"wexp", "enscale", "kpol", "pair_scale_default", "rep_kexp",
+                                "rep_klight", "es3_s", "es3_p", "es3_d", "mp_dmp3", "mp_dmp5",
+                                "mp_kexp", "mp_shift", "mp_rmax", "d4_a1", "d4_a2", "d4_s6",
+                                "d4_s8", "d4_s9", "es2_gexp"};
+
+ModelConstants make_constants() {
+  ModelConstants m{};
+  const double* g = kP_gfn2_globals;
+  m.wexp = g[0];
+  m.enscale = g[1];
+  m.kpol = g[2];
+  m.pair_scale_default = g[3];
+  for (int i = 0; i < 9; ++i) m.shell_pair_scale[i] = kP_gfn2_shell_pair_scale[i];
+  m.rep_kexp = g[4];
+  m.rep_klight = g[5];
+  m.es3_scale[0] = g[6];
+  m.es3_scale[1] = g[7];
+  m.es3_scale[2] = g[8];
+  m.mp_kexp = g[11];
+  m.mp_shift = g[12];
+  m.mp_rmax = g[13];
+  m.d4_a1 = g[14];
+  m.d4_a2 = g[15];
+  m.d4_s6 = g[16];
+  m.d4_s8 = g[17];
+  m.d4_s9 = g[18];
+  (void)kGlobalNames;
+  return m;
+}
+
+size_t host_bytes_of(const xtbloom_const_buffer_t& b) { return b.size_bytes; }
+
+}  // namespace
+
+struct Engine::Impl {
+  ModelConstants model = make_constants();
+  // static parameter tables on the device
+  Dbuf d4_rcov, d4_en, d4_zeff, d4_eta, d4_r4r2, d4_roff, d4_rcnt, ref_cn, ref_q, ref_ng, ref_c6;
+  bool tables_ready = false;
+
+  // topology (host copies used for caching and sizes)
+  HostBatch topo;
+  bool topo_valid = false;
+  int64_t nsys = 0, natoms = 0, nshells = 0, naos = 0, total_mat = 0, total_gam = 0, total_vec = 0,
+          total_scr = 0, total_prim = 0;
+  int max_n = 0, max_atoms = 0, max_shells = 0, max_dim = 0;
+  int64_t max_pairs = 0;
+  std::vector<int32_t> h_nao, h_order;
+  std::vector<double> h_nel_a, h_nel_b;
+
+  // device topology arrays
+  Dbuf atom_off, shell_off, ao_off, mat_off, gam_off, vec_off, scr_off, nao, nel_a, nel_b, qmol;
+  Dbuf Z, atom_sh, pos, at_en, at_rad, at_rcov, at_mprad, at_mpvcn, at_dk, at_qk, at_rep_sa, at_rep_z;
+  Dbuf sh_atom, sh_l, sh_ao, sh_p0, sh_np, sh_level, sh_kcn, sh_shpoly, sh_zeta, sh_eta, sh_g3,
+      sh_refocc, p_alpha, p_coeff, ao_sh, ao_at, order;
+  // state
+  Dbuf list, count, status, iterations, converged, nvec;
+  Dbuf cn, cn_d4, mrad, dmrad, gam;
+  Dbuf S, D, Q, H0, H, X, T, A, Zv, C, P, W;
+  Dbuf d, e, tau, eig, occ, occ_eps, entropy, scratch;
+  Dbuf qsh, dip, qp, pop_sh, pop_dip, pop_qp, e_core, vsh, vd, vq;
+  Dbuf free_energy, terms;
+  Dbuf mx_cur, mx_prev, mx_res, mx_df, mx_u, mx_omega;
+  Dbuf grad, acn, acn_d4;
+  Dbuf out_energy, out_forces, out_charges;
+  int32_t* h_count = nullptr;   // pinned
+  int last_memory = 0;
+  bool have_results = false;
+
+  DevTopo devtopo() const {
+    DevTopo t{};
+    t.m = model;
+    t.nsys = (int32_t)nsys;
+    t.total_atoms = natoms;
+    t.total_shells = nshells;
+    t.total_aos = naos;
+    t.atom_off = atom_off.as<int64_t>();
+    t.shell_off = shell_off.as<int64_t>();
+    t.ao_off = ao_off.as<int64_t>();
+    t.mat_off = mat_off.as<int64_t>();
+    t.gam_off = gam_off.as<int64_t>();
+    t.vec_off = vec_off.as<int64_t>();
+    t.nao = nao.as<int32_t>();
+    t.nel_a = nel_a.as<double>();
+    t.nel_b = nel_b.as<double>();
+    t.qmol = qmol.as<double>();
+    t.Z = Z.as<int32_t>();
+    t.atom_sh = atom_sh.as<int32_t>();
+    t.pos = pos.as<double>();
+    t.at_en = at_en.as<double>();
+    t.at_rad = at_rad.as<double>();
+    t.at_rcov = at_rcov.as<double>();
+    t.at_mprad = at_mprad.as<double>();
+    t.at_mpvcn = at_mpvcn.as<double>();
+    t.at_dk = at_dk.as<double>();
+    t.at_qk = at_qk.as<double>();
+    t.at_rep_sa = at_rep_sa.as<double>();
+    t.at_rep_z = at_rep_z.as<double>();
+    t.d4_rcov = d4_rcov.as<double>();
+    t.d4_en = d4_en.as<double>();
+    t.d4_zeff = d4_zeff.as<double>();
+    t.d4_eta = d4_eta.as<double>();
+    t.d4_r4r2 = d4_r4r2.as<double>();
+    t.d4_roff = d4_roff.as<int32_t>();
+    t.d4_rcnt = d4_rcnt.as<int32_t>();
+    t.sh_atom = sh_atom.as<int32_t>();
+    t.sh_l = sh_l.as<int32_t>();
+    t.sh_ao = sh_ao.as<int32_t>();
+    t.sh_p0 = sh_p0.as<int32_t>();
+    t.sh_np = sh_np.as<int32_t>();
+    t.sh_level = sh_level.as<double>();
+    t.sh_kcn = sh_kcn.as<double>();
+    t.sh_shpoly = sh_shpoly.as<double>();
+    t.sh_zeta = sh_zeta.as<double>();
+    t.sh_eta = sh_eta.as<double>();
+    t.sh_g3 = sh_g3.as<double>();
+    t.sh_refocc = sh_refocc.as<double>();
+    t.p_alpha = p_alpha.as<double>();
+    t.p_coeff = p_coeff.as<double>();
+    t.ao_sh = ao_sh.as<int32_t>();
+    t.ao_at = ao_at.as<int32_t>();
+    t.ref_cn = ref_cn.as<double>();
+    t.ref_q = ref_q.as<double>();
+    t.ref_ng = ref_ng.as<int32_t>();
+    t.ref_c6 = ref_c6.as<double>();
+    t.ref_count = 262;
+    return t;
+  }
+};
+
+Engine::Engine(int device, cudaStream_t stream) : impl_(new Impl), device_(device), stream_(stream) {
+  cudaMallocHost(&impl_->h_count, 4 * sizeof(int32_t));
+}
+
+Engine::~Engine() {
+  if (impl_->h_count) cudaFreeHost(impl_->h_count);
+  delete impl_;
+}
+
+namespace {
+
+bool ensure_tables(Engine::Impl& m, cudaStream_t s) {
+  if (m.tables_ready) return true;
+  auto upd = [&](Dbuf& b, const double* src, size_t n) {
+    return b.reserve(n * sizeof(double)) &&
+           cudaMemcpyAsync(b.p, src, n * sizeof(double), cudaMemcpyHostToDevice, s) == cudaSuccess;
+  };
+  auto upi = [&](Dbuf& b, const int* src, size_t n) {
+    return b.reserve(n * sizeof(int)) &&
+           cudaMemcpyAsync(b.p, src, n * sizeof(int), cudaMemcpyHostToDevice, s) == cudaSuccess;
+  };
+  bool ok = upd(m.d4_rcov, kP_d4_rcov, 86) && upd(m.d4_en, kP_d4_en, 86) &&
+            upd(m.d4_zeff, kP_d4_zeff, 86) && upd(m.d4_eta, kP_d4_eta, 86) &&
+            upd(m.d4_r4r2, kP_d4_r4r2, 86) && upi(m.d4_roff, kP_d4_ref_offset, 86) &&
+            upi(m.d4_rcnt, kP_d4_ref_count, 86) && upd(m.ref_cn, kP_d4_ref_cn, 262) &&
+            upd(m.ref_q, kP_d4_ref_q, 262) && upi(m.ref_ng, kP_d4_ref_ngauss, 262) &&
+            upd(m.ref_c6, kP_d4_ref_c6, 262 * 262);
+  m.tables_ready = ok;
+  return ok;
+}
+
+bool same_topology(const HostBatch& a, const HostBatch& b) {
+  return a.nsys == b.nsys && a.atom_off == b.atom_off && a.Z == b.Z && a.qmol == b.qmol &&
+         a.uhf == b.uhf;
+}
+
+xtbloom_status_t build_topology(Engine::Impl& m, const HostBatch& hb, cudaStream_t s,
+                                std::string& error) {
+  const int64_t B = hb.nsys;
+  const int64_t N = hb.atom_off[B];
+  std::vector<int64_t> atom_off = hb.atom_off, shell_off(B + 1), ao_off(B + 1), mat_off(B + 1),
+                       gam_off(B + 1), vec_off(B + 1), scr_off(B + 1);
+  std::vector<int32_t> nao(B), Zv(hb.Z.begin(), hb.Z.end()), atom_sh(N + 1);
+  std::vector<double> nel_a(B), nel_b(B), qmol(hb.qmol.begin(), hb.qmol.end());
+  std::vector<double> at_en(N), at_rad(N), at_rcov(N), at_mprad(N), at_mpvcn(N), at_dk(N), at_qk(N),
+      at_rep_sa(N), at_rep_z(N);
+  std::vector<int32_t> sh_atom, sh_l, sh_ao, sh_p0, sh_np, ao_sh, ao_at;
+  std::vector<double> sh_level, sh_kcn, sh_shpoly, sh_zeta, sh_eta, sh_g3, sh_refocc, p_alpha, p_coeff;
+  int64_t shell = 0;
+  int max_n = 0, max_atoms = 0, max_shells = 0, max_dim = 0;
+  int64_t max_pairs = 0;
+  for (int64_t sy = 0; sy < B; ++sy) {
+    shell_off[sy] = shell;
+    ao_off[sy] = (int64_t)ao_sh.size();
+    int ao_local = 0;
+    double nel = 0.0;
+    for (int64_t a = atom_off[sy]; a < atom_off[sy + 1]; ++a) {
+      const int z = Zv[a];
+      const int zi = z - 1;
+      atom_sh[a] = (int32_t)shell;
+      at_en[a] = kP_gfn2_en[zi];
+      at_rad[a] = kP_atomic_radii_angstrom[zi] * kAngstromToBohr;
+      at_rcov[a] = (4.0 / 3.0) * kAngstromToBohr * kP_covalent_radii_angstrom[zi];
+      at_mprad[a] = kP_gfn2_mprad[zi];
+      at_mpvcn[a] = kP_gfn2_mpvcn[zi];
+      at_dk[a] = kP_gfn2_dkernel[zi];
+      at_qk[a] = kP_gfn2_qkernel[zi];
+      at_rep_sa[a] = std::sqrt(kP_gfn2_arep[zi]);
+      at_rep_z[a] = kP_gfn2_zeff[zi];
+      const int nsh = kP_gfn2_nshell[zi];
+      int first_of_l[5] = {-1, -1, -1, -1, -1};
+      for (int k = 0; k < nsh; ++k) {
+        const int l = kP_gfn2_shell_l[3 * zi + k];
+        const int pn = kP_gfn2_shell_n[3 * zi + k];
+        const int ng = kP_gfn2_shell_ngauss[3 * zi + k];
+        const double zeta = kP_gfn2_shell_slater[3 * zi + k];
+        std::vector<double> al, co;
+        if (!sto_expand(pn, l, ng, zeta, al, co)) {
+          error = "unsupported STO-nG shell in the parameter tables";
+          return XTBLOOM_STATUS_INTERNAL_ERROR;
+        }
+        if (first_of_l[l] >= 0) {
+          const int f = first_of_l[l];
+          std::vector<double> a1(p_alpha.begin() + sh_p0[f], p_alpha.begin() + sh_p0[f] + sh_np[f]);
+          std::vector<double> c1(p_coeff.begin() + sh_p0[f], p_coeff.begin() + sh_p0[f] + sh_np[f]);
+          orthogonalize_to_first(a1, c1, al, co);
+        } else {
+          first_of_l[l] = (int)shell;
+        }
+        sh_atom.push_back((int32_t)a);
+        sh_l.push_back(l);
+        sh_ao.push_back(ao_local);
+        sh_p0.push_back((int32_t)p_alpha.size());
+        sh_np.push_back((int32_t)al.size());
+        p_alpha.insert(p_alpha.end(), al.begin(), al.end());
+        p_coeff.insert(p_coeff.end(), co.begin(), co.end());
+        sh_level.push_back(kP_gfn2_shell_level[3 * zi + k] * kEvToHartree);
+        sh_kcn.push_back(kP_gfn2_shell_kcn[3 * zi + k] * kEvToHartree);
+        sh_shpoly.push_back(kP_gfn2_shell_shpoly[3 * zi + k]);
+        sh_zeta.push_back(zeta);
+        sh_eta.push_back(kP_gfn2_gam[zi] * kP_gfn2_shell_hubbard_scale[3 * zi + k]);
+        sh_g3.push_back(kP_gfn2_gam3[zi] * m.model.es3_scale[l]);
+        const double ro = kP_gfn2_shell_refocc[3 * zi + k];
+        sh_refocc.push_back(ro);
+        nel += ro;
+        for (int q = 0; q < 2 * l + 1; ++q) {
+          ao_sh.push_back((int32_t)shell);
+          ao_at.push_back((int32_t)a);
+        }
+        ao_local += 2 * l + 1;
+        ++shell;
+      }
+    }
+    const int na = (int)(atom_off[sy + 1] - atom_off[sy]);
+    const int ns = (int)(shell - shell_off[sy]);
+    nao[sy] = ao_local;
+    nel -= qmol[sy];
+    const double u = hb.uhf[sy];
+    if (!(nel >= 0.0) || u < 0 || u > nel + 1e-12) {
+      error = "molecular charge or unpaired electrons are incompatible with the electron count";
+      return XTBLOOM_STATUS_INVALID_ARGUMENT;
+    }
+    nel_a[sy] = 0.5 * (nel + u);
+    nel_b[sy] = 0.5 * (nel - u);
+    max_n = std::max(max_n, ao_local);
+    max_atoms = std::max(max_atoms, na);
+    max_shells = std::max(max_shells, ns);
+    max_dim = std::max(max_dim, ns + 9 * na);
+    max_pairs = std::max<int64_t>(max_pairs, (int64_t)na * (na + 1) / 2);
+  }
+  shell_off[B] = shell;
+  ao_off[B] = (int64_t)ao_sh.size();
+  atom_sh[N] = (int32_t)shell;
+  mat_off[0] = gam_off[0] = vec_off[0] = scr_off[0] = 0;
+  for (int64_t sy = 0; sy < B; ++sy) {
+    const int64_t n = nao[sy];
+    const int64_t k = shell_off[sy + 1] - shell_off[sy];
+    const int64_t na = atom_off[sy + 1] - atom_off[sy];
+    mat_off[sy + 1] = mat_off[sy] + n * n;
+    gam_off[sy + 1] = gam_off[sy] + k * k;
+    vec_off[sy + 1] = vec_off[sy] + k + 9 * na;
+    scr_off[sy + 1] = scr_off[sy] + 128 * 5 * n;
+  }
+  // largest systems first
+  std::vector<int32_t> order(B);
+  std::iota(order.begin(), order.end(), 0);
+  std::stable_sort(order.begin(), order.end(), [&](int32_t a, int32_t b) { return nao[a] > nao[b]; });
+
+  m.nsys = B;
+  m.natoms = N;
+  m.nshells = shell;
+  m.naos = ao_off[B];
+  m.total_mat = mat_off[B];
+  m.total_gam = gam_off[B];
+  m.total_vec = vec_off[B];
+  m.total_scr = scr_off[B];
+  m.total_prim = (int64_t)p_alpha.size();
+  m.max_n = max_n;
+  m.max_atoms = max_atoms;
+  m.max_shells = max_shells;
+  m.max_dim = max_dim;
+  m.max_pairs = max_pairs;
+  m.h_nao = nao;
+  m.h_order = order;
+  m.h_nel_a = nel_a;
+  m.h_nel_b = nel_b;
+
+  bool ok = upload(m.atom_off, atom_off, s) && upload(m.shell_off, shell_off, s) &&
+            upload(m.ao_off, ao_off, s) && upload(m.mat_off, mat_off, s) &&
+            upload(m.gam_off, gam_off, s) && upload(m.vec_off, vec_off, s) &&
+            upload(m.scr_off, scr_off, s) && upload(m.nao, nao, s) && upload(m.nel_a, nel_a, s) &&
+            upload(m.nel_b, nel_b, s) && upload(m.qmol, qmol, s) && upload(m.Z, Zv, s) &&
+            upload(m.atom_sh, atom_sh, s) && upload(m.at_en, at_en, s) &&
+            upload(m.at_rad, at_rad, s) && upload(m.at_rcov, at_rcov, s) &&
+            upload(m.at_mprad, at_mprad, s) && upload(m.at_mpvcn, at_mpvcn, s) &&
+            upload(m.at_dk, at_dk, s) && upload(m.at_qk, at_qk, s) &&
+            upload(m.at_rep_sa, at_rep_sa, s) && upload(m.at_rep_z, at_rep_z, s) &&
+            upload(m.sh_atom, sh_atom, s) && upload(m.sh_l, sh_l, s) && upload(m.sh_ao, sh_ao, s) &&
+            upload(m.sh_p0, sh_p0, s) && upload(m.sh_np, sh_np, s) &&
+            upload(m.sh_level, sh_level, s) && upload(m.sh_kcn, sh_kcn, s) &&
+            upload(m.sh_shpoly, sh_shpoly, s) && upload(m.sh_zeta, sh_zeta, s) &&
+            upload(m.sh_eta, sh_eta, s) && upload(m.sh_g3, sh_g3, s) &&
+            upload(m.sh_refocc, sh_refocc, s) && upload(m.p_alpha, p_alpha, s) &&
+            upload(m.p_coeff, p_coeff, s) && upload(m.ao_sh, ao_sh, s) &&
+            upload(m.ao_at, ao_at, s) && upload(m.order, order, s);
+  const size_t d8 = sizeof(double);
+  const size_t mat = (size_t)m.total_mat * d8;
+  ok = ok && m.pos.reserve((size_t)N * 3 * d8) && m.list.reserve((size_t)B * 4) &&
+       m.count.reserve(16) && m.status.reserve((size_t)B * 4) && m.iterations.reserve((size_t)B * 4) &&
+       m.converged.reserve((size_t)B) && m.nvec.reserve((size_t)B * 4) && m.cn.reserve(N * d8) &&
+       m.cn_d4.reserve(N * d8) && m.mrad.reserve(N * d8) && m.dmrad.reserve(N * d8) &&
+       m.gam.reserve((size_t)m.total_gam * d8) && m.S.reserve(mat) && m.D.reserve(3 * mat) &&
+       m.Q.reserve(6 * mat) && m.H0.reserve(mat) && m.H.reserve(mat) && m.X.reserve(mat) &&
+       m.T.reserve(mat) && m.A.reserve(mat) && m.Zv.reserve(mat) && m.C.reserve(mat) &&
+       m.P.reserve(mat) && m.W.reserve(mat) && m.d.reserve(m.naos * d8) && m.e.reserve(m.naos * d8) &&
+       m.tau.reserve(m.naos * d8) && m.eig.reserve(m.naos * d8) && m.occ.reserve(m.naos * d8) &&
+       m.occ_eps.reserve(m.naos * d8) && m.entropy.reserve(B * d8) &&
+       m.scratch.reserve((size_t)m.total_scr * d8) && m.qsh.reserve(shell * d8) &&
+       m.dip.reserve(3 * N * d8) && m.qp.reserve(6 * N * d8) && m.pop_sh.reserve(shell * d8) &&
+       m.pop_dip.reserve(3 * N * d8) && m.pop_qp.reserve(6 * N * d8) && m.e_core.reserve(B * d8) &&
+       m.vsh.reserve(shell * d8) && m.vd.reserve(3 * N * d8) && m.vq.reserve(6 * N * d8) &&
+       m.free_energy.reserve(B * d8) && m.terms.reserve(8 * B * d8) &&
+       m.mx_cur.reserve((size_t)m.total_vec * d8) && m.mx_prev.reserve((size_t)m.total_vec * d8) &&
+       m.mx_res.reserve((size_t)m.total_vec * d8) && m.grad.reserve(3 * N * d8) &&
+       m.acn.reserve(N * d8) && m.acn_d4.reserve(N * d8) && m.out_energy.reserve(B * d8) &&
+       m.out_forces.reserve(3 * N * d8) && m.out_charges.reserve(N * d8);
+  if (!ok) {
+    error = "device allocation for the batch failed";
+    return XTBLOOM_STATUS_ALLOCATION_FAILED;
+  }
+  return XTBLOOM_STATUS_SUCCESS;
+}
+
+bool read_input(const xtbloom_const_buffer_t& b, void* dst, size_t bytes, cudaStream_t s) {
+  if (bytes == 0) return true;
+  const cudaMemcpyKind kind =
+      b.memory_space == XTBLOOM_MEMORY_CUDA_DEVICE ? cudaMemcpyDeviceToHost : cudaMemcpyHostToHost;
+  if (kind == cudaMemcpyHostToHost) {
+    std::memcpy(dst, b.data, bytes);
+    return true;
+  }
+  return cudaMemcpyAsync(dst, b.data, bytes, kind, s) == cudaSuccess && cudaStreamSynchronize(s) == cudaSuccess;
+}
+
+__global__ void k_publish(DevTopo t, const int32_t* status, const double* free_energy,
+                          const double* terms, const double* grad, const double* qsh,
+                          double* energy, double* forces, double* charges) {
+  const int s = blockIdx.x;
+  const bool ok = status[s] == kOk;
+  const double nan = __longlong_as_double(0x7ff8000000000000ll);
+  const int64_t a0 = t.atom_off[s], a1 = t.atom_off[s + 1];
+  if (threadIdx.x == 0) energy[s] = ok ? free_energy[s] + terms[8 * (int64_t)s + 6] + terms[8 * (int64_t)s + 7] : nan;
+  for (int64_t a = a0 + threadIdx.x; a < a1; a += blockDim.x) {
+    double q = 0.0;
+    for (int sh = t.atom_sh[a]; sh < t.atom_sh[a + 1]; ++sh) q += qsh[sh];
+    charges[a] = ok ? q : nan;
+    for (int c = 0; c < 3; ++c) forces[3 * a + c] = ok ? -grad[3 * a + c] : nan;
+  }
+}
+
+__global__ void k_fill_status(const int32_t* order, int nsys, int32_t* status, int32_t value) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < nsys) status[order[i]] = value;
+}
+
+__global__ void k_finalize_status(int nsys, int32_t* status, const uint8_t* converged) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < nsys && status[i] == kOk && !converged[i]) status[i] = kNotConverged;
+}
+
+// Converged systems only (status ok), in cost order.
+__global__ void k_list_ok(const int32_t* order, int nsys, const int32_t* status, int32_t* list,
+                          int32_t* count) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  int c = 0;
+  for (int i = 0; i < nsys; ++i)
+    if (status[order[i]] == kOk) list[c++] = order[i];
+  count[0] = c;
+}
+
+}  // namespace
+
+xtbloom_status_t Engine::compute(const ComputeRequest& req, std::string& error) {
+  Impl& m = *impl_;
+  cudaStream_t s = stream_;
+  cudaSetDevice(device_);
+  const xtbloom_batch_t& b = *req.batch;
+  const int64_t B = b.batch_size;
+  const int64_t N = b.total_atoms;
+  if (!ensure_tables(m, s)) {
+    error = "failed to upload parameter tables";
+    return XTBLOOM_STATUS_ALLOCATION_FAILED;
+  }
+  // ---- stage topology descriptors on the host ----
+  HostBatch hb;
+  hb.nsys = B;
+  hb.atom_off.resize(B + 1);
+  hb.Z.resize(N);
+  hb.qmol.resize(B);
+  hb.uhf.resize(B, 0);
+  if (!read_input(b.atom_offsets, hb.atom_off.data(), (B + 1) * 8, s) ||
+      !read_input(b.atomic_numbers, hb.Z.data(), N * 4, s) ||
+      !read_input(b.molecular_charges, hb.qmol.data(), B * 8, s) ||
+      (b.unpaired_electrons.data && !read_input(b.unpaired_electrons, hb.uhf.data(), B * 4, s))) {
+    error = "failed to read the batch descriptors";
+    return XTBLOOM_STATUS_INVALID_ARGUMENT;
+  }
+  if (hb.atom_off[0] != 0 || hb.atom_off[B] != N) {
+    error = "atom_offsets must start at zero and end at total_atoms";
+    return XTBLOOM_STATUS_INVALID_ARGUMENT;
+  }
+  for (int64_t i = 0; i < B; ++i) {
+    if (hb.atom_off[i + 1] <= hb.atom_off[i]) {
+      error = "atom_offsets must be strictly increasing (every system needs an atom)";
+      return XTBLOOM_STATUS_INVALID_ARGUMENT;
+    }
+    if (!std::isfinite(hb.qmol[i])) {
+      error = "molecular_charges must be finite";
+      return XTBLOOM_STATUS_INVALID_ARGUMENT;
+    }
+    if (hb.uhf[i] < 0) {
+      error = "unpaired_electrons must be nonnegative";
+      return XTBLOOM_STATUS_INVALID_ARGUMENT;
+    }
+  }
+  for (int64_t a = 0; a < N; ++a) {
+    if (hb.Z[a] < 1 || hb.Z[a] > 86) {
+      error = "atomic_numbers must be in [1, 86]";
+      return XTBLOOM_STATUS_INVALID_ARGUMENT;
+    }
+  }
+  if (!m.topo_valid || !same_topology(m.topo, hb)) {
+    m.topo_valid = false;
+    xtbloom_status_t st = build_topology(m, hb, s, error);
+    if (st != XTBLOOM_STATUS_SUCCESS) return st;
+    m.topo = hb;
+    m.topo_valid = true;
+  }
+  // ---- positions ----
+  {
+    const cudaMemcpyKind kind = b.positions.memory_space == XTBLOOM_MEMORY_CUDA_DEVICE
+                                    ? cudaMemcpyDeviceToDevice
+                                    : cudaMemcpyHostToDevice;
+    if (cudaMemcpyAsync(m.pos.p, b.positions.data, (size_t)N * 3 * 8, kind, s) != cudaSuccess) {
+      error = "failed to stage positions";
+      return XTBLOOM_STATUS_INVALID_ARGUMENT;
+    }
+  }
+  // Broyden history sized by the requested memory
+  const int M = req.memory;
+  if (!m.mx_df.reserve((size_t)m.total_vec * M * 8) || !m.mx_u.reserve((size_t)m.total_vec * M * 8) ||
+      !m.mx_omega.reserve((size_t)B * M * 8)) {
+    error = "device allocation for the mixer history failed";
+    return XTBLOOM_STATUS_ALLOCATION_FAILED;
+  }
+  const DevTopo t = m.devtopo();
+  const int nsys = (int)B;
+  int32_t* list = m.list.as<int32_t>();
+  int32_t* dcount = m.count.as<int32_t>();
+  int32_t* status = m.status.as<int32_t>();
+  const int32_t* order = m.order.as<int32_t>();
+  cudaMemsetAsync(status, 0, B * 4, s);
+  cudaMemsetAsync(m.converged.p, 0, B, s);
+  cudaMemsetAsync(m.iterations.p, 0, B * 4, s);
+  cudaMemsetAsync(m.terms.p, 0, 8 * B * 8, s);
+  cudaMemcpyAsync(list, order, B * 4, cudaMemcpyDeviceToDevice, s);
+
+  // ---- geometry setup ----
+  launch_setup(t, list, nsys, m.max_atoms, m.max_pairs, m.max_shells, m.cn.as<double>(),
+               m.cn_d4.as<double>(), m.mrad.as<double>(), m.dmrad.as<double>(), m.S.as<double>(),
+               m.D.as<double>(), m.Q.as<double>(), m.H0.as<double>(), m.gam.as<double>(),
+               m.total_mat, s);
+
+  EigArgs eg{};
+  eg.list = list;
+  eg.nao = m.nao.as<int32_t>();
+  eg.mat_off = m.mat_off.as<int64_t>();
+  eg.ao_off = m.ao_off.as<int64_t>();
+  eg.A = m.A.as<double>();
+  eg.d = m.d.as<double>();
+  eg.e = m.e.as<double>();
+  eg.tau = m.tau.as<double>();
+  eg.eig = m.eig.as<double>();
+  eg.occ = m.occ.as<double>();
+  eg.occ_eps = m.occ_eps.as<double>();
+  eg.entropy = m.entropy.as<double>();
+  eg.nvec = m.nvec.as<int32_t>();
+  eg.Z = m.Zv.as<double>();
+  eg.scratch = m.scratch.as<double>();
+  eg.scratch_off = m.scr_off.as<int64_t>();
+  eg.nel_a = m.nel_a.as<double>();
+  eg.nel_b = m.nel_b.as<double>();
+  const int tiles = ((m.max_n + 63) / 64) * ((m.max_n + 63) / 64);
+  auto gemm = [&](const double* A, const double* Bm, double* C, const int32_t* dm, const int32_t* dn,
+                  const int32_t* dk, bool ta, const double* w, int count) {
+    GemmArgs g{};
+    g.list = list;
+    g.nao = m.nao.as<int32_t>();
+    g.dm = dm;
+    g.dn = dn;
+    g.dk = dk;
+    g.A = A;
+    g.offA = m.mat_off.as<int64_t>();
+    g.B = Bm;
+    g.offB = m.mat_off.as<int64_t>();
+    g.C = C;
+    g.offC = m.mat_off.as<int64_t>();
+    g.w = w;
+    g.offW = m.ao_off.as<int64_t>();
+    launch_gemm(g, ta, w != nullptr, tiles, count, s);
+  };
+  const int32_t* dnao = m.nao.as<int32_t>();
+  const int32_t* dnvec = m.nvec.as<int32_t>();
+
+  // ---- Loewdin orthogonaliser X = U s^-1/2 U^T ----
+  cudaMemcpyAsync(m.A.p, m.S.p, (size_t)m.total_mat * 8, cudaMemcpyDeviceToDevice, s);
+  launch_tridiag(eg, nsys, m.max_n, s);
+  launch_eigvals(eg, 1, 0.0, nsys, m.max_n, s);
+  launch_inverse_iteration(eg, nsys, s);
+  launch_backtransform(eg, nsys, m.max_n, s);
+  launch_lowdin_weights(eg, status, nsys, s);
+  gemm(m.Zv.as<double>(), m.Zv.as<double>(), m.X.as<double>(), dnao, dnao, dnao, true,
+       m.occ.as<double>(), nsys);
+
+  // ---- SCC ----
+  SccArgs a{};
+  a.t = t;
+  a.list = list;
+  a.qsh = m.qsh.as<double>();
+  a.dip = m.dip.as<double>();
+  a.qp = m.qp.as<double>();
+  a.pop_sh = m.pop_sh.as<double>();
+  a.pop_dip = m.pop_dip.as<double>();
+  a.pop_qp = m.pop_qp.as<double>();
+  a.e_core = m.e_core.as<double>();
+  a.vsh = m.vsh.as<double>();
+  a.vd = m.vd.as<double>();
+  a.vq = m.vq.as<double>();
+  a.gam = m.gam.as<double>();
+  a.mrad = m.mrad.as<double>();
+  a.cn_d4 = m.cn_d4.as<double>();
+  a.S = m.S.as<double>();
+  a.D = m.D.as<double>();
+  a.Q = m.Q.as<double>();
+  a.H0 = m.H0.as<double>();
+  a.H = m.H.as<double>();
+  a.P = m.P.as<double>();
+  a.total_mat = m.total_mat;
+  a.entropy = m.entropy.as<double>();
+  a.free_energy = m.free_energy.as<double>();
+  a.terms = m.terms.as<double>();
+  a.iterations = m.iterations.as<int32_t>();
+  a.status = status;
+  a.converged = m.converged.as<uint8_t>();
+  a.mx_cur = m.mx_cur.as<double>();
+  a.mx_prev = m.mx_prev.as<double>();
+  a.mx_res = m.mx_res.as<double>();
+  a.mx_df = m.mx_df.as<double>();
+  a.mx_u = m.mx_u.as<double>();
+  a.mx_omega = m.mx_omega.as<double>();
+  a.memory = M;
+  a.damping = req.damping;
+  a.ctol = req.ctol;
+  a.etol = req.etol;
+  a.kt = req.kt;
+  a.max_iter = req.max_iter;
+
+  launch_compact(order, nsys, status, a.converged, a.iterations, req.max_iter, list, dcount, s);
+  cudaMemcpyAsync(m.h_count, dcount, 4, cudaMemcpyDeviceToHost, s);
+  cudaStreamSynchronize(s);
+  int count = m.h_count[0];
+  a.count = count;
+  launch_sad_init(a, s);
+  for (int it = 0; it < req.max_iter && count > 0; ++it) {
+    a.count = count;
+    launch_potential(a, a.qsh, a.dip, a.qp, m.max_atoms, m.max_shells, s);
+    launch_fock(a, m.max_n, s);
+    gemm(m.H.as<double>(), m.X.as<double>(), m.T.as<double>(), dnao, dnao, dnao, false, nullptr, count);
+    gemm(m.X.as<double>(), m.T.as<double>(), m.A.as<double>(), dnao, dnao, dnao, false, nullptr, count);
+    launch_tridiag(eg, count, m.max_n, s);
+    launch_eigvals(eg, 0, req.kt, count, m.max_n, s);
+    launch_inverse_iteration(eg, count, s);
+    launch_backtransform(eg, count, m.max_n, s);
+    gemm(m.Zv.as<double>(), m.X.as<double>(), m.C.as<double>(), dnvec, dnao, dnao, false, nullptr, count);
+    gemm(m.C.as<double>(), m.C.as<double>(), m.P.as<double>(), dnao, dnao, dnvec, true,
+         m.occ.as<double>(), count);
+    cudaMemsetAsync(m.pop_sh.p, 0, m.nshells * 8, s);
+    cudaMemsetAsync(m.pop_dip.p, 0, 3 * m.natoms * 8, s);
+    cudaMemsetAsync(m.pop_qp.p, 0, 6 * m.natoms * 8, s);
+    cudaMemsetAsync(m.e_core.p, 0, B * 8, s);
+    launch_mulliken(a, m.max_n, s);
+    launch_energy_mixer(a, m.max_atoms, m.max_shells, m.max_dim, it == 0, s);
+    launch_compact(order, nsys, status, a.converged, a.iterations, req.max_iter, list, dcount, s);
+    cudaMemcpyAsync(m.h_count, dcount, 4, cudaMemcpyDeviceToHost, s);
+    cudaStreamSynchronize(s);
+    count = m.h_count[0];
+  }
+  k_finalize_status<<<(nsys + 255) / 256, 256, 0, s>>>(nsys, status, a.converged);
+
+  // ---- energy/force terms on converged systems ----
+  k_list_ok<<<1, 32, 0, s>>>(order, nsys, status, list, dcount);
+  cudaMemcpyAsync(m.h_count, dcount, 4, cudaMemcpyDeviceToHost, s);
+  cudaStreamSynchronize(s);
+  count = m.h_count[0];
+  const bool want_forces = (req.flags & XTBLOOM_COMPUTE_FORCES) != 0;
+  cudaMemsetAsync(m.grad.p, 0, 3 * N * 8, s);
+  cudaMemsetAsync(m.acn.p, 0, N * 8, s);
+  cudaMemsetAsync(m.acn_d4.p, 0, N * 8, s);
+  ForceArgs f{};
+  f.t = t;
+  f.list = list;
+  f.count = count;
+  f.cn = m.cn.as<double>();
+  f.cn_d4 = m.cn_d4.as<double>();
+  f.mrad = m.mrad.as<double>();
+  f.dmrad = m.dmrad.as<double>();
+  f.S = m.S.as<double>();
+  f.P = m.P.as<double>();
+  f.W = m.W.as<double>();
+  f.vsh = m.vsh.as<double>();
+  f.vd = m.vd.as<double>();
+  f.vq = m.vq.as<double>();
+  f.qsh = m.qsh.as<double>();
+  f.dip = m.dip.as<double>();
+  f.qp = m.qp.as<double>();
+  f.gam = m.gam.as<double>();
+  f.grad = m.grad.as<double>();
+  f.acn = m.acn.as<double>();
+  f.acn_d4 = m.acn_d4.as<double>();
+  f.terms = m.terms.as<double>();
+  f.want_grad = want_forces ? 1 : 0;
+  if (want_forces && count > 0) {
+    a.count = count;
+    launch_potential(a, a.qsh, a.dip, a.qp, m.max_atoms, m.max_shells, s);
+    gemm(m.C.as<double>(), m.C.as<double>(), m.W.as<double>(), dnao, dnao, dnvec, true,
+         m.occ_eps.as<double>(), count);
+    launch_force_pairs(f, m.max_pairs, s);
+  }
+  launch_classical(f, m.max_atoms, m.max_shells, s);
+  if (want_forces) launch_cn_chain(f, m.max_atoms, s);
+  k_publish<<<nsys, 128, 0, s>>>(t, status, m.free_energy.as<double>(), m.terms.as<double>(),
+                                  m.grad.as<double>(), m.qsh.as<double>(), m.out_energy.as<double>(),
+                                  m.out_forces.as<double>(), m.out_charges.as<double>());
+  // ---- copy into caller buffers ----
+  const xtbloom_batch_result_t& r = *req.result;
+  auto put = [&](const xtbloom_buffer_t& dst, const void* src, size_t bytes) {
+    if (!dst.data || bytes == 0) return cudaSuccess;
+    const cudaMemcpyKind kind =
+        dst.memory_space == XTBLOOM_MEMORY_CUDA_DEVICE ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost;
+    return cudaMemcpyAsync(dst.data, src, bytes, kind, s);
+  };
+  if (req.flags & XTBLOOM_COMPUTE_ENERGY) put(r.energies, m.out_energy.p, B * 8);
+  if (req.flags & XTBLOOM_COMPUTE_FORCES) put(r.forces, m.out_forces.p, 3 * N * 8);
+  if (req.flags & XTBLOOM_COMPUTE_ATOMIC_CHARGES) put(r.atomic_charges, m.out_charges.p, N * 8);
+  put(r.scc_iterations, m.iterations.p, B * 4);
+  put(r.scc_converged, m.converged.p, B);
+  put(r.per_system_status, status, B * 4);
+  const cudaError_t ce = cudaStreamSynchronize(s);
+  if (ce != cudaSuccess) {
+    error = std::string("CUDA failure: ") + cudaGetErrorString(ce);
+    return XTBLOOM_STATUS_INTERNAL_ERROR;
+  }
+  const cudaError_t le = cudaGetLastError();
+  if (le != cudaSuccess) {
+    error = std::string("CUDA launch failure: ") + cudaGetErrorString(le);
+    return XTBLOOM_STATUS_INTERNAL_ERROR;
+  }
+  m.have_results = true;
+  return XTBLOOM_STATUS_SUCCESS;
+}
+
+xtbloom_status_t Engine::debug_fetch(const std::string& name, int64_t system, double* out,
+                                     size_t capacity, size_t* count, std::string& error) {
+  Impl& m = *impl_;
+  if (!m.have_results || system < 0 || system >= m.nsys) {
+    error = "no retained results for that system";
+    return XTBLOOM_STATUS_INVALID_ARGUMENT;
+  }
+  cudaSetDevice(device_);
+  const int64_t a0 = m.topo.atom_off[system], na = m.topo.atom_off[system + 1] - a0;
+  std::vector<int64_t> mat_off(m.nsys + 1), ao_off(m.nsys + 1), sh_off(m.nsys + 1);
+  cudaMemcpy(mat_off.data(), m.mat_off.p, (m.nsys + 1) * 8, cudaMemcpyDeviceToHost);
+  cudaMemcpy(ao_off.data(), m.ao_off.p, (m.nsys + 1) * 8, cudaMemcpyDeviceToHost);
+  cudaMemcpy(sh_off.data(), m.shell_off.p, (m.nsys + 1) * 8, cudaMemcpyDeviceToHost);
+  const int64_t n = m.h_nao[system];
+  const double* src = nullptr;
+  size_t len = 0;
+  if (name == "cn") { src = m.cn.as<double>() + a0; len = na; }
+  else if (name == "cn_d4") { src = m.cn_d4.as<double>() + a0; len = na; }
+  else if (name == "overlap") { src = m.S.as<double>() + mat_off[system]; len = n * n; }
+  else if (name == "h0") { src = m.H0.as<double>() + mat_off[system]; len = n * n; }
+  else if (name == "x") { src = m.X.as<double>() + mat_off[system]; len = n * n; }
+  else if (name == "density") { src = m.P.as<double>() + mat_off[system]; len = n * n; }
+  else if (name == "hamiltonian") { src = m.H.as<double>() + mat_off[system]; len = n * n; }
+  else if (name == "eigenvalues") { src = m.eig.as<double>() + ao_off[system]; len = n; }
+  else if (name == "occupations") { src = m.occ.as<double>() + ao_off[system]; len = n; }
+  else if (name == "qsh") { src = m.qsh.as<double>() + sh_off[system]; len = sh_off[system + 1] - sh_off[system]; }
+  else if (name == "dipoles") { src = m.dip.as<double>() + 3 * a0; len = 3 * na; }
+  else if (name == "quadrupoles") { src = m.qp.as<double>() + 6 * a0; len = 6 * na; }
+  else if (name == "energy_terms") { src = m.terms.as<double>() + 8 * system; len = 8; }
+  else if (name == "gradient") { src = m.grad.as<double>() + 3 * a0; len = 3 * na; }
+  else if (name == "dipole_integrals") {
+    if (capacity < 3 * (size_t)(n * n)) { error = "capacity too small"; return XTBLOOM_STATUS_INVALID_ARGUMENT; }
+    for (int c = 0; c < 3; ++c)
+      cudaMemcpy(out + c * n * n, m.D.as<double>() + c * m.total_mat + mat_off[system], n * n * 8, cudaMemcpyDeviceToHost);
+    *count = 3 * n * n;
+    return XTBLOOM_STATUS_SUCCESS;
+  } else if (name == "quadrupole_integrals") {
+    if (capacity < 6 * (size_t)(n * n)) { error = "capacity too small"; return XTBLOOM_STATUS_INVALID_ARGUMENT; }
+    for (int c = 0; c < 6; ++c)
+      cudaMemcpy(out + c * n * n, m.Q.as<double>() + c * m.total_mat + mat_off[system], n * n * 8, cudaMemcpyDeviceToHost);
+    *count = 6 * n * n;
+    return XTBLOOM_STATUS_SUCCESS;
+  } else {
+    error = "unknown diagnostics name";
+    return XTBLOOM_STATUS_INVALID_ARGUMENT;
+  }
+  if (capacity < len) {
+    error = "capacity too small";
+    return XTBLOOM_STATUS_INVALID_ARGUMENT;
+  }
+  cudaMemcpy(out, src, len * 8, cudaMemcpyDeviceToHost);
+  *count = len;
+  return XTBLOOM_STATUS_SUCCESS;
+}
+
+}  // namespace xtb

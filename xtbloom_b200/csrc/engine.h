@@ -1,0 +1,56 @@
+// Host orchestration of the batched GFN2-xTB single point on one GPU.
+#pragma once
+
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include <cuda_runtime.h>
+
+#include "xtbloom.h"
+
+namespace xtb {
+
+struct HostBatch {
+  int64_t nsys = 0;
+  std::vector<int64_t> atom_off;
+  std::vector<int32_t> Z;
+  std::vector<double> qmol;
+  std::vector<int32_t> uhf;
+};
+
+struct ComputeRequest {
+  const xtbloom_batch_t* batch = nullptr;
+  const xtbloom_compute_options_t* options = nullptr;
+  const xtbloom_batch_result_t* result = nullptr;
+  // normalised options
+  uint32_t flags = 0;
+  int32_t max_iter = 250;
+  double ctol = 1e-6, etol = 1e-8, kt = 0.0;
+  int32_t memory = 8;
+  double damping = 0.4;
+};
+
+class Engine {
+ public:
+  Engine(int device, cudaStream_t stream);
+  ~Engine();
+  Engine(const Engine&) = delete;
+  Engine& operator=(const Engine&) = delete;
+
+  // Runs one batch; returns an ABI status and fills error on failure.
+  xtbloom_status_t compute(const ComputeRequest& req, std::string& error);
+  xtbloom_status_t debug_fetch(const std::string& name, int64_t system, double* out,
+                               size_t capacity, size_t* count, std::string& error);
+  int device() const { return device_; }
+  cudaStream_t stream() const { return stream_; }
+
+  struct Impl;
+
+ private:
+  Impl* impl_;
+  int device_;
+  cudaStream_t stream_;
+};
+
+}  // namespace xtb

@@ -1,0 +1,440 @@
+// Analytic gradient of the converged GFN2 energy.
+//
+//  * k_force_pairs: one thread per atom pair recomputes the shell-pair
+//    overlap/multipole integrals with their derivatives and contracts them on
+//    the fly with the adjoints P*dH0/dS - W and the stationary S/D/Q
+//    potential adjoints (so dS/dR is never stored), adds the H0 distance
+//    polynomial term and accumulates dE/dCN (model/gfn2/force.cpp:256-300,
+//    520-560; model/gfn2/h0.cpp:469-597; common/integrals.cpp:440-496,867-1145).
+//  * k_classical: ES2, AES2 (with the multipole-radius CN chain), D4
+//    two-body at fixed charges, D4 ATM and repulsion energies/gradients
+//    (model/gfn2/es2.cpp:1040-1110, aes2.cpp:596-713, d4.cpp:1034-1362,
+//    repulsion.cpp:93-176).
+//  * k_cn_chain: chain rule through both coordination numbers.
+#include "classical.cuh"
+#include "integrals.cuh"
+#include "kernels.cuh"
+
+namespace xtb {
+
+__device__ __forceinline__ double lev(const DevTopo& t, int sh, const double* cn) {
+  return t.sh_level[sh] - t.sh_kcn[sh] * cn[t.sh_atom[sh]];
+}
+
+__global__ void __launch_bounds__(128) k_force_pairs(ForceArgs f) {
+  const DevTopo& t = f.t;
+  const int s = f.list[blockIdx.y];
+  const int64_t a0 = t.atom_off[s], na = t.atom_off[s + 1] - a0;
+  const int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= na * (na + 1) / 2) return;
+  int64_t A = (int64_t)((sqrt(1.0 + 8.0 * (double)p) - 1.0) * 0.5);
+  while (A * (A + 1) / 2 > p) --A;
+  while ((A + 1) * (A + 2) / 2 <= p) ++A;
+  const int64_t B = p - A * (A + 1) / 2;
+  const int64_t gA = a0 + A, gB = a0 + B;
+  const int n = t.nao[s];
+  const int64_t mo = t.mat_off[s];
+  const double* P = f.P + mo;
+  const double* W = f.W + mo;
+  if (A == B) return;   // onsite blocks: k_force_onsite
+  const double v[3] = {t.pos[3 * gA] - t.pos[3 * gB], t.pos[3 * gA + 1] - t.pos[3 * gB + 1],
+                       t.pos[3 * gA + 2] - t.pos[3 * gB + 2]};
+  const double r = sqrt(v[0] * v[0] + v[1] * v[1] + v[2] * v[2]);
+  const double* vdA = f.vd + 3 * gA;
+  const double* vdB = f.vd + 3 * gB;
+  const double* vqA = f.vq + 6 * gA;
+  const double* vqB = f.vq + 6 * gB;
+  double g[3] = {0.0, 0.0, 0.0};
+  double cnA = 0.0, cnB = 0.0;
+  for (int ks = t.atom_sh[gA]; ks < t.atom_sh[gA + 1]; ++ks) {
+    const int lk = t.sh_l[ks];
+    const int npk = t.sh_np[ks];
+    const double* ak = t.p_alpha + t.sh_p0[ks];
+    const double* ck = t.p_coeff + t.sh_p0[ks];
+    const double vk = f.vsh[ks];
+    for (int bs = t.atom_sh[gB]; bs < t.atom_sh[gB + 1]; ++bs) {
+      const int lb = t.sh_l[bs];
+      const int npb = t.sh_np[bs];
+      const double* ab = t.p_alpha + t.sh_p0[bs];
+      const double* cb = t.p_coeff + t.sh_p0[bs];
+      const double vb = f.vsh[bs];
+      // H0 factor pieces
+      const double avg = 0.5 * (lev(t, bs, f.cn) + lev(t, ks, f.cn));
+      const double zi = t.sh_zeta[bs], zj = t.sh_zeta[ks];
+      const double zs = pow(2.0 * sqrt(zi * zj) / (zi + zj), t.m.wexp);
+      const double den = t.at_en[gB] - t.at_en[gA];
+      const double ps = zs * (1.0 + t.m.enscale * den * den) *
+                        t.m.shell_pair_scale[lb * 3 + lk] * t.m.pair_scale_default;
+      const double rr = sqrt(r / (t.at_rad[gB] + t.at_rad[gA]));
+      const double p1 = 1.0 + t.sh_shpoly[bs] * rr, p2 = 1.0 + t.sh_shpoly[ks] * rr;
+      const double spat = ps * p1 * p2;
+      const double dspat = ps * (t.sh_shpoly[bs] * p2 + t.sh_shpoly[ks] * p1) * rr / (2.0 * r);
+      const double fac = avg * spat;
+      double bw = 0.0;
+      for (int ib = 0; ib < 2 * lb + 1; ++ib) {
+        const int64_t row = t.sh_ao[bs] + ib;
+        for (int ik = 0; ik < 2 * lk + 1; ++ik) {
+          const int64_t col = t.sh_ao[ks] + ik;
+          const double Pv = P[row * n + col];
+          const double Wv = W[row * n + col];
+          double val[10], dv[3][10];
+          sph_pair<true>(lb, ib, lk, ik, ab, cb, npb, ak, ck, npk, v, val, dv);
+          const double S = val[0];
+          bw += Pv * S;
+          const double sA = 2.0 * (Pv * fac - Wv) - Pv * (vb + vk);
+          double fD[3], rD[3], qadj[6], rQ[6];
+#pragma unroll
+          for (int c = 0; c < 3; ++c) {
+            fD[c] = -Pv * vdA[c];
+            rD[c] = -Pv * vdB[c];
+          }
+#pragma unroll
+          for (int c = 0; c < 6; ++c) {
+            rQ[c] = -Pv * vqB[c];
+            qadj[c] = -Pv * vqA[c] + rQ[c];
+          }
+          const double dsum = rQ[0] + rQ[2] + rQ[5];
+          const double axx = 1.5 * rQ[0] - 0.5 * dsum, axy = 1.5 * rQ[1];
+          const double ayy = 1.5 * rQ[2] - 0.5 * dsum, axz = 1.5 * rQ[3];
+          const double ayz = 1.5 * rQ[4], azz = 1.5 * rQ[5] - 0.5 * dsum;
+          const double x = v[0], y = v[1], z = v[2];
+          const double sadj = sA + rD[0] * x + rD[1] * y + rD[2] * z + axx * x * x + axy * x * y +
+                              ayy * y * y + axz * x * z + ayz * y * z + azz * z * z;
+          const double dadj[3] = {fD[0] + rD[0] + 2.0 * axx * x + axy * y + axz * z,
+                                  fD[1] + rD[1] + axy * x + 2.0 * ayy * y + ayz * z,
+                                  fD[2] + rD[2] + axz * x + ayz * y + 2.0 * azz * z};
+          const double Dx = val[1], Dy = val[2], Dz = val[3];
+          const double vadj[3] = {
+              rD[0] * S + axx * (2.0 * Dx + 2.0 * x * S) + axy * (Dy + y * S) + axz * (Dz + z * S),
+              rD[1] * S + axy * (Dx + x * S) + ayy * (2.0 * Dy + 2.0 * y * S) + ayz * (Dz + z * S),
+              rD[2] * S + axz * (Dx + x * S) + ayz * (Dy + y * S) + azz * (2.0 * Dz + 2.0 * z * S)};
+#pragma unroll
+          for (int c = 0; c < 3; ++c) {
+            double acc = vadj[c] + sadj * dv[c][0];
+#pragma unroll
+            for (int k = 0; k < 3; ++k) acc += dadj[k] * dv[c][1 + k];
+#pragma unroll
+            for (int k = 0; k < 6; ++k) acc += qadj[k] * dv[c][4 + k];
+            g[c] += acc;
+          }
+        }
+      }
+      const double rad = 2.0 * bw * avg * dspat / r;
+      g[0] += rad * v[0];
+      g[1] += rad * v[1];
+      g[2] += rad * v[2];
+      cnB -= t.sh_kcn[bs] * bw * spat;
+      cnA -= t.sh_kcn[ks] * bw * spat;
+    }
+  }
+  if (f.want_grad) {
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      atomicAdd(&f.grad[3 * gA + c], g[c]);
+      atomicAdd(&f.grad[3 * gB + c], -g[c]);
+    }
+  }
+  atomicAdd(&f.acn[gA], cnA);
+  atomicAdd(&f.acn[gB], cnB);
+}
+
+// Onsite CN adjoint of the shell levels: one thread per atom.
+__global__ void k_force_onsite(ForceArgs f) {
+  const DevTopo& t = f.t;
+  const int s = f.list[blockIdx.y];
+  const int64_t a0 = t.atom_off[s], na = t.atom_off[s + 1] - a0;
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= na) return;
+  const int64_t gA = a0 + i;
+  const int n = t.nao[s];
+  const double* P = f.P + t.mat_off[s];
+  const double* S = f.S + t.mat_off[s];
+  double acc = 0.0;
+  for (int x = t.atom_sh[gA]; x < t.atom_sh[gA + 1]; ++x) {
+    for (int y = t.atom_sh[gA]; y < t.atom_sh[gA + 1]; ++y) {
+      double bw = 0.0;
+      for (int k = 0; k < 2 * t.sh_l[x] + 1; ++k)
+        for (int l = 0; l < 2 * t.sh_l[y] + 1; ++l) {
+          const int64_t idx = (int64_t)(t.sh_ao[x] + k) * n + t.sh_ao[y] + l;
+          bw += P[idx] * S[idx];
+        }
+      acc -= 0.5 * bw * (t.sh_kcn[x] + t.sh_kcn[y]);
+    }
+  }
+  atomicAdd(&f.acn[gA], acc);
+}
+
+void launch_force_pairs(const ForceArgs& f, int64_t max_pairs, cudaStream_t stream) {
+  if (f.count == 0) return;
+  const int tpb = 128;
+  dim3 grid((unsigned)((max_pairs + tpb - 1) / tpb), f.count);
+  k_force_pairs<<<grid, tpb, 0, stream>>>(f);
+}
+
+// ---------------------------------------------------------------------------
+// Classical terms: one CTA per system, gradients accumulated in shared memory.
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(256) k_classical(ForceArgs f) {
+  extern __shared__ double sm[];
+  const DevTopo& t = f.t;
+  const int s = f.list[blockIdx.x];
+  const int64_t a0 = t.atom_off[s];
+  const int na = (int)(t.atom_off[s + 1] - a0);
+  const int64_t s0 = t.shell_off[s];
+  const int ns = (int)(t.shell_off[s + 1] - s0);
+  double* gr = sm;                         // 3 na
+  double* acn = gr + 3 * na;               // na (dexp)
+  double* acn4 = acn + na;                 // na (D4)
+  double* qat = acn4 + na;                 // na
+  double* w = qat + na;                    // 7 na (charged weights)
+  double* wcn = w + kMaxD4Refs * na;       // 7 na (d w / d cn)
+  double* w0 = wcn + kMaxD4Refs * na;      // 7 na (zero-charge weights)
+  double* w0cn = w0 + kMaxD4Refs * na;     // 7 na
+  double* red = w0cn + kMaxD4Refs * na;    // 40
+  const int tid = threadIdx.x, bs = blockDim.x;
+  const bool grad = f.want_grad != 0;
+  for (int i = tid; i < na; i += bs) {
+    const int64_t g = a0 + i;
+    gr[3 * i] = gr[3 * i + 1] = gr[3 * i + 2] = 0.0;
+    acn[i] = 0.0;
+    acn4[i] = 0.0;
+    double q = 0.0;
+    for (int sh = t.atom_sh[g]; sh < t.atom_sh[g + 1]; ++sh) q += f.qsh[sh];
+    qat[i] = q;
+    d4_weights(t, t.Z[g], f.cn_d4[g], q, w + kMaxD4Refs * i, wcn + kMaxD4Refs * i, nullptr);
+    d4_weights(t, t.Z[g], f.cn_d4[g], 0.0, w0 + kMaxD4Refs * i, w0cn + kMaxD4Refs * i, nullptr);
+  }
+  __syncthreads();
+  double erep = 0.0, eatm = 0.0;
+  const double* gam = f.gam + t.gam_off[s];
+  const int64_t npair = (int64_t)na * (na - 1) / 2;
+  for (int64_t p = tid; p < npair; p += bs) {
+    int64_t ii, jj;
+    pair_from_index(p, ii, jj);     // ii > jj
+    const int i = (int)ii, j = (int)jj;
+    const int64_t gi = a0 + i, gj = a0 + j;
+    const double d[3] = {t.pos[3 * gi] - t.pos[3 * gj], t.pos[3 * gi + 1] - t.pos[3 * gj + 1],
+                         t.pos[3 * gi + 2] - t.pos[3 * gj + 2]};
+    const double r2 = d[0] * d[0] + d[1] * d[1] + d[2] * d[2];
+    const double r = sqrt(r2);
+    double gs = 0.0;   // scalar multiplying d for pair (i <- j)
+    // repulsion
+    if (r2 <= 625.0) {
+      const bool light = t.Z[gi] <= 2 && t.Z[gj] <= 2;
+      const double k = light ? t.m.rep_klight : t.m.rep_kexp;
+      const double rp = light ? r : r * sqrt(r);
+      const double pa = t.at_rep_sa[gi] * t.at_rep_sa[gj];
+      const double pe = t.at_rep_z[gi] * t.at_rep_z[gj] * exp(-pa * rp) / r;
+      erep += pe;
+      gs -= (pa * k * rp + 1.0) * pe / r2;
+    }
+    if (grad) {
+      // ES2 at fixed shell charges
+      double wsum = 0.0;
+      for (int x = t.atom_sh[gi]; x < t.atom_sh[gi + 1]; ++x)
+        for (int y = t.atom_sh[gj]; y < t.atom_sh[gj + 1]; ++y) {
+          const double gv = gam[(int64_t)(x - s0) * ns + (y - s0)];
+          wsum += f.qsh[x] * f.qsh[y] * gv * gv * gv;
+        }
+      gs -= wsum;
+      // D4 two-body at fixed charges; pair orientation (first = j, second = i)
+      double damp, ddamp;
+      d4_pair_damping(t, t.Z[gj], t.Z[gi], r2, damp, ddamp);
+      if (damp != 0.0) {
+        double cj, ci;
+        const double c6 = d4_c6(t, t.Z[gj], t.Z[gi], w + kMaxD4Refs * j, w + kMaxD4Refs * i,
+                                wcn + kMaxD4Refs * j, wcn + kMaxD4Refs * i, &cj, &ci);
+        // gradient[first=j] += -c6*ddamp*(R_j - R_i), i.e. gradient[i] += -c6*ddamp*d
+        gs -= c6 * ddamp;
+        atomicAdd(&acn4[j], -cj * damp);
+        atomicAdd(&acn4[i], -ci * damp);
+      }
+      // AES2: first = j, second = i, displacement dd = R_j - R_i = -d
+      {
+        const double dd[3] = {-d[0], -d[1], -d[2]};
+        const double R = 0.5 * (f.mrad[gj] + f.mrad[gi]);
+        double k3, k5;
+        aes2_kernels(r, R, k3, k5);
+        const double sc = R / r;
+        const double f3 = 1.0 / (1.0 + 6.0 * sc * sc * sc);
+        const double f5 = 1.0 / (1.0 + 6.0 * sc * sc * sc * sc);
+        const double* dpf = f.dip + 3 * gj;
+        const double* dps = f.dip + 3 * gi;
+        const double* qf = f.qp + 6 * gj;
+        const double* qs = f.qp + 6 * gi;
+        const double qfv = qat[j], qsv = qat[i];
+        double cdv[3], pf = 0.0, ps = 0.0, ddt = 0.0;
+        for (int c = 0; c < 3; ++c) {
+          cdv[c] = qfv * dps[c] - qsv * dpf[c];
+          pf += dd[c] * dpf[c];
+          ps += dd[c] * dps[c];
+          ddt += dpf[c] * dps[c];
+        }
+        const double cdn = dd[0] * cdv[0] + dd[1] * cdv[1] + dd[2] * cdv[2];
+        const double ddn = r2 * ddt - 3.0 * pf * ps;
+        double T[6];
+        for (int c = 0; c < 6; ++c) T[c] = qfv * qs[c] + qsv * qf[c];
+        const double tv[3] = {T[0] * dd[0] + T[1] * dd[1] + T[3] * dd[2],
+                              T[1] * dd[0] + T[2] * dd[1] + T[4] * dd[2],
+                              T[3] * dd[0] + T[4] * dd[1] + T[5] * dd[2]};
+        const double cqn = dd[0] * tv[0] + dd[1] * tv[1] + dd[2] * tv[2];
+        const double k3d = -3.0 * f3 * k3 / r;
+        const double k5d = -(1.0 + 4.0 * f5) * k5 / r;
+        const double k3r = -3.0 * (1.0 - f3) * k3 / R;
+        const double k5r = -4.0 * (1.0 - f5) * k5 / R;
+        const double k5n = ddn + cqn;
+        const double erd = k3r * cdn + k5r * k5n;
+        for (int c = 0; c < 3; ++c) {
+          const double ddd = 2.0 * ddt * dd[c] - 3.0 * (pf * dps[c] + ps * dpf[c]);
+          const double gc = k3 * cdv[c] + k3d * cdn * dd[c] / r + k5 * (ddd + 2.0 * tv[c]) +
+                            k5d * k5n * dd[c] / r;
+          atomicAdd(&gr[3 * j + c], gc);
+          atomicAdd(&gr[3 * i + c], -gc);
+        }
+        atomicAdd(&acn[j], 0.5 * erd * f.dmrad[gj]);
+        atomicAdd(&acn[i], 0.5 * erd * f.dmrad[gi]);
+      }
+    }
+    if (grad) {
+      for (int c = 0; c < 3; ++c) {
+        atomicAdd(&gr[3 * i + c], gs * d[c]);
+        atomicAdd(&gr[3 * j + c], -gs * d[c]);
+      }
+    }
+    // ATM triples (i > j > k) with all three distances within 25 bohr
+    if (r2 > 625.0) continue;
+    const int zi = t.Z[gi], zj = t.Z[gj];
+    double cij_i, cij_j;
+    const double cij = d4_c6(t, zi, zj, w0 + kMaxD4Refs * i, w0 + kMaxD4Refs * j,
+                             w0cn + kMaxD4Refs * i, w0cn + kMaxD4Refs * j, &cij_i, &cij_j);
+    const double r0ij = d4_r0(t, zi, zj);
+    for (int k = 0; k < j; ++k) {
+      const int64_t gk = a0 + k;
+      const double vik[3] = {t.pos[3 * gk] - t.pos[3 * gi], t.pos[3 * gk + 1] - t.pos[3 * gi + 1],
+                             t.pos[3 * gk + 2] - t.pos[3 * gi + 2]};
+      const double vjk[3] = {t.pos[3 * gk] - t.pos[3 * gj], t.pos[3 * gk + 1] - t.pos[3 * gj + 1],
+                             t.pos[3 * gk + 2] - t.pos[3 * gj + 2]};
+      const double r2ik = vik[0] * vik[0] + vik[1] * vik[1] + vik[2] * vik[2];
+      const double r2jk = vjk[0] * vjk[0] + vjk[1] * vjk[1] + vjk[2] * vjk[2];
+      if (r2ik > 625.0 || r2jk > 625.0) continue;
+      const int zk = t.Z[gk];
+      double cik_i, cik_k, cjk_j, cjk_k;
+      const double cik = d4_c6(t, zi, zk, w0 + kMaxD4Refs * i, w0 + kMaxD4Refs * k,
+                               w0cn + kMaxD4Refs * i, w0cn + kMaxD4Refs * k, &cik_i, &cik_k);
+      const double cjk = d4_c6(t, zj, zk, w0 + kMaxD4Refs * j, w0 + kMaxD4Refs * k,
+                               w0cn + kMaxD4Refs * j, w0cn + kMaxD4Refs * k, &cjk_j, &cjk_k);
+      const double r0ik = d4_r0(t, zi, zk), r0jk = d4_r0(t, zj, zk);
+      const double r2ij = r2;
+      const double r2p = r2ij * r2ik * r2jk;
+      const double r1p = sqrt(r2p);
+      const double r3p = r2p * r1p;
+      const double r5p = r3p * r2p;
+      const double ratio = r0ij * r0ik * r0jk / r1p;
+      const double rpow = pow(ratio, 16.0 / 3.0);
+      const double damp = 1.0 / (1.0 + 6.0 * rpow);
+      const double ang = 0.375 * (r2ij + r2jk - r2ik) * (r2ij - r2jk + r2ik) * (-r2ij + r2jk + r2ik) / r5p +
+                         1.0 / r3p;
+      const double prod = cij * cik * cjk;
+      const double c9 = -t.m.d4_s9 * sqrt(fabs(prod));
+      eatm -= ang * damp * c9;
+      if (!grad || !(cij > 0.0) || !(cik > 0.0) || !(cjk > 0.0)) continue;
+      const double ddmp = -2.0 * 16.0 * rpow * damp * damp;
+      auto dg = [&](double tt, double o1, double o2) {
+        const double dang = -0.375 *
+                            (tt * tt * tt + tt * tt * (o1 + o2) + tt * (3.0 * o1 * o1 + 2.0 * o1 * o2 + 3.0 * o2 * o2) -
+                             5.0 * (o1 - o2) * (o1 - o2) * (o1 + o2)) / r5p;
+        return c9 * (-dang * damp + ang * ddmp) / tt;
+      };
+      // vij = R_i - R_j in the reference's pair cache (first = j, second = i)
+      const double vij[3] = {t.pos[3 * gj] - t.pos[3 * gi], t.pos[3 * gj + 1] - t.pos[3 * gi + 1],
+                             t.pos[3 * gj + 2] - t.pos[3 * gi + 2]};
+      const double sij = dg(r2ij, r2jk, r2ik);
+      const double sik = dg(r2ik, r2jk, r2ij);
+      const double sjk = dg(r2jk, r2ik, r2ij);
+      for (int c = 0; c < 3; ++c) {
+        const double gij = sij * vij[c], gik = sik * vik[c], gjk = sjk * vjk[c];
+        atomicAdd(&gr[3 * i + c], -(gij + gik));
+        atomicAdd(&gr[3 * j + c], gij - gjk);
+        atomicAdd(&gr[3 * k + c], gik + gjk);
+      }
+      const double de = ang * damp * c9;
+      atomicAdd(&acn4[i], -0.5 * de * (cij_i / cij + cik_i / cik));
+      atomicAdd(&acn4[j], -0.5 * de * (cij_j / cij + cjk_j / cjk));
+      atomicAdd(&acn4[k], -0.5 * de * (cik_k / cik + cjk_k / cjk));
+    }
+  }
+  erep = block_sum(erep, red);
+  eatm = block_sum(eatm, red);
+  if (tid == 0) {
+    f.terms[8 * (int64_t)s + 6] = erep;
+    f.terms[8 * (int64_t)s + 7] = eatm;
+  }
+  if (!grad) return;
+  for (int i = tid; i < na; i += bs) {
+    const int64_t g = a0 + i;
+    for (int c = 0; c < 3; ++c) atomicAdd(&f.grad[3 * g + c], gr[3 * i + c]);
+    atomicAdd(&f.acn[g], acn[i]);
+    atomicAdd(&f.acn_d4[g], acn4[i]);
+  }
+}
+
+void launch_classical(const ForceArgs& f, int max_atoms, int max_shells, cudaStream_t stream) {
+  (void)max_shells;
+  if (f.count == 0) return;
+  const size_t sm = ((size_t)(7 + 4 * kMaxD4Refs) * max_atoms + 48) * sizeof(double);
+  static const bool attr = cudaFuncSetAttribute(k_classical, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024) == cudaSuccess;
+  (void)attr;
+  k_classical<<<f.count, 256, sm, stream>>>(f);
+}
+
+// Chain rule through the double-exponential CN (acn) and the D4 CN (acn_d4).
+__global__ void __launch_bounds__(256) k_cn_chain(ForceArgs f) {
+  const DevTopo& t = f.t;
+  const int s = f.list[blockIdx.x];
+  const int64_t a0 = t.atom_off[s];
+  const int na = (int)(t.atom_off[s + 1] - a0);
+  const int64_t npair = (int64_t)na * (na - 1) / 2;
+  for (int64_t p = threadIdx.x; p < npair; p += blockDim.x) {
+    int64_t ii, jj;
+    pair_from_index(p, ii, jj);
+    const int64_t gi = a0 + ii, gj = a0 + jj;
+    const double d[3] = {t.pos[3 * gi] - t.pos[3 * gj], t.pos[3 * gi + 1] - t.pos[3 * gj + 1],
+                         t.pos[3 * gi + 2] - t.pos[3 * gj + 2]};
+    const double r2 = d[0] * d[0] + d[1] * d[1] + d[2] * d[2];
+    const double r = sqrt(r2);
+    double sc = 0.0;
+    if (r2 <= 625.0) {
+      const double rad = t.at_rcov[gi] + t.at_rcov[gj];
+      const double f1 = logistic(10.0 * (rad / r - 1.0));
+      const double f2 = logistic(20.0 * ((rad + 2.0) / r - 1.0));
+      const double dv = -(10.0 * rad * f1 * (1.0 - f1) * f2 + 20.0 * (rad + 2.0) * f2 * (1.0 - f2) * f1) / r2;
+      sc += (f.acn[gi] + f.acn[gj]) * dv / r;
+    }
+    if (r2 <= 900.0) {
+      const int zi = t.Z[gi] - 1, zj = t.Z[gj] - 1;
+      const double rc = t.d4_rcov[zi] + t.d4_rcov[zj];
+      const double den = fabs(t.d4_en[zi] - t.d4_en[zj]);
+      const double enf = 4.10451 * exp(-(den + 19.08857) * (den + 19.08857) / (2.0 * 11.28174 * 11.28174));
+      const double x = 7.5 * (r - rc) / rc;
+      const double dv = -enf * 7.5 * exp(-x * x) / sqrt(kPi) / rc;
+      sc += (f.acn_d4[gi] + f.acn_d4[gj]) * dv / r;
+    }
+    if (sc != 0.0) {
+      for (int c = 0; c < 3; ++c) {
+        atomicAdd(&f.grad[3 * gi + c], sc * d[c]);
+        atomicAdd(&f.grad[3 * gj + c], -sc * d[c]);
+      }
+    }
+  }
+}
+
+void launch_cn_chain(const ForceArgs& f, int max_atoms, cudaStream_t stream) {
+  if (f.count == 0) return;
+  (void)max_atoms;
+  // onsite shell-level CN adjoints first, then the pair chain rule
+  dim3 g1((unsigned)((max_atoms + 127) / 128), f.count);
+  k_force_onsite<<<g1, 128, 0, stream>>>(f);
+  k_cn_chain<<<f.count, 256, 0, stream>>>(f);
+}
+
+}  // namespace xtb

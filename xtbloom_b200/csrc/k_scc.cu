@@ -1,0 +1,610 @@
+// Per-iteration SCC kernels: SAD start, potentials (ES2 + ES3 + AES2 + D4),
+// Fock build, Mulliken populations with the band trace, and the fused energy
+// functional + modified-Broyden mixer + convergence gate.
+//
+// Restated from model/gfn2/scc_driver.cpp:706-960 (iteration order),
+// 2105-2560 (energy functional, potentials), model/gfn2/mulliken_kernels_impl.hpp
+// (population and Hamiltonian contractions), model/gfn2/aes2.cpp:451-594
+// (AES2 potentials/energy), model/gfn2/d4.cpp:730-980 (self-consistent D4),
+// model/gfn2/es3.cpp:190-230 and common/scc_mixer.cpp:559-740 (Broyden).
+#include "classical.cuh"
+#include "kernels.cuh"
+
+#include <cfloat>
+
+namespace xtb {
+
+__global__ void k_sad_init(SccArgs a) {
+  const int s = a.list[blockIdx.x];
+  const DevTopo& t = a.t;
+  const int64_t a0 = t.atom_off[s], na = t.atom_off[s + 1] - a0;
+  const int64_t s0 = t.shell_off[s], ns = t.shell_off[s + 1] - s0;
+  const int64_t v0 = t.vec_off[s];
+  const double qa = t.qmol[s] / (double)na;
+  for (int64_t i = threadIdx.x; i < na; i += blockDim.x) {
+    const int64_t g = a0 + i;
+    double ref = 0.0;
+    for (int sh = t.atom_sh[g]; sh < t.atom_sh[g + 1]; ++sh) ref += t.sh_refocc[sh];
+    for (int sh = t.atom_sh[g]; sh < t.atom_sh[g + 1]; ++sh) {
+      const double q = t.sh_refocc[sh] / ref * qa;
+      a.qsh[sh] = q;
+      a.mx_cur[v0 + (sh - s0)] = q;
+    }
+    for (int c = 0; c < 3; ++c) {
+      a.dip[3 * g + c] = 0.0;
+      a.mx_cur[v0 + ns + 3 * i + c] = 0.0;
+    }
+    for (int c = 0; c < 6; ++c) {
+      a.qp[6 * g + c] = 0.0;
+      a.mx_cur[v0 + ns + 3 * na + 6 * i + c] = 0.0;
+    }
+  }
+  if (threadIdx.x == 0) {
+    a.iterations[s] = 0;
+    a.converged[s] = 0;
+    a.free_energy[s] = 0.0;
+  }
+}
+
+void launch_sad_init(const SccArgs& a, cudaStream_t stream) {
+  if (a.count == 0) return;
+  k_sad_init<<<a.count, 128, 0, stream>>>(a);
+}
+
+// ---------------------------------------------------------------------------
+// Potentials from (qsh, dip, qp): vsh = gamma q + g3 q^2 + vat(atom);
+// vat, vd, vq from AES2 and the D4 charge response.
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(256) k_potential(SccArgs a, const double* qsh, const double* dip,
+                                                   const double* qp) {
+  extern __shared__ double sm[];
+  const DevTopo& t = a.t;
+  const int s = a.list[blockIdx.x];
+  const int64_t a0 = t.atom_off[s];
+  const int na = (int)(t.atom_off[s + 1] - a0);
+  const int64_t s0 = t.shell_off[s];
+  const int ns = (int)(t.shell_off[s + 1] - s0);
+  double* qat = sm;
+  double* vat = qat + na;
+  double* svd = vat + na;
+  double* svq = svd + 3 * na;
+  double* w = svq + 6 * na;                 // na * 7
+  double* dwq = w + kMaxD4Refs * na;        // na * 7
+  double* sq = dwq + kMaxD4Refs * na;       // ns
+  const int tid = threadIdx.x, bs = blockDim.x;
+  for (int i = tid; i < na; i += bs) {
+    const int64_t g = a0 + i;
+    double q = 0.0;
+    for (int sh = t.atom_sh[g]; sh < t.atom_sh[g + 1]; ++sh) q += qsh[sh];
+    qat[i] = q;
+    vat[i] = 0.0;
+    const double dk2 = 2.0 * t.at_dk[g], qk2 = 2.0 * t.at_qk[g];
+    for (int c = 0; c < 3; ++c) svd[3 * i + c] = dk2 * dip[3 * g + c];
+    const double scl[6] = {1.0, 2.0, 1.0, 2.0, 2.0, 1.0};
+    for (int c = 0; c < 6; ++c) svq[6 * i + c] = qk2 * scl[c] * qp[6 * g + c];
+    const int z = t.Z[g];
+    d4_weights(t, z, a.cn_d4[g], q, w + kMaxD4Refs * i, nullptr, dwq + kMaxD4Refs * i);
+  }
+  for (int i = tid; i < ns; i += bs) sq[i] = qsh[s0 + i];
+  __syncthreads();
+  const int64_t npair = (int64_t)na * (na - 1) / 2;
+  for (int64_t p = tid; p < npair; p += bs) {
+    int64_t si, fi;
+    pair_from_index(p, si, fi);      // si > fi
+    const int f = (int)fi, sc = (int)si;
+    const int64_t gf = a0 + f, gs = a0 + sc;
+    const double d[3] = {t.pos[3 * gf] - t.pos[3 * gs], t.pos[3 * gf + 1] - t.pos[3 * gs + 1],
+                         t.pos[3 * gf + 2] - t.pos[3 * gs + 2]};
+    const double r2 = d[0] * d[0] + d[1] * d[1] + d[2] * d[2];
+    const double r = sqrt(r2);
+    // AES2
+    double k3, k5;
+    aes2_kernels(r, 0.5 * (a.mrad[gf] + a.mrad[gs]), k3, k5);
+    const double* df = dip + 3 * gf;
+    const double* ds = dip + 3 * gs;
+    const double* qf = qp + 6 * gf;
+    const double* qs = qp + 6 * gs;
+    const double sqv[6] = {d[0] * d[0] * k5, 2.0 * d[0] * d[1] * k5, d[1] * d[1] * k5,
+                           2.0 * d[0] * d[2] * k5, 2.0 * d[1] * d[2] * k5, d[2] * d[2] * k5};
+    const double iso = r2 * k5;
+    double pf = 0.0, ps = 0.0, sdf = 0.0, sds = 0.0, tqf = 0.0, tqs = 0.0;
+    for (int c = 0; c < 3; ++c) {
+      pf += d[c] * df[c];
+      ps += d[c] * ds[c];
+      sdf += d[c] * k3 * df[c];
+      sds += d[c] * k3 * ds[c];
+    }
+    for (int c = 0; c < 6; ++c) {
+      tqf += sqv[c] * qf[c];
+      tqs += sqv[c] * qs[c];
+    }
+    double vf = sds + tqs;
+    double vs = -sdf + tqf;
+    for (int c = 0; c < 3; ++c) {
+      atomicAdd(&svd[3 * f + c], -qat[sc] * d[c] * k3 + iso * ds[c] - 3.0 * k5 * d[c] * ps);
+      atomicAdd(&svd[3 * sc + c], qat[f] * d[c] * k3 + iso * df[c] - 3.0 * k5 * d[c] * pf);
+    }
+    for (int c = 0; c < 6; ++c) {
+      atomicAdd(&svq[6 * f + c], qat[sc] * sqv[c]);
+      atomicAdd(&svq[6 * sc + c], qat[f] * sqv[c]);
+    }
+    // D4 charge response
+    double damp, ddamp;
+    const int zf = t.Z[gf], zs = t.Z[gs];
+    d4_pair_damping(t, zf, zs, r2, damp, ddamp);
+    if (damp != 0.0) {
+      double cf, cs;
+      d4_c6(t, zf, zs, w + kMaxD4Refs * f, w + kMaxD4Refs * sc, dwq + kMaxD4Refs * f,
+            dwq + kMaxD4Refs * sc, &cf, &cs);
+      vf -= cf * damp;
+      vs -= cs * damp;
+    }
+    atomicAdd(&vat[f], vf);
+    atomicAdd(&vat[sc], vs);
+  }
+  __syncthreads();
+  // shell potentials: ES2 (warp per shell row) + ES3 + atomic potential
+  const double* gam = a.gam + t.gam_off[s];
+  const int lane = tid & 31, warp = tid >> 5, nw = bs >> 5;
+  for (int i = warp; i < ns; i += nw) {
+    const double* row = gam + (int64_t)i * ns;
+    double acc = 0.0;
+    for (int j = lane; j < ns; j += 32) acc = fma(row[j], sq[j], acc);
+    acc = warp_sum(acc);
+    if (lane == 0) {
+      const int sh = (int)(s0 + i);
+      const double q = sq[i];
+      a.vsh[sh] = acc + t.sh_g3[sh] * q * q + vat[t.sh_atom[sh] - a0];
+    }
+  }
+  for (int i = tid; i < na; i += bs) {
+    const int64_t g = a0 + i;
+    for (int c = 0; c < 3; ++c) a.vd[3 * g + c] = svd[3 * i + c];
+    for (int c = 0; c < 6; ++c) a.vq[6 * g + c] = svq[6 * i + c];
+  }
+}
+
+void launch_potential(const SccArgs& a, const double* qsh, const double* dip, const double* qp,
+                      int max_atoms, int max_shells, cudaStream_t stream) {
+  if (a.count == 0) return;
+  const size_t sm = ((size_t)(11 + 2 * kMaxD4Refs) * max_atoms + max_shells + 8) * sizeof(double);
+  static const bool attr = cudaFuncSetAttribute(k_potential, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024) == cudaSuccess;
+  (void)attr;
+  k_potential<<<a.count, 256, sm, stream>>>(a, qsh, dip, qp);
+}
+
+// ---------------------------------------------------------------------------
+// Fock build on 32x32 tiles of the upper tile triangle:
+//   H = H0 - S (v_mu + v_nu)/2 - (G + G^T)/2,
+//   G[x][y] = sum_c D_c[x][y] vd_c(atom y) + Q_c[x][y] vq_c(atom y).
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ double g_element(const SccArgs& a, int64_t idx, int atom) {
+  double g = 0.0;
+#pragma unroll
+  for (int c = 0; c < 3; ++c) g = fma(a.D[c * a.total_mat + idx], a.vd[3 * atom + c], g);
+#pragma unroll
+  for (int c = 0; c < 6; ++c) g = fma(a.Q[c * a.total_mat + idx], a.vq[6 * atom + c], g);
+  return g;
+}
+
+__global__ void __launch_bounds__(256) k_fock(SccArgs a) {
+  __shared__ double sg[32][33];
+  const DevTopo& t = a.t;
+  const int s = a.list[blockIdx.y];
+  const int n = t.nao[s];
+  const int T = (n + 31) / 32;
+  const int64_t p = blockIdx.x;
+  if (p >= (int64_t)T * (T + 1) / 2) return;
+  // p -> (ti <= tj): p = tj (tj + 1)/2 + ti
+  int tj = (int)((sqrt(8.0 * (double)p + 1.0) - 1.0) * 0.5);
+  while ((int64_t)tj * (tj + 1) / 2 > p) --tj;
+  while ((int64_t)(tj + 1) * (tj + 2) / 2 <= p) ++tj;
+  const int ti = (int)(p - (int64_t)tj * (tj + 1) / 2);
+  const int row0 = ti * 32, col0 = tj * 32;
+  const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
+  const int64_t mo = t.mat_off[s];
+  const int64_t ao0 = t.ao_off[s];
+  // transposed tile: G(col0 + r, row0 + c) -> sg[r][c]
+  for (int r = ty; r < 32; r += 8) {
+    const int x = col0 + r, y = row0 + tx;
+    double g = 0.0;
+    if (x < n && y < n) g = g_element(a, mo + (int64_t)x * n + y, t.ao_at[ao0 + y]);
+    sg[r][tx] = g;
+  }
+  __syncthreads();
+  double h[4];
+  const int y = col0 + tx;
+  const bool yin = y < n;
+  const double vy = yin ? a.vsh[t.ao_sh[ao0 + y]] : 0.0;
+  const int aty = yin ? t.ao_at[ao0 + y] : 0;
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    const int r = ty + 8 * k;
+    const int x = row0 + r;
+    h[k] = 0.0;
+    if (x < n && yin) {
+      const int64_t idx = mo + (int64_t)x * n + y;
+      const double g1 = g_element(a, idx, aty);
+      const double vx = a.vsh[t.ao_sh[ao0 + x]];
+      h[k] = a.H0[idx] - 0.5 * a.S[idx] * (vx + vy) - 0.5 * (g1 + sg[tx][r]);
+      a.H[idx] = h[k];
+    }
+  }
+  if (ti == tj) return;
+  __syncthreads();
+#pragma unroll
+  for (int k = 0; k < 4; ++k) sg[tx][ty + 8 * k] = h[k];
+  __syncthreads();
+  for (int r = ty; r < 32; r += 8) {
+    const int x = col0 + r, yy = row0 + tx;
+    if (x < n && yy < n) a.H[mo + (int64_t)x * n + yy] = sg[r][tx];
+  }
+}
+
+void launch_fock(const SccArgs& a, int max_n, cudaStream_t stream) {
+  if (a.count == 0) return;
+  const int T = (max_n + 31) / 32;
+  dim3 grid((unsigned)(T * (T + 1) / 2), a.count);
+  k_fock<<<grid, 256, 0, stream>>>(a);
+}
+
+// ---------------------------------------------------------------------------
+// Mulliken populations (column reductions) and the band trace Tr(P H0).
+// ---------------------------------------------------------------------------
+constexpr int kMullRows = 64;
+
+__global__ void __launch_bounds__(128) k_mulliken(SccArgs a) {
+  const DevTopo& t = a.t;
+  const int s = a.list[blockIdx.z];
+  const int n = t.nao[s];
+  const int col = blockIdx.x * blockDim.x + threadIdx.x;
+  const int r0 = blockIdx.y * kMullRows;
+  if (r0 >= n) return;
+  const int r1 = min(n, r0 + kMullRows);
+  const int64_t mo = t.mat_off[s];
+  double ps = 0.0, ph = 0.0, pd[3] = {0, 0, 0}, pq[6] = {0, 0, 0, 0, 0, 0};
+  if (col < n) {
+    for (int r = r0; r < r1; ++r) {
+      const int64_t idx = mo + (int64_t)r * n + col;
+      const double pv = a.P[idx];
+      ps = fma(pv, a.S[idx], ps);
+      ph = fma(pv, a.H0[idx], ph);
+#pragma unroll
+      for (int c = 0; c < 3; ++c) pd[c] = fma(pv, a.D[c * a.total_mat + idx], pd[c]);
+#pragma unroll
+      for (int c = 0; c < 6; ++c) pq[c] = fma(pv, a.Q[c * a.total_mat + idx], pq[c]);
+    }
+    const int64_t gao = t.ao_off[s] + col;
+    const int sh = t.ao_sh[gao], at = t.ao_at[gao];
+    atomicAdd(&a.pop_sh[sh], ps);
+#pragma unroll
+    for (int c = 0; c < 3; ++c) atomicAdd(&a.pop_dip[3 * at + c], pd[c]);
+#pragma unroll
+    for (int c = 0; c < 6; ++c) atomicAdd(&a.pop_qp[6 * at + c], pq[c]);
+  }
+  ph = warp_sum(ph);
+  if ((threadIdx.x & 31) == 0) atomicAdd(&a.e_core[s], ph);
+}
+
+void launch_mulliken(const SccArgs& a, int max_n, cudaStream_t stream) {
+  if (a.count == 0) return;
+  dim3 grid((unsigned)((max_n + 127) / 128), (unsigned)((max_n + kMullRows - 1) / kMullRows), a.count);
+  k_mulliken<<<grid, 128, 0, stream>>>(a);
+}
+
+// ---------------------------------------------------------------------------
+// Energy functional from the raw populations, Broyden mixing, convergence.
+// ---------------------------------------------------------------------------
+__device__ bool cholesky_solve_small(double* B, double* c, int n) {
+  for (int r = 0; r < n; ++r) {
+    for (int col = 0; col <= r; ++col) {
+      double v = B[r * 8 + col];
+      for (int k = 0; k < col; ++k) v -= B[r * 8 + k] * B[col * 8 + k];
+      if (r == col) {
+        if (!(v > 0.0)) return false;
+        B[r * 8 + col] = sqrt(v);
+      } else {
+        B[r * 8 + col] = v / B[col * 8 + col];
+      }
+    }
+  }
+  for (int r = 0; r < n; ++r) {
+    double v = c[r];
+    for (int k = 0; k < r; ++k) v -= B[r * 8 + k] * c[k];
+    c[r] = v / B[r * 8 + r];
+  }
+  for (int r = n - 1; r >= 0; --r) {
+    double v = c[r];
+    for (int k = r + 1; k < n; ++k) v -= B[k * 8 + r] * c[k];
+    c[r] = v / B[r * 8 + r];
+  }
+  return true;
+}
+
+__global__ void __launch_bounds__(256) k_energy_mixer(SccArgs a) {
+  extern __shared__ double sm[];
+  const DevTopo& t = a.t;
+  const int s = a.list[blockIdx.x];
+  const int64_t a0 = t.atom_off[s];
+  const int na = (int)(t.atom_off[s + 1] - a0);
+  const int64_t s0 = t.shell_off[s];
+  const int ns = (int)(t.shell_off[s + 1] - s0);
+  const int dim = ns + 9 * na;
+  double* raw = sm;                       // dim: [qsh, dip (3na), qp (6na)]
+  double* qat = raw + dim;                // na
+  double* w = qat + na;                   // 7 na
+  double* red = w + kMaxD4Refs * na;      // 64 + 8*64
+  const int tid = threadIdx.x, bs = blockDim.x;
+  const int lane = tid & 31, warp = tid >> 5, nw = bs >> 5;
+  for (int i = tid; i < ns; i += bs) raw[i] = t.sh_refocc[s0 + i] - a.pop_sh[s0 + i];
+  for (int i = tid; i < 3 * na; i += bs) raw[ns + i] = -a.pop_dip[3 * a0 + i];
+  for (int i = tid; i < 6 * na; i += bs) raw[ns + 3 * na + i] = -a.pop_qp[6 * a0 + i];
+  __syncthreads();
+  for (int i = tid; i < na; i += bs) {
+    const int64_t g = a0 + i;
+    double q = 0.0;
+    for (int sh = t.atom_sh[g]; sh < t.atom_sh[g + 1]; ++sh) q += raw[sh - s0];
+    qat[i] = q;
+    d4_weights(t, t.Z[g], a.cn_d4[g], q, w + kMaxD4Refs * i, nullptr, nullptr);
+  }
+  __syncthreads();
+  // ES2 and ES3
+  double e2 = 0.0, e3 = 0.0, ea = 0.0, ed = 0.0;
+  const double* gam = a.gam + t.gam_off[s];
+  for (int i = warp; i < ns; i += nw) {
+    const double* row = gam + (int64_t)i * ns;
+    double acc = 0.0;
+    for (int j = lane; j < ns; j += 32) acc = fma(row[j], raw[j], acc);
+    acc = warp_sum(acc);
+    if (lane == 0) {
+      const double q = raw[i];
+      e2 += 0.5 * q * acc;
+      e3 += t.sh_g3[s0 + i] * q * q * q / 3.0;
+    }
+  }
+  // AES2 onsite
+  const double* rd = raw + ns;
+  const double* rq = raw + ns + 3 * na;
+  const double scl[6] = {1.0, 2.0, 1.0, 2.0, 2.0, 1.0};
+  for (int i = tid; i < na; i += bs) {
+    const int64_t g = a0 + i;
+    double d2 = 0.0, q2 = 0.0;
+    for (int c = 0; c < 3; ++c) d2 += rd[3 * i + c] * rd[3 * i + c];
+    for (int c = 0; c < 6; ++c) q2 += scl[c] * rq[6 * i + c] * rq[6 * i + c];
+    ea += t.at_dk[g] * d2 + t.at_qk[g] * q2;
+  }
+  // pairs: AES2 and D4 two-body
+  const int64_t npair = (int64_t)na * (na - 1) / 2;
+  for (int64_t p = tid; p < npair; p += bs) {
+    int64_t si, fi;
+    pair_from_index(p, si, fi);
+    const int f = (int)fi, sc = (int)si;
+    const int64_t gf = a0 + f, gs = a0 + sc;
+    const double d[3] = {t.pos[3 * gf] - t.pos[3 * gs], t.pos[3 * gf + 1] - t.pos[3 * gs + 1],
+                         t.pos[3 * gf + 2] - t.pos[3 * gs + 2]};
+    const double r2 = d[0] * d[0] + d[1] * d[1] + d[2] * d[2];
+    const double r = sqrt(r2);
+    double k3, k5;
+    aes2_kernels(r, 0.5 * (a.mrad[gf] + a.mrad[gs]), k3, k5);
+    const double* df = rd + 3 * f;
+    const double* ds = rd + 3 * sc;
+    double pf = 0.0, ps = 0.0, dd = 0.0, cdn = 0.0;
+    for (int c = 0; c < 3; ++c) {
+      pf += d[c] * df[c];
+      ps += d[c] * ds[c];
+      dd += df[c] * ds[c];
+      cdn += d[c] * (qat[f] * ds[c] - qat[sc] * df[c]);
+    }
+    const double sqv[6] = {d[0] * d[0] * k5, 2.0 * d[0] * d[1] * k5, d[1] * d[1] * k5,
+                           2.0 * d[0] * d[2] * k5, 2.0 * d[1] * d[2] * k5, d[2] * d[2] * k5};
+    double tq = 0.0;
+    for (int c = 0; c < 6; ++c) tq += qat[f] * sqv[c] * rq[6 * sc + c] + qat[sc] * sqv[c] * rq[6 * f + c];
+    ea += k3 * cdn + k5 * (r2 * dd - 3.0 * pf * ps) + tq;
+    double damp, ddamp;
+    const int zf = t.Z[gf], zs = t.Z[gs];
+    d4_pair_damping(t, zf, zs, r2, damp, ddamp);
+    if (damp != 0.0) {
+      ed -= d4_c6(t, zf, zs, w + kMaxD4Refs * f, w + kMaxD4Refs * sc, nullptr, nullptr, nullptr,
+                  nullptr) * damp;
+    }
+  }
+  e2 = block_sum(e2, red);
+  e3 = block_sum(e3, red);
+  ea = block_sum(ea, red);
+  ed = block_sum(ed, red);
+  const double ecore = a.e_core[s];
+  const double ts = -a.kt * a.entropy[s];
+  const double F = ecore + e2 + e3 + ea + ed + ts;
+
+  // ---- modified Broyden (Johnson) ----
+  const int64_t v0 = t.vec_off[s];
+  const int M = a.memory;
+  double* cur = a.mx_cur + v0;
+  double* prv = a.mx_prev + v0;
+  double* pres = a.mx_res + v0;
+  double* dfh = a.mx_df + v0 * M;
+  double* uh = a.mx_u + v0 * M;
+  double* om = a.mx_omega + (int64_t)s * M;
+  const int it = a.iterations[s];
+  // residual norm
+  double r2p = 0.0;
+  for (int i = tid; i < dim; i += bs) {
+    const double r = raw[i] - cur[i];
+    r2p += r * r;
+  }
+  const double nrm = sqrt(block_sum(r2p, red));
+  const double rms = nrm / sqrt((double)dim);
+  __shared__ double s_c[8];
+  __shared__ int s_hc, s_ok;
+  int hc = 0;
+  if (it > 0) {
+    double f2p = 0.0;
+    for (int i = tid; i < dim; i += bs) {
+      const double r = raw[i] - cur[i];
+      const double df = r - pres[i];
+      f2p += df * df;
+    }
+    const double inv = 1.0 / fmax(sqrt(block_sum(f2p, red)), DBL_EPSILON);
+    const double omega = nrm > 0.01 / 100000.0 ? fmax(1.0, 0.01 / nrm) : 100000.0;
+    hc = min(M, it);
+    const int new_slot = (it - 1) % M;
+    for (int i = tid; i < dim; i += bs) {
+      const double r = raw[i] - cur[i];
+      const double df = (r - pres[i]) * inv;
+      dfh[(int64_t)new_slot * dim + i] = df;
+      uh[(int64_t)new_slot * dim + i] = a.damping * df + inv * (cur[i] - prv[i]);
+    }
+    if (tid == 0) om[new_slot] = omega;
+    __syncthreads();
+    // dot products: c_h = df_h . res, B_hk = df_h . df_k
+    const int first = it - hc + 1;
+    int slot[8];
+    for (int h = 0; h < 8; ++h) slot[h] = (h < hc) ? (first + h - 1) % M : 0;
+    double part[8 + 36];
+    for (int q = 0; q < 44; ++q) part[q] = 0.0;
+    for (int i = tid; i < dim; i += bs) {
+      const double r = raw[i] - cur[i];
+      double dv[8];
+#pragma unroll
+      for (int h = 0; h < 8; ++h) dv[h] = (h < hc) ? dfh[(int64_t)slot[h] * dim + i] : 0.0;
+      int q = 8;
+#pragma unroll
+      for (int h = 0; h < 8; ++h) {
+        part[h] += dv[h] * r;
+#pragma unroll
+        for (int k = 0; k <= h; ++k) part[q++] += dv[h] * dv[k];
+      }
+    }
+    double* wsum = red + 64;   // [nw][44]
+#pragma unroll
+    for (int q = 0; q < 44; ++q) {
+      const double v = warp_sum(part[q]);
+      if (lane == 0) wsum[warp * 44 + q] = v;
+    }
+    __syncthreads();
+    if (tid == 0) {
+      double tot[44];
+      for (int q = 0; q < 44; ++q) {
+        double v = 0.0;
+        for (int ww = 0; ww < nw; ++ww) v += wsum[ww * 44 + q];
+        tot[q] = v;
+      }
+      double B[64], c[8];
+      int q = 8;
+      for (int h = 0; h < 8; ++h) {
+        for (int k = 0; k <= h; ++k) {
+          if (h < hc && k < hc) {
+            const double val = om[slot[h]] * om[slot[k]] * tot[q] + (h == k ? 1e-4 : 0.0);
+            B[h * 8 + k] = val;
+            B[k * 8 + h] = val;
+          }
+          ++q;
+        }
+        if (h < hc) c[h] = om[slot[h]] * tot[h];
+      }
+      const bool ok = cholesky_solve_small(B, c, hc);
+      for (int h = 0; h < 8; ++h) s_c[h] = (h < hc) ? om[slot[h]] * c[h] : 0.0;
+      s_ok = ok ? 1 : 0;
+      s_hc = hc;
+    }
+    __syncthreads();
+    hc = s_hc;
+    if (!s_ok) hc = -1;
+  }
+  // mixed = cur + damp * res - sum_h omega_h c_h u_h ; shift history
+  const double Fold = (it == 0) ? 0.0 : a.free_energy[s];
+  const bool conv = (rms < a.ctol) && (fabs(F - Fold) < a.etol) && hc >= 0;
+  const bool failed = hc < 0 || !isfinite(F) || !isfinite(nrm);
+  const int first = it - (hc > 0 ? hc : 0) + 1;
+  for (int i = tid; i < dim; i += bs) {
+    const double r = raw[i] - cur[i];
+    double mixed = cur[i] + a.damping * r;
+    for (int h = 0; h < hc; ++h) {
+      const int sl = (first + h - 1) % M;
+      mixed -= s_c[h] * uh[(int64_t)sl * dim + i];
+    }
+    prv[i] = cur[i];
+    pres[i] = r;
+    cur[i] = mixed;
+    const double out = conv ? raw[i] : mixed;
+    if (i < ns) {
+      a.qsh[s0 + i] = out;
+    } else if (i < ns + 3 * na) {
+      a.dip[3 * a0 + (i - ns)] = out;
+    } else {
+      a.qp[6 * a0 + (i - ns - 3 * na)] = out;
+    }
+  }
+  if (tid == 0) {
+    a.free_energy[s] = F;
+    a.iterations[s] = it + 1;
+    double* tm = a.terms + 8 * (int64_t)s;
+    tm[0] = ecore; tm[1] = e2; tm[2] = e3; tm[3] = ea; tm[4] = ed; tm[5] = ts;
+    if (failed) {
+      a.status[s] = kInternal;
+    } else if (conv) {
+      a.converged[s] = 1;
+    } else if (it + 1 >= a.max_iter) {
+      a.status[s] = kNotConverged;
+    }
+  }
+}
+
+void launch_energy_mixer(const SccArgs& a, int max_atoms, int max_shells, int max_dim,
+                         int first_iteration, cudaStream_t stream) {
+  (void)first_iteration;
+  if (a.count == 0) return;
+  const size_t sm = ((size_t)max_dim + (1 + kMaxD4Refs) * max_atoms + 64 + 8 * 44 + 8) * sizeof(double);
+  static const bool attr = cudaFuncSetAttribute(k_energy_mixer, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024) == cudaSuccess;
+  (void)attr;
+  k_energy_mixer<<<a.count, 256, sm, stream>>>(a);
+}
+
+// ---------------------------------------------------------------------------
+// Active-list compaction in the (cost-descending) system order.
+// ---------------------------------------------------------------------------
+__global__ void k_compact(const int32_t* order, int nsys, const int32_t* status,
+                          const uint8_t* converged, const int32_t* iterations, int max_iter,
+                          int32_t* list, int32_t* count) {
+  __shared__ int wtot[32];
+  __shared__ int base, chunk_total;
+  if (threadIdx.x == 0) base = 0;
+  __syncthreads();
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  for (int c0 = 0; c0 < nsys; c0 += blockDim.x) {
+    const int i = c0 + threadIdx.x;
+    int sys = -1;
+    bool act = false;
+    if (i < nsys) {
+      sys = order[i];
+      act = status[sys] == kOk && converged[sys] == 0 && iterations[sys] < max_iter;
+    }
+    const unsigned b = __ballot_sync(0xffffffffu, act);
+    const int pre = __popc(b & ((1u << lane) - 1u));
+    if (lane == 0) wtot[warp] = __popc(b);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      int acc = 0;
+      for (int w = 0; w < (int)(blockDim.x >> 5); ++w) {
+        const int v = wtot[w];
+        wtot[w] = acc;
+        acc += v;
+      }
+      chunk_total = acc;
+    }
+    __syncthreads();
+    if (act) list[base + wtot[warp] + pre] = sys;
+    __syncthreads();
+    if (threadIdx.x == 0) base += chunk_total;
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) count[0] = base;
+}
+
+void launch_compact(const int32_t* order, int nsys, const int32_t* status, const uint8_t* converged,
+                    const int32_t* iterations, int max_iter, int32_t* list, int32_t* count,
+                    cudaStream_t stream) {
+  k_compact<<<1, 1024, 0, stream>>>(order, nsys, status, converged, iterations, max_iter, list, count);
+}
+
+}  // namespace xtb

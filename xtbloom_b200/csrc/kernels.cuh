@@ -1,0 +1,146 @@
+// Kernel argument blocks and host launch entry points of the CUDA path.
+#pragma once
+
+#include "common.cuh"
+
+namespace xtb {
+
+struct GemmArgs {
+  const int32_t* list;     // active systems (blockIdx.y -> system)
+  const int32_t* nao;      // leading dimension of every matrix of a system
+  const int32_t* dm;       // rows of C
+  const int32_t* dn;       // columns of C
+  const int32_t* dk;       // contraction length
+  const double* A;
+  const int64_t* offA;
+  const double* B;
+  const int64_t* offB;
+  double* C;
+  const int64_t* offC;
+  const double* w;         // per-k weight (weighted form)
+  const int64_t* offW;
+};
+
+struct EigArgs {
+  const int32_t* list;
+  const int32_t* nao;
+  const int64_t* mat_off;
+  const int64_t* ao_off;
+  double* A;          // matrix to tridiagonalise (destroyed: holds reflectors)
+  double* d;
+  double* e;
+  double* tau;
+  double* eig;        // eigenvalues (ao-indexed)
+  double* occ;        // occupations (ao-indexed); Loewdin weights in setup
+  double* occ_eps;    // occupation * eigenvalue
+  double* entropy;    // per system
+  int32_t* nvec;      // per system: number of eigenvectors formed
+  double* Z;          // eigenvector-major n x n blocks
+  double* scratch;    // inverse-iteration workspace
+  const int64_t* scratch_off;
+  const double* nel_a;
+  const double* nel_b;
+};
+
+struct SccArgs {
+  DevTopo t;
+  const int32_t* list;
+  int32_t count;
+  // state (mixed input) and raw populations
+  double* qsh;        // per shell
+  double* dip;        // 3 per atom
+  double* qp;         // 6 per atom
+  double* pop_sh;     // accumulated sum_mu P S per shell (zeroed each iteration)
+  double* pop_dip;
+  double* pop_qp;
+  double* e_core;     // per system Tr(P H0)
+  // potentials
+  double* vsh;        // per shell (scalar shell + atomic potential)
+  double* vd;
+  double* vq;
+  // geometry caches
+  const double* gam;
+  const double* mrad;
+  const double* cn_d4;
+  // matrices
+  const double* S;
+  const double* D;
+  const double* Q;
+  const double* H0;
+  double* H;
+  const double* P;
+  int64_t total_mat;
+  // per system energies / status
+  const double* entropy;
+  double* free_energy;
+  double* terms;      // 8 per system: core, es2, es3, aes2, d4, -kTS, rep, atm
+  int32_t* iterations;
+  int32_t* status;
+  uint8_t* converged;
+  // Broyden state
+  double* mx_cur;
+  double* mx_prev;
+  double* mx_res;
+  double* mx_df;      // memory x dim per system, at vec_off * memory
+  double* mx_u;
+  double* mx_omega;   // memory per system
+  int32_t memory;
+  double damping;
+  double ctol, etol, kt;
+  int32_t max_iter;
+};
+
+void launch_setup(const DevTopo& t, const int32_t* list, int count, int max_atoms,
+                  int64_t max_pairs, int64_t max_shells, double* cn, double* cn_d4, double* mrad,
+                  double* dmrad, double* S, double* D, double* Q, double* H0, double* gam,
+                  int64_t total_mat, cudaStream_t stream);
+
+void launch_gemm(const GemmArgs& g, bool transA, bool weighted, int max_tiles, int count,
+                 cudaStream_t stream);
+void launch_tridiag(const EigArgs& g, int count, int max_n, cudaStream_t stream);
+void launch_eigvals(const EigArgs& g, int mode, double kt, int count, int max_n, cudaStream_t stream);
+void launch_inverse_iteration(const EigArgs& g, int count, cudaStream_t stream);
+void launch_backtransform(const EigArgs& g, int count, int max_n, cudaStream_t stream);
+void launch_lowdin_weights(const EigArgs& g, int32_t* status, int count, cudaStream_t stream);
+
+void launch_sad_init(const SccArgs& a, cudaStream_t stream);
+void launch_potential(const SccArgs& a, const double* qsh, const double* dip, const double* qp,
+                      int max_atoms, int max_shells, cudaStream_t stream);
+void launch_fock(const SccArgs& a, int max_n, cudaStream_t stream);
+void launch_mulliken(const SccArgs& a, int max_n, cudaStream_t stream);
+void launch_energy_mixer(const SccArgs& a, int max_atoms, int max_shells, int max_dim,
+                         int first_iteration, cudaStream_t stream);
+void launch_compact(const int32_t* order, int nsys, const int32_t* status, const uint8_t* converged,
+                    const int32_t* iterations, int max_iter, int32_t* list, int32_t* count,
+                    cudaStream_t stream);
+
+struct ForceArgs {
+  DevTopo t;
+  const int32_t* list;
+  int32_t count;
+  const double* cn;
+  const double* cn_d4;
+  const double* mrad;
+  const double* dmrad;
+  const double* S;
+  const double* P;
+  const double* W;
+  const double* vsh;
+  const double* vd;
+  const double* vq;
+  const double* qsh;
+  const double* dip;
+  const double* qp;
+  const double* gam;
+  double* grad;       // 3 per atom (dE/dR), accumulated
+  double* acn;        // dE/dCN (dexp) per atom, accumulated
+  double* acn_d4;     // dE/dCN (D4) per atom, accumulated
+  double* terms;      // per-system energy terms (rep, atm written)
+  int32_t want_grad;
+};
+
+void launch_force_pairs(const ForceArgs& f, int64_t max_pairs, cudaStream_t stream);
+void launch_classical(const ForceArgs& f, int max_atoms, int max_shells, cudaStream_t stream);
+void launch_cn_chain(const ForceArgs& f, int max_atoms, cudaStream_t stream);
+
+}  // namespace xtb
