@@ -1,0 +1,350 @@
+#!/usr/bin/env python
+"""Throughput benchmark of the batched GFN2-xTB energy+forces path.
+
+Workload: the 4096-system ragged batch of hetero-alkane chains (C3..C40,
+10 % of interior CH2 replaced by O or NH, seed 1), GFN2-xTB energy + analytic
+forces + Mulliken charges to SCC convergence (charge 1e-6, energy 1e-8, 300 K,
+Broyden 8/0.4).  One step = one ``xtbloom_compute`` call over the whole batch.
+
+  python bench.py [--gpus N --steps K --warmup W]        # this library (CUDA)
+  python bench.py --impl reference [...]                 # reference CPU library
+
+``value`` is measured with positions and outputs resident in HBM; ``e2e`` is
+the same call with host positions and host outputs (the library's own
+host<->device copies inside the timed region).  Multi-GPU runs shard the
+independent systems (each rank its own 4096-system batch, no collective in
+the data path) and report the whole-job throughput from the slowest rank.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes as C
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+from xtbloom_b200 import abi  # noqa: E402
+from xtbloom_b200 import workloads as W  # noqa: E402
+
+METRIC = ("GFN2 E+F systems/s on 1 B200: mixed vs FP64 path at |ΔE|≤1e-6 Eh; roofline %")
+STAGES = ["setup_integrals", "lowdin", "potential", "fock", "gemm_transform", "tridiag", "eigvals",
+          "inverse_iteration", "backtransform", "gemm_density", "mulliken", "energy_mixer",
+          "compact", "force_pairs", "classical", "cn_chain", "publish"]
+REF_LIB = ROOT / "oracle" / "_ref" / "libxtbloom_ref.so"
+WORKLOAD = ("GFN2-xTB E+F+q, ragged batch of 4096 hetero-alkane chains C_nH_(2n+2), n uniform "
+            "in 3..40, 10% interior CH2 -> O/NH, seed 1; SCC 1e-6/1e-8, 300 K, Broyden 8/0.4")
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=3)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    p.add_argument("--systems", type=int, default=4096)
+    p.add_argument("--cpu-sample", type=int, default=192)
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    return p.parse_args()
+
+
+def dist_setup(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    return world, rank, local
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def allreduce_max(x: float, world: int) -> float:
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def fetch(lib, name, cap=256):
+    f = lib.lib.xtbloom_b200_debug_fetch
+    f.restype = C.c_int32
+    f.argtypes = [C.c_void_p, C.c_char_p, C.c_int64, C.POINTER(C.c_double), C.c_size_t,
+                  C.POINTER(C.c_size_t)]
+    out = np.zeros(cap)
+    cnt = C.c_size_t()
+    f(lib.ctx, name.encode(), 0, out.ctypes.data_as(C.POINTER(C.c_double)), cap, C.byref(cnt))
+    return out[:cnt.value].copy()
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms."""
+
+    def __init__(self, device: int):
+        self.path = Path(tempfile.gettempdir()) / f"xtb_clocks_{os.getpid()}.csv"
+        q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+             "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+             "clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={device}", f"--query-gpu={q}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+
+    def stop(self) -> dict:
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        self.proc.wait(timeout=10)
+        rows = []
+        for line in self.path.read_text().splitlines():
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) == 7:
+                rows.append(parts)
+        self.path.unlink(missing_ok=True)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": []}
+        sm = [float(r[0]) for r in rows if r[0].replace(".", "").isdigit()]
+        mx = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[3 + i].lower() == "active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(mx) if mx else None, "reasons": reasons, "samples": len(rows)}
+
+
+def stage_work(n: np.ndarray, iters: np.ndarray, nocc: np.ndarray) -> dict:
+    """Algorithmic FP64 flops and HBM bytes per stage over one step (all systems)."""
+    n = n.astype(float)
+    it = iters.astype(float)
+    m = nocc.astype(float)
+    d8 = 8.0
+    return {
+        "gemm_transform": {"flops": float(np.sum(it * 4 * n ** 3)), "bytes": float(np.sum(it * 6 * n * n * d8))},
+        "tridiag": {"flops": float(np.sum((it + 1) * 4 / 3 * n ** 3)), "bytes": float(np.sum((it + 1) * 2 * n * n * d8))},
+        "backtransform": {"flops": float(np.sum(it * 2 * n * n * m)), "bytes": float(np.sum(it * 3 * n * m * d8))},
+        "gemm_density": {"flops": float(np.sum(it * 4 * n * n * m)), "bytes": float(np.sum(it * (3 * n * n + 2 * n * m) * d8))},
+        "fock": {"flops": float(np.sum(it * 22 * n * n)), "bytes": float(np.sum(it * 12 * n * n * d8))},
+        "mulliken": {"flops": float(np.sum(it * 22 * n * n)), "bytes": float(np.sum(it * 11 * n * n * d8))},
+    }
+
+
+def load_peaks() -> dict:
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return {"hbm_gbs": d.get("hbm_gbs", 6650.0), "source": "measured"}
+    return {"hbm_gbs": 6650.0, "source": "fallback"}
+
+
+def reference_sample(batch, count: int):
+    idx = np.linspace(0, batch.batch_size - 1, count).round().astype(int)
+    return W.subset(batch, idx), idx
+
+
+def cpu_run(sample, threads: int = 0) -> tuple[float, dict]:
+    lib = abi.Library(str(REF_LIB), backend=abi.BACKEND_CPU, cpu_threads=threads)
+    warm = W.subset(sample, range(min(4, sample.batch_size)))
+    lib.compute(warm)
+    t0 = time.perf_counter()
+    out = lib.compute(sample)
+    dt = time.perf_counter() - t0
+    lib.close()
+    return dt, out
+
+
+def host_cores() -> int:
+    try:
+        return min(len(os.sched_getaffinity(0)), 64)
+    except AttributeError:
+        return min(os.cpu_count() or 1, 64)
+
+
+def run_reference(args, world, rank):
+    if rank != 0:
+        return
+    if not REF_LIB.exists():
+        print(json.dumps({"impl": "reference",
+                          "unavailable": "oracle/_ref/libxtbloom_ref.so was not built (build() builds it from the reference sources)"}))
+        return
+    batch = W.config1(args.systems, seed=1)
+    sample, _ = reference_sample(batch, args.cpu_sample)
+    lib = abi.Library(str(REF_LIB), backend=abi.BACKEND_CPU, cpu_threads=0)
+    for _ in range(args.warmup):
+        lib.compute(W.subset(sample, range(min(8, sample.batch_size))))
+    times = []
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        lib.compute(sample)
+        times.append(time.perf_counter() - t0)
+    t = statistics.median(times)
+    value = sample.batch_size / t
+    cores = host_cores()
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "systems/s",
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": 1e3 * t, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "global_batch": args.systems,
+                   "sample_per_step": sample.batch_size},
+        "cpu_baseline": {"value": value, "unit": "systems/s", "cores": cores, "kind": "reference",
+                         "sample": f"{sample.batch_size} evenly spaced systems of the 4096-system batch per step, cpu_threads=0 (affinity count, capped at 64)"},
+        "e2e": {"value": value, "unit": "systems/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line))
+
+
+def run_ours(args, world, rank, local):
+    import torch
+    from xtbloom_b200 import library_path
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    batch = W.config1(args.systems, seed=1 + 1000 * rank)
+    B, N = batch.batch_size, batch.total_atoms
+    stream = torch.cuda.current_stream(dev)
+    lib = abi.Library(library_path(), backend=abi.BACKEND_CUDA, device_id=local,
+                      stream=stream.cuda_stream)
+    opts = lib.make_options()
+    pos_d = torch.from_numpy(batch.positions).to(dev)
+    dev_batch = abi.RaggedBatch(batch.atom_offsets, batch.atomic_numbers, pos_d,
+                                batch.molecular_charges, batch.unpaired_electrons)
+    outs_d = {"energies": torch.empty(B, dtype=torch.float64, device=dev),
+              "forces": torch.empty(3 * N, dtype=torch.float64, device=dev),
+              "atomic_charges": torch.empty(N, dtype=torch.float64, device=dev),
+              "scc_iterations": torch.empty(B, dtype=torch.int32, device=dev),
+              "scc_converged": torch.empty(B, dtype=torch.uint8, device=dev),
+              "per_system_status": torch.empty(B, dtype=torch.int32, device=dev)}
+    for _ in range(args.warmup):
+        lib.compute(dev_batch, opts, outs_d)
+    torch.cuda.synchronize()
+    fetch(lib, "reset_counters")
+    clocks = ClockSampler(local)
+    barrier(world)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        lib.compute(dev_batch, opts, outs_d)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    barrier(world)
+    clk = clocks.stop()
+    ms = e0.elapsed_time(e1) / args.steps
+    ms_max = allreduce_max(ms, world)
+    stage = fetch(lib, "kernel_times").reshape(-1, 2)
+    launches = int(fetch(lib, "launch_count")[0])
+    timing_on = bool(fetch(lib, "launch_count")[1])
+    # end-to-end: host positions in, host results out
+    host_outs = {"energies": np.empty(B), "forces": np.empty(3 * N), "atomic_charges": np.empty(N),
+                 "scc_iterations": np.empty(B, np.int32), "scc_converged": np.empty(B, np.uint8),
+                 "per_system_status": np.empty(B, np.int32)}
+    lib.compute(batch, opts, host_outs)
+    torch.cuda.synchronize()
+    barrier(world)
+    e0.record(stream)
+    for _ in range(args.steps):
+        lib.compute(batch, opts, host_outs)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    barrier(world)
+    ms_e2e = allreduce_max(e0.elapsed_time(e1) / args.steps, world)
+    h2d = (B + 1) * 8 + N * 4 + 3 * N * 8 + B * 8 + B * 4
+    d2h = B * 8 + 3 * N * 8 + N * 8 + B * 4 + B + B * 4
+    if rank != 0:
+        return
+    energies = host_outs["energies"]
+    status = host_outs["per_system_status"]
+    iters = host_outs["scc_iterations"]
+    n_ao = np.array([int(np.sum([{1: 1}.get(int(z), 4) for z in W.molecule(batch, i)[0]]))
+                     for i in range(B)])
+    nocc = n_ao // 2 + 1
+    work = stage_work(n_ao, iters, nocc)
+    per_stage_ms = {STAGES[i]: float(stage[i, 0]) / args.steps for i in range(len(STAGES))} if timing_on else {}
+    total_stage = sum(per_stage_ms.values()) or 1.0
+    peaks = load_peaks()
+    roofline = None
+    if timing_on:
+        dom = max(per_stage_ms, key=per_stage_ms.get)
+        dom_ms = per_stage_ms[dom]
+        calls = float(stage[STAGES.index(dom), 1]) / args.steps
+        if dom in work:
+            byts = work[dom]["bytes"]
+            achieved = byts / (dom_ms / 1e3) / 1e9
+            roofline = {"kernel": dom, "bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"],
+                        "unit": "GB/s", "frac": achieved / peaks["hbm_gbs"], "traffic": None,
+                        "peak_source": peaks["source"],
+                        "fp64_tflops": work[dom]["flops"] / (dom_ms / 1e3) / 1e12,
+                        "share_of_step": dom_ms / ms, "launches_per_step": calls}
+        else:
+            roofline = {"kernel": dom, "bound": "hbm", "achieved": None, "peak": peaks["hbm_gbs"],
+                        "unit": "GB/s", "frac": None, "traffic": None, "share_of_step": dom_ms / ms}
+    cpu = None
+    dE = None
+    if world == 1 and not args.no_cpu_baseline and REF_LIB.exists():
+        sample, idx = reference_sample(batch, args.cpu_sample)
+        t, ref = cpu_run(sample, 0)
+        ok = (ref["per_system_status"] == 0) & (status[idx] == 0)
+        dE = float(np.max(np.abs(ref["energies"][ok] - energies[idx][ok]))) if ok.any() else None
+        cpu = {"value": sample.batch_size / t, "unit": "systems/s", "cores": host_cores(),
+               "kind": "reference",
+               "sample": f"{sample.batch_size} evenly spaced systems of the same batch, one call, cpu_threads=0"}
+    line = {
+        "metric": METRIC, "value": world * B / (ms_max / 1e3), "unit": "systems/s",
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_max,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic",
+        "config": {"workload": WORKLOAD, "global_batch": world * B, "atoms_per_rank": int(N),
+                   "path": "FP64 (all stages)", "l2": "inputs larger than L2 (~11 GB of packed matrices per step)",
+                   "parallelism": f"dp{world} (independent systems, no collective)"},
+        "roofline": roofline,
+        "cpu_baseline": cpu,
+        "e2e": {"value": world * B / (ms_e2e / 1e3), "unit": "systems/s",
+                "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)},
+        "gpu_launches": launches // max(args.steps, 1) * args.steps if timing_on else launches,
+        "clocks": clk,
+        "parity": {"max_abs_dE_vs_reference_Eh": dE,
+                   "converged": int(np.sum(status == 0)), "systems": int(B),
+                   "mean_scc_iterations": float(np.mean(iters))},
+        "stage_ms_per_step": per_stage_ms,
+        "stage_share": {k: v / total_stage for k, v in per_stage_ms.items()},
+    }
+    print(json.dumps(line))
+    sys.stdout.flush()
+
+
+def main():
+    args = parse()
+    world, rank, local = dist_setup(args)
+    if args.impl == "reference":
+        run_reference(args, world, rank)
+    else:
+        os.environ.setdefault("XTBLOOM_B200_KERNEL_TIMING", "1")
+        run_ours(args, world, rank, local)
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -304,9 +304,9 @@ class Library:
             if b.point_charge_offsets is not None and options.flags & COMPUTE_POINT_CHARGE_FORCES:
                 outputs["point_charge_forces"] = np.empty(3 * len(b.point_charge_values))
         batch = self.make_batch(b)
-        res = self.make_result(outputs)
+        res = self.make_result({k: v for k, v in outputs.items() if k in RESULT_BUFFERS})
         self._check(self.lib.xtbloom_compute(self.ctx, C.byref(batch), C.byref(options), C.byref(res)))
-        outputs["result_flags"] = res.flags
+        self.last_result_flags = res.flags
         return outputs
 
 

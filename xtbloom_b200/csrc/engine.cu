@@ -140,7 +140,57 @@ ModelConstants make_constants() {
   return m;
 }
 
-size_t host_bytes_of(const xtbloom_const_buffer_t& b) { return b.size_bytes; }
+// Optional live kernel timing with CUDA events on the engine stream, grouped
+// by pipeline stage; enabled with XTBLOOM_B200_KERNEL_TIMING=1.
+enum Stage : int {
+  kStSetup, kStLowdin, kStPotential, kStFock, kStTransform, kStTridiag, kStEigvals, kStInvIter,
+  kStBacktransform, kStDensity, kStMulliken, kStEnergyMixer, kStCompact, kStForcePairs,
+  kStClassical, kStCnChain, kStPublish, kStageCount
+};
+const char* kStageNames[kStageCount] = {
+    "setup_integrals", "lowdin", "potential", "fock", "gemm_transform", "tridiag", "eigvals",
+    "inverse_iteration", "backtransform", "gemm_density", "mulliken", "energy_mixer", "compact",
+    "force_pairs", "classical", "cn_chain", "publish"};
+
+struct Profiler {
+  bool on = false;
+  std::vector<cudaEvent_t> pool;
+  size_t used = 0;
+  std::vector<std::pair<int, size_t>> marks;   // stage, index of start event (end = +1)
+  double total_ms[kStageCount] = {};
+  int64_t calls[kStageCount] = {};
+  int64_t launches = 0;
+  cudaEvent_t next() {
+    if (used == pool.size()) {
+      cudaEvent_t e;
+      cudaEventCreate(&e);
+      pool.push_back(e);
+    }
+    return pool[used++];
+  }
+  void begin(int stage, cudaStream_t s) {
+    if (!on) return;
+    marks.push_back({stage, used});
+    cudaEventRecord(next(), s);
+  }
+  void end(cudaStream_t s) {
+    if (!on) return;
+    cudaEventRecord(next(), s);
+  }
+  void collect() {
+    for (auto& m : marks) {
+      float ms = 0.f;
+      cudaEventElapsedTime(&ms, pool[m.second], pool[m.second + 1]);
+      total_ms[m.first] += ms;
+      calls[m.first] += 1;
+    }
+    marks.clear();
+    used = 0;
+  }
+  ~Profiler() {
+    for (auto e : pool) cudaEventDestroy(e);
+  }
+};
 
 }  // namespace
 
@@ -178,6 +228,7 @@ struct Engine::Impl {
   int32_t* h_count = nullptr;   // pinned
   int last_memory = 0;
   bool have_results = false;
+  Profiler prof;
 
   DevTopo devtopo() const {
     DevTopo t{};
@@ -242,6 +293,8 @@ struct Engine::Impl {
 
 Engine::Engine(int device, cudaStream_t stream) : impl_(new Impl), device_(device), stream_(stream) {
   cudaMallocHost(&impl_->h_count, 4 * sizeof(int32_t));
+  const char* env = std::getenv("XTBLOOM_B200_KERNEL_TIMING");
+  impl_->prof.on = env != nullptr && env[0] == '1';
 }
 
 Engine::~Engine() {
@@ -587,11 +640,19 @@ xtbloom_status_t Engine::compute(const ComputeRequest& req, std::string& error) 
   cudaMemsetAsync(m.terms.p, 0, 8 * B * 8, s);
   cudaMemcpyAsync(list, order, B * 4, cudaMemcpyDeviceToDevice, s);
 
+#define XTB_STAGE(id, nk, ...)        \
+  do {                                \
+    m.prof.begin(id, s);              \
+    __VA_ARGS__;                      \
+    m.prof.end(s);                    \
+    m.prof.launches += (nk);          \
+  } while (0)
   // ---- geometry setup ----
-  launch_setup(t, list, nsys, m.max_atoms, m.max_pairs, m.max_shells, m.cn.as<double>(),
-               m.cn_d4.as<double>(), m.mrad.as<double>(), m.dmrad.as<double>(), m.S.as<double>(),
-               m.D.as<double>(), m.Q.as<double>(), m.H0.as<double>(), m.gam.as<double>(),
-               m.total_mat, s);
+  XTB_STAGE(kStSetup, 3,
+            launch_setup(t, list, nsys, m.max_atoms, m.max_pairs, m.max_shells, m.cn.as<double>(),
+                         m.cn_d4.as<double>(), m.mrad.as<double>(), m.dmrad.as<double>(),
+                         m.S.as<double>(), m.D.as<double>(), m.Q.as<double>(), m.H0.as<double>(),
+                         m.gam.as<double>(), m.total_mat, s));
 
   EigArgs eg{};
   eg.list = list;
@@ -636,13 +697,11 @@ xtbloom_status_t Engine::compute(const ComputeRequest& req, std::string& error) 
 
   // ---- Loewdin orthogonaliser X = U s^-1/2 U^T ----
   cudaMemcpyAsync(m.A.p, m.S.p, (size_t)m.total_mat * 8, cudaMemcpyDeviceToDevice, s);
-  launch_tridiag(eg, nsys, m.max_n, s);
-  launch_eigvals(eg, 1, 0.0, nsys, m.max_n, s);
-  launch_inverse_iteration(eg, nsys, s);
-  launch_backtransform(eg, nsys, m.max_n, s);
-  launch_lowdin_weights(eg, status, nsys, s);
-  gemm(m.Zv.as<double>(), m.Zv.as<double>(), m.X.as<double>(), dnao, dnao, dnao, true,
-       m.occ.as<double>(), nsys);
+  XTB_STAGE(kStLowdin, 6, launch_tridiag(eg, nsys, m.max_n, s);
+            launch_eigvals(eg, 1, 0.0, nsys, m.max_n, s); launch_inverse_iteration(eg, nsys, s);
+            launch_backtransform(eg, nsys, m.max_n, s); launch_lowdin_weights(eg, status, nsys, s);
+            gemm(m.Zv.as<double>(), m.Zv.as<double>(), m.X.as<double>(), dnao, dnao, dnao, true,
+                 m.occ.as<double>(), nsys));
 
   // ---- SCC ----
   SccArgs a{};
@@ -687,40 +746,51 @@ xtbloom_status_t Engine::compute(const ComputeRequest& req, std::string& error) 
   a.kt = req.kt;
   a.max_iter = req.max_iter;
 
-  launch_compact(order, nsys, status, a.converged, a.iterations, req.max_iter, list, dcount, s);
+  XTB_STAGE(kStCompact, 1,
+            launch_compact(order, nsys, status, a.converged, a.iterations, req.max_iter, list,
+                           dcount, s));
   cudaMemcpyAsync(m.h_count, dcount, 4, cudaMemcpyDeviceToHost, s);
   cudaStreamSynchronize(s);
   int count = m.h_count[0];
   a.count = count;
-  launch_sad_init(a, s);
+  XTB_STAGE(kStPotential, 1, launch_sad_init(a, s));
   for (int it = 0; it < req.max_iter && count > 0; ++it) {
     a.count = count;
-    launch_potential(a, a.qsh, a.dip, a.qp, m.max_atoms, m.max_shells, s);
-    launch_fock(a, m.max_n, s);
-    gemm(m.H.as<double>(), m.X.as<double>(), m.T.as<double>(), dnao, dnao, dnao, false, nullptr, count);
-    gemm(m.X.as<double>(), m.T.as<double>(), m.A.as<double>(), dnao, dnao, dnao, false, nullptr, count);
-    launch_tridiag(eg, count, m.max_n, s);
-    launch_eigvals(eg, 0, req.kt, count, m.max_n, s);
-    launch_inverse_iteration(eg, count, s);
-    launch_backtransform(eg, count, m.max_n, s);
-    gemm(m.Zv.as<double>(), m.X.as<double>(), m.C.as<double>(), dnvec, dnao, dnao, false, nullptr, count);
-    gemm(m.C.as<double>(), m.C.as<double>(), m.P.as<double>(), dnao, dnao, dnvec, true,
-         m.occ.as<double>(), count);
+    XTB_STAGE(kStPotential, 1, launch_potential(a, a.qsh, a.dip, a.qp, m.max_atoms, m.max_shells, s));
+    XTB_STAGE(kStFock, 1, launch_fock(a, m.max_n, s));
+    XTB_STAGE(kStTransform, 2,
+              gemm(m.H.as<double>(), m.X.as<double>(), m.T.as<double>(), dnao, dnao, dnao, false,
+                   nullptr, count);
+              gemm(m.X.as<double>(), m.T.as<double>(), m.A.as<double>(), dnao, dnao, dnao, false,
+                   nullptr, count));
+    XTB_STAGE(kStTridiag, 1, launch_tridiag(eg, count, m.max_n, s));
+    XTB_STAGE(kStEigvals, 1, launch_eigvals(eg, 0, req.kt, count, m.max_n, s));
+    XTB_STAGE(kStInvIter, 1, launch_inverse_iteration(eg, count, s));
+    XTB_STAGE(kStBacktransform, 1, launch_backtransform(eg, count, m.max_n, s));
+    XTB_STAGE(kStDensity, 2,
+              gemm(m.Zv.as<double>(), m.X.as<double>(), m.C.as<double>(), dnvec, dnao, dnao, false,
+                   nullptr, count);
+              gemm(m.C.as<double>(), m.C.as<double>(), m.P.as<double>(), dnao, dnao, dnvec, true,
+                   m.occ.as<double>(), count));
     cudaMemsetAsync(m.pop_sh.p, 0, m.nshells * 8, s);
     cudaMemsetAsync(m.pop_dip.p, 0, 3 * m.natoms * 8, s);
     cudaMemsetAsync(m.pop_qp.p, 0, 6 * m.natoms * 8, s);
     cudaMemsetAsync(m.e_core.p, 0, B * 8, s);
-    launch_mulliken(a, m.max_n, s);
-    launch_energy_mixer(a, m.max_atoms, m.max_shells, m.max_dim, it == 0, s);
-    launch_compact(order, nsys, status, a.converged, a.iterations, req.max_iter, list, dcount, s);
+    XTB_STAGE(kStMulliken, 1, launch_mulliken(a, m.max_n, s));
+    XTB_STAGE(kStEnergyMixer, 1, launch_energy_mixer(a, m.max_atoms, m.max_shells, m.max_dim, it == 0, s));
+    XTB_STAGE(kStCompact, 1,
+              launch_compact(order, nsys, status, a.converged, a.iterations, req.max_iter, list,
+                             dcount, s));
     cudaMemcpyAsync(m.h_count, dcount, 4, cudaMemcpyDeviceToHost, s);
     cudaStreamSynchronize(s);
     count = m.h_count[0];
   }
   k_finalize_status<<<(nsys + 255) / 256, 256, 0, s>>>(nsys, status, a.converged);
+  m.prof.launches += 1;
 
   // ---- energy/force terms on converged systems ----
   k_list_ok<<<1, 32, 0, s>>>(order, nsys, status, list, dcount);
+  m.prof.launches += 1;
   cudaMemcpyAsync(m.h_count, dcount, 4, cudaMemcpyDeviceToHost, s);
   cudaStreamSynchronize(s);
   count = m.h_count[0];
@@ -753,16 +823,20 @@ xtbloom_status_t Engine::compute(const ComputeRequest& req, std::string& error) 
   f.want_grad = want_forces ? 1 : 0;
   if (want_forces && count > 0) {
     a.count = count;
-    launch_potential(a, a.qsh, a.dip, a.qp, m.max_atoms, m.max_shells, s);
-    gemm(m.C.as<double>(), m.C.as<double>(), m.W.as<double>(), dnao, dnao, dnvec, true,
-         m.occ_eps.as<double>(), count);
-    launch_force_pairs(f, m.max_pairs, s);
+    XTB_STAGE(kStForcePairs, 3,
+              launch_potential(a, a.qsh, a.dip, a.qp, m.max_atoms, m.max_shells, s);
+              gemm(m.C.as<double>(), m.C.as<double>(), m.W.as<double>(), dnao, dnao, dnvec, true,
+                   m.occ_eps.as<double>(), count);
+              launch_force_pairs(f, m.max_pairs, s));
   }
-  launch_classical(f, m.max_atoms, m.max_shells, s);
-  if (want_forces) launch_cn_chain(f, m.max_atoms, s);
-  k_publish<<<nsys, 128, 0, s>>>(t, status, m.free_energy.as<double>(), m.terms.as<double>(),
-                                  m.grad.as<double>(), m.qsh.as<double>(), m.out_energy.as<double>(),
-                                  m.out_forces.as<double>(), m.out_charges.as<double>());
+  if (count > 0) XTB_STAGE(kStClassical, 1, launch_classical(f, m.max_atoms, m.max_shells, s));
+  if (want_forces && count > 0) XTB_STAGE(kStCnChain, 2, launch_cn_chain(f, m.max_atoms, s));
+  XTB_STAGE(kStPublish, 1,
+            k_publish<<<nsys, 128, 0, s>>>(t, status, m.free_energy.as<double>(),
+                                           m.terms.as<double>(), m.grad.as<double>(),
+                                           m.qsh.as<double>(), m.out_energy.as<double>(),
+                                           m.out_forces.as<double>(), m.out_charges.as<double>()));
+#undef XTB_STAGE
   // ---- copy into caller buffers ----
   const xtbloom_batch_result_t& r = *req.result;
   auto put = [&](const xtbloom_buffer_t& dst, const void* src, size_t bytes) {
@@ -787,6 +861,7 @@ xtbloom_status_t Engine::compute(const ComputeRequest& req, std::string& error) 
     error = std::string("CUDA launch failure: ") + cudaGetErrorString(le);
     return XTBLOOM_STATUS_INTERNAL_ERROR;
   }
+  if (m.prof.on) m.prof.collect();
   m.have_results = true;
   return XTBLOOM_STATUS_SUCCESS;
 }
@@ -794,6 +869,34 @@ xtbloom_status_t Engine::compute(const ComputeRequest& req, std::string& error) 
 xtbloom_status_t Engine::debug_fetch(const std::string& name, int64_t system, double* out,
                                      size_t capacity, size_t* count, std::string& error) {
   Impl& m = *impl_;
+  if (name == "kernel_times" || name == "launch_count" || name == "reset_counters") {
+    // Accumulated since the last reset: [ms, calls] per stage, or total launches.
+    if (name == "reset_counters") {
+      for (int i = 0; i < kStageCount; ++i) {
+        m.prof.total_ms[i] = 0.0;
+        m.prof.calls[i] = 0;
+      }
+      m.prof.launches = 0;
+      *count = 0;
+      return XTBLOOM_STATUS_SUCCESS;
+    }
+    const size_t len = name == "launch_count" ? 2 : 2 * (size_t)kStageCount;
+    if (capacity < len) {
+      error = "capacity too small";
+      return XTBLOOM_STATUS_INVALID_ARGUMENT;
+    }
+    if (name == "launch_count") {
+      out[0] = (double)m.prof.launches;
+      out[1] = m.prof.on ? 1.0 : 0.0;
+    } else {
+      for (int i = 0; i < kStageCount; ++i) {
+        out[2 * i] = m.prof.total_ms[i];
+        out[2 * i + 1] = (double)m.prof.calls[i];
+      }
+    }
+    *count = len;
+    return XTBLOOM_STATUS_SUCCESS;
+  }
   if (!m.have_results || system < 0 || system >= m.nsys) {
     error = "no retained results for that system";
     return XTBLOOM_STATUS_INVALID_ARGUMENT;
