@@ -1075,5 +1075,5 @@ def singlepoint(numbers, pos, charge=0.0, uhf=0, kt=300.0 * PR.KELVIN_TO_HARTREE
         repulsion(numbers, pos, grad=grad)
     if debug:
         dbg.update(cn=cn, S=S, D=D, Q=Q, H0=H0, P=P, W=W, eps=eps, qsh=qsh, dip=dip, qp=qp,
-                   gam=gam, cn_d4=d4.cn)
+                   gam=gam, cn_d4=d4.cn, nel=nel)
     return Result(energy, grad, qat, it, converged, terms, dbg)

@@ -1,0 +1,59 @@
+"""Pins of the CPU oracle (numpy restatement) against the reference's own outputs."""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+from conftest import as_molecule
+from oracle import gfn2
+
+FAST = ["c10h22_conformer_0", "c10h22_conformer_3", "hetero_chain_7", "h3_plus", "ketene",
+        "nenacl", "sif5_minus", "oh_radical", "zn_atom", "i_anion", "rn_atom"]
+
+
+@pytest.mark.parametrize("name", FAST)
+def test_oracle_matches_reference_library(fixtures, name):
+    """Energy, forces, charges and iteration count equal the compiled reference library."""
+    sys_ = next(s for s in fixtures if s["name"] == name)
+    z, x, q, u = as_molecule(sys_)
+    r = gfn2.singlepoint(z, x, charge=q, uhf=u)
+    assert r.converged
+    assert abs(r.energy - sys_["energy"]) < 1e-9
+    assert np.abs(-r.gradient.ravel() - np.asarray(sys_["forces"])).max() < 1e-8
+    assert np.abs(r.charges - np.asarray(sys_["charges"])).max() < 1e-8
+    assert r.iterations == sys_["scc_iterations"]
+
+
+def test_oracle_matches_tblite_goldens(fixtures, tblite_goldens):
+    """The oracle reproduces the pinned tblite 0.7.0 conformance energies and forces (5e-7)."""
+    for case in tblite_goldens:
+        sys_ = next(s for s in fixtures if s["name"] == case["name"])
+        z, x, q, u = as_molecule(sys_)
+        r = gfn2.singlepoint(z, x, charge=q, uhf=u)
+        assert abs(r.energy - case["energy"]) < 5e-7, case["name"]
+        assert np.abs(-r.gradient.ravel() - np.asarray(case["forces"])).max() < 5e-7, case["name"]
+
+
+def test_oracle_gradient_is_derivative_of_energy(fixtures):
+    """Central finite differences (h = 1e-4 bohr) of the oracle energy match its analytic gradient."""
+    sys_ = next(s for s in fixtures if s["name"] == "ketene")
+    z, x, q, u = as_molecule(sys_)
+    r = gfn2.singlepoint(z, x, charge=q, uhf=u, ctol=1e-10, etol=1e-12)
+    h = 1e-4
+    fd = np.zeros_like(x)
+    for a in range(len(z)):
+        for c in range(3):
+            xp, xm = x.copy(), x.copy()
+            xp[a, c] += h
+            xm[a, c] -= h
+            ep = gfn2.singlepoint(z, xp, q, u, ctol=1e-10, etol=1e-12, forces=False).energy
+            em = gfn2.singlepoint(z, xm, q, u, ctol=1e-10, etol=1e-12, forces=False).energy
+            fd[a, c] = (ep - em) / (2 * h)
+    assert np.abs(fd - r.gradient).max() < 2e-6
+
+
+def test_integer_layout_of_basis():
+    """AO/shell counts per element follow the GFN2 basis (H: 1s; C, N, O: 2s2p; Cl: 3s3p3d)."""
+    for z, nsh, nao in [(1, 1, 1), (6, 2, 4), (7, 2, 4), (8, 2, 4), (17, 3, 9)]:
+        b = gfn2.make_basis(np.array([z]))
+        assert len(b.sh_l) == nsh and b.nao == nao

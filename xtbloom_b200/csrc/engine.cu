@@ -11,7 +11,10 @@
 #include "engine.h"
 
 #include <algorithm>
+#include <chrono>
 #include <cmath>
+#include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <limits>
 #include <map>
@@ -226,8 +229,11 @@ struct Engine::Impl {
   Dbuf grad, acn, acn_d4;
   Dbuf out_energy, out_forces, out_charges;
   int32_t* h_count = nullptr;   // pinned
+  int32_t* h_list = nullptr;    // pinned copy of the active list
+  int64_t h_list_cap = 0;
   int last_memory = 0;
   bool have_results = false;
+  bool trace = false;
   Profiler prof;
 
   DevTopo devtopo() const {
@@ -295,10 +301,13 @@ Engine::Engine(int device, cudaStream_t stream) : impl_(new Impl), device_(devic
   cudaMallocHost(&impl_->h_count, 4 * sizeof(int32_t));
   const char* env = std::getenv("XTBLOOM_B200_KERNEL_TIMING");
   impl_->prof.on = env != nullptr && env[0] == '1';
+  const char* tr = std::getenv("XTBLOOM_B200_TRACE");
+  impl_->trace = tr != nullptr && tr[0] == '1';
 }
 
 Engine::~Engine() {
   if (impl_->h_count) cudaFreeHost(impl_->h_count);
+  if (impl_->h_list) cudaFreeHost(impl_->h_list);
   delete impl_;
 }
 
@@ -559,6 +568,7 @@ xtbloom_status_t Engine::compute(const ComputeRequest& req, std::string& error) 
   Impl& m = *impl_;
   cudaStream_t s = stream_;
   cudaSetDevice(device_);
+  const auto t_start = std::chrono::steady_clock::now();
   const xtbloom_batch_t& b = *req.batch;
   const int64_t B = b.batch_size;
   const int64_t N = b.total_atoms;
@@ -695,11 +705,81 @@ xtbloom_status_t Engine::compute(const ComputeRequest& req, std::string& error) 
   const int32_t* dnao = m.nao.as<int32_t>();
   const int32_t* dnvec = m.nvec.as<int32_t>();
 
+  // AO-count buckets of the (n-descending) active list: each bucket gets its
+  // own launch geometry and shared-memory footprint.
+  if (m.h_list_cap < B) {
+    if (m.h_list) cudaFreeHost(m.h_list);
+    cudaMallocHost(&m.h_list, B * sizeof(int32_t));
+    m.h_list_cap = B;
+  }
+  struct Bucket {
+    int start, count, max_n, max_m;
+  };
+  auto buckets = [&](int count) {
+    static const int kEdges[] = {230, 192, 160, 128, 96, 64, 0};
+    std::vector<Bucket> out;
+    int i = 0;
+    if (count <= 296) {
+      // at most two waves: one launch, so few large systems run concurrently
+      Bucket bk{0, count, count > 0 ? m.h_nao[m.h_list[0]] : 0, 0};
+      for (int k = 0; k < count; ++k) {
+        const int sy = m.h_list[k];
+        bk.max_m = std::max(bk.max_m, (int)std::ceil(std::max(m.h_nel_a[sy], m.h_nel_b[sy])) + 4);
+      }
+      if (count > 0) out.push_back(bk);
+      return out;
+    }
+    while (i < count) {
+      const int n0 = m.h_nao[m.h_list[i]];
+      int lo_edge = 0;
+      for (int e : kEdges)
+        if (n0 > e) { lo_edge = e; break; }
+      Bucket bk{i, 0, n0, 0};
+      while (i < count && m.h_nao[m.h_list[i]] > lo_edge) {
+        const int sy = m.h_list[i];
+        bk.max_m = std::max(bk.max_m, (int)std::ceil(std::max(m.h_nel_a[sy], m.h_nel_b[sy])) + 4);
+        ++bk.count;
+        ++i;
+      }
+      out.push_back(bk);
+    }
+    return out;
+  };
+  // tridiagonalise, eigenvalues (+ occupations), eigenvectors, back-transform
+  auto eigensolve = [&](int count, int mode, double kt, double ortol_rel, int stage_base) {
+    const std::vector<Bucket> bks = buckets(count);
+    auto sub = [&](const Bucket& bk) {
+      EigArgs gb = eg;
+      gb.list = list + bk.start;
+      return gb;
+    };
+    XTB_STAGE(stage_base == kStLowdin ? kStLowdin : kStTridiag, (int)bks.size(), for (const Bucket& bk : bks) {
+      const EigArgs gb = sub(bk);
+      if (bk.max_n <= 230) launch_tridiag_smem(gb, gb.list, bk.count, bk.max_n, s);
+      else launch_tridiag(gb, bk.count, bk.max_n, s);
+    });
+    XTB_STAGE(stage_base == kStLowdin ? kStLowdin : kStEigvals, (int)bks.size(),
+              for (const Bucket& bk : bks) launch_eigvals(sub(bk), mode, kt, bk.count, bk.max_n, s));
+    XTB_STAGE(stage_base == kStLowdin ? kStLowdin : kStInvIter, (int)bks.size(),
+              for (const Bucket& bk : bks) launch_inverse_iteration(sub(bk), bk.count, ortol_rel, s));
+    XTB_STAGE(stage_base == kStLowdin ? kStLowdin : kStBacktransform, (int)bks.size(), for (const Bucket& bk : bks) {
+      const EigArgs gb = sub(bk);
+      const int want = mode == 1 ? bk.max_n : std::min(bk.max_m, bk.max_n);
+      const long budget = 220L * 1024 / 8 - (long)bk.max_n * 33 - 2 * 32 * 33 - 8;
+      const int wcap = (int)std::min<long>(want, budget / 32);
+      if (wcap >= 8) {
+        launch_backtransform_wy(gb, bk.count, bk.max_n, wcap, s);
+      } else {
+        launch_backtransform(gb, gb.list, bk.count, bk.max_n, 0, s);
+      }
+    });
+  };
+
   // ---- Loewdin orthogonaliser X = U s^-1/2 U^T ----
   cudaMemcpyAsync(m.A.p, m.S.p, (size_t)m.total_mat * 8, cudaMemcpyDeviceToDevice, s);
-  XTB_STAGE(kStLowdin, 6, launch_tridiag(eg, nsys, m.max_n, s);
-            launch_eigvals(eg, 1, 0.0, nsys, m.max_n, s); launch_inverse_iteration(eg, nsys, s);
-            launch_backtransform(eg, nsys, m.max_n, s); launch_lowdin_weights(eg, status, nsys, s);
+  std::memcpy(m.h_list, m.h_order.data(), B * sizeof(int32_t));
+  eigensolve(nsys, 1, 0.0, 2e-6, kStLowdin);
+  XTB_STAGE(kStLowdin, 2, launch_lowdin_weights(eg, status, nsys, s);
             gemm(m.Zv.as<double>(), m.Zv.as<double>(), m.X.as<double>(), dnao, dnao, dnao, true,
                  m.occ.as<double>(), nsys));
 
@@ -750,6 +830,7 @@ xtbloom_status_t Engine::compute(const ComputeRequest& req, std::string& error) 
             launch_compact(order, nsys, status, a.converged, a.iterations, req.max_iter, list,
                            dcount, s));
   cudaMemcpyAsync(m.h_count, dcount, 4, cudaMemcpyDeviceToHost, s);
+  cudaMemcpyAsync(m.h_list, list, B * sizeof(int32_t), cudaMemcpyDeviceToHost, s);
   cudaStreamSynchronize(s);
   int count = m.h_count[0];
   a.count = count;
@@ -763,10 +844,7 @@ xtbloom_status_t Engine::compute(const ComputeRequest& req, std::string& error) 
                    nullptr, count);
               gemm(m.X.as<double>(), m.T.as<double>(), m.A.as<double>(), dnao, dnao, dnao, false,
                    nullptr, count));
-    XTB_STAGE(kStTridiag, 1, launch_tridiag(eg, count, m.max_n, s));
-    XTB_STAGE(kStEigvals, 1, launch_eigvals(eg, 0, req.kt, count, m.max_n, s));
-    XTB_STAGE(kStInvIter, 1, launch_inverse_iteration(eg, count, s));
-    XTB_STAGE(kStBacktransform, 1, launch_backtransform(eg, count, m.max_n, s));
+    eigensolve(count, 0, req.kt, 2e-7, kStTridiag);
     XTB_STAGE(kStDensity, 2,
               gemm(m.Zv.as<double>(), m.X.as<double>(), m.C.as<double>(), dnvec, dnao, dnao, false,
                    nullptr, count);
@@ -782,7 +860,13 @@ xtbloom_status_t Engine::compute(const ComputeRequest& req, std::string& error) 
               launch_compact(order, nsys, status, a.converged, a.iterations, req.max_iter, list,
                              dcount, s));
     cudaMemcpyAsync(m.h_count, dcount, 4, cudaMemcpyDeviceToHost, s);
+    cudaMemcpyAsync(m.h_list, list, B * sizeof(int32_t), cudaMemcpyDeviceToHost, s);
     cudaStreamSynchronize(s);
+    if (m.trace) {
+      std::fprintf(stderr, "[xtbloom_b200] iteration %d active %d -> %d  t=%.3f ms\n", it, a.count,
+                   m.h_count[0],
+                   std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t_start).count());
+    }
     count = m.h_count[0];
   }
   k_finalize_status<<<(nsys + 255) / 256, 256, 0, s>>>(nsys, status, a.converged);

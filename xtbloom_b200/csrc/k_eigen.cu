@@ -17,6 +17,7 @@
 // eigenpairs are basis independent.
 #include "kernels.cuh"
 
+#include <algorithm>
 #include <cfloat>
 
 namespace xtb {
@@ -193,6 +194,126 @@ __global__ void __launch_bounds__(512) k_tridiag(EigArgs g) {
 }
 
 // ---------------------------------------------------------------------------
+// Shared-memory variant: the symmetric matrix lives in packed lower storage
+// (element (r, c), r >= c, at r(r+1)/2 + c) inside one CTA's shared memory, so
+// every Householder step touches only on-chip data.  The symmetric matvec uses
+// per-warp private accumulators for the transposed half (no atomics).  The
+// reflectors are written to the global matrix in the layout k_backtransform
+// reads.  Requires n(n+1)/2 + (2 + nwarps) n + 40 doubles of shared memory.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ int64_t pk(int r, int c) { return (int64_t)r * (r + 1) / 2 + c; }
+
+__global__ void __launch_bounds__(256) k_tridiag_smem(EigArgs g, const int32_t* list) {
+  extern __shared__ double sm[];
+  const int s = list[blockIdx.x];
+  const int n = g.nao[s];
+  double* ga = g.A + g.mat_off[s];
+  double* d = g.d + g.ao_off[s];
+  double* e = g.e + g.ao_off[s];
+  double* tau = g.tau + g.ao_off[s];
+  const int tid = threadIdx.x, bs = blockDim.x;
+  const int lane = tid & 31, warp = tid >> 5, nw = bs >> 5;
+  double* L = sm;
+  double* v = L + pk(n, 0);
+  double* p = v + n;
+  double* priv = p + n;          // nw x n
+  double* red = priv + (int64_t)nw * n;
+  // load the lower triangle
+  for (int r = warp; r < n; r += nw)
+    for (int c = lane; c <= r; c += 32) L[pk(r, c)] = ga[(int64_t)r * n + c];
+  for (int k = tid; k < nw * n; k += bs) priv[k] = 0.0;
+  __syncthreads();
+  for (int i = 0; i + 2 < n; ++i) {
+    const int m = n - i - 1;
+    const int o = i + 1;                       // first row/col of the trailing block
+    double part = 0.0;
+    for (int k = tid; k < m; k += bs) {
+      const double x = L[pk(o + k, i)];
+      v[k] = x;
+      if (k >= 1) part += x * x;
+    }
+    const double xn2 = block_sum(part, red);
+    const double alpha = v[0];
+    double ti = 0.0, beta = alpha;
+    if (xn2 > 0.0) {
+      beta = -copysign(sqrt(alpha * alpha + xn2), alpha);
+      ti = (beta - alpha) / beta;
+      const double sc = 1.0 / (alpha - beta);
+      for (int k = tid; k < m; k += bs) {
+        if (k >= 1) {
+          const double vk = v[k] * sc;
+          v[k] = vk;
+          ga[(int64_t)i * n + o + k] = vk;
+        }
+      }
+    }
+    __syncthreads();
+    if (tid == 0) {
+      v[0] = 1.0;
+      d[i] = L[pk(i, i)];
+      e[i] = beta;
+      tau[i] = ti;
+    }
+    __syncthreads();
+    if (ti == 0.0) continue;
+    // p = tau * A22 v with A22 symmetric, stored lower
+    for (int r = warp; r < m; r += nw) {
+      const double* row = L + pk(o + r, o);
+      const double vr = v[r];
+      double acc = 0.0;
+      for (int c = lane; c <= r; c += 32) {
+        const double a = row[c];
+        acc = fma(a, v[c], acc);
+        if (c < r) priv[warp * n + c] = fma(a, vr, priv[warp * n + c]);
+      }
+      acc = warp_sum(acc);
+      if (lane == 0) p[r] = acc;
+    }
+    __syncthreads();
+    double pv = 0.0;
+    for (int k = tid; k < m; k += bs) {
+      double t = p[k];
+      for (int w = 0; w < nw; ++w) {
+        t += priv[w * n + k];
+        priv[w * n + k] = 0.0;
+      }
+      t *= ti;
+      p[k] = t;
+      pv += t * v[k];
+    }
+    const double K = 0.5 * ti * block_sum(pv, red);
+    for (int k = tid; k < m; k += bs) p[k] -= K * v[k];
+    __syncthreads();
+    for (int r = warp; r < m; r += nw) {
+      double* row = L + pk(o + r, o);
+      const double vr = v[r], wr = p[r];
+      for (int c = lane; c <= r; c += 32) row[c] -= vr * p[c] + wr * v[c];
+    }
+    __syncthreads();
+  }
+  if (tid == 0) {
+    if (n >= 2) {
+      d[n - 2] = L[pk(n - 2, n - 2)];
+      e[n - 2] = L[pk(n - 1, n - 2)];
+      tau[n - 2] = 0.0;
+    }
+    d[n - 1] = L[pk(n - 1, n - 1)];
+    e[n - 1] = 0.0;
+    tau[n - 1] = 0.0;
+  }
+}
+
+size_t tridiag_smem_bytes(int n) { return ((size_t)n * (n + 1) / 2 + (2 + 8) * (size_t)n + 40) * sizeof(double); }
+
+void launch_tridiag_smem(const EigArgs& g, const int32_t* list, int count, int max_n, cudaStream_t stream) {
+  if (count == 0) return;
+  static const bool attr = cudaFuncSetAttribute(k_tridiag_smem, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                227 * 1024) == cudaSuccess;
+  (void)attr;
+  k_tridiag_smem<<<count, 256, tridiag_smem_bytes(max_n), stream>>>(g, list);
+}
+
+// ---------------------------------------------------------------------------
 // Eigenvalues (bisection), occupations and the number of needed eigenvectors.
 // ---------------------------------------------------------------------------
 __device__ __forceinline__ int sturm_count(const double* d, const double* e2, int n, double x,
@@ -207,6 +328,57 @@ __device__ __forceinline__ int sturm_count(const double* d, const double* e2, in
     if (q < 0.0) ++c;
   }
   return c;
+}
+
+// Number of eigenvalues below x for four shifts at once, from the sign changes
+// of the three-term (Givens) Sturm sequence p_{k+1} = (d_k - x) p_k - e_{k-1}^2 p_{k-1},
+// p_0 = 1.  No divisions.  The caller scales T by a power of two so that its
+// spectrum lies in [-1, 1] and floors e^2 at 1e-40: then |p| grows at most
+// 3x and shrinks at most 3e40x per step, and rescaling the pair (p_{k-1}, p_k)
+// by a power of two every fourth step (exact, sign-preserving) keeps it far
+// from overflow and underflow.  Sign changes are read from the sign bits.  An
+// exact zero inside the sequence lies between two terms of opposite sign
+// (p_{k+1} = -e_k^2 p_{k-1}, and e^2 > 0), so the sign it is given does not
+// change the count; a zero last term means x is an eigenvalue, which either
+// count brackets correctly.
+__device__ __forceinline__ void rescale_pair(double& a, double& b) {
+  const int ea = __double2hiint(a) & 0x7ff00000;
+  const int eb = __double2hiint(b) & 0x7ff00000;
+  // 2^-(exponent of max(|a|, |b|)); 2^1023 when both are zero or subnormal
+  const double f = __hiloint2double(0x7fe00000 - max(ea, eb), 0);
+  a *= f;
+  b *= f;
+}
+
+__device__ __forceinline__ void sturm4(const double* d, const double* e2, int n, const double x[4],
+                                       int c[4]) {
+  double p0[4], p1[4];
+#pragma unroll
+  for (int q = 0; q < 4; ++q) {
+    p0[q] = 1.0;
+    p1[q] = d[0] - x[q];
+    c[q] = (int)((unsigned)__double2hiint(p1[q]) >> 31);
+  }
+  auto step = [&](int k) {
+    const double dk = d[k], ek = e2[k - 1];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      const double p2 = fma(dk - x[q], p1[q], -ek * p0[q]);
+      c[q] += (int)((unsigned)(__double2hiint(p2) ^ __double2hiint(p1[q])) >> 31);
+      p0[q] = p1[q];
+      p1[q] = p2;
+    }
+  };
+  int k = 1;
+  for (; k + 4 <= n; k += 4) {
+    step(k);
+    step(k + 1);
+    step(k + 2);
+    step(k + 3);
+#pragma unroll
+    for (int q = 0; q < 4; ++q) rescale_pair(p0[q], p1[q]);
+  }
+  for (; k < n; ++k) step(k);
 }
 
 __device__ __forceinline__ double fermi_f(double de, double kt) {
@@ -274,18 +446,27 @@ __device__ void warp_fermi(const double* eps, int n, double nel, double kt, doub
   __syncwarp();
 }
 
-// mode 0: SCC (occupations, needed vectors); mode 1: all vectors, no occupations.
-__global__ void __launch_bounds__(256) k_tridiag_eigvals(EigArgs g, int mode, double kt) {
-  extern __shared__ double sm[];
-  const int s = g.list[blockIdx.x];
-  const int n = g.nao[s];
-  const int64_t o = g.ao_off[s];
-  double* d = sm;
-  double* e2 = sm + n;
-  double* ev = sm + 2 * n;
-  double* fa = sm + 3 * n;
-  double* fb = sm + 4 * n;
-  double* red = sm + 5 * n;
+__device__ void bisect_range(const double* d, const double* e2, int n, double glo, double ghi,
+                             double pivmin, int j0, int j1, double unscale, int tpe_max, double* ev);
+
+// Number of eigenvalues the SCC needs: the occupied levels and eight above
+// them (mode 0); all of them for the overlap (mode 1).
+__device__ __forceinline__ int levels_needed(const EigArgs& g, int s, int n, int mode) {
+  if (mode != 0) return n;
+  return min(n, (int)ceil(fmax(g.nel_a[s], g.nel_b[s])) + 8);
+}
+
+struct ScaledTridiag {
+  double glo, ghi;     // bracket of the whole spectrum (scaled)
+  double pivmin;       // (scaled)
+  double unscale;      // 2^ex: eigenvalue of T = scaled eigenvalue * unscale
+};
+
+// Loads the tridiagonal of system s into shared memory as T / 2^ex with the
+// spectrum inside [-1, 1] (exact; see sturm4): d, e2 = squared off-diagonal
+// floored at 1e-40.  Gershgorin bounds give the bracket.  Block-wide.
+__device__ ScaledTridiag load_scaled_tridiag(const EigArgs& g, int64_t o, int n, double* d, double* e2,
+                                             double* red) {
   const int tid = threadIdx.x, bs = blockDim.x;
   double lo_b = DBL_MAX, hi_b = -DBL_MAX, emax = 0.0;
   for (int k = tid; k < n; k += bs) {
@@ -303,43 +484,149 @@ __global__ void __launch_bounds__(256) k_tridiag_eigvals(EigArgs g, int mode, do
   const double e2max = block_max(emax, red);
   const double pivmin = DBL_MIN * fmax(1.0, e2max);
   const double tnorm = fmax(fabs(gl), fabs(gu));
-  const double glo = gl - 2.0 * tnorm * DBL_EPSILON * n - 4.0 * pivmin;
-  const double ghi = gu + 2.0 * tnorm * DBL_EPSILON * n + 4.0 * pivmin;
-  for (int j = tid; j < n; j += bs) {
-    double lo = glo, hi = ghi;
-    for (int it = 0; it < 256; ++it) {
-      if (hi - lo <= 2.0 * DBL_EPSILON * fmax(fabs(lo), fabs(hi)) + 4.0 * pivmin) break;
-      const double mid = 0.5 * (lo + hi);
-      if (mid <= lo || mid >= hi) break;
-      if (sturm_count(d, e2, n, mid, pivmin) > j) hi = mid; else lo = mid;
-    }
-    ev[j] = 0.5 * (lo + hi);
+  int ex = 0;
+  frexp(tnorm, &ex);
+  const double sc = ldexp(1.0, -ex);
+  for (int k = tid; k < n; k += bs) {
+    d[k] *= sc;
+    e2[k] = fmax(e2[k] * sc * sc, 1e-40);
   }
   __syncthreads();
-  for (int j = tid; j < n; j += bs) g.eig[o + j] = ev[j];
+  ScaledTridiag t;
+  t.glo = (gl - 2.0 * tnorm * DBL_EPSILON * n - 4.0 * pivmin) * sc;
+  t.ghi = (gu + 2.0 * tnorm * DBL_EPSILON * n + 4.0 * pivmin) * sc;
+  t.pivmin = pivmin * sc * sc;
+  t.unscale = ldexp(1.0, ex);
+  return t;
+}
+
+// Latency form for few systems: part blockIdx.x of `parts` CTAs of system
+// blockIdx.y bisects a contiguous slice of the needed eigenvalues, with up to
+// a warp per eigenvalue, and writes them to g.eig.
+__global__ void __launch_bounds__(256) k_eigvals_part(EigArgs g, int mode, int parts) {
+  extern __shared__ double sm[];
+  const int s = g.list[blockIdx.y];
+  const int n = g.nao[s];
+  const int64_t o = g.ao_off[s];
+  const int nk = levels_needed(g, s, n, mode);
+  const int per = (nk + parts - 1) / parts;
+  const int j0 = blockIdx.x * per, j1 = min(nk, j0 + per);
+  if (j0 >= j1) return;   // uniform over the block
+  double* d = sm;
+  double* e2 = sm + n;
+  double* red = sm + 2 * n;
+  const ScaledTridiag t = load_scaled_tridiag(g, o, n, d, e2, red);
+  bisect_range(d, e2, n, t.glo, t.ghi, t.pivmin, j0, j1, t.unscale, 32, g.eig + o);
+}
+
+// mode 0: SCC (occupations, needed vectors); mode 1: all vectors, no occupations.
+// have != 0: the needed eigenvalues are already in g.eig (k_eigvals_part).
+// Bisection here uses at most tpe_max threads per eigenvalue.
+__global__ void __launch_bounds__(256) k_tridiag_eigvals(EigArgs g, int mode, double kt, int have,
+                                                         int tpe_max) {
+  extern __shared__ double sm[];
+  const int s = g.list[blockIdx.x];
+  const int n = g.nao[s];
+  const int64_t o = g.ao_off[s];
+  double* d = sm;
+  double* e2 = sm + n;
+  double* ev = sm + 2 * n;
+  double* fa = sm + 3 * n;
+  double* fb = sm + 4 * n;
+  double* red = sm + 5 * n;
+  const int tid = threadIdx.x, bs = blockDim.x;
+  const ScaledTridiag t = load_scaled_tridiag(g, o, n, d, e2, red);
+  // In the SCC only the occupied eigenpairs and a few above them are needed:
+  // the Fermi level is found on that partial spectrum (the higher levels count
+  // as empty) and the rest is computed only if the last one is not empty.
+  int nk = levels_needed(g, s, n, mode);
+  if (have) {
+    for (int j = tid; j < nk; j += bs) ev[j] = g.eig[o + j];
+  } else {
+    bisect_range(d, e2, n, t.glo, t.ghi, t.pivmin, 0, nk, t.unscale, tpe_max, ev);
+  }
+  __syncthreads();
   if (mode == 1) {
+    if (!have)
+      for (int j = tid; j < n; j += bs) g.eig[o + j] = ev[j];
     if (tid == 0) g.nvec[s] = n;
     return;
   }
   const int warp = tid >> 5;
-  double ent = 0.0;
-  if (warp == 0) warp_fermi(ev, n, g.nel_a[s], kt, fa, ent);
-  if (warp == 1) warp_fermi(ev, n, g.nel_b[s], kt, fb, ent);
-  if ((tid & 31) == 0 && warp < 2) red[warp] = ent;
-  __syncthreads();
   __shared__ int last;
-  if (tid == 0) last = -1;
-  __syncthreads();
+  __shared__ int need_more;
+  for (int pass = 0; pass < 2; ++pass) {
+    double ent = 0.0;
+    if (warp == 0) warp_fermi(ev, nk, g.nel_a[s], kt, fa, ent);
+    if (warp == 1) warp_fermi(ev, nk, g.nel_b[s], kt, fb, ent);
+    if ((tid & 31) == 0 && warp < 2) red[warp] = ent;
+    __syncthreads();
+    if (tid == 0) {
+      last = -1;
+      need_more = (nk < n && fa[nk - 1] + fb[nk - 1] > 1e-14) ? 1 : 0;
+    }
+    __syncthreads();
+    if (!need_more) break;
+    bisect_range(d, e2, n, t.glo, t.ghi, t.pivmin, nk, n, t.unscale, 8, ev);
+    nk = n;
+    __syncthreads();
+  }
   for (int j = tid; j < n; j += bs) {
-    const double f = fa[j] + fb[j];
+    const double f = j < nk ? fa[j] + fb[j] : 0.0;
+    g.eig[o + j] = j < nk ? ev[j] : DBL_MAX;
     g.occ[o + j] = f;
-    g.occ_eps[o + j] = f * ev[j];
+    g.occ_eps[o + j] = j < nk ? f * ev[j] : 0.0;
     if (f > 1e-14) atomicMax(&last, j);
   }
   __syncthreads();
   if (tid == 0) {
     g.nvec[s] = last + 1;
     g.entropy[s] = red[0] + red[1];
+  }
+}
+
+// Eigenvalues j0..j1-1 (ascending) of the scaled symmetric tridiagonal (d, e2)
+// by multisection.  A group of tpe threads (a power of two, as many as the
+// block has to spare, at most tpe_max <= 32) shares one eigenvalue: each thread evaluates
+// four interleaved Sturm sequences (sturm4), so a round cuts the interval into
+// 4 tpe + 1 parts.  Results are written unscaled (times `unscale`).
+__device__ void bisect_range(const double* d, const double* e2, int n, double glo, double ghi,
+                             double pivmin, int j0, int j1, double unscale, int tpe_max, double* ev) {
+  const int cnt = j1 - j0;
+  if (cnt <= 0) return;
+  int tpe = 1;
+  while (tpe < tpe_max && cnt * tpe * 2 <= (int)blockDim.x) tpe *= 2;
+  const int r = threadIdx.x & (tpe - 1);
+  const int lane = threadIdx.x & 31;
+  const unsigned gmask = (tpe == 32 ? 0xffffffffu : ((1u << tpe) - 1u)) << (lane & ~(tpe - 1));
+  const double inv_parts = 1.0 / (4 * tpe + 1);
+  for (int jj = threadIdx.x / tpe; jj < cnt; jj += blockDim.x / tpe) {
+    const int j = j0 + jj;
+    double lo = glo, hi = ghi;
+    for (int it = 0; it < 80; ++it) {
+      const double w = hi - lo;
+      if (w <= 2.0 * DBL_EPSILON * fmax(fabs(lo), fabs(hi)) + 4.0 * pivmin) break;
+      double x[4];
+      int c[4];
+#pragma unroll
+      for (int q = 0; q < 4; ++q) x[q] = lo + (4 * r + q + 1) * inv_parts * w;
+      sturm4(d, e2, n, x, c);
+      double nlo = lo, nhi = hi;
+#pragma unroll
+      for (int q = 0; q < 4; ++q)
+        if (c[q] <= j) nlo = x[q];
+#pragma unroll
+      for (int q = 3; q >= 0; --q)
+        if (c[q] > j) nhi = x[q];
+      for (int off = 1; off < tpe; off <<= 1) {
+        nlo = fmax(nlo, __shfl_xor_sync(gmask, nlo, off));
+        nhi = fmin(nhi, __shfl_xor_sync(gmask, nhi, off));
+      }
+      if (!(nlo > lo) && !(nhi < hi)) break;   // resolution limit reached
+      lo = nlo;
+      hi = nhi;
+    }
+    if (r == 0) ev[j] = 0.5 * (lo + hi) * unscale;
   }
 }
 
@@ -353,7 +640,11 @@ __device__ __forceinline__ double hash_unit(uint32_t a, uint32_t b) {
   return (double)h * (2.0 / 4294967296.0) - 1.0;
 }
 
-__global__ void __launch_bounds__(128) k_inverse_iteration(EigArgs g) {
+// ortol_rel: eigenvalues closer than ortol_rel * ||T||_1 form a cluster whose
+// vectors are re-orthogonalised.  Outside clusters inverse-iteration vectors
+// are orthogonal to ~eps ||T|| / gap, i.e. better than 1e-9 for the
+// thresholds used (2e-7 for Hamiltonians, 2e-6 for overlap matrices).
+__global__ void __launch_bounds__(128) k_inverse_iteration(EigArgs g, double ortol_rel) {
   const int s = g.list[blockIdx.x];
   const int n = g.nao[s];
   const int m = g.nvec[s];
@@ -362,12 +653,16 @@ __global__ void __launch_bounds__(128) k_inverse_iteration(EigArgs g) {
   const double* e = g.e + o;
   const double* ev = g.eig + o;
   double* Z = g.Z + g.mat_off[s];
-  double* scr = g.scratch + g.scratch_off[s] + (int64_t)threadIdx.x * 5 * n;
-  double* u1 = scr;
-  double* u2 = scr + n;
-  double* u3 = scr + 2 * n;
-  double* lm = scr + 3 * n;
-  double* pv = scr + 4 * n;
+  // Per-thread work vectors interleaved across the CTA's threads (element k of
+  // array a for thread t at ((a*n + k) * 128 + t)) so that every sequential
+  // sweep over k is a coalesced warp access.
+  double* scr = g.scratch + g.scratch_off[s] + threadIdx.x;
+  const int64_t ld = 128;
+  auto U1 = [&](int k) -> double& { return scr[((int64_t)0 * n + k) * ld]; };
+  auto U2 = [&](int k) -> double& { return scr[((int64_t)1 * n + k) * ld]; };
+  auto U3 = [&](int k) -> double& { return scr[((int64_t)2 * n + k) * ld]; };
+  auto LM = [&](int k) -> double& { return scr[((int64_t)3 * n + k) * ld]; };
+  auto Y = [&](int k) -> double& { return scr[((int64_t)4 * n + k) * ld]; };
   // one-norm of T and the cluster threshold
   __shared__ double s_onenrm;
   if (threadIdx.x == 0) {
@@ -380,7 +675,7 @@ __global__ void __launch_bounds__(128) k_inverse_iteration(EigArgs g) {
   }
   __syncthreads();
   const double onenrm = s_onenrm;
-  const double ortol = 1e-5 * onenrm;
+  const double ortol = ortol_rel * onenrm;
   const double tiny = DBL_EPSILON * onenrm;
   for (int lead = threadIdx.x; lead < m; lead += blockDim.x) {
     if (lead > 0 && ev[lead] - ev[lead - 1] <= ortol) continue;   // not a cluster leader
@@ -390,63 +685,91 @@ __global__ void __launch_bounds__(128) k_inverse_iteration(EigArgs g) {
       double x = ev[j];
       if (j > lead && x - xprev < 10.0 * DBL_EPSILON * fabs(x)) x = xprev + 10.0 * DBL_EPSILON * fabs(x);
       xprev = x;
-      // LU with partial pivoting of T - xI
+      // LU with partial pivoting of T - xI; U1 holds reciprocal pivots and the
+      // sign of LM encodes the row interchange (pivoted rows store -l - 4; both |l| <= 1).
       double diag = d[0] - x, sup = n > 1 ? e[0] : 0.0;
       for (int k = 0; k < n - 1; ++k) {
         const double ck = e[k];
         const double nd = d[k + 1] - x;
         const double ns = (k + 1 < n - 1) ? e[k + 1] : 0.0;
+        double u1, l;
         if (fabs(diag) >= fabs(ck)) {
-          const double l = diag != 0.0 ? ck / diag : 0.0;
-          u1[k] = diag; u2[k] = sup; u3[k] = 0.0; pv[k] = 0.0; lm[k] = l;
+          l = diag != 0.0 ? ck / diag : 0.0;
+          u1 = diag; U2(k) = sup; U3(k) = 0.0; LM(k) = l;
           diag = nd - l * sup;
           sup = ns;
         } else {
-          const double l = diag / ck;
-          u1[k] = ck; u2[k] = nd; u3[k] = ns; pv[k] = 1.0; lm[k] = l;
+          l = diag / ck;
+          u1 = ck; U2(k) = nd; U3(k) = ns; LM(k) = -l - 4.0;
           diag = sup - l * nd;
           sup = -l * ns;
         }
+        if (fabs(u1) < tiny) u1 = u1 < 0.0 ? -tiny : tiny;
+        U1(k) = 1.0 / u1;
       }
-      u1[n - 1] = diag;
-      for (int k = 0; k < n; ++k)
-        if (fabs(u1[k]) < tiny) u1[k] = u1[k] < 0.0 ? -tiny : tiny;
-      double* y = Z + (int64_t)j * n;
-      for (int k = 0; k < n; ++k) y[k] = hash_unit((uint32_t)k, (uint32_t)(j * 7919 + s));
-      const int iters = (j > lead) ? 4 : 3;
+      {
+        double u1 = diag;
+        if (fabs(u1) < tiny) u1 = u1 < 0.0 ? -tiny : tiny;
+        U1(n - 1) = 1.0 / u1;
+      }
+      for (int k = 0; k < n; ++k) Y(k) = hash_unit((uint32_t)k, (uint32_t)(j * 7919 + s));
+      const int iters = (j > lead) ? 3 : 2;
       for (int it = 0; it < iters; ++it) {
-        // forward elimination
+        // forward elimination with the recorded interchanges
+        double yk = Y(0);
         for (int k = 0; k < n - 1; ++k) {
-          if (pv[k] != 0.0) {
-            const double tmp = y[k];
-            y[k] = y[k + 1];
-            y[k + 1] = tmp;
+          double yn = Y(k + 1);
+          const double lk = LM(k);
+          if (lk < -2.0) {
+            const double tmp = yk;
+            yk = yn;
+            yn = tmp - (-lk - 4.0) * yk;
+          } else {
+            yn -= lk * yk;
           }
-          y[k + 1] -= lm[k] * y[k];
+          Y(k) = yk;
+          yk = yn;
         }
+        Y(n - 1) = yk;
         // back substitution
-        y[n - 1] /= u1[n - 1];
-        if (n >= 2) y[n - 2] = (y[n - 2] - u2[n - 2] * y[n - 1]) / u1[n - 2];
-        for (int k = n - 3; k >= 0; --k) y[k] = (y[k] - u2[k] * y[k + 1] - u3[k] * y[k + 2]) / u1[k];
-        // orthogonalise against the earlier members of the cluster
-        for (int q = lead; q < j; ++q) {
-          const double* zq = Z + (int64_t)q * n;
-          double dot = 0.0;
-          for (int k = 0; k < n; ++k) dot += y[k] * zq[k];
-          for (int k = 0; k < n; ++k) y[k] -= dot * zq[k];
+        double y2 = 0.0, y1 = Y(n - 1) * U1(n - 1);
+        Y(n - 1) = y1;
+        if (n >= 2) {
+          const double y0 = (Y(n - 2) - U2(n - 2) * y1) * U1(n - 2);
+          Y(n - 2) = y0;
+          y2 = y1;
+          y1 = y0;
         }
-        double nrm = 0.0;
-        for (int k = 0; k < n; ++k) nrm += y[k] * y[k];
+        double nrm = y1 * y1 + (n >= 2 ? y2 * y2 : 0.0);
+        for (int k = n - 3; k >= 0; --k) {
+          const double y0 = (Y(k) - U2(k) * y1 - U3(k) * y2) * U1(k);
+          Y(k) = y0;
+          nrm += y0 * y0;
+          y2 = y1;
+          y1 = y0;
+        }
+        // orthogonalise against the earlier members of the cluster
+        if (j > lead) {
+          for (int q = lead; q < j; ++q) {
+            const double* zq = Z + (int64_t)q * n;
+            double dot = 0.0;
+            for (int k = 0; k < n; ++k) dot += Y(k) * zq[k];
+            for (int k = 0; k < n; ++k) Y(k) -= dot * zq[k];
+          }
+          nrm = 0.0;
+          for (int k = 0; k < n; ++k) nrm += Y(k) * Y(k);
+        }
         const double inv = 1.0 / sqrt(nrm);
-        for (int k = 0; k < n; ++k) y[k] *= inv;
+        for (int k = 0; k < n; ++k) Y(k) *= inv;
       }
-      // sign convention: largest component positive
+      // sign convention: largest component positive; publish row j of Z
       int kmax = 0;
       double amax = 0.0;
       for (int k = 0; k < n; ++k)
-        if (fabs(y[k]) > amax) { amax = fabs(y[k]); kmax = k; }
-      if (y[kmax] < 0.0)
-        for (int k = 0; k < n; ++k) y[k] = -y[k];
+        if (fabs(Y(k)) > amax) { amax = fabs(Y(k)); kmax = k; }
+      const double sgn = Y(kmax) < 0.0 ? -1.0 : 1.0;
+      double* y = Z + (int64_t)j * n;
+      for (int k = 0; k < n; ++k) y[k] = sgn * Y(k);
     }
   }
 }
@@ -454,16 +777,23 @@ __global__ void __launch_bounds__(128) k_inverse_iteration(EigArgs g) {
 // ---------------------------------------------------------------------------
 // Back-transform Z <- H_0 H_1 ... H_{n-3} Z (eigenvector-major rows of Z).
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(256) k_backtransform(EigArgs g) {
+// mcap > 0: the m formed eigenvectors are staged in shared memory (m <= mcap),
+// applied there and written back once; otherwise they are updated in place.
+__global__ void __launch_bounds__(256) k_backtransform(EigArgs g, const int32_t* list, int mcap) {
   extern __shared__ double sm[];
-  const int s = g.list[blockIdx.x];
+  const int s = list[blockIdx.x];
   const int n = g.nao[s];
   const int m = g.nvec[s];
   const double* a = g.A + g.mat_off[s];
   const double* tau = g.tau + g.ao_off[s];
-  double* Z = g.Z + g.mat_off[s];
+  double* gZ = g.Z + g.mat_off[s];
   double* v = sm;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nw = blockDim.x >> 5;
+  const bool staged = mcap > 0 && m <= mcap;
+  double* Z = staged ? sm + n + 8 : gZ;
+  if (staged) {
+    for (int64_t k = tid; k < (int64_t)m * n; k += blockDim.x) Z[k] = gZ[k];
+  }
   for (int i = n - 3; i >= 0; --i) {
     const double ti = tau[i];
     if (ti == 0.0) continue;
@@ -479,6 +809,121 @@ __global__ void __launch_bounds__(256) k_backtransform(EigArgs g) {
       for (int k = lane; k < L; k += 32) z[k] -= acc * v[k];
     }
   }
+  if (staged) {
+    __syncthreads();
+    for (int64_t k = tid; k < (int64_t)m * n; k += blockDim.x) gZ[k] = Z[k];
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Blocked back-transform (compact WY form, LAPACK larft/larfb order): the
+// reflectors H_i0 ... H_i0+31 of one block are I - V T V^T with T upper
+// triangular, so each block costs one pass over Z: Z <- Z - V (T (V^T Z)).
+// Blocks are applied from the last to the first.
+// ---------------------------------------------------------------------------
+constexpr int WB = 32;
+
+size_t backtransform_wy_bytes(int n, int m) {
+  return ((size_t)n * (WB + 1) + 2 * WB * (WB + 1) + (size_t)WB * m + 8) * sizeof(double);
+}
+
+__global__ void __launch_bounds__(256) k_backtransform_wy(EigArgs g, int wcap) {
+  extern __shared__ double sm[];
+  const int s = g.list[blockIdx.x];
+  const int n = g.nao[s];
+  const int m = g.nvec[s];
+  const double* a = g.A + g.mat_off[s];
+  const double* tau = g.tau + g.ao_off[s];
+  double* Z = g.Z + g.mat_off[s];
+  const int nr = n - 2;
+  if (nr <= 0 || m <= 0) return;
+  const int tid = threadIdx.x, bs = blockDim.x, lane = tid & 31, warp = tid >> 5, nw = bs >> 5;
+  constexpr int P = WB + 1;
+  double* V = sm;                       // n x P
+  double* T = V + (size_t)n * P;        // WB x P
+  double* G = T + WB * P;               // WB x P
+  double* W = G + WB * P;               // WB x m
+  const int nblk = (nr + WB - 1) / WB;
+  for (int b = nblk - 1; b >= 0; --b) {
+    const int i0 = b * WB;
+    const int k = min(WB, nr - i0);
+    const int L = n - i0 - 1;
+    for (int idx = tid; idx < L * WB; idx += bs) {
+      const int r = idx / WB, c = idx - (idx / WB) * WB;
+      double val = 0.0;
+      if (c < k) {
+        if (r == c) val = 1.0;
+        else if (r > c) val = a[(int64_t)(i0 + c) * n + i0 + 1 + r];
+      }
+      V[r * P + c] = val;
+    }
+    __syncthreads();
+    for (int idx = tid; idx < WB * WB; idx += bs) {
+      const int p = idx / WB, q = idx - (idx / WB) * WB;
+      if (p < q && q < k) {
+        double acc = 0.0;
+        for (int r = q; r < L; ++r) acc = fma(V[r * P + p], V[r * P + q], acc);
+        G[p * P + q] = acc;
+      }
+    }
+    __syncthreads();
+    if (warp == 0) {
+      for (int j = 0; j < WB; ++j) {
+        const double tj = j < k ? tau[i0 + j] : 0.0;
+        double t = 0.0;
+        if (lane < j && j < k) {
+          for (int q = lane; q < j; ++q) t = fma(T[lane * P + q], G[q * P + j], t);
+          t *= -tj;
+        }
+        if (lane == j) t = tj;
+        T[lane * P + j] = (lane <= j) ? t : 0.0;
+        __syncwarp();
+      }
+    }
+    __syncthreads();
+    // eigenvectors in chunks of at most wcap (the W buffer's capacity)
+    for (int j0 = 0; j0 < m; j0 += wcap) {
+    const int jc = min(wcap, m - j0);
+    // W = T (V^T Z_block): one warp per eigenvector, lane = reflector
+    for (int jj = warp; jj < jc; jj += nw) {
+      const int j = j0 + jj;
+      const double* z = Z + (int64_t)j * n + i0 + 1;
+      double acc = 0.0;
+      for (int r0 = 0; r0 < L; r0 += 32) {
+        const double zv = (r0 + lane < L) ? z[r0 + lane] : 0.0;
+        const int rmax = min(32, L - r0);
+        for (int rr = 0; rr < rmax; ++rr) {
+          const double zr = __shfl_sync(0xffffffffu, zv, rr);
+          const int r = r0 + rr;
+          if (lane < k && r >= lane) acc = fma(V[r * P + lane], zr, acc);
+        }
+      }
+      double w2 = 0.0;
+      for (int q = 0; q < WB; ++q) {
+        const double w1 = __shfl_sync(0xffffffffu, acc, q);
+        if (q >= lane) w2 = fma(T[lane * P + q], w1, w2);
+      }
+      W[lane * wcap + jj] = w2;
+    }
+    __syncthreads();
+    for (int64_t idx = tid; idx < (int64_t)jc * L; idx += bs) {
+      const int jj = (int)(idx / L), r = (int)(idx - (idx / L) * L);
+      const int amax = min(k, r + 1);
+      double acc = 0.0;
+      for (int q = 0; q < amax; ++q) acc = fma(V[r * P + q], W[q * wcap + jj], acc);
+      Z[(int64_t)(j0 + jj) * n + i0 + 1 + r] -= acc;
+    }
+    __syncthreads();
+    }
+  }
+}
+
+void launch_backtransform_wy(const EigArgs& g, int count, int max_n, int max_m, cudaStream_t stream) {
+  if (count == 0) return;
+  static const bool attr = cudaFuncSetAttribute(k_backtransform_wy, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                227 * 1024) == cudaSuccess;
+  (void)attr;
+  k_backtransform_wy<<<count, 256, backtransform_wy_bytes(max_n, max_m), stream>>>(g, max_m);
 }
 
 // Loewdin weights s^-1/2 with the overlap condition guard; failed systems are flagged.
@@ -507,22 +952,51 @@ void launch_tridiag(const EigArgs& g, int count, int max_n, cudaStream_t stream)
   k_tridiag<<<count, 512, sm, stream>>>(g);
 }
 
+int sm_count() {
+  static const int n = [] {
+    int dev = 0, v = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess ||
+        cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || v <= 0)
+      v = 148;
+    return v;
+  }();
+  return n;
+}
+
 void launch_eigvals(const EigArgs& g, int mode, double kt, int count, int max_n, cudaStream_t stream) {
   if (count == 0) return;
+  const int kNumSMs = sm_count();
   const size_t sm = (5 * (size_t)max_n + 40) * sizeof(double);
   static const bool attr = cudaFuncSetAttribute(k_tridiag_eigvals, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024) == cudaSuccess;
   (void)attr;
-  k_tridiag_eigvals<<<count, 256, sm, stream>>>(g, mode, kt);
+  // Enough systems to fill the GPU: one CTA each, one thread per eigenvalue
+  // (fewest Sturm sequences in total).  Few systems: spread each system's
+  // eigenvalues over several CTAs, up to a warp per eigenvalue (fewest rounds).
+  if (count >= kNumSMs) {
+    k_tridiag_eigvals<<<count, 256, sm, stream>>>(g, mode, kt, 0, 1);
+    return;
+  }
+  const int need = mode == 0 ? max_n / 2 + 16 : max_n;
+  const int parts = std::max(1, std::min((need + 7) / 8, 2 * kNumSMs / count));
+  const size_t smp = (2 * (size_t)max_n + 40) * sizeof(double);
+  k_eigvals_part<<<dim3(parts, count), 256, smp, stream>>>(g, mode, parts);
+  k_tridiag_eigvals<<<count, 256, sm, stream>>>(g, mode, kt, 1, 8);
 }
 
-void launch_inverse_iteration(const EigArgs& g, int count, cudaStream_t stream) {
+void launch_inverse_iteration(const EigArgs& g, int count, double ortol_rel, cudaStream_t stream) {
   if (count == 0) return;
-  k_inverse_iteration<<<count, 128, 0, stream>>>(g);
+  k_inverse_iteration<<<count, 128, 0, stream>>>(g, ortol_rel);
 }
 
-void launch_backtransform(const EigArgs& g, int count, int max_n, cudaStream_t stream) {
+void launch_backtransform(const EigArgs& g, const int32_t* list, int count, int max_n, int mcap,
+                          cudaStream_t stream) {
   if (count == 0) return;
-  k_backtransform<<<count, 256, ((size_t)max_n + 8) * sizeof(double), stream>>>(g);
+  static const bool attr = cudaFuncSetAttribute(k_backtransform, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                227 * 1024) == cudaSuccess;
+  (void)attr;
+  size_t bytes = ((size_t)max_n + 8) * sizeof(double);
+  if (mcap > 0) bytes += (size_t)mcap * max_n * sizeof(double);
+  k_backtransform<<<count, 256, bytes, stream>>>(g, list, mcap);
 }
 
 void launch_lowdin_weights(const EigArgs& g, int32_t* status, int count, cudaStream_t stream) {
