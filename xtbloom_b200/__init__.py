@@ -3,8 +3,8 @@
 The compute path is the in-tree CUDA library ``libxtbloom_b200.so`` behind the
 versioned caller-buffer C ABI declared in ``include/xtbloom.h``.  This package
 is the Python host side: a ctypes binding (``abi``), a ``Calculator`` /
-``BatchCalculator`` mirroring the reference's Python interface, seeded
-synthetic workloads, and an optional torch autograd wrapper.
+``BatchCalculator`` mirroring the reference's Python interface, and seeded
+synthetic workloads.
 """
 from __future__ import annotations
 
