@@ -336,6 +336,28 @@ XTBLOOM_API xtbloom_status_t xtbloom_b200_debug_fetch(xtbloom_context_t* context
                                                       int64_t system, double* out,
                                                       size_t capacity, size_t* count);
 
+/*
+ * Allocation-free eigenvectors of one symmetric tridiagonal matrix (no
+ * counterpart in the reference ABI).  For callers that may not allocate device
+ * memory once set up: cudaMalloc/cudaFree can synchronise the device and fail
+ * under a committed memory budget.  Inverse iteration for eigenvectors
+ * 0..m-1 of T = tridiag(offdiagonal[n-1], diagonal[n], offdiagonal[n-1]) with
+ * ascending eigenvalues[m]; vector j goes to vectors[j*n .. j*n+n), largest
+ * component positive.  All pointers are CUDA device memory of the current
+ * device (offdiagonal may be NULL when n == 1); the work is enqueued on
+ * cuda_stream (a cudaStream_t, NULL for the default stream) and the call
+ * returns without waiting.  cluster_tolerance (0 selects 2e-7) is relative to
+ * ||T||_1: eigenvalues closer than that are re-orthogonalised together.
+ * Work vectors live in a fixed 1.25 MiB array of the library's device memory,
+ * so n is limited to 256 (INVALID_ARGUMENT beyond, before anything runs);
+ * nothing in it has to start at zero.  Calls that overlap on one device race
+ * on that array: serialise them.  The first call on each device looks the
+ * array up (and may load the module): make it before any stream capture.
+ */
+XTBLOOM_API xtbloom_status_t xtbloom_b200_tridiag_eigenvectors_static(
+    const double* diagonal, const double* offdiagonal, const double* eigenvalues, int32_t n,
+    int32_t m, double* vectors, double cluster_tolerance, void* cuda_stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -16,6 +16,7 @@
 #include <cuda_runtime.h>
 
 #include "engine.h"
+#include "static_eigvec.h"
 #include "xtbloom.h"
 
 namespace {
@@ -630,6 +631,27 @@ xtbloom_status_t xtbloom_b200_debug_fetch(xtbloom_context_t* context, const char
   const xtbloom_status_t st = context->engine->debug_fetch(name, system, out, capacity, count, err);
   if (st != XTBLOOM_STATUS_SUCCESS) return fail(st, err);
   return st;
+}
+
+xtbloom_status_t xtbloom_b200_tridiag_eigenvectors_static(const double* diagonal,
+                                                          const double* offdiagonal,
+                                                          const double* eigenvalues, int32_t n,
+                                                          int32_t m, double* vectors,
+                                                          double cluster_tolerance,
+                                                          void* cuda_stream) {
+  if (diagonal == nullptr || eigenvalues == nullptr || vectors == nullptr ||
+      (offdiagonal == nullptr && n > 1))
+    return fail(XTBLOOM_STATUS_INVALID_ARGUMENT, "NULL argument");
+  if (!(cluster_tolerance >= 0.0) || !std::isfinite(cluster_tolerance))
+    return fail(XTBLOOM_STATUS_INVALID_ARGUMENT, "cluster_tolerance must be finite and >= 0");
+  std::string err;
+  const int rc = xtb::static_eigvec_run(diagonal, offdiagonal, eigenvalues, n, m, vectors,
+                                        cluster_tolerance > 0.0 ? cluster_tolerance : 2e-7,
+                                        static_cast<cudaStream_t>(cuda_stream), err);
+  if (rc == 1) return fail(XTBLOOM_STATUS_INVALID_ARGUMENT, err);
+  if (rc == 2) return fail(XTBLOOM_STATUS_BACKEND_UNAVAILABLE, err);
+  if (rc != 0) return fail(XTBLOOM_STATUS_INTERNAL_ERROR, err);
+  return XTBLOOM_STATUS_SUCCESS;
 }
 
 }  // extern "C"

@@ -1,0 +1,155 @@
+// Inverse iteration for eigenvectors of a symmetric tridiagonal matrix: the
+// block-wide routine shared by the batched SCC kernel and the single-matrix
+// static-scratch entry point.
+#pragma once
+
+#include <cfloat>
+#include <cstdint>
+
+namespace xtb {
+
+// ---------------------------------------------------------------------------
+// Inverse iteration for eigenvectors 0..nvec-1 of the tridiagonal matrix.
+// One thread per eigenvalue cluster; output ZT[j][0..n) (eigenvector-major).
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ double hash_unit(uint32_t a, uint32_t b) {
+  uint32_t h = a * 0x9E3779B1u ^ (b + 0x7F4A7C15u + (a << 6) + (a >> 2));
+  h ^= h >> 16; h *= 0x85EBCA6Bu; h ^= h >> 13; h *= 0xC2B2AE35u; h ^= h >> 16;
+  return (double)h * (2.0 / 4294967296.0) - 1.0;
+}
+
+// ortol_rel: eigenvalues closer than ortol_rel * ||T||_1 form a cluster whose
+// vectors are re-orthogonalised.  Outside clusters inverse-iteration vectors
+// are orthogonal to ~eps ||T|| / gap, i.e. better than 1e-9 for the
+// thresholds used (2e-7 for Hamiltonians, 2e-6 for overlap matrices).
+//
+// Block-wide (128 threads): eigenvectors 0..m-1 of the n x n tridiagonal
+// (d, e) for the ascending eigenvalues ev, written as rows Z[j*n .. j*n+n).
+// scratch holds 5 n 128 doubles: per-thread work vectors interleaved across
+// the CTA's threads (element k of array a for thread t at ((a*n + k) * 128 + t))
+// so that every sequential sweep over k is a coalesced warp access.  Every
+// scratch element is written before it is read.  seed varies the start vectors.
+__device__ __forceinline__ void inverse_iteration_block(const double* d, const double* e,
+                                                        const double* ev, int n, int m, double* Z,
+                                                        double* scratch, double ortol_rel,
+                                                        uint32_t seed) {
+  double* scr = scratch + threadIdx.x;
+  const int64_t ld = 128;
+  auto U1 = [&](int k) -> double& { return scr[((int64_t)0 * n + k) * ld]; };
+  auto U2 = [&](int k) -> double& { return scr[((int64_t)1 * n + k) * ld]; };
+  auto U3 = [&](int k) -> double& { return scr[((int64_t)2 * n + k) * ld]; };
+  auto LM = [&](int k) -> double& { return scr[((int64_t)3 * n + k) * ld]; };
+  auto Y = [&](int k) -> double& { return scr[((int64_t)4 * n + k) * ld]; };
+  // one-norm of T and the cluster threshold
+  __shared__ double s_onenrm;
+  if (threadIdx.x == 0) {
+    double nm = 0.0;
+    for (int k = 0; k < n; ++k) {
+      const double c = fabs(d[k]) + (k > 0 ? fabs(e[k - 1]) : 0.0) + (k < n - 1 ? fabs(e[k]) : 0.0);
+      nm = fmax(nm, c);
+    }
+    s_onenrm = fmax(nm, DBL_MIN);
+  }
+  __syncthreads();
+  const double onenrm = s_onenrm;
+  const double ortol = ortol_rel * onenrm;
+  const double tiny = DBL_EPSILON * onenrm;
+  for (int lead = threadIdx.x; lead < m; lead += blockDim.x) {
+    if (lead > 0 && ev[lead] - ev[lead - 1] <= ortol) continue;   // not a cluster leader
+    double xprev = -DBL_MAX;
+    for (int j = lead; j < m; ++j) {
+      if (j > lead && ev[j] - ev[j - 1] > ortol) break;
+      double x = ev[j];
+      if (j > lead && x - xprev < 10.0 * DBL_EPSILON * fabs(x)) x = xprev + 10.0 * DBL_EPSILON * fabs(x);
+      xprev = x;
+      // LU with partial pivoting of T - xI; U1 holds reciprocal pivots and the
+      // sign of LM encodes the row interchange (pivoted rows store -l - 4; both |l| <= 1).
+      double diag = d[0] - x, sup = n > 1 ? e[0] : 0.0;
+      for (int k = 0; k < n - 1; ++k) {
+        const double ck = e[k];
+        const double nd = d[k + 1] - x;
+        const double ns = (k + 1 < n - 1) ? e[k + 1] : 0.0;
+        double u1, l;
+        if (fabs(diag) >= fabs(ck)) {
+          l = diag != 0.0 ? ck / diag : 0.0;
+          u1 = diag; U2(k) = sup; U3(k) = 0.0; LM(k) = l;
+          diag = nd - l * sup;
+          sup = ns;
+        } else {
+          l = diag / ck;
+          u1 = ck; U2(k) = nd; U3(k) = ns; LM(k) = -l - 4.0;
+          diag = sup - l * nd;
+          sup = -l * ns;
+        }
+        if (fabs(u1) < tiny) u1 = u1 < 0.0 ? -tiny : tiny;
+        U1(k) = 1.0 / u1;
+      }
+      {
+        double u1 = diag;
+        if (fabs(u1) < tiny) u1 = u1 < 0.0 ? -tiny : tiny;
+        U1(n - 1) = 1.0 / u1;
+      }
+      for (int k = 0; k < n; ++k) Y(k) = hash_unit((uint32_t)k, (uint32_t)j * 7919u + seed);
+      const int iters = (j > lead) ? 3 : 2;
+      for (int it = 0; it < iters; ++it) {
+        // forward elimination with the recorded interchanges
+        double yk = Y(0);
+        for (int k = 0; k < n - 1; ++k) {
+          double yn = Y(k + 1);
+          const double lk = LM(k);
+          if (lk < -2.0) {
+            const double tmp = yk;
+            yk = yn;
+            yn = tmp - (-lk - 4.0) * yk;
+          } else {
+            yn -= lk * yk;
+          }
+          Y(k) = yk;
+          yk = yn;
+        }
+        Y(n - 1) = yk;
+        // back substitution
+        double y2 = 0.0, y1 = Y(n - 1) * U1(n - 1);
+        Y(n - 1) = y1;
+        if (n >= 2) {
+          const double y0 = (Y(n - 2) - U2(n - 2) * y1) * U1(n - 2);
+          Y(n - 2) = y0;
+          y2 = y1;
+          y1 = y0;
+        }
+        double nrm = y1 * y1 + (n >= 2 ? y2 * y2 : 0.0);
+        for (int k = n - 3; k >= 0; --k) {
+          const double y0 = (Y(k) - U2(k) * y1 - U3(k) * y2) * U1(k);
+          Y(k) = y0;
+          nrm += y0 * y0;
+          y2 = y1;
+          y1 = y0;
+        }
+        // orthogonalise against the earlier members of the cluster
+        if (j > lead) {
+          for (int q = lead; q < j; ++q) {
+            const double* zq = Z + (int64_t)q * n;
+            double dot = 0.0;
+            for (int k = 0; k < n; ++k) dot += Y(k) * zq[k];
+            for (int k = 0; k < n; ++k) Y(k) -= dot * zq[k];
+          }
+          nrm = 0.0;
+          for (int k = 0; k < n; ++k) nrm += Y(k) * Y(k);
+        }
+        const double inv = 1.0 / sqrt(nrm);
+        for (int k = 0; k < n; ++k) Y(k) *= inv;
+      }
+      // sign convention: largest component positive; publish row j of Z
+      int kmax = 0;
+      double amax = 0.0;
+      for (int k = 0; k < n; ++k)
+        if (fabs(Y(k)) > amax) { amax = fabs(Y(k)); kmax = k; }
+      const double sgn = Y(kmax) < 0.0 ? -1.0 : 1.0;
+      double* y = Z + (int64_t)j * n;
+      for (int k = 0; k < n; ++k) y[k] = sgn * Y(k);
+    }
+  }
+}
+
+
+}  // namespace xtb
