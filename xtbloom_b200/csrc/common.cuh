@@ -17,6 +17,20 @@
 
 namespace xtb {
 
+// Lets `func` use as much dynamic shared memory as the device allows beside
+// its static shared memory; returns that limit in bytes.
+template <class F>
+inline size_t allow_max_dynamic_smem(F func) {
+  int dev = 0, optin = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+  cudaFuncAttributes fa{};
+  cudaFuncGetAttributes(&fa, func);
+  const size_t cap = (size_t)optin > fa.sharedSizeBytes ? (size_t)optin - fa.sharedSizeBytes : 0;
+  cudaFuncSetAttribute(func, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)cap);
+  return cap;
+}
+
 constexpr int kMaxD4Refs = 7;
 constexpr double kPi = 3.141592653589793238462643383279502884;
 constexpr double kSqrtPi3 = 5.5683279968317061;   // pi^(3/2)

@@ -650,12 +650,17 @@ xtbloom_status_t Engine::compute(const ComputeRequest& req, std::string& error) 
   cudaMemsetAsync(m.terms.p, 0, 8 * B * 8, s);
   cudaMemcpyAsync(list, order, B * 4, cudaMemcpyDeviceToDevice, s);
 
-#define XTB_STAGE(id, nk, ...)        \
-  do {                                \
-    m.prof.begin(id, s);              \
-    __VA_ARGS__;                      \
-    m.prof.end(s);                    \
-    m.prof.launches += (nk);          \
+  // first launch failure of any stage (a launch that fails does not run and
+  // leaves its outputs unwritten, so the call must fail)
+  cudaError_t launch_error = cudaSuccess;
+#define XTB_STAGE(id, nk, ...)                                                     \
+  do {                                                                             \
+    m.prof.begin(id, s);                                                           \
+    __VA_ARGS__;                                                                   \
+    m.prof.end(s);                                                                 \
+    m.prof.launches += (nk);                                                       \
+    if (const cudaError_t le_ = cudaGetLastError(); le_ != cudaSuccess && !launch_error) \
+      launch_error = le_;                                                          \
   } while (0)
   // ---- geometry setup ----
   XTB_STAGE(kStSetup, 3,
@@ -755,20 +760,21 @@ xtbloom_status_t Engine::compute(const ComputeRequest& req, std::string& error) 
     };
     XTB_STAGE(stage_base == kStLowdin ? kStLowdin : kStTridiag, (int)bks.size(), for (const Bucket& bk : bks) {
       const EigArgs gb = sub(bk);
-      if (bk.max_n <= 230) launch_tridiag_smem(gb, gb.list, bk.count, bk.max_n, s);
-      else launch_tridiag(gb, bk.count, bk.max_n, s);
+      launch_tridiag_smem(gb, gb.list, bk.count, bk.max_n, s);
     });
     XTB_STAGE(stage_base == kStLowdin ? kStLowdin : kStEigvals, (int)bks.size(),
               for (const Bucket& bk : bks) launch_eigvals(sub(bk), mode, kt, bk.count, bk.max_n, s));
     XTB_STAGE(stage_base == kStLowdin ? kStLowdin : kStInvIter, (int)bks.size(),
-              for (const Bucket& bk : bks) launch_inverse_iteration(sub(bk), bk.count, ortol_rel, s));
+              for (const Bucket& bk : bks) launch_inverse_iteration(
+                  sub(bk), bk.count, bk.max_n, mode == 1 ? bk.max_n : std::min(bk.max_m + 4, bk.max_n),
+                  ortol_rel, s));
     XTB_STAGE(stage_base == kStLowdin ? kStLowdin : kStBacktransform, (int)bks.size(), for (const Bucket& bk : bks) {
       const EigArgs gb = sub(bk);
       const int want = mode == 1 ? bk.max_n : std::min(bk.max_m, bk.max_n);
       const long budget = 220L * 1024 / 8 - (long)bk.max_n * 33 - 2 * 32 * 33 - 8;
       const int wcap = (int)std::min<long>(want, budget / 32);
       if (wcap >= 8) {
-        launch_backtransform_wy(gb, bk.count, bk.max_n, wcap, s);
+        launch_backtransform_wy(gb, bk.count, bk.max_n, wcap, want, s);
       } else {
         launch_backtransform(gb, gb.list, bk.count, bk.max_n, 0, s);
       }
@@ -868,6 +874,7 @@ xtbloom_status_t Engine::compute(const ComputeRequest& req, std::string& error) 
                    std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t_start).count());
     }
     count = m.h_count[0];
+    if (launch_error) break;
   }
   k_finalize_status<<<(nsys + 255) / 256, 256, 0, s>>>(nsys, status, a.converged);
   m.prof.launches += 1;
@@ -921,6 +928,12 @@ xtbloom_status_t Engine::compute(const ComputeRequest& req, std::string& error) 
                                            m.qsh.as<double>(), m.out_energy.as<double>(),
                                            m.out_forces.as<double>(), m.out_charges.as<double>()));
 #undef XTB_STAGE
+  if (launch_error == cudaSuccess) launch_error = cudaGetLastError();
+  if (launch_error != cudaSuccess) {
+    cudaStreamSynchronize(s);
+    error = std::string("kernel launch failed: ") + cudaGetErrorString(launch_error);
+    return XTBLOOM_STATUS_INTERNAL_ERROR;
+  }
   // ---- copy into caller buffers ----
   const xtbloom_batch_result_t& r = *req.result;
   auto put = [&](const xtbloom_buffer_t& dst, const void* src, size_t bytes) {

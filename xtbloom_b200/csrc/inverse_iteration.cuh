@@ -23,18 +23,21 @@ __device__ __forceinline__ double hash_unit(uint32_t a, uint32_t b) {
 // are orthogonal to ~eps ||T|| / gap, i.e. better than 1e-9 for the
 // thresholds used (2e-7 for Hamiltonians, 2e-6 for overlap matrices).
 //
-// Block-wide (128 threads): eigenvectors 0..m-1 of the n x n tridiagonal
-// (d, e) for the ascending eigenvalues ev, written as rows Z[j*n .. j*n+n).
-// scratch holds 5 n 128 doubles: per-thread work vectors interleaved across
-// the CTA's threads (element k of array a for thread t at ((a*n + k) * 128 + t))
-// so that every sequential sweep over k is a coalesced warp access.  Every
-// scratch element is written before it is read.  seed varies the start vectors.
+// Block-wide: eigenvectors of the n x n tridiagonal (d, e) for the ascending
+// eigenvalues ev[0..m), written as rows Z[j*n .. j*n+n).  Thread t of the
+// block leads the clusters starting at lead0 + t, lead0 + t + lead_step, ...
+// scratch holds 5 n LD doubles: per-thread work vectors interleaved across
+// the CTA's LD thread slots (element k of array a for thread t at
+// ((a*n + k) * LD + t)) so that every sequential sweep over k is a coalesced
+// access.  Every scratch element is written before it is read.  seed varies
+// the start vectors.
+template <int LD>
 __device__ __forceinline__ void inverse_iteration_block(const double* d, const double* e,
                                                         const double* ev, int n, int m, double* Z,
                                                         double* scratch, double ortol_rel,
-                                                        uint32_t seed) {
+                                                        uint32_t seed, int lead0, int lead_step) {
   double* scr = scratch + threadIdx.x;
-  const int64_t ld = 128;
+  constexpr int64_t ld = LD;
   auto U1 = [&](int k) -> double& { return scr[((int64_t)0 * n + k) * ld]; };
   auto U2 = [&](int k) -> double& { return scr[((int64_t)1 * n + k) * ld]; };
   auto U3 = [&](int k) -> double& { return scr[((int64_t)2 * n + k) * ld]; };
@@ -54,7 +57,7 @@ __device__ __forceinline__ void inverse_iteration_block(const double* d, const d
   const double onenrm = s_onenrm;
   const double ortol = ortol_rel * onenrm;
   const double tiny = DBL_EPSILON * onenrm;
-  for (int lead = threadIdx.x; lead < m; lead += blockDim.x) {
+  for (int lead = lead0 + threadIdx.x; lead < m; lead += lead_step) {
     if (lead > 0 && ev[lead] - ev[lead - 1] <= ortol) continue;   // not a cluster leader
     double xprev = -DBL_MAX;
     for (int j = lead; j < m; ++j) {

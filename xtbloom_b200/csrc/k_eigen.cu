@@ -114,10 +114,15 @@ void launch_gemm(const GemmArgs& g, bool transA, bool weighted, int max_tiles, i
 // Reflector i (v[0] = 1 at row i+1, v[k] stored in A[i][i+1+k], k >= 1) and
 // tau_i; d, e receive the tridiagonal.
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(512) k_tridiag(EigArgs g) {
+// nloc > 0: only the first n - nloc columns are reduced here (systems with
+// n <= nloc return at once); the shared-memory kernel finishes the trailing
+// nloc x nloc block, which this kernel has updated in place.
+__global__ void __launch_bounds__(512) k_tridiag(EigArgs g, int nloc) {
   extern __shared__ double sm[];
   const int s = g.list[blockIdx.x];
   const int n = g.nao[s];
+  const int i_end = nloc > 0 ? n - nloc : n - 2;
+  if (i_end <= 0 && nloc > 0) return;
   double* a = g.A + g.mat_off[s];
   double* d = g.d + g.ao_off[s];
   double* e = g.e + g.ao_off[s];
@@ -127,7 +132,7 @@ __global__ void __launch_bounds__(512) k_tridiag(EigArgs g) {
   double* red = sm + 2 * n;
   const int tid = threadIdx.x, bs = blockDim.x;
   const int lane = tid & 31, warp = tid >> 5, nw = bs >> 5;
-  for (int i = 0; i + 2 < n; ++i) {
+  for (int i = 0; i < i_end && i + 2 < n; ++i) {
     const int m = n - i - 1;
     double* row = a + (int64_t)i * n + (i + 1);
     double part = 0.0;
@@ -182,6 +187,7 @@ __global__ void __launch_bounds__(512) k_tridiag(EigArgs g) {
     }
     __syncthreads();
   }
+  if (nloc > 0) return;
   if (tid == 0) {
     if (n >= 2) {
       d[n - 2] = a[(int64_t)(n - 2) * n + (n - 2)];
@@ -195,123 +201,216 @@ __global__ void __launch_bounds__(512) k_tridiag(EigArgs g) {
 }
 
 // ---------------------------------------------------------------------------
-// Shared-memory variant: the symmetric matrix lives in packed lower storage
-// (element (r, c), r >= c, at r(r+1)/2 + c) inside one CTA's shared memory, so
-// every Householder step touches only on-chip data.  The symmetric matvec uses
-// per-warp private accumulators for the transposed half (no atomics).  The
-// reflectors are written to the global matrix in the layout k_backtransform
-// reads.  Requires n(n+1)/2 + (2 + nwarps) n + 40 doubles of shared memory.
+// Shared-memory Householder tridiagonalisation.  The trailing nl x nl block
+// (rows/columns i0..n-1, i0 = max(0, n - nloc)) lives in packed lower storage
+// (local element (r, c), r >= c, at r(r+1)/2 + c) in one CTA's shared memory.
+// Step i applies reflector i's rank-2 update and forms the product of the next
+// reflector with the updated block in the same pass over the packed triangle:
+//   (A) update the block's first column with (v_i, w_i); it gives x_{i+1};
+//   (B) v_{i+1}, tau_{i+1} from x_{i+1};
+//   (C) 32 x 32 tiles of the rest, dealt round-robin to the warps: update with
+//       (v_i, w_i), then accumulate A v_{i+1} (see fused_tile);
+//   (D) w_{i+1} = tau p - (tau/2)(p.v) v.
+// Reflectors are stored in the global matrix in the layout the back-transform
+// reads (row i, columns i+2..): the same as the global-memory kernel.
 // ---------------------------------------------------------------------------
-__device__ __forceinline__ int64_t pk(int r, int c) { return (int64_t)r * (r + 1) / 2 + c; }
+__device__ __forceinline__ int pk32(int r, int c) { return r * (r + 1) / 2 + c; }
 
-__global__ void __launch_bounds__(256) k_tridiag_smem(EigArgs g, const int32_t* list) {
+// One tile (rows R0.., columns C0.., R0 >= C0, local to the block that starts
+// at row/column o of the packed triangle, size m) for one warp: update every
+// element with (vi, wi), then lane j accumulates the transposed part of A vn
+// for column C0+j directly and keeps 32 row partials, which a butterfly
+// reduce-scatter (31 exchanges) leaves with lane i holding row R0+i.  Diagonal
+// tiles use their lower triangle once.  Results go to the warp's pw.
+__device__ __forceinline__ void fused_tile(double* L, int o, int m, int R0, int C0,
+                                           const double* vi, const double* wi, const double* vn,
+                                           double* pw, int lane, bool want_mv) {
+  const int cj = C0 + lane;
+  const bool cok = cj < m;
+  const double vn_c = cok ? vn[cj] : 0.0;
+  const double vi_c = cok ? vi[cj] : 0.0;
+  const double wi_c = cok ? wi[cj] : 0.0;
+  const bool diag = R0 == C0;
+  double rp[32];
+  double col = 0.0;
+  int base = pk32(o + R0, o);
+#pragma unroll
+  for (int i = 0; i < 32; ++i) {
+    const int r = R0 + i;
+    const bool ok = r < m && cok && (!diag || lane <= i);
+    double a = 0.0;
+    const double vr = r < m ? vi[r] : 0.0, wr = r < m ? wi[r] : 0.0, nr = r < m ? vn[r] : 0.0;
+    if (ok) {
+      a = L[base + cj];
+      a -= vr * wi_c + wr * vi_c;
+      L[base + cj] = a;
+    }
+    rp[i] = a * vn_c;
+    if (!diag || lane < i) col = fma(a, nr, col);
+    base += o + r + 1;
+  }
+  if (!want_mv) return;
+#pragma unroll
+  for (int sh = 16; sh >= 1; sh >>= 1) {
+    const bool up = (lane & sh) != 0;
+#pragma unroll
+    for (int k = 0; k < sh; ++k) {
+      const double send = up ? rp[k] : rp[k + sh];
+      const double keep = up ? rp[k + sh] : rp[k];
+      rp[k] = keep + __shfl_xor_sync(0xffffffffu, send, sh);
+    }
+  }
+  if (R0 + lane < m) pw[R0 + lane] += rp[0];
+  if (cok) pw[cj] += col;
+}
+
+template <int NT>
+__global__ void __launch_bounds__(NT) k_tridiag_smem(EigArgs g, const int32_t* list, int nloc) {
   extern __shared__ double sm[];
+  constexpr int nw = NT / 32;
   const int s = list[blockIdx.x];
   const int n = g.nao[s];
+  const int i0 = n > nloc ? n - nloc : 0;
+  const int nl = n - i0;
   double* ga = g.A + g.mat_off[s];
-  double* d = g.d + g.ao_off[s];
-  double* e = g.e + g.ao_off[s];
-  double* tau = g.tau + g.ao_off[s];
-  const int tid = threadIdx.x, bs = blockDim.x;
-  const int lane = tid & 31, warp = tid >> 5, nw = bs >> 5;
+  double* d = g.d + g.ao_off[s] + i0;
+  double* e = g.e + g.ao_off[s] + i0;
+  double* tau = g.tau + g.ao_off[s] + i0;
+  const int tid = threadIdx.x;
+  const int lane = tid & 31, warp = tid >> 5;
   double* L = sm;
-  double* v = L + pk(n, 0);
-  double* p = v + n;
-  double* priv = p + n;          // nw x n
-  double* red = priv + (int64_t)nw * n;
-  // load the lower triangle
-  for (int r = warp; r < n; r += nw)
-    for (int c = lane; c <= r; c += 32) L[pk(r, c)] = ga[(int64_t)r * n + c];
-  for (int k = tid; k < nw * n; k += bs) priv[k] = 0.0;
+  double* vb0 = L + pk32(nl, 0);
+  double* vb1 = vb0 + nl;
+  double* wb0 = vb1 + nl;
+  double* wb1 = wb0 + nl;
+  double* priv = wb1 + nl;            // nw x nl
+  double* red = priv + nw * nl;       // 33
+  __shared__ double s_alpha;
+  for (int r = warp; r < nl; r += nw)
+    for (int c = lane; c <= r; c += 32) L[pk32(r, c)] = ga[(int64_t)(i0 + r) * n + i0 + c];
+  for (int k = tid; k < nw * nl; k += NT) priv[k] = 0.0;
+  for (int k = tid; k < nl; k += NT) vb0[k] = wb0[k] = vb1[k] = wb1[k] = 0.0;
   __syncthreads();
-  for (int i = 0; i + 2 < n; ++i) {
-    const int m = n - i - 1;
-    const int o = i + 1;                       // first row/col of the trailing block
+  if (nl == 1) {
+    if (tid == 0) { d[0] = L[0]; e[0] = 0.0; tau[0] = 0.0; }
+    return;
+  }
+  int cur = 0;
+  // Step i = -1 applies no update; its column gives reflector 0 of the block.
+  for (int i = -1; i + 2 < nl; ++i) {
+    const int o = i + 1, m = nl - o;
+    const double* vi = cur ? vb1 : vb0;
+    const double* wi = cur ? wb1 : wb0;
+    double* vn = cur ? vb0 : vb1;
+    double* wn = cur ? wb0 : wb1;
+    const bool next = o + 3 <= nl;      // reflector o exists
+    // (A)
     double part = 0.0;
-    for (int k = tid; k < m; k += bs) {
-      const double x = L[pk(o + k, i)];
-      v[k] = x;
-      if (k >= 1) part += x * x;
+    const double vi0 = vi[0], wi0 = wi[0];
+    for (int r = tid; r < m; r += NT) {
+      const int idx = pk32(o + r, o);
+      const double c = L[idx] - (vi[r] * wi0 + wi[r] * vi0);
+      L[idx] = c;
+      if (r == 0) d[o] = c;
+      if (r >= 1) vn[r - 1] = c;
+      if (r == 1) s_alpha = c;
+      if (r >= 2) part += c * c;
     }
     const double xn2 = block_sum(part, red);
-    const double alpha = v[0];
-    double ti = 0.0, beta = alpha;
-    if (xn2 > 0.0) {
-      beta = -copysign(sqrt(alpha * alpha + xn2), alpha);
-      ti = (beta - alpha) / beta;
-      const double sc = 1.0 / (alpha - beta);
-      for (int k = tid; k < m; k += bs) {
-        if (k >= 1) {
-          const double vk = v[k] * sc;
-          v[k] = vk;
-          ga[(int64_t)i * n + o + k] = vk;
+    // (B)
+    double ti = 0.0;
+    if (next) {
+      const double alpha = s_alpha;
+      double beta = alpha;
+      if (xn2 > 0.0) {
+        beta = -copysign(sqrt(alpha * alpha + xn2), alpha);
+        ti = (beta - alpha) / beta;
+        const double sc = 1.0 / (alpha - beta);
+        for (int k = tid + 1; k < m - 1; k += NT) {
+          const double vk = vn[k] * sc;
+          vn[k] = vk;
+          ga[(int64_t)(i0 + o) * n + i0 + o + 1 + k] = vk;
         }
+      } else {
+        for (int k = tid + 1; k < m - 1; k += NT) vn[k] = 0.0;
+      }
+      if (tid == 0) {
+        vn[0] = 1.0;
+        e[o] = beta;
+        tau[o] = ti;
+      }
+    } else {
+      for (int k = tid; k < m; k += NT) vn[k] = 0.0;
+    }
+    __syncthreads();
+    // (C)
+    const int m1 = m - 1;
+    {
+      const int nt = (m1 + 31) >> 5;
+      const int ntiles = nt * (nt + 1) / 2;
+      double* pw = priv + warp * nl;
+      const bool mv = next && ti != 0.0;
+      for (int tl = warp; tl < ntiles; tl += nw) {
+        int R = (int)((sqrt(8.0 * tl + 1.0) - 1.0) * 0.5);   // tile row: R(R+1)/2 <= tl
+        while ((R + 1) * (R + 2) / 2 <= tl) ++R;
+        while (R * (R + 1) / 2 > tl) --R;
+        const int C = tl - R * (R + 1) / 2;
+        fused_tile(L, o + 1, m1, R << 5, C << 5, vi + 1, wi + 1, vn, pw, lane, mv);
       }
     }
     __syncthreads();
-    if (tid == 0) {
-      v[0] = 1.0;
-      d[i] = L[pk(i, i)];
-      e[i] = beta;
-      tau[i] = ti;
-    }
-    __syncthreads();
-    if (ti == 0.0) continue;
-    // p = tau * A22 v with A22 symmetric, stored lower
-    for (int r = warp; r < m; r += nw) {
-      const double* row = L + pk(o + r, o);
-      const double vr = v[r];
-      double acc = 0.0;
-      for (int c = lane; c <= r; c += 32) {
-        const double a = row[c];
-        acc = fma(a, v[c], acc);
-        if (c < r) priv[warp * n + c] = fma(a, vr, priv[warp * n + c]);
-      }
-      acc = warp_sum(acc);
-      if (lane == 0) p[r] = acc;
-    }
-    __syncthreads();
+    if (!next) break;
+    // (D)
     double pv = 0.0;
-    for (int k = tid; k < m; k += bs) {
-      double t = p[k];
+    for (int k = tid; k < m1; k += NT) {
+      double t = 0.0;
+#pragma unroll
       for (int w = 0; w < nw; ++w) {
-        t += priv[w * n + k];
-        priv[w * n + k] = 0.0;
+        t += priv[w * nl + k];
+        priv[w * nl + k] = 0.0;
       }
       t *= ti;
-      p[k] = t;
-      pv += t * v[k];
+      wn[k] = t;
+      pv += t * vn[k];
     }
     const double K = 0.5 * ti * block_sum(pv, red);
-    for (int k = tid; k < m; k += bs) p[k] -= K * v[k];
+    for (int k = tid; k < m1; k += NT) wn[k] -= K * vn[k];
+    for (int k = m1 + tid; k < nl; k += NT) wn[k] = vn[k] = 0.0;
     __syncthreads();
-    for (int r = warp; r < m; r += nw) {
-      double* row = L + pk(o + r, o);
-      const double vr = v[r], wr = p[r];
-      for (int c = lane; c <= r; c += 32) row[c] -= vr * p[c] + wr * v[c];
-    }
-    __syncthreads();
+    cur ^= 1;
   }
   if (tid == 0) {
-    if (n >= 2) {
-      d[n - 2] = L[pk(n - 2, n - 2)];
-      e[n - 2] = L[pk(n - 1, n - 2)];
-      tau[n - 2] = 0.0;
-    }
-    d[n - 1] = L[pk(n - 1, n - 1)];
-    e[n - 1] = 0.0;
-    tau[n - 1] = 0.0;
+    e[nl - 2] = L[pk32(nl - 1, nl - 2)];
+    tau[nl - 2] = 0.0;
+    d[nl - 1] = L[pk32(nl - 1, nl - 1)];
+    e[nl - 1] = 0.0;
+    tau[nl - 1] = 0.0;
   }
 }
 
-size_t tridiag_smem_bytes(int n) { return ((size_t)n * (n + 1) / 2 + (2 + 8) * (size_t)n + 40) * sizeof(double); }
+size_t tridiag_smem_bytes(int nl, int nt) {
+  return ((size_t)nl * (nl + 1) / 2 + (4 + nt / 32) * (size_t)nl + 40) * sizeof(double);
+}
+
+// Largest trailing block the shared-memory kernel holds (227 KB per CTA).
+constexpr int kTridiagSmemMax = 228;
 
 void launch_tridiag_smem(const EigArgs& g, const int32_t* list, int count, int max_n, cudaStream_t stream) {
   if (count == 0) return;
-  static const bool attr = cudaFuncSetAttribute(k_tridiag_smem, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                                227 * 1024) == cudaSuccess;
-  (void)attr;
-  k_tridiag_smem<<<count, 256, tridiag_smem_bytes(max_n), stream>>>(g, list);
+  static const size_t cap256 = allow_max_dynamic_smem(k_tridiag_smem<256>);
+  static const size_t cap512 = allow_max_dynamic_smem(k_tridiag_smem<512>);
+  int nloc = std::min(max_n, kTridiagSmemMax);
+  while (nloc > 2 && tridiag_smem_bytes(nloc, 256) > cap256) --nloc;
+  if (max_n > nloc) {
+    // columns that do not fit: reduced in global memory first
+    const size_t sm = (2 * (size_t)max_n + 40) * sizeof(double);
+    k_tridiag<<<count, 512, sm, stream>>>(g, nloc);
+  }
+  if (tridiag_smem_bytes(nloc, 512) <= cap512) {
+    k_tridiag_smem<512><<<count, 512, tridiag_smem_bytes(nloc, 512), stream>>>(g, list, nloc);
+  } else {
+    k_tridiag_smem<256><<<count, 256, tridiag_smem_bytes(nloc, 256), stream>>>(g, list, nloc);
+  }
 }
 
 // ---------------------------------------------------------------------------
@@ -634,8 +733,23 @@ __device__ void bisect_range(const double* d, const double* e2, int n, double gl
 __global__ void __launch_bounds__(128) k_inverse_iteration(EigArgs g, double ortol_rel) {
   const int s = g.list[blockIdx.x];
   const int64_t o = g.ao_off[s];
-  inverse_iteration_block(g.d + o, g.e + o, g.eig + o, g.nao[s], g.nvec[s], g.Z + g.mat_off[s],
-                          g.scratch + g.scratch_off[s], ortol_rel, (uint32_t)s);
+  inverse_iteration_block<128>(g.d + o, g.e + o, g.eig + o, g.nao[s], g.nvec[s],
+                               g.Z + g.mat_off[s], g.scratch + g.scratch_off[s], ortol_rel,
+                               (uint32_t)s, 0, 128);
+}
+
+// Latency form for few systems: grid (parts, systems) of 16-thread CTAs whose
+// work vectors live in shared memory (5 n 16 doubles) instead of global
+// scratch; part p leads the clusters starting at p*16 + t, stepping 16 parts.
+constexpr int kInvSmemThreads = 16;
+__global__ void __launch_bounds__(kInvSmemThreads) k_inverse_iteration_smem(EigArgs g, double ortol_rel) {
+  extern __shared__ double sm[];
+  const int s = g.list[blockIdx.y];
+  const int64_t o = g.ao_off[s];
+  inverse_iteration_block<kInvSmemThreads>(g.d + o, g.e + o, g.eig + o, g.nao[s], g.nvec[s],
+                                           g.Z + g.mat_off[s], sm, ortol_rel, (uint32_t)s,
+                                           blockIdx.x * kInvSmemThreads,
+                                           gridDim.x * kInvSmemThreads);
 }
 
 // ---------------------------------------------------------------------------
@@ -691,14 +805,20 @@ size_t backtransform_wy_bytes(int n, int m) {
   return ((size_t)n * (WB + 1) + 2 * WB * (WB + 1) + (size_t)WB * m + 8) * sizeof(double);
 }
 
+// Grid (parts, systems): part blockIdx.x transforms its contiguous slice of
+// the system's eigenvectors (parts > 1 only when few systems are active, so
+// that one system's vectors are spread over several SMs).
 __global__ void __launch_bounds__(256) k_backtransform_wy(EigArgs g, int wcap) {
   extern __shared__ double sm[];
-  const int s = g.list[blockIdx.x];
+  const int s = g.list[blockIdx.y];
   const int n = g.nao[s];
-  const int m = g.nvec[s];
+  const int mt = g.nvec[s];
+  const int per = (mt + gridDim.x - 1) / gridDim.x;
+  const int jbeg = blockIdx.x * per;
+  const int m = min(mt - jbeg, per);
   const double* a = g.A + g.mat_off[s];
   const double* tau = g.tau + g.ao_off[s];
-  double* Z = g.Z + g.mat_off[s];
+  double* Z = g.Z + g.mat_off[s] + (int64_t)jbeg * n;
   const int nr = n - 2;
   if (nr <= 0 || m <= 0) return;
   const int tid = threadIdx.x, bs = blockDim.x, lane = tid & 31, warp = tid >> 5, nw = bs >> 5;
@@ -782,12 +902,15 @@ __global__ void __launch_bounds__(256) k_backtransform_wy(EigArgs g, int wcap) {
   }
 }
 
-void launch_backtransform_wy(const EigArgs& g, int count, int max_n, int max_m, cudaStream_t stream) {
+void launch_backtransform_wy(const EigArgs& g, int count, int max_n, int max_m, int want_m,
+                             cudaStream_t stream) {
   if (count == 0) return;
-  static const bool attr = cudaFuncSetAttribute(k_backtransform_wy, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                                227 * 1024) == cudaSuccess;
-  (void)attr;
-  k_backtransform_wy<<<count, 256, backtransform_wy_bytes(max_n, max_m), stream>>>(g, max_m);
+  static const size_t cap = allow_max_dynamic_smem(k_backtransform_wy);
+  (void)cap;
+  // Few systems: split each system's vectors over CTAs, at least 8 vectors each.
+  const int sms = sm_count();
+  const int parts = count >= sms ? 1 : std::max(1, std::min((want_m + 7) / 8, 2 * sms / count));
+  k_backtransform_wy<<<dim3(parts, count), 256, backtransform_wy_bytes(max_n, max_m), stream>>>(g, max_m);
 }
 
 // Loewdin weights s^-1/2 with the overlap condition guard; failed systems are flagged.
@@ -811,9 +934,9 @@ __global__ void k_lowdin_weights(EigArgs g, int32_t* status) {
 void launch_tridiag(const EigArgs& g, int count, int max_n, cudaStream_t stream) {
   if (count == 0) return;
   const size_t sm = (2 * (size_t)max_n + 40) * sizeof(double);
-  static const bool attr = cudaFuncSetAttribute(k_tridiag, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024) == cudaSuccess;
-  (void)attr;
-  k_tridiag<<<count, 512, sm, stream>>>(g);
+  static const size_t cap = allow_max_dynamic_smem(k_tridiag);
+  (void)cap;
+  k_tridiag<<<count, 512, sm, stream>>>(g, 0);
 }
 
 int sm_count() {
@@ -831,8 +954,8 @@ void launch_eigvals(const EigArgs& g, int mode, double kt, int count, int max_n,
   if (count == 0) return;
   const int kNumSMs = sm_count();
   const size_t sm = (5 * (size_t)max_n + 40) * sizeof(double);
-  static const bool attr = cudaFuncSetAttribute(k_tridiag_eigvals, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024) == cudaSuccess;
-  (void)attr;
+  static const size_t cap = allow_max_dynamic_smem(k_tridiag_eigvals);
+  (void)cap;
   // Enough systems to fill the GPU: one CTA each, one thread per eigenvalue
   // (fewest Sturm sequences in total).  Few systems: spread each system's
   // eigenvalues over several CTAs, up to a warp per eigenvalue (fewest rounds).
@@ -847,16 +970,23 @@ void launch_eigvals(const EigArgs& g, int mode, double kt, int count, int max_n,
   k_tridiag_eigvals<<<count, 256, sm, stream>>>(g, mode, kt, 1, 8);
 }
 
-void launch_inverse_iteration(const EigArgs& g, int count, double ortol_rel, cudaStream_t stream) {
+void launch_inverse_iteration(const EigArgs& g, int count, int max_n, int want_m, double ortol_rel,
+                              cudaStream_t stream) {
   if (count == 0) return;
+  const size_t smem = (size_t)5 * max_n * kInvSmemThreads * sizeof(double);
+  static const size_t cap = allow_max_dynamic_smem(k_inverse_iteration_smem);
+  if (count < sm_count() && smem <= cap) {
+    const int parts = std::max(1, (want_m + kInvSmemThreads - 1) / kInvSmemThreads);
+    k_inverse_iteration_smem<<<dim3(parts, count), kInvSmemThreads, smem, stream>>>(g, ortol_rel);
+    return;
+  }
   k_inverse_iteration<<<count, 128, 0, stream>>>(g, ortol_rel);
 }
 
 void launch_backtransform(const EigArgs& g, const int32_t* list, int count, int max_n, int mcap,
                           cudaStream_t stream) {
   if (count == 0) return;
-  static const bool attr = cudaFuncSetAttribute(k_backtransform, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                                227 * 1024) == cudaSuccess;
+  static const size_t attr = allow_max_dynamic_smem(k_backtransform);
   (void)attr;
   size_t bytes = ((size_t)max_n + 8) * sizeof(double);
   if (mcap > 0) bytes += (size_t)mcap * max_n * sizeof(double);

@@ -382,7 +382,7 @@ void launch_classical(const ForceArgs& f, int max_atoms, int max_shells, cudaStr
   (void)max_shells;
   if (f.count == 0) return;
   const size_t sm = ((size_t)(7 + 4 * kMaxD4Refs) * max_atoms + 48) * sizeof(double);
-  static const bool attr = cudaFuncSetAttribute(k_classical, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024) == cudaSuccess;
+  static const size_t attr = allow_max_dynamic_smem(k_classical);
   (void)attr;
   k_classical<<<f.count, 256, sm, stream>>>(f);
 }

@@ -168,7 +168,7 @@ void launch_potential(const SccArgs& a, const double* qsh, const double* dip, co
                       int max_atoms, int max_shells, cudaStream_t stream) {
   if (a.count == 0) return;
   const size_t sm = ((size_t)(11 + 2 * kMaxD4Refs) * max_atoms + max_shells + 8) * sizeof(double);
-  static const bool attr = cudaFuncSetAttribute(k_potential, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024) == cudaSuccess;
+  static const size_t attr = allow_max_dynamic_smem(k_potential);
   (void)attr;
   k_potential<<<a.count, 256, sm, stream>>>(a, qsh, dip, qp);
 }
@@ -555,7 +555,7 @@ void launch_energy_mixer(const SccArgs& a, int max_atoms, int max_shells, int ma
   (void)first_iteration;
   if (a.count == 0) return;
   const size_t sm = ((size_t)max_dim + (1 + kMaxD4Refs) * max_atoms + 64 + 8 * 44 + 8) * sizeof(double);
-  static const bool attr = cudaFuncSetAttribute(k_energy_mixer, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024) == cudaSuccess;
+  static const size_t attr = allow_max_dynamic_smem(k_energy_mixer);
   (void)attr;
   k_energy_mixer<<<a.count, 256, sm, stream>>>(a);
 }

@@ -99,13 +99,15 @@ void launch_gemm(const GemmArgs& g, bool transA, bool weighted, int max_tiles, i
                  cudaStream_t stream);
 void launch_tridiag(const EigArgs& g, int count, int max_n, cudaStream_t stream);
 void launch_tridiag_smem(const EigArgs& g, const int32_t* list, int count, int max_n, cudaStream_t stream);
-size_t tridiag_smem_bytes(int n);
+size_t tridiag_smem_bytes(int nl, int nt);
 int sm_count();   // multiprocessors of the current device (cached)
 void launch_eigvals(const EigArgs& g, int mode, double kt, int count, int max_n, cudaStream_t stream);
-void launch_inverse_iteration(const EigArgs& g, int count, double ortol_rel, cudaStream_t stream);
+void launch_inverse_iteration(const EigArgs& g, int count, int max_n, int want_m, double ortol_rel,
+                              cudaStream_t stream);
 void launch_backtransform(const EigArgs& g, const int32_t* list, int count, int max_n, int mcap,
                           cudaStream_t stream);
-void launch_backtransform_wy(const EigArgs& g, int count, int max_n, int max_m, cudaStream_t stream);
+void launch_backtransform_wy(const EigArgs& g, int count, int max_n, int max_m, int want_m,
+                             cudaStream_t stream);
 size_t backtransform_wy_bytes(int n, int m);
 void launch_lowdin_weights(const EigArgs& g, int32_t* status, int count, cudaStream_t stream);
 

@@ -44,7 +44,7 @@ double* g_scratch_ptr[kMaxDevices] = {};
 __global__ void __launch_bounds__(kThreads)
     k_inverse_iteration_static(const double* d, const double* e, const double* ev, int n, int m,
                                double* Z, double* scratch, double ortol_rel) {
-  inverse_iteration_block(d, e, ev, n, m, Z, scratch, ortol_rel, 0u);
+  inverse_iteration_block<kThreads>(d, e, ev, n, m, Z, scratch, ortol_rel, 0u, 0, kThreads);
 }
 
 }  // namespace
