@@ -690,8 +690,9 @@ xtbloom_status_t Engine::compute(const ComputeRequest& req, std::string& error) 
   eg.nel_b = m.nel_b.as<double>();
   const int tiles = ((m.max_n + 63) / 64) * ((m.max_n + 63) / 64);
   auto gemm = [&](const double* A, const double* Bm, double* C, const int32_t* dm, const int32_t* dn,
-                  const int32_t* dk, bool ta, const double* w, int count) {
+                  const int32_t* dk, bool ta, const double* w, int count, bool sym = false) {
     GemmArgs g{};
+    g.sym = sym ? 1 : 0;
     g.list = list;
     g.nao = m.nao.as<int32_t>();
     g.dm = dm;
@@ -787,7 +788,7 @@ xtbloom_status_t Engine::compute(const ComputeRequest& req, std::string& error) 
   eigensolve(nsys, 1, 0.0, 2e-6, kStLowdin);
   XTB_STAGE(kStLowdin, 2, launch_lowdin_weights(eg, status, nsys, s);
             gemm(m.Zv.as<double>(), m.Zv.as<double>(), m.X.as<double>(), dnao, dnao, dnao, true,
-                 m.occ.as<double>(), nsys));
+                 m.occ.as<double>(), nsys, true));
 
   // ---- SCC ----
   SccArgs a{};
@@ -849,13 +850,13 @@ xtbloom_status_t Engine::compute(const ComputeRequest& req, std::string& error) 
               gemm(m.H.as<double>(), m.X.as<double>(), m.T.as<double>(), dnao, dnao, dnao, false,
                    nullptr, count);
               gemm(m.X.as<double>(), m.T.as<double>(), m.A.as<double>(), dnao, dnao, dnao, false,
-                   nullptr, count));
+                   nullptr, count, true));
     eigensolve(count, 0, req.kt, 2e-7, kStTridiag);
     XTB_STAGE(kStDensity, 2,
               gemm(m.Zv.as<double>(), m.X.as<double>(), m.C.as<double>(), dnvec, dnao, dnao, false,
                    nullptr, count);
               gemm(m.C.as<double>(), m.C.as<double>(), m.P.as<double>(), dnao, dnao, dnvec, true,
-                   m.occ.as<double>(), count));
+                   m.occ.as<double>(), count, true));
     cudaMemsetAsync(m.pop_sh.p, 0, m.nshells * 8, s);
     cudaMemsetAsync(m.pop_dip.p, 0, 3 * m.natoms * 8, s);
     cudaMemsetAsync(m.pop_qp.p, 0, 6 * m.natoms * 8, s);
@@ -917,7 +918,7 @@ xtbloom_status_t Engine::compute(const ComputeRequest& req, std::string& error) 
     XTB_STAGE(kStForcePairs, 3,
               launch_potential(a, a.qsh, a.dip, a.qp, m.max_atoms, m.max_shells, s);
               gemm(m.C.as<double>(), m.C.as<double>(), m.W.as<double>(), dnao, dnao, dnvec, true,
-                   m.occ_eps.as<double>(), count);
+                   m.occ_eps.as<double>(), count, true);
               launch_force_pairs(f, m.max_pairs, s));
   }
   if (count > 0) XTB_STAGE(kStClassical, 1, launch_classical(f, m.max_atoms, m.max_shells, s));

@@ -19,13 +19,17 @@
 #include "kernels.cuh"
 
 #include <algorithm>
+#include <cmath>
 #include <cfloat>
 
 namespace xtb {
 
 // ---------------------------------------------------------------------------
 // Ragged batched GEMM.  C = op(A) * diag(w) * B with op(A) = A or A^T.
-// Every matrix of system s is row-major with leading dimension nao[s].
+// Every matrix of system s is row-major with leading dimension nao[s].  With
+// g.sym the product is known to be symmetric (M = N): only the tiles on and
+// below the diagonal are computed and each off-diagonal tile is also stored
+// transposed.
 // ---------------------------------------------------------------------------
 constexpr int GB = 64, GK = 16;
 
@@ -36,8 +40,19 @@ __global__ void __launch_bounds__(256) k_gemm(GemmArgs g) {
   const int ld = g.nao[s];
   const int tn = (N + GB - 1) / GB;
   const int tm = (M + GB - 1) / GB;
-  if ((int)blockIdx.x >= tm * tn) return;
-  const int ti = blockIdx.x / tn, tj = blockIdx.x % tn;
+  int ti, tj;
+  if (g.sym) {
+    const int t = blockIdx.x;
+    if (t >= tm * (tm + 1) / 2) return;
+    ti = (int)((sqrt(8.0 * t + 1.0) - 1.0) * 0.5);   // ti(ti+1)/2 <= t
+    while ((ti + 1) * (ti + 2) / 2 <= t) ++ti;
+    while (ti * (ti + 1) / 2 > t) --ti;
+    tj = t - ti * (ti + 1) / 2;
+  } else {
+    if ((int)blockIdx.x >= tm * tn) return;
+    ti = blockIdx.x / tn;
+    tj = blockIdx.x % tn;
+  }
   const double* A = g.A + g.offA[s];
   const double* B = g.B + g.offB[s];
   double* C = g.C + g.offC[s];
@@ -87,6 +102,7 @@ __global__ void __launch_bounds__(256) k_gemm(GemmArgs g) {
     }
     __syncthreads();
   }
+  const bool mirror = g.sym && ti != tj;
 #pragma unroll
   for (int i = 0; i < 4; ++i) {
     const int gi = i0 + ty + 16 * i;
@@ -94,7 +110,10 @@ __global__ void __launch_bounds__(256) k_gemm(GemmArgs g) {
 #pragma unroll
     for (int j = 0; j < 4; ++j) {
       const int gj = j0 + tx + 16 * j;
-      if (gj < N) C[(int64_t)gi * ld + gj] = acc[i][j];
+      if (gj < N) {
+        C[(int64_t)gi * ld + gj] = acc[i][j];
+        if (mirror) C[(int64_t)gj * ld + gi] = acc[i][j];
+      }
     }
   }
 }
@@ -102,6 +121,10 @@ __global__ void __launch_bounds__(256) k_gemm(GemmArgs g) {
 void launch_gemm(const GemmArgs& g, bool transA, bool weighted, int max_tiles, int count,
                  cudaStream_t stream) {
   if (count == 0) return;
+  if (g.sym) {
+    const int tm = (int)std::lround(std::sqrt((double)max_tiles));   // max_tiles = tm * tm
+    max_tiles = tm * (tm + 1) / 2;
+  }
   dim3 grid(max_tiles, count);
   if (transA && weighted) k_gemm<true, true><<<grid, 256, 0, stream>>>(g);
   else if (transA) k_gemm<true, false><<<grid, 256, 0, stream>>>(g);
@@ -406,7 +429,9 @@ void launch_tridiag_smem(const EigArgs& g, const int32_t* list, int count, int m
     const size_t sm = (2 * (size_t)max_n + 40) * sizeof(double);
     k_tridiag<<<count, 512, sm, stream>>>(g, nloc);
   }
-  if (tridiag_smem_bytes(nloc, 512) <= cap512) {
+  // 512 threads shorten one system's critical path (few systems active);
+  // with many systems, several 256-thread CTAs per SM give more throughput.
+  if (count < sm_count() && tridiag_smem_bytes(nloc, 512) <= cap512) {
     k_tridiag_smem<512><<<count, 512, tridiag_smem_bytes(nloc, 512), stream>>>(g, list, nloc);
   } else {
     k_tridiag_smem<256><<<count, 256, tridiag_smem_bytes(nloc, 256), stream>>>(g, list, nloc);

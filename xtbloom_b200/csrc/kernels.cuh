@@ -19,6 +19,7 @@ struct GemmArgs {
   const int64_t* offC;
   const double* w;         // per-k weight (weighted form)
   const int64_t* offW;
+  int32_t sym;             // C is symmetric: compute the lower tiles, mirror them
 };
 
 struct EigArgs {
