@@ -935,6 +935,26 @@ class Broyden:
 # Single point (runtime/gfn2_cpu_execution.cpp:1218-1460, model/gfn2/scc_driver.cpp:706-960,
 # 2105-2560, model/gfn2/force.cpp:336-645)
 # --------------------------------------------------------------------------
+def pc_setup(basis, pos, pc_pos, pc_gam):
+    """Softened shell-point Coulomb kernel K[s, p] = (|R_A - R_p|^2 + a_sp^2)^-1/2 with
+    a_sp = 2 / (eta_s + gamma_p), eta_s the GFN2 shell hardness
+    (model/gfn2/external_point_charges.cpp:277-327, docs/theory/qmmm.md)."""
+    eta = shell_hardness(basis)
+    d = pos[basis.sh_atom][:, None, :] - pc_pos[None, :, :]
+    a = 2.0 / (eta[:, None] + pc_gam[None, :])
+    D = np.sum(d * d, axis=-1) + a * a
+    return 1.0 / np.sqrt(D), d, D
+
+
+def pc_gradients(basis, qsh, pc_q, K, d, D, grad):
+    """Adds dE_pc/dR_A to grad; returns dE_pc/dR_p and dE_pc/dQ_p
+    (external_point_charges.cpp:389-490; dE/dQ_p = sum_s q_s K_sp)."""
+    w = qsh[:, None] * pc_q[None, :] * D ** -1.5
+    f = w[:, :, None] * d
+    np.add.at(grad, basis.sh_atom, -f.sum(axis=1))
+    return f.sum(axis=0), qsh @ K
+
+
 @dataclass
 class Result:
     energy: float
@@ -944,11 +964,13 @@ class Result:
     converged: bool
     terms: dict = field(default_factory=dict)
     debug: dict = field(default_factory=dict)
+    pc_gradient: np.ndarray | None = None
+    pc_dq: np.ndarray | None = None
 
 
 def singlepoint(numbers, pos, charge=0.0, uhf=0, kt=300.0 * PR.KELVIN_TO_HARTREE,
                 ctol=1e-6, etol=1e-8, maxiter=250, memory=8, damping=0.4,
-                forces=True, debug=False) -> Result:
+                forces=True, debug=False, pc_pos=None, pc_q=None, pc_gam=None) -> Result:
     numbers = np.asarray(numbers, int)
     pos = np.asarray(pos, float).reshape(-1, 3)
     nat = len(numbers)
@@ -963,6 +985,15 @@ def singlepoint(numbers, pos, charge=0.0, uhf=0, kt=300.0 * PR.KELVIN_TO_HARTREE
     d4 = d4_setup(numbers, pos)
     ao_at, ao_sh = basis.ao_atom, basis.ao_shell
     ns = len(basis.sh_l)
+    have_pc = pc_q is not None and len(pc_q) > 0
+    if have_pc:
+        pc_pos = np.asarray(pc_pos, float).reshape(-1, 3)
+        pc_q = np.asarray(pc_q, float)
+        pc_gam = np.asarray(pc_gam, float)
+        Kpc, dpc, Dpc = pc_setup(basis, pos, pc_pos, pc_gam)
+        vpc = Kpc @ pc_q
+    else:
+        vpc = np.zeros(ns)
     nel = basis.refocc.sum() - charge
     na, nb = 0.5 * (nel + uhf), 0.5 * (nel - uhf)
 
@@ -986,7 +1017,7 @@ def singlepoint(numbers, pos, charge=0.0, uhf=0, kt=300.0 * PR.KELVIN_TO_HARTREE
         vat, vd, vq = aes2_potential(aes, qat, dip, qp)
         _, vd4 = d4_two_body(d4, qat)
         vat = vat + vd4
-        return vsh + vat[basis.sh_atom], vd, vq
+        return vsh + vat[basis.sh_atom] + vpc, vd, vq
 
     def fock(vs, vd, vq):
         v = vs[ao_sh]
@@ -1031,7 +1062,8 @@ def singlepoint(numbers, pos, charge=0.0, uhf=0, kt=300.0 * PR.KELVIN_TO_HARTREE
         e_es3 = np.sum(g3 * rqsh ** 3) / 3.0
         e_aes2 = aes2_energy(aes, rqat, rdip, rqp)
         e_d4, _ = d4_two_body(d4, rqat)
-        free = e_core + e_es2 + e_es3 + e_aes2 + e_d4 - kt * ent
+        e_pc = rqsh @ vpc
+        free = e_core + e_es2 + e_es3 + e_aes2 + e_d4 + e_pc - kt * ent
         raw = np.concatenate([rqsh, rdip.ravel(), rqp.ravel()])
         mixed, rms = mixer.step(raw)
         de = free - (0.0 if it == 0 else fold)
@@ -1050,8 +1082,9 @@ def singlepoint(numbers, pos, charge=0.0, uhf=0, kt=300.0 * PR.KELVIN_TO_HARTREE
     e_atm = d4_atm(d4)
     energy = free + e_rep + e_atm
     terms = dict(core=e_core, es2=e_es2, es3=e_es3, aes2=e_aes2, d4=e_d4, entropy=-kt * ent,
-                 rep=e_rep, atm=e_atm, free=free)
+                 rep=e_rep, atm=e_atm, pc=e_pc, free=free)
     grad = np.zeros((nat, 3))
+    pc_grad = pc_dq = None
     if forces and converged:
         vs, vd, vq = potentials(qsh, dip, qp)
         # electronic part: H0 VJP, -W, stationary S/D/Q adjoints (model/gfn2/force.cpp:256-300,520-560)
@@ -1073,7 +1106,9 @@ def singlepoint(numbers, pos, charge=0.0, uhf=0, kt=300.0 * PR.KELVIN_TO_HARTREE
         d4_two_body(d4, qat, grad=grad)
         d4_atm(d4, grad=grad)
         repulsion(numbers, pos, grad=grad)
+        if have_pc:
+            pc_grad, pc_dq = pc_gradients(basis, qsh, pc_q, Kpc, dpc, Dpc, grad)
     if debug:
         dbg.update(cn=cn, S=S, D=D, Q=Q, H0=H0, P=P, W=W, eps=eps, qsh=qsh, dip=dip, qp=qp,
                    gam=gam, cn_d4=d4.cn, nel=nel)
-    return Result(energy, grad, qat, it, converged, terms, dbg)
+    return Result(energy, grad, qat, it, converged, terms, dbg, pc_grad, pc_dq)

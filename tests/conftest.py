@@ -29,6 +29,16 @@ def fixtures():
 
 
 @pytest.fixture(scope="session")
+def pc_fixtures():
+    return json.loads((GOLDEN / "pc_fixtures.json").read_text())["systems"]
+
+
+def as_pc(sys_):
+    return (np.asarray(sys_["pc_positions"], float).reshape(-1, 3), np.asarray(sys_["pc_charges"], float),
+            np.asarray(sys_["pc_gammas"], float))
+
+
+@pytest.fixture(scope="session")
 def tblite_goldens():
     return json.loads((GOLDEN / "tblite_goldens.json").read_text())["cases"]
 

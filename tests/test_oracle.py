@@ -4,7 +4,7 @@ from __future__ import annotations
 import numpy as np
 import pytest
 
-from conftest import as_molecule
+from conftest import as_molecule, as_pc
 from oracle import gfn2
 
 FAST = ["c10h22_conformer_0", "c10h22_conformer_3", "hetero_chain_7", "h3_plus", "ketene",
@@ -57,3 +57,50 @@ def test_integer_layout_of_basis():
     for z, nsh, nao in [(1, 1, 1), (6, 2, 4), (7, 2, 4), (8, 2, 4), (17, 3, 9)]:
         b = gfn2.make_basis(np.array([z]))
         assert len(b.sh_l) == nsh and b.nao == nao
+
+
+PC_FAST = ["water_one_pc_gamma999", "water_one_pc_close_hardness", "water_one_pc_coincident_hardness",
+           "water_dimer_6pc_hardness", "water_dimer_6pc_gamma999", "hetero_chain_7_pc30_gamma999",
+           "hetero_chain_3001_pc30_gamma0.8"]
+
+
+@pytest.mark.parametrize("name", PC_FAST)
+def test_oracle_point_charges_match_reference_library(pc_fixtures, name):
+    """Embedded energies, forces, charges and point-charge forces equal the compiled reference."""
+    sys_ = next(s for s in pc_fixtures if s["name"] == name)
+    z, x, q, u = as_molecule(sys_)
+    pp, pq, pg = as_pc(sys_)
+    r = gfn2.singlepoint(z, x, charge=q, uhf=u, pc_pos=pp, pc_q=pq, pc_gam=pg)
+    assert r.converged and r.iterations == sys_["scc_iterations"]
+    assert abs(r.energy - sys_["energy"]) < 1e-9
+    assert np.abs(-r.gradient.ravel() - np.asarray(sys_["forces"])).max() < 1e-8
+    assert np.abs(r.charges - np.asarray(sys_["charges"])).max() < 1e-8
+    assert np.abs(-r.pc_gradient.ravel() - np.asarray(sys_["pc_forces"])).max() < 1e-8
+    if "xtb_energy" in sys_:   # the reference's xTB 6.7.1 QM/MM goldens
+        assert abs(r.energy - sys_["xtb_energy"]) < 5e-7
+        assert np.abs(-r.gradient.ravel() - np.asarray(sys_["xtb_forces"])).max() < 5e-7
+        assert np.abs(-r.pc_gradient.ravel() - np.asarray(sys_["xtb_pc_forces"])).max() < 5e-7
+
+
+def test_oracle_point_charge_derivatives_are_finite_differences(pc_fixtures):
+    """dE/dQ_p and dE/dR_p from central differences (h = 1e-4) of the oracle energy."""
+    sys_ = next(s for s in pc_fixtures if s["name"] == "water_dimer_6pc_hardness")
+    z, x, q, u = as_molecule(sys_)
+    pp, pq, pg = as_pc(sys_)
+    tight = dict(charge=q, uhf=u, ctol=1e-10, etol=1e-12, pc_gam=pg)
+    r = gfn2.singlepoint(z, x, pc_pos=pp, pc_q=pq, **tight)
+    h = 1e-4
+    for p in range(len(pq)):
+        qp, qm = pq.copy(), pq.copy()
+        qp[p] += h
+        qm[p] -= h
+        ep = gfn2.singlepoint(z, x, pc_pos=pp, pc_q=qp, forces=False, **tight).energy
+        em = gfn2.singlepoint(z, x, pc_pos=pp, pc_q=qm, forces=False, **tight).energy
+        assert abs((ep - em) / (2 * h) - r.pc_dq[p]) < 1e-6
+    for p, c in [(0, 0), (3, 2)]:
+        xp, xm = pp.copy(), pp.copy()
+        xp[p, c] += h
+        xm[p, c] -= h
+        ep = gfn2.singlepoint(z, x, pc_pos=xp, pc_q=pq, forces=False, **tight).energy
+        em = gfn2.singlepoint(z, x, pc_pos=xm, pc_q=pq, forces=False, **tight).energy
+        assert abs((ep - em) / (2 * h) - r.pc_gradient[p, c]) < 1e-6

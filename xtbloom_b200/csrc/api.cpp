@@ -181,9 +181,15 @@ xtbloom_status_t validate_and_normalise(const xtbloom_batch_t* batch,
       }
     }
   }
-  if (batch->total_point_charges != 0 || buffer_active(batch->point_charge_offsets)) {
-    err = "external point charges are not implemented in this CUDA path";
-    return XTBLOOM_STATUS_NOT_IMPLEMENTED;
+  const size_t P = static_cast<size_t>(batch->total_point_charges);
+  if (P != 0 || buffer_active(batch->point_charge_offsets)) {
+    if (!check_in(batch->point_charge_offsets, (B + 1) * 8, "point_charge_offsets", err))
+      return XTBLOOM_STATUS_INVALID_ARGUMENT;
+  }
+  if (P != 0 && (!check_in(batch->point_charge_positions, P * 24, "point_charge_positions", err) ||
+                 !check_in(batch->point_charge_values, P * 8, "point_charge_values", err) ||
+                 !check_in(batch->point_charge_gammas, P * 8, "point_charge_gammas", err))) {
+    return XTBLOOM_STATUS_INVALID_ARGUMENT;
   }
   if (batch->total_charge_response_elements != 0 || buffer_active(batch->atomic_potential_shifts) ||
       buffer_active(batch->charge_response_offsets) || buffer_active(batch->charge_response_matrix)) {
@@ -214,10 +220,6 @@ xtbloom_status_t validate_and_normalise(const xtbloom_batch_t* batch,
                          XTBLOOM_COMPUTE_DIPOLE_MOMENTS;
   if ((options->flags & ~known) != 0 || options->reserved != 0) {
     err = "compute flags contain reserved bits";
-    return XTBLOOM_STATUS_INVALID_ARGUMENT;
-  }
-  if (options->flags & XTBLOOM_COMPUTE_POINT_CHARGE_FORCES) {
-    err = "point-charge forces were requested without point charges";
     return XTBLOOM_STATUS_INVALID_ARGUMENT;
   }
   if (options->flags & XTBLOOM_COMPUTE_DIPOLE_MOMENTS) {
@@ -273,6 +275,8 @@ xtbloom_status_t validate_and_normalise(const xtbloom_batch_t* batch,
       !check_out(result->forces, N * 24, (f & XTBLOOM_COMPUTE_FORCES) != 0, "forces", err) ||
       !check_out(result->atomic_charges, N * 8, (f & XTBLOOM_COMPUTE_ATOMIC_CHARGES) != 0,
                  "atomic_charges", err) ||
+      !check_out(result->point_charge_forces, P * 24,
+                 (f & XTBLOOM_COMPUTE_POINT_CHARGE_FORCES) != 0 && P != 0, "point_charge_forces", err) ||
       !check_out(result->scc_iterations, B * 4, true, "scc_iterations", err) ||
       !check_out(result->scc_converged, B, true, "scc_converged", err) ||
       !check_out(result->per_system_status, B * 4, true, "per_system_status", err)) {

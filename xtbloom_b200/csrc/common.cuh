@@ -105,6 +105,18 @@ struct DevTopo {
   const int32_t* ref_ng;
   const double* ref_c6;       // 262 x 262
   int32_t ref_count;
+  // external point charges (per system ranges; empty when pc_off is null)
+  const int64_t* pc_off;      // nsys + 1
+  const double* pc_pos;       // 3 per charge
+  const double* pc_q;
+  const double* pc_gam;
+  const double* vpc;          // per shell: potential of the point charges
+};
+
+// Per-system energy terms (terms[kTermCount * s + k]).
+enum TermIndex : int {
+  kTermCore = 0, kTermEs2 = 1, kTermEs3 = 2, kTermAes2 = 3, kTermD4 = 4, kTermEntropy = 5,
+  kTermRep = 6, kTermAtm = 7, kTermPc = 8, kTermCount = 9
 };
 
 __device__ __forceinline__ double logistic(double x) {

@@ -228,6 +228,11 @@ struct Engine::Impl {
   Dbuf mx_cur, mx_prev, mx_res, mx_df, mx_u, mx_omega;
   Dbuf grad, acn, acn_d4;
   Dbuf out_energy, out_forces, out_charges;
+  // external point charges of the current call
+  Dbuf pc_off, pc_pos, pc_q, pc_gam, vpc, pc_grad, pc_dq, out_pcf;
+  bool have_pc = false;
+  int64_t npc = 0;
+  std::vector<int64_t> h_pc_off;
   int32_t* h_count = nullptr;   // pinned
   int32_t* h_list = nullptr;    // pinned copy of the active list
   int64_t h_list_cap = 0;
@@ -282,6 +287,11 @@ struct Engine::Impl {
     t.sh_shpoly = sh_shpoly.as<double>();
     t.sh_zeta = sh_zeta.as<double>();
     t.sh_eta = sh_eta.as<double>();
+    t.pc_off = have_pc ? pc_off.as<int64_t>() : nullptr;
+    t.pc_pos = have_pc ? pc_pos.as<double>() : nullptr;
+    t.pc_q = have_pc ? pc_q.as<double>() : nullptr;
+    t.pc_gam = have_pc ? pc_gam.as<double>() : nullptr;
+    t.vpc = have_pc ? vpc.as<double>() : nullptr;
     t.sh_g3 = sh_g3.as<double>();
     t.sh_refocc = sh_refocc.as<double>();
     t.p_alpha = p_alpha.as<double>();
@@ -503,7 +513,7 @@ xtbloom_status_t build_topology(Engine::Impl& m, const HostBatch& hb, cudaStream
        m.dip.reserve(3 * N * d8) && m.qp.reserve(6 * N * d8) && m.pop_sh.reserve(shell * d8) &&
        m.pop_dip.reserve(3 * N * d8) && m.pop_qp.reserve(6 * N * d8) && m.e_core.reserve(B * d8) &&
        m.vsh.reserve(shell * d8) && m.vd.reserve(3 * N * d8) && m.vq.reserve(6 * N * d8) &&
-       m.free_energy.reserve(B * d8) && m.terms.reserve(8 * B * d8) &&
+       m.free_energy.reserve(B * d8) && m.terms.reserve(kTermCount * B * d8) &&
        m.mx_cur.reserve((size_t)m.total_vec * d8) && m.mx_prev.reserve((size_t)m.total_vec * d8) &&
        m.mx_res.reserve((size_t)m.total_vec * d8) && m.grad.reserve(3 * N * d8) &&
        m.acn.reserve(N * d8) && m.acn_d4.reserve(N * d8) && m.out_energy.reserve(B * d8) &&
@@ -533,7 +543,10 @@ __global__ void k_publish(DevTopo t, const int32_t* status, const double* free_e
   const bool ok = status[s] == kOk;
   const double nan = __longlong_as_double(0x7ff8000000000000ll);
   const int64_t a0 = t.atom_off[s], a1 = t.atom_off[s + 1];
-  if (threadIdx.x == 0) energy[s] = ok ? free_energy[s] + terms[8 * (int64_t)s + 6] + terms[8 * (int64_t)s + 7] : nan;
+  if (threadIdx.x == 0)
+    energy[s] = ok ? free_energy[s] + terms[kTermCount * (int64_t)s + kTermRep] +
+                         terms[kTermCount * (int64_t)s + kTermAtm]
+               : nan;
   for (int64_t a = a0 + threadIdx.x; a < a1; a += blockDim.x) {
     double q = 0.0;
     for (int sh = t.atom_sh[a]; sh < t.atom_sh[a + 1]; ++sh) q += qsh[sh];
@@ -631,6 +644,53 @@ xtbloom_status_t Engine::compute(const ComputeRequest& req, std::string& error) 
       return XTBLOOM_STATUS_INVALID_ARGUMENT;
     }
   }
+  // ---- external point charges (validated here, before any output is touched) ----
+  {
+    const int64_t P = b.total_point_charges;
+    m.have_pc = P > 0;
+    m.npc = P;
+    if (P > 0) {
+      m.h_pc_off.assign(B + 1, 0);
+      std::vector<double> ppos(3 * P), pq(P), pg(P);
+      if (!read_input(b.point_charge_offsets, m.h_pc_off.data(), (B + 1) * 8, s) ||
+          !read_input(b.point_charge_positions, ppos.data(), 3 * P * 8, s) ||
+          !read_input(b.point_charge_values, pq.data(), P * 8, s) ||
+          !read_input(b.point_charge_gammas, pg.data(), P * 8, s)) {
+        error = "failed to read the point-charge inputs";
+        return XTBLOOM_STATUS_INVALID_ARGUMENT;
+      }
+      if (m.h_pc_off[0] != 0 || m.h_pc_off[B] != P) {
+        error = "point_charge_offsets must start at zero and end at total_point_charges";
+        return XTBLOOM_STATUS_INVALID_ARGUMENT;
+      }
+      for (int64_t i = 0; i < B; ++i)
+        if (m.h_pc_off[i + 1] < m.h_pc_off[i]) {
+          error = "point_charge_offsets must be nondecreasing";
+          return XTBLOOM_STATUS_INVALID_ARGUMENT;
+        }
+      for (int64_t i = 0; i < 3 * P; ++i)
+        if (!std::isfinite(ppos[i])) {
+          error = "external point-charge positions contain NaN or infinity";
+          return XTBLOOM_STATUS_INVALID_ARGUMENT;
+        }
+      for (int64_t i = 0; i < P; ++i)
+        if (!std::isfinite(pq[i]) || !(pg[i] > 0.0) || !std::isfinite(pg[i])) {
+          error = "external point-charge values must be finite and hardnesses must be finite positive";
+          return XTBLOOM_STATUS_INVALID_ARGUMENT;
+        }
+      if (!upload(m.pc_off, m.h_pc_off, s) || !upload(m.pc_pos, ppos, s) || !upload(m.pc_q, pq, s) ||
+          !upload(m.pc_gam, pg, s) || !m.vpc.reserve((size_t)m.nshells * 8) ||
+          !m.pc_grad.reserve((size_t)P * 24) || !m.pc_dq.reserve((size_t)P * 8) ||
+          !m.out_pcf.reserve((size_t)P * 24)) {
+        error = "device allocation for the point charges failed";
+        return XTBLOOM_STATUS_ALLOCATION_FAILED;
+      }
+      cudaMemsetAsync(m.pc_grad.p, 0, (size_t)P * 24, s);
+      cudaMemsetAsync(m.pc_dq.p, 0, (size_t)P * 8, s);
+      // the host vectors must outlive the asynchronous uploads
+      cudaStreamSynchronize(s);
+    }
+  }
   // Broyden history sized by the requested memory
   const int M = req.memory;
   if (!m.mx_df.reserve((size_t)m.total_vec * M * 8) || !m.mx_u.reserve((size_t)m.total_vec * M * 8) ||
@@ -647,7 +707,7 @@ xtbloom_status_t Engine::compute(const ComputeRequest& req, std::string& error) 
   cudaMemsetAsync(status, 0, B * 4, s);
   cudaMemsetAsync(m.converged.p, 0, B, s);
   cudaMemsetAsync(m.iterations.p, 0, B * 4, s);
-  cudaMemsetAsync(m.terms.p, 0, 8 * B * 8, s);
+  cudaMemsetAsync(m.terms.p, 0, kTermCount * B * 8, s);
   cudaMemcpyAsync(list, order, B * 4, cudaMemcpyDeviceToDevice, s);
 
   // first launch failure of any stage (a launch that fails does not run and
@@ -667,7 +727,8 @@ xtbloom_status_t Engine::compute(const ComputeRequest& req, std::string& error) 
             launch_setup(t, list, nsys, m.max_atoms, m.max_pairs, m.max_shells, m.cn.as<double>(),
                          m.cn_d4.as<double>(), m.mrad.as<double>(), m.dmrad.as<double>(),
                          m.S.as<double>(), m.D.as<double>(), m.Q.as<double>(), m.H0.as<double>(),
-                         m.gam.as<double>(), m.total_mat, s));
+                         m.gam.as<double>(), m.total_mat, s);
+            if (m.have_pc) launch_pc_potential(t, list, nsys, m.vpc.as<double>(), s));
 
   EigArgs eg{};
   eg.list = list;
@@ -923,6 +984,14 @@ xtbloom_status_t Engine::compute(const ComputeRequest& req, std::string& error) 
   }
   if (count > 0) XTB_STAGE(kStClassical, 1, launch_classical(f, m.max_atoms, m.max_shells, s));
   if (want_forces && count > 0) XTB_STAGE(kStCnChain, 2, launch_cn_chain(f, m.max_atoms, s));
+  const bool want_pcf = (req.flags & XTBLOOM_COMPUTE_POINT_CHARGE_FORCES) != 0;
+  if (m.have_pc && (want_forces || want_pcf) && count > 0)
+    XTB_STAGE(kStClassical, 1,
+              launch_pc_forces(t, list, count, m.qsh.as<double>(), m.grad.as<double>(),
+                               m.pc_grad.as<double>(), m.pc_dq.as<double>(), s));
+  if (m.have_pc && want_pcf)
+    XTB_STAGE(kStPublish, 1,
+              launch_pc_publish(t, status, nsys, m.pc_grad.as<double>(), m.out_pcf.as<double>(), s));
   XTB_STAGE(kStPublish, 1,
             k_publish<<<nsys, 128, 0, s>>>(t, status, m.free_energy.as<double>(),
                                            m.terms.as<double>(), m.grad.as<double>(),
@@ -946,6 +1015,8 @@ xtbloom_status_t Engine::compute(const ComputeRequest& req, std::string& error) 
   if (req.flags & XTBLOOM_COMPUTE_ENERGY) put(r.energies, m.out_energy.p, B * 8);
   if (req.flags & XTBLOOM_COMPUTE_FORCES) put(r.forces, m.out_forces.p, 3 * N * 8);
   if (req.flags & XTBLOOM_COMPUTE_ATOMIC_CHARGES) put(r.atomic_charges, m.out_charges.p, N * 8);
+  if ((req.flags & XTBLOOM_COMPUTE_POINT_CHARGE_FORCES) && m.have_pc)
+    put(r.point_charge_forces, m.out_pcf.p, (size_t)m.npc * 24);
   put(r.scc_iterations, m.iterations.p, B * 4);
   put(r.scc_converged, m.converged.p, B);
   put(r.per_system_status, status, B * 4);
@@ -1020,7 +1091,20 @@ xtbloom_status_t Engine::debug_fetch(const std::string& name, int64_t system, do
   else if (name == "qsh") { src = m.qsh.as<double>() + sh_off[system]; len = sh_off[system + 1] - sh_off[system]; }
   else if (name == "dipoles") { src = m.dip.as<double>() + 3 * a0; len = 3 * na; }
   else if (name == "quadrupoles") { src = m.qp.as<double>() + 6 * a0; len = 6 * na; }
-  else if (name == "energy_terms") { src = m.terms.as<double>() + 8 * system; len = 8; }
+  else if (name == "point_charge_dq" || name == "point_charge_potential") {
+    if (!m.have_pc) {
+      error = "the most recent compute had no point charges";
+      return XTBLOOM_STATUS_INVALID_ARGUMENT;
+    }
+    if (name == "point_charge_dq") {
+      src = m.pc_dq.as<double>() + m.h_pc_off[system];
+      len = m.h_pc_off[system + 1] - m.h_pc_off[system];
+    } else {
+      src = m.vpc.as<double>() + sh_off[system];
+      len = sh_off[system + 1] - sh_off[system];
+    }
+  }
+  else if (name == "energy_terms") { src = m.terms.as<double>() + kTermCount * system; len = kTermCount; }
   else if (name == "gradient") { src = m.grad.as<double>() + 3 * a0; len = 3 * na; }
   else if (name == "dipole_integrals") {
     if (capacity < 3 * (size_t)(n * n)) { error = "capacity too small"; return XTBLOOM_STATUS_INVALID_ARGUMENT; }

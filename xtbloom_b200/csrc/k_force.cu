@@ -366,8 +366,8 @@ __global__ void __launch_bounds__(256) k_classical(ForceArgs f) {
   erep = block_sum(erep, red);
   eatm = block_sum(eatm, red);
   if (tid == 0) {
-    f.terms[8 * (int64_t)s + 6] = erep;
-    f.terms[8 * (int64_t)s + 7] = eatm;
+    f.terms[kTermCount * (int64_t)s + kTermRep] = erep;
+    f.terms[kTermCount * (int64_t)s + kTermAtm] = eatm;
   }
   if (!grad) return;
   for (int i = tid; i < na; i += bs) {

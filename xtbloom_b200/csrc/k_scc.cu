@@ -154,7 +154,8 @@ __global__ void __launch_bounds__(256) k_potential(SccArgs a, const double* qsh,
     if (lane == 0) {
       const int sh = (int)(s0 + i);
       const double q = sq[i];
-      a.vsh[sh] = acc + t.sh_g3[sh] * q * q + vat[t.sh_atom[sh] - a0];
+      a.vsh[sh] = acc + t.sh_g3[sh] * q * q + vat[t.sh_atom[sh] - a0] +
+                  (t.vpc != nullptr ? t.vpc[sh] : 0.0);
     }
   }
   for (int i = tid; i < na; i += bs) {
@@ -408,13 +409,18 @@ __global__ void __launch_bounds__(256) k_energy_mixer(SccArgs a) {
                   nullptr) * damp;
     }
   }
+  // external point charges: E_pc = sum_s q_s V_s (potential fixed by the geometry)
+  double ep = 0.0;
+  if (t.vpc != nullptr)
+    for (int i = tid; i < ns; i += bs) ep += raw[i] * t.vpc[s0 + i];
   e2 = block_sum(e2, red);
   e3 = block_sum(e3, red);
   ea = block_sum(ea, red);
   ed = block_sum(ed, red);
+  ep = block_sum(ep, red);
   const double ecore = a.e_core[s];
   const double ts = -a.kt * a.entropy[s];
-  const double F = ecore + e2 + e3 + ea + ed + ts;
+  const double F = ecore + e2 + e3 + ea + ed + ep + ts;
 
   // ---- modified Broyden (Johnson) ----
   const int64_t v0 = t.vec_off[s];
@@ -538,8 +544,14 @@ __global__ void __launch_bounds__(256) k_energy_mixer(SccArgs a) {
   if (tid == 0) {
     a.free_energy[s] = F;
     a.iterations[s] = it + 1;
-    double* tm = a.terms + 8 * (int64_t)s;
-    tm[0] = ecore; tm[1] = e2; tm[2] = e3; tm[3] = ea; tm[4] = ed; tm[5] = ts;
+    double* tm = a.terms + kTermCount * (int64_t)s;
+    tm[kTermCore] = ecore;
+    tm[kTermEs2] = e2;
+    tm[kTermEs3] = e3;
+    tm[kTermAes2] = ea;
+    tm[kTermD4] = ed;
+    tm[kTermEntropy] = ts;
+    tm[kTermPc] = ep;
     if (failed) {
       a.status[s] = kInternal;
     } else if (conv) {

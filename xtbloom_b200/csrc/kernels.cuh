@@ -149,6 +149,14 @@ struct ForceArgs {
 };
 
 void launch_force_pairs(const ForceArgs& f, int64_t max_pairs, cudaStream_t stream);
+
+// external point charges (k_pc.cu)
+void launch_pc_potential(const DevTopo& t, const int32_t* list, int count, double* vpc,
+                         cudaStream_t stream);
+void launch_pc_forces(const DevTopo& t, const int32_t* list, int count, const double* qsh,
+                      double* grad, double* pc_grad, double* pc_dq, cudaStream_t stream);
+void launch_pc_publish(const DevTopo& t, const int32_t* status, int nsys, const double* pc_grad,
+                       double* out, cudaStream_t stream);
 void launch_classical(const ForceArgs& f, int max_atoms, int max_shells, cudaStream_t stream);
 void launch_cn_chain(const ForceArgs& f, int max_atoms, cudaStream_t stream);
 
