@@ -329,8 +329,10 @@ XTBLOOM_API xtbloom_status_t xtbloom_result_owner_export_dltensor(
  * retained per-system intermediate of the context's most recent compute into
  * host memory, for stage-by-stage parity tests.  name is one of "cn",
  * "overlap", "h0", "density", "eigenvalues", "qsh", "dipoles", "quadrupoles",
- * "energy_terms", "gradient_terms".  Returns INVALID_ARGUMENT when the name,
- * system or capacity is wrong.  *count receives the number of doubles.
+ * "energy_terms", "point_charge_potential" (per shell), "point_charge_dq"
+ * (dE/dQ per point charge; system -1 returns every charge of the batch).
+ * Returns INVALID_ARGUMENT when the name, system or capacity is wrong.
+ * *count receives the number of doubles.
  */
 XTBLOOM_API xtbloom_status_t xtbloom_b200_debug_fetch(xtbloom_context_t* context, const char* name,
                                                       int64_t system, double* out,

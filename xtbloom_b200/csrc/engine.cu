@@ -1066,6 +1066,24 @@ xtbloom_status_t Engine::debug_fetch(const std::string& name, int64_t system, do
     *count = len;
     return XTBLOOM_STATUS_SUCCESS;
   }
+  if (name == "point_charge_dq" && system == -1) {
+    // the whole batch: dE/dQ for every point charge of the most recent call
+    if (!m.have_results || !m.have_pc) {
+      error = "the most recent compute had no point charges";
+      return XTBLOOM_STATUS_INVALID_ARGUMENT;
+    }
+    if (capacity < (size_t)m.npc) {
+      error = "capacity too small";
+      return XTBLOOM_STATUS_INVALID_ARGUMENT;
+    }
+    cudaSetDevice(device_);
+    if (cudaMemcpy(out, m.pc_dq.p, (size_t)m.npc * 8, cudaMemcpyDeviceToHost) != cudaSuccess) {
+      error = "device read failed";
+      return XTBLOOM_STATUS_INTERNAL_ERROR;
+    }
+    *count = (size_t)m.npc;
+    return XTBLOOM_STATUS_SUCCESS;
+  }
   if (!m.have_results || system < 0 || system >= m.nsys) {
     error = "no retained results for that system";
     return XTBLOOM_STATUS_INVALID_ARGUMENT;
