@@ -226,7 +226,7 @@ struct Engine::Impl {
   Dbuf qsh, dip, qp, pop_sh, pop_dip, pop_qp, e_core, vsh, vd, vq;
   Dbuf free_energy, terms;
   Dbuf mx_cur, mx_prev, mx_res, mx_df, mx_u, mx_omega;
-  Dbuf grad, acn, acn_d4;
+  Dbuf grad, acn, acn_d4, pot_acc;
   Dbuf out_energy, out_forces, out_charges;
   // external point charges of the current call
   Dbuf pc_off, pc_pos, pc_q, pc_gam, vpc, pc_grad, pc_dq, out_pcf;
@@ -516,7 +516,8 @@ xtbloom_status_t build_topology(Engine::Impl& m, const HostBatch& hb, cudaStream
        m.free_energy.reserve(B * d8) && m.terms.reserve(kTermCount * B * d8) &&
        m.mx_cur.reserve((size_t)m.total_vec * d8) && m.mx_prev.reserve((size_t)m.total_vec * d8) &&
        m.mx_res.reserve((size_t)m.total_vec * d8) && m.grad.reserve(3 * N * d8) &&
-       m.acn.reserve(N * d8) && m.acn_d4.reserve(N * d8) && m.out_energy.reserve(B * d8) &&
+       m.acn.reserve(N * d8) && m.acn_d4.reserve(N * d8) && m.pot_acc.reserve(10 * N * d8) &&
+       cudaMemsetAsync(m.pot_acc.p, 0, 10 * N * d8, s) == cudaSuccess && m.out_energy.reserve(B * d8) &&
        m.out_forces.reserve(3 * N * d8) && m.out_charges.reserve(N * d8);
   if (!ok) {
     error = "device allocation for the batch failed";
@@ -708,6 +709,7 @@ xtbloom_status_t Engine::compute(const ComputeRequest& req, std::string& error) 
   cudaMemsetAsync(m.converged.p, 0, B, s);
   cudaMemsetAsync(m.iterations.p, 0, B * 4, s);
   cudaMemsetAsync(m.terms.p, 0, kTermCount * B * 8, s);
+  cudaMemsetAsync(m.pot_acc.p, 0, 10 * N * 8, s);
   cudaMemcpyAsync(list, order, B * 4, cudaMemcpyDeviceToDevice, s);
 
   // first launch failure of any stage (a launch that fails does not run and
@@ -875,6 +877,7 @@ xtbloom_status_t Engine::compute(const ComputeRequest& req, std::string& error) 
   a.H = m.H.as<double>();
   a.P = m.P.as<double>();
   a.total_mat = m.total_mat;
+  a.pot_acc = m.pot_acc.as<double>();
   a.entropy = m.entropy.as<double>();
   a.free_energy = m.free_energy.as<double>();
   a.terms = m.terms.as<double>();

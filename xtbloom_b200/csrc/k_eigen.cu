@@ -231,60 +231,119 @@ __global__ void __launch_bounds__(512) k_tridiag(EigArgs g, int nloc) {
 // reflector with the updated block in the same pass over the packed triangle:
 //   (A) update the block's first column with (v_i, w_i); it gives x_{i+1};
 //   (B) v_{i+1}, tau_{i+1} from x_{i+1};
-//   (C) 32 x 32 tiles of the rest, dealt round-robin to the warps: update with
+//   (C) 16 x 32 tiles of the rest, dealt round-robin to the warps: update with
 //       (v_i, w_i), then accumulate A v_{i+1} (see fused_tile);
-//   (D) w_{i+1} = tau p - (tau/2)(p.v) v.
+//   (D) w_{i+1} = tau p - (tau/2)(p.v) v, kept as tau p and the scalar
+//       (tau/2)(p.v); readers of w apply the correction.
+// Four barriers per column: after (A)'s norm, (B), (C) and (D)'s dot product.
 // Reflectors are stored in the global matrix in the layout the back-transform
 // reads (row i, columns i+2..): the same as the global-memory kernel.
 // ---------------------------------------------------------------------------
 __device__ __forceinline__ int pk32(int r, int c) { return r * (r + 1) / 2 + c; }
 
-// One tile (rows R0.., columns C0.., R0 >= C0, local to the block that starts
-// at row/column o of the packed triangle, size m) for one warp: update every
-// element with (vi, wi), then lane j accumulates the transposed part of A vn
-// for column C0+j directly and keeps 32 row partials, which a butterfly
-// reduce-scatter (31 exchanges) leaves with lane i holding row R0+i.  Diagonal
-// tiles use their lower triangle once.  Results go to the warp's pw.
+// Block-wide sum with a single barrier: every warp posts its partial to
+// buf[warp] and every thread adds the posted partials.  Two reductions that
+// use the same buf must be separated by another barrier (the kernel below
+// alternates two buffers between its two reductions per column).
+template <int NW>
+__device__ __forceinline__ double block_sum1(double v, double* buf) {
+  v = warp_sum(v);
+  if ((threadIdx.x & 31) == 0) buf[threadIdx.x >> 5] = v;
+  __syncthreads();
+  double t = 0.0;
+#pragma unroll
+  for (int w = 0; w < NW; ++w) t += buf[w];
+  return t;
+}
+
+// One tile of 16 rows (R0..) and 32 columns (C0..) of the lower triangle of
+// the block that starts at row/column o of the packed storage (size m), for
+// one warp: update every element with (vi, wi), then lane j accumulates the
+// transposed part of A vn for column C0+j directly and keeps 16 row partials,
+// which a butterfly reduce-scatter (15 exchanges, then one across the half
+// warps) leaves with lane i (and i+16) holding row R0+i.  Elements on the
+// diagonal count once.  Results go to the warp's pw.  wi holds w + kw v (the
+// previous reflector's correction kw is applied here).  The tile's elements
+// are all loaded before any is stored and the row values come from registers
+// by shuffles, so the shared-memory loads issue back to back.
+constexpr int kTileRows = 16;
 __device__ __forceinline__ void fused_tile(double* L, int o, int m, int R0, int C0,
-                                           const double* vi, const double* wi, const double* vn,
-                                           double* pw, int lane, bool want_mv) {
+                                           const double* vi, const double* wi, double kw,
+                                           const double* vn, double* pw, int lane, bool want_mv) {
   const int cj = C0 + lane;
   const bool cok = cj < m;
   const double vn_c = cok ? vn[cj] : 0.0;
   const double vi_c = cok ? vi[cj] : 0.0;
-  const double wi_c = cok ? wi[cj] : 0.0;
-  const bool diag = R0 == C0;
-  double rp[32];
-  double col = 0.0;
-  int base = pk32(o + R0, o);
+  const double wi_c = cok ? fma(-kw, vi_c, wi[cj]) : 0.0;
+  const int rl = R0 + (lane & (kTileRows - 1));
+  const double vi_r = rl < m ? vi[rl] : 0.0;
+  const double wi_r = rl < m ? fma(-kw, vi_r, wi[rl]) : 0.0;
+  const double vn_r = rl < m ? vn[rl] : 0.0;
+  const int rows = min(kTileRows, m - R0);
+  const int dcol = cj - R0;            // element (R0+i, cj) is on/below the diagonal iff dcol <= i
+  double a[kTileRows];
+  const int base0 = pk32(o + R0, o) + cj;
+  {
+    int base = base0;
 #pragma unroll
-  for (int i = 0; i < 32; ++i) {
-    const int r = R0 + i;
-    const bool ok = r < m && cok && (!diag || lane <= i);
-    double a = 0.0;
-    const double vr = r < m ? vi[r] : 0.0, wr = r < m ? wi[r] : 0.0, nr = r < m ? vn[r] : 0.0;
-    if (ok) {
-      a = L[base + cj];
-      a -= vr * wi_c + wr * vi_c;
-      L[base + cj] = a;
+    for (int i = 0; i < kTileRows; ++i) {
+      const bool ok = i < rows && cok && dcol <= i;
+      a[i] = ok ? L[base] : 0.0;
+      base += o + R0 + i + 1;
     }
-    rp[i] = a * vn_c;
-    if (!diag || lane < i) col = fma(a, nr, col);
-    base += o + r + 1;
+  }
+  double col = 0.0;
+#pragma unroll
+  for (int i = 0; i < kTileRows; ++i) {
+    const double vr = __shfl_sync(0xffffffffu, vi_r, i);
+    const double wr = __shfl_sync(0xffffffffu, wi_r, i);
+    const double nr = __shfl_sync(0xffffffffu, vn_r, i);
+    const double u = a[i] - (vr * wi_c + wr * vi_c);
+    a[i] = dcol > i ? 0.0 : u;   // rows past m and columns past m give 0
+    if (dcol < i) col = fma(a[i], nr, col);
+  }
+  {
+    int base = base0;
+#pragma unroll
+    for (int i = 0; i < kTileRows; ++i) {
+      const bool ok = i < rows && cok && dcol <= i;
+      if (ok) L[base] = a[i];
+      base += o + R0 + i + 1;
+    }
   }
   if (!want_mv) return;
 #pragma unroll
-  for (int sh = 16; sh >= 1; sh >>= 1) {
+  for (int i = 0; i < kTileRows; ++i) a[i] *= vn_c;
+#pragma unroll
+  for (int sh = kTileRows / 2; sh >= 1; sh >>= 1) {
     const bool up = (lane & sh) != 0;
 #pragma unroll
     for (int k = 0; k < sh; ++k) {
-      const double send = up ? rp[k] : rp[k + sh];
-      const double keep = up ? rp[k + sh] : rp[k];
-      rp[k] = keep + __shfl_xor_sync(0xffffffffu, send, sh);
+      const double send = up ? a[k] : a[k + sh];
+      const double keep = up ? a[k + sh] : a[k];
+      a[k] = keep + __shfl_xor_sync(0xffffffffu, send, sh);
     }
   }
-  if (R0 + lane < m) pw[R0 + lane] += rp[0];
+  a[0] += __shfl_xor_sync(0xffffffffu, a[0], 16);
+  if (lane < kTileRows && rl < m) pw[rl] += a[0];
   if (cok) pw[cj] += col;
+}
+
+// Tiles of the lower triangle of an m x m block: row blocks of 16, column
+// blocks of 32; row blocks 2p and 2p+1 hold p+1 tiles each, so the tiles of
+// row blocks below 2p number p(p+1).
+__device__ __forceinline__ int tri_tiles(int m) {
+  const int nr = (m + kTileRows - 1) / kTileRows;
+  const int p = nr >> 1;
+  return p * (p + 1) + ((nr & 1) ? p + 1 : 0);
+}
+__device__ __forceinline__ void tri_tile(int tl, int& R, int& C) {
+  int p = (int)((sqrtf(4.0f * tl + 1.0f) - 1.0f) * 0.5f);
+  while ((p + 1) * (p + 2) <= tl) ++p;
+  while (p * (p + 1) > tl) --p;
+  const int rem = tl - p * (p + 1);
+  R = 2 * p + (rem > p ? 1 : 0);
+  C = rem > p ? rem - (p + 1) : rem;
 }
 
 template <int NT>
@@ -307,7 +366,7 @@ __global__ void __launch_bounds__(NT) k_tridiag_smem(EigArgs g, const int32_t* l
   double* wb0 = vb1 + nl;
   double* wb1 = wb0 + nl;
   double* priv = wb1 + nl;            // nw x nl
-  double* red = priv + nw * nl;       // 33
+  double* red = priv + nw * nl;       // 2 x 32 (alternating reduction buffers)
   __shared__ double s_alpha;
   for (int r = warp; r < nl; r += nw)
     for (int c = lane; c <= r; c += 32) L[pk32(r, c)] = ga[(int64_t)(i0 + r) * n + i0 + c];
@@ -319,6 +378,9 @@ __global__ void __launch_bounds__(NT) k_tridiag_smem(EigArgs g, const int32_t* l
     return;
   }
   int cur = 0;
+  // w of the current reflector is stored as tau p; kw = (tau/2)(tau p . v) is
+  // the correction w = tau p - kw v, applied where w is read.
+  double kw = 0.0;
   // Step i = -1 applies no update; its column gives reflector 0 of the block.
   for (int i = -1; i + 2 < nl; ++i) {
     const int o = i + 1, m = nl - o;
@@ -327,19 +389,20 @@ __global__ void __launch_bounds__(NT) k_tridiag_smem(EigArgs g, const int32_t* l
     double* vn = cur ? vb0 : vb1;
     double* wn = cur ? wb0 : wb1;
     const bool next = o + 3 <= nl;      // reflector o exists
-    // (A)
+    // (A) update the block's first column; its tail gives the next reflector
     double part = 0.0;
-    const double vi0 = vi[0], wi0 = wi[0];
+    const double vi0 = vi[0], wi0 = fma(-kw, vi0, wi[0]);
     for (int r = tid; r < m; r += NT) {
       const int idx = pk32(o + r, o);
-      const double c = L[idx] - (vi[r] * wi0 + wi[r] * vi0);
+      const double vr = vi[r];
+      const double c = L[idx] - (vr * wi0 + fma(-kw, vr, wi[r]) * vi0);
       L[idx] = c;
       if (r == 0) d[o] = c;
       if (r >= 1) vn[r - 1] = c;
       if (r == 1) s_alpha = c;
       if (r >= 2) part += c * c;
     }
-    const double xn2 = block_sum(part, red);
+    const double xn2 = block_sum1<nw>(part, red);
     // (B)
     double ti = 0.0;
     if (next) {
@@ -366,24 +429,21 @@ __global__ void __launch_bounds__(NT) k_tridiag_smem(EigArgs g, const int32_t* l
       for (int k = tid; k < m; k += NT) vn[k] = 0.0;
     }
     __syncthreads();
-    // (C)
+    // (C) rank-2 update of the rest of the block, fused with A v_next
     const int m1 = m - 1;
     {
-      const int nt = (m1 + 31) >> 5;
-      const int ntiles = nt * (nt + 1) / 2;
+      const int ntiles = tri_tiles(m1);
       double* pw = priv + warp * nl;
       const bool mv = next && ti != 0.0;
       for (int tl = warp; tl < ntiles; tl += nw) {
-        int R = (int)((sqrt(8.0 * tl + 1.0) - 1.0) * 0.5);   // tile row: R(R+1)/2 <= tl
-        while ((R + 1) * (R + 2) / 2 <= tl) ++R;
-        while (R * (R + 1) / 2 > tl) --R;
-        const int C = tl - R * (R + 1) / 2;
-        fused_tile(L, o + 1, m1, R << 5, C << 5, vi + 1, wi + 1, vn, pw, lane, mv);
+        int R, C;
+        tri_tile(tl, R, C);
+        fused_tile(L, o + 1, m1, R * kTileRows, C << 5, vi + 1, wi + 1, kw, vn, pw, lane, mv);
       }
     }
     __syncthreads();
     if (!next) break;
-    // (D)
+    // (D) w_next = tau p (stored) and its correction kw = (tau/2)(tau p . v)
     double pv = 0.0;
     for (int k = tid; k < m1; k += NT) {
       double t = 0.0;
@@ -396,10 +456,7 @@ __global__ void __launch_bounds__(NT) k_tridiag_smem(EigArgs g, const int32_t* l
       wn[k] = t;
       pv += t * vn[k];
     }
-    const double K = 0.5 * ti * block_sum(pv, red);
-    for (int k = tid; k < m1; k += NT) wn[k] -= K * vn[k];
-    for (int k = m1 + tid; k < nl; k += NT) wn[k] = vn[k] = 0.0;
-    __syncthreads();
+    kw = 0.5 * ti * block_sum1<nw>(pv, red + 32);
     cur ^= 1;
   }
   if (tid == 0) {
@@ -412,7 +469,7 @@ __global__ void __launch_bounds__(NT) k_tridiag_smem(EigArgs g, const int32_t* l
 }
 
 size_t tridiag_smem_bytes(int nl, int nt) {
-  return ((size_t)nl * (nl + 1) / 2 + (4 + nt / 32) * (size_t)nl + 40) * sizeof(double);
+  return ((size_t)nl * (nl + 1) / 2 + (4 + nt / 32) * (size_t)nl + 72) * sizeof(double);
 }
 
 // Largest trailing block the shared-memory kernel holds (227 KB per CTA).

@@ -10,6 +10,7 @@
 #include "classical.cuh"
 #include "kernels.cuh"
 
+#include <algorithm>
 #include <cfloat>
 
 namespace xtb {
@@ -55,6 +56,106 @@ void launch_sad_init(const SccArgs& a, cudaStream_t stream) {
 // Potentials from (qsh, dip, qp): vsh = gamma q + g3 q^2 + vat(atom);
 // vat, vd, vq from AES2 and the D4 charge response.
 // ---------------------------------------------------------------------------
+// Per-atom inputs of the pair loop, system-local, in shared memory: atomic
+// charges, D4 reference weights and their charge derivatives.
+__device__ __forceinline__ void potential_atoms(const SccArgs& a, const double* qsh, int64_t a0,
+                                                int na, double* qat, double* w, double* dwq) {
+  const DevTopo& t = a.t;
+  for (int i = threadIdx.x; i < na; i += blockDim.x) {
+    const int64_t g = a0 + i;
+    double q = 0.0;
+    for (int sh = t.atom_sh[g]; sh < t.atom_sh[g + 1]; ++sh) q += qsh[sh];
+    qat[i] = q;
+    d4_weights(t, t.Z[g], a.cn_d4[g], q, w + kMaxD4Refs * i, nullptr, dwq + kMaxD4Refs * i);
+  }
+}
+
+// Pair (si > fi) contributions to the atomic potential vat, the dipole
+// potential svd and the quadrupole potential svq (shared-memory atomics).
+__device__ __forceinline__ void potential_pair(const SccArgs& a, const double* dip, const double* qp,
+                                               int64_t a0, int64_t p, const double* qat,
+                                               const double* w, const double* dwq, double* vat,
+                                               double* svd, double* svq) {
+  const DevTopo& t = a.t;
+  int64_t si, fi;
+  pair_from_index(p, si, fi);      // si > fi
+  const int f = (int)fi, sc = (int)si;
+  const int64_t gf = a0 + f, gs = a0 + sc;
+  const double d[3] = {t.pos[3 * gf] - t.pos[3 * gs], t.pos[3 * gf + 1] - t.pos[3 * gs + 1],
+                       t.pos[3 * gf + 2] - t.pos[3 * gs + 2]};
+  const double r2 = d[0] * d[0] + d[1] * d[1] + d[2] * d[2];
+  const double r = sqrt(r2);
+  // AES2
+  double k3, k5;
+  aes2_kernels(r, 0.5 * (a.mrad[gf] + a.mrad[gs]), k3, k5);
+  const double* df = dip + 3 * gf;
+  const double* ds = dip + 3 * gs;
+  const double* qf = qp + 6 * gf;
+  const double* qs = qp + 6 * gs;
+  const double sqv[6] = {d[0] * d[0] * k5, 2.0 * d[0] * d[1] * k5, d[1] * d[1] * k5,
+                         2.0 * d[0] * d[2] * k5, 2.0 * d[1] * d[2] * k5, d[2] * d[2] * k5};
+  const double iso = r2 * k5;
+  double pf = 0.0, ps = 0.0, sdf = 0.0, sds = 0.0, tqf = 0.0, tqs = 0.0;
+  for (int c = 0; c < 3; ++c) {
+    pf += d[c] * df[c];
+    ps += d[c] * ds[c];
+    sdf += d[c] * k3 * df[c];
+    sds += d[c] * k3 * ds[c];
+  }
+  for (int c = 0; c < 6; ++c) {
+    tqf += sqv[c] * qf[c];
+    tqs += sqv[c] * qs[c];
+  }
+  double vf = sds + tqs;
+  double vs = -sdf + tqf;
+  for (int c = 0; c < 3; ++c) {
+    atomicAdd(&svd[3 * f + c], -qat[sc] * d[c] * k3 + iso * ds[c] - 3.0 * k5 * d[c] * ps);
+    atomicAdd(&svd[3 * sc + c], qat[f] * d[c] * k3 + iso * df[c] - 3.0 * k5 * d[c] * pf);
+  }
+  for (int c = 0; c < 6; ++c) {
+    atomicAdd(&svq[6 * f + c], qat[sc] * sqv[c]);
+    atomicAdd(&svq[6 * sc + c], qat[f] * sqv[c]);
+  }
+  // D4 charge response
+  double damp, ddamp;
+  const int zf = t.Z[gf], zs = t.Z[gs];
+  d4_pair_damping(t, zf, zs, r2, damp, ddamp);
+  if (damp != 0.0) {
+    double cf, cs;
+    d4_c6(t, zf, zs, w + kMaxD4Refs * f, w + kMaxD4Refs * sc, dwq + kMaxD4Refs * f,
+          dwq + kMaxD4Refs * sc, &cf, &cs);
+    vf -= cf * damp;
+    vs -= cs * damp;
+  }
+  atomicAdd(&vat[f], vf);
+  atomicAdd(&vat[sc], vs);
+}
+
+// Shell potentials of system s from the finished atomic potentials: ES2 (warp
+// per shell row) + ES3 + atomic potential (+ external point charges).
+__device__ __forceinline__ void potential_shells(const SccArgs& a, int s, const double* sq,
+                                                 const double* vat) {
+  const DevTopo& t = a.t;
+  const int64_t a0 = t.atom_off[s];
+  const int64_t s0 = t.shell_off[s];
+  const int ns = (int)(t.shell_off[s + 1] - s0);
+  const double* gam = a.gam + t.gam_off[s];
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nw = blockDim.x >> 5;
+  for (int i = warp; i < ns; i += nw) {
+    const double* row = gam + (int64_t)i * ns;
+    double acc = 0.0;
+    for (int j = lane; j < ns; j += 32) acc = fma(row[j], sq[j], acc);
+    acc = warp_sum(acc);
+    if (lane == 0) {
+      const int sh = (int)(s0 + i);
+      const double q = sq[i];
+      a.vsh[sh] = acc + t.sh_g3[sh] * q * q + vat[t.sh_atom[sh] - a0] +
+                  (t.vpc != nullptr ? t.vpc[sh] : 0.0);
+    }
+  }
+}
+
+// One CTA per system.
 __global__ void __launch_bounds__(256) k_potential(SccArgs a, const double* qsh, const double* dip,
                                                    const double* qp) {
   extern __shared__ double sm[];
@@ -72,92 +173,22 @@ __global__ void __launch_bounds__(256) k_potential(SccArgs a, const double* qsh,
   double* dwq = w + kMaxD4Refs * na;        // na * 7
   double* sq = dwq + kMaxD4Refs * na;       // ns
   const int tid = threadIdx.x, bs = blockDim.x;
+  potential_atoms(a, qsh, a0, na, qat, w, dwq);
   for (int i = tid; i < na; i += bs) {
     const int64_t g = a0 + i;
-    double q = 0.0;
-    for (int sh = t.atom_sh[g]; sh < t.atom_sh[g + 1]; ++sh) q += qsh[sh];
-    qat[i] = q;
     vat[i] = 0.0;
     const double dk2 = 2.0 * t.at_dk[g], qk2 = 2.0 * t.at_qk[g];
     for (int c = 0; c < 3; ++c) svd[3 * i + c] = dk2 * dip[3 * g + c];
     const double scl[6] = {1.0, 2.0, 1.0, 2.0, 2.0, 1.0};
     for (int c = 0; c < 6; ++c) svq[6 * i + c] = qk2 * scl[c] * qp[6 * g + c];
-    const int z = t.Z[g];
-    d4_weights(t, z, a.cn_d4[g], q, w + kMaxD4Refs * i, nullptr, dwq + kMaxD4Refs * i);
   }
   for (int i = tid; i < ns; i += bs) sq[i] = qsh[s0 + i];
   __syncthreads();
   const int64_t npair = (int64_t)na * (na - 1) / 2;
-  for (int64_t p = tid; p < npair; p += bs) {
-    int64_t si, fi;
-    pair_from_index(p, si, fi);      // si > fi
-    const int f = (int)fi, sc = (int)si;
-    const int64_t gf = a0 + f, gs = a0 + sc;
-    const double d[3] = {t.pos[3 * gf] - t.pos[3 * gs], t.pos[3 * gf + 1] - t.pos[3 * gs + 1],
-                         t.pos[3 * gf + 2] - t.pos[3 * gs + 2]};
-    const double r2 = d[0] * d[0] + d[1] * d[1] + d[2] * d[2];
-    const double r = sqrt(r2);
-    // AES2
-    double k3, k5;
-    aes2_kernels(r, 0.5 * (a.mrad[gf] + a.mrad[gs]), k3, k5);
-    const double* df = dip + 3 * gf;
-    const double* ds = dip + 3 * gs;
-    const double* qf = qp + 6 * gf;
-    const double* qs = qp + 6 * gs;
-    const double sqv[6] = {d[0] * d[0] * k5, 2.0 * d[0] * d[1] * k5, d[1] * d[1] * k5,
-                           2.0 * d[0] * d[2] * k5, 2.0 * d[1] * d[2] * k5, d[2] * d[2] * k5};
-    const double iso = r2 * k5;
-    double pf = 0.0, ps = 0.0, sdf = 0.0, sds = 0.0, tqf = 0.0, tqs = 0.0;
-    for (int c = 0; c < 3; ++c) {
-      pf += d[c] * df[c];
-      ps += d[c] * ds[c];
-      sdf += d[c] * k3 * df[c];
-      sds += d[c] * k3 * ds[c];
-    }
-    for (int c = 0; c < 6; ++c) {
-      tqf += sqv[c] * qf[c];
-      tqs += sqv[c] * qs[c];
-    }
-    double vf = sds + tqs;
-    double vs = -sdf + tqf;
-    for (int c = 0; c < 3; ++c) {
-      atomicAdd(&svd[3 * f + c], -qat[sc] * d[c] * k3 + iso * ds[c] - 3.0 * k5 * d[c] * ps);
-      atomicAdd(&svd[3 * sc + c], qat[f] * d[c] * k3 + iso * df[c] - 3.0 * k5 * d[c] * pf);
-    }
-    for (int c = 0; c < 6; ++c) {
-      atomicAdd(&svq[6 * f + c], qat[sc] * sqv[c]);
-      atomicAdd(&svq[6 * sc + c], qat[f] * sqv[c]);
-    }
-    // D4 charge response
-    double damp, ddamp;
-    const int zf = t.Z[gf], zs = t.Z[gs];
-    d4_pair_damping(t, zf, zs, r2, damp, ddamp);
-    if (damp != 0.0) {
-      double cf, cs;
-      d4_c6(t, zf, zs, w + kMaxD4Refs * f, w + kMaxD4Refs * sc, dwq + kMaxD4Refs * f,
-            dwq + kMaxD4Refs * sc, &cf, &cs);
-      vf -= cf * damp;
-      vs -= cs * damp;
-    }
-    atomicAdd(&vat[f], vf);
-    atomicAdd(&vat[sc], vs);
-  }
+  for (int64_t p = tid; p < npair; p += bs)
+    potential_pair(a, dip, qp, a0, p, qat, w, dwq, vat, svd, svq);
   __syncthreads();
-  // shell potentials: ES2 (warp per shell row) + ES3 + atomic potential
-  const double* gam = a.gam + t.gam_off[s];
-  const int lane = tid & 31, warp = tid >> 5, nw = bs >> 5;
-  for (int i = warp; i < ns; i += nw) {
-    const double* row = gam + (int64_t)i * ns;
-    double acc = 0.0;
-    for (int j = lane; j < ns; j += 32) acc = fma(row[j], sq[j], acc);
-    acc = warp_sum(acc);
-    if (lane == 0) {
-      const int sh = (int)(s0 + i);
-      const double q = sq[i];
-      a.vsh[sh] = acc + t.sh_g3[sh] * q * q + vat[t.sh_atom[sh] - a0] +
-                  (t.vpc != nullptr ? t.vpc[sh] : 0.0);
-    }
-  }
+  potential_shells(a, s, sq, vat);
   for (int i = tid; i < na; i += bs) {
     const int64_t g = a0 + i;
     for (int c = 0; c < 3; ++c) a.vd[3 * g + c] = svd[3 * i + c];
@@ -165,13 +196,97 @@ __global__ void __launch_bounds__(256) k_potential(SccArgs a, const double* qsh,
   }
 }
 
+// Latency form for few systems: blockIdx.x of gridDim.x CTAs of system
+// blockIdx.y takes a contiguous slice of the atom pairs and adds its partial
+// atomic, dipole and quadrupole potentials to acc (10 per atom, zero on entry).
+__global__ void __launch_bounds__(256) k_potential_pairs(SccArgs a, const double* qsh,
+                                                         const double* dip, const double* qp,
+                                                         double* acc) {
+  extern __shared__ double sm[];
+  const DevTopo& t = a.t;
+  const int s = a.list[blockIdx.y];
+  const int64_t a0 = t.atom_off[s];
+  const int na = (int)(t.atom_off[s + 1] - a0);
+  const int64_t npair = (int64_t)na * (na - 1) / 2;
+  const int64_t per = (npair + gridDim.x - 1) / gridDim.x;
+  const int64_t p0 = (int64_t)blockIdx.x * per, p1 = min(npair, p0 + per);
+  if (p0 >= p1) return;   // uniform over the block
+  double* qat = sm;
+  double* loc = qat + na;                   // na * 10: vat, svd[3], svq[6] per atom
+  double* w = loc + 10 * na;                // na * 7
+  double* dwq = w + kMaxD4Refs * na;        // na * 7
+  double* vat = loc;
+  double* svd = loc + na;
+  double* svq = loc + 4 * na;
+  const int tid = threadIdx.x, bs = blockDim.x;
+  potential_atoms(a, qsh, a0, na, qat, w, dwq);
+  for (int i = tid; i < 10 * na; i += bs) loc[i] = 0.0;
+  __syncthreads();
+  for (int64_t p = p0 + tid; p < p1; p += bs)
+    potential_pair(a, dip, qp, a0, p, qat, w, dwq, vat, svd, svq);
+  __syncthreads();
+  for (int i = tid; i < na; i += bs) {
+    double* dst = acc + 10 * (a0 + i);
+    atomicAdd(dst, vat[i]);
+    for (int c = 0; c < 3; ++c) atomicAdd(dst + 1 + c, svd[3 * i + c]);
+    for (int c = 0; c < 6; ++c) atomicAdd(dst + 4 + c, svq[6 * i + c]);
+  }
+}
+
+// Completes the latency form: onsite multipole terms, shell potentials, and
+// clears acc for the next use.
+__global__ void __launch_bounds__(256) k_potential_finish(SccArgs a, const double* qsh,
+                                                          const double* dip, const double* qp,
+                                                          double* acc) {
+  extern __shared__ double sm[];
+  const DevTopo& t = a.t;
+  const int s = a.list[blockIdx.x];
+  const int64_t a0 = t.atom_off[s];
+  const int na = (int)(t.atom_off[s + 1] - a0);
+  const int64_t s0 = t.shell_off[s];
+  const int ns = (int)(t.shell_off[s + 1] - s0);
+  double* vat = sm;
+  double* sq = vat + na;
+  const int tid = threadIdx.x, bs = blockDim.x;
+  const double scl[6] = {1.0, 2.0, 1.0, 2.0, 2.0, 1.0};
+  for (int i = tid; i < na; i += bs) {
+    const int64_t g = a0 + i;
+    double* src = acc + 10 * g;
+    vat[i] = src[0];
+    const double dk2 = 2.0 * t.at_dk[g], qk2 = 2.0 * t.at_qk[g];
+    for (int c = 0; c < 3; ++c) a.vd[3 * g + c] = dk2 * dip[3 * g + c] + src[1 + c];
+    for (int c = 0; c < 6; ++c) a.vq[6 * g + c] = qk2 * scl[c] * qp[6 * g + c] + src[4 + c];
+    for (int c = 0; c < 10; ++c) src[c] = 0.0;
+  }
+  for (int i = tid; i < ns; i += bs) sq[i] = qsh[s0 + i];
+  __syncthreads();
+  potential_shells(a, s, sq, vat);
+}
+
 void launch_potential(const SccArgs& a, const double* qsh, const double* dip, const double* qp,
                       int max_atoms, int max_shells, cudaStream_t stream) {
   if (a.count == 0) return;
-  const size_t sm = ((size_t)(11 + 2 * kMaxD4Refs) * max_atoms + max_shells + 8) * sizeof(double);
-  static const size_t attr = allow_max_dynamic_smem(k_potential);
-  (void)attr;
-  k_potential<<<a.count, 256, sm, stream>>>(a, qsh, dip, qp);
+  const int sms = sm_count();
+  const int64_t max_pairs = (int64_t)max_atoms * (max_atoms - 1) / 2;
+  // With fewer systems than SMs, spread each system's pairs over CTAs (at
+  // least 64 pairs each) so that the whole GPU works on the few systems left.
+  const int parts = a.count * 2 > sms || a.pot_acc == nullptr
+                        ? 1
+                        : (int)std::max<int64_t>(1, std::min<int64_t>((max_pairs + 63) / 64,
+                                                                      2 * sms / a.count));
+  if (parts == 1) {
+    const size_t sm = ((size_t)(11 + 2 * kMaxD4Refs) * max_atoms + max_shells + 8) * sizeof(double);
+    static const size_t attr = allow_max_dynamic_smem(k_potential);
+    (void)attr;
+    k_potential<<<a.count, 256, sm, stream>>>(a, qsh, dip, qp);
+    return;
+  }
+  const size_t sm1 = ((size_t)(11 + 2 * kMaxD4Refs) * max_atoms + 8) * sizeof(double);
+  static const size_t attr1 = allow_max_dynamic_smem(k_potential_pairs);
+  (void)attr1;
+  k_potential_pairs<<<dim3(parts, a.count), 256, sm1, stream>>>(a, qsh, dip, qp, a.pot_acc);
+  const size_t sm2 = ((size_t)max_atoms + max_shells + 8) * sizeof(double);
+  k_potential_finish<<<a.count, 256, sm2, stream>>>(a, qsh, dip, qp, a.pot_acc);
 }
 
 // ---------------------------------------------------------------------------

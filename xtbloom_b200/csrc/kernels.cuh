@@ -71,6 +71,7 @@ struct SccArgs {
   double* H;
   const double* P;
   int64_t total_mat;
+  double* pot_acc;    // 10 per atom, all zero between uses (pair-split potential)
   // per system energies / status
   const double* entropy;
   double* free_energy;
