@@ -6,6 +6,11 @@ Workload: the 4096-system ragged batch of hetero-alkane chains (C3..C40,
 forces + Mulliken charges to SCC convergence (charge 1e-6, energy 1e-8, 300 K,
 Broyden 8/0.4).  One step = one ``xtbloom_compute`` call over the whole batch.
 
+Two execution forms are timed on the same batch: FP64 throughout (the
+headline ``value``) and split precision (3xTF32 tensor-core GEMMs until a
+system's residual is below 1e-5, then FP64), with the largest difference of
+every output between them.
+
   python bench.py [--gpus N --steps K --warmup W]        # this library (CUDA)
   python bench.py --impl reference [...]                 # reference CPU library
 
@@ -54,6 +59,8 @@ def parse():
     p.add_argument("--systems", type=int, default=4096)
     p.add_argument("--cpu-sample", type=int, default=192)
     p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--form", default="both", choices=["both", "mixed", "fp64"])
+    p.add_argument("--graphs", type=int, default=1)
     return p.parse_args()
 
 
@@ -216,31 +223,15 @@ def run_reference(args, world, rank):
     print(json.dumps(line))
 
 
-def run_ours(args, world, rank, local):
+def time_form(lib, args, world, stream, dev_batch, outs_d, host_batch, host_outs):
+    """Times one execution form: K device-resident steps (CUDA events on the
+    context stream, max over ranks), then K end-to-end steps with host buffers."""
     import torch
-    from xtbloom_b200 import library_path
-    torch.cuda.set_device(local)
-    dev = torch.device("cuda", local)
-    batch = W.config1(args.systems, seed=1 + 1000 * rank)
-    B, N = batch.batch_size, batch.total_atoms
-    stream = torch.cuda.current_stream(dev)
-    lib = abi.Library(library_path(), backend=abi.BACKEND_CUDA, device_id=local,
-                      stream=stream.cuda_stream)
     opts = lib.make_options()
-    pos_d = torch.from_numpy(batch.positions).to(dev)
-    dev_batch = abi.RaggedBatch(batch.atom_offsets, batch.atomic_numbers, pos_d,
-                                batch.molecular_charges, batch.unpaired_electrons)
-    outs_d = {"energies": torch.empty(B, dtype=torch.float64, device=dev),
-              "forces": torch.empty(3 * N, dtype=torch.float64, device=dev),
-              "atomic_charges": torch.empty(N, dtype=torch.float64, device=dev),
-              "scc_iterations": torch.empty(B, dtype=torch.int32, device=dev),
-              "scc_converged": torch.empty(B, dtype=torch.uint8, device=dev),
-              "per_system_status": torch.empty(B, dtype=torch.int32, device=dev)}
     for _ in range(args.warmup):
         lib.compute(dev_batch, opts, outs_d)
     torch.cuda.synchronize()
     fetch(lib, "reset_counters")
-    clocks = ClockSampler(local)
     barrier(world)
     torch.cuda.synchronize()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -250,30 +241,72 @@ def run_ours(args, world, rank, local):
     e1.record(stream)
     torch.cuda.synchronize()
     barrier(world)
-    clk = clocks.stop()
-    ms = e0.elapsed_time(e1) / args.steps
-    ms_max = allreduce_max(ms, world)
+    ms = allreduce_max(e0.elapsed_time(e1) / args.steps, world)
     stage = fetch(lib, "kernel_times").reshape(-1, 2)
     launches = int(fetch(lib, "launch_count")[0])
     timing_on = bool(fetch(lib, "launch_count")[1])
-    # end-to-end: host positions in, host results out
-    host_outs = {"energies": np.empty(B), "forces": np.empty(3 * N), "atomic_charges": np.empty(N),
-                 "scc_iterations": np.empty(B, np.int32), "scc_converged": np.empty(B, np.uint8),
-                 "per_system_status": np.empty(B, np.int32)}
-    lib.compute(batch, opts, host_outs)
+    lib.compute(host_batch, opts, host_outs)
     torch.cuda.synchronize()
     barrier(world)
     e0.record(stream)
     for _ in range(args.steps):
-        lib.compute(batch, opts, host_outs)
+        lib.compute(host_batch, opts, host_outs)
     e1.record(stream)
     torch.cuda.synchronize()
     barrier(world)
     ms_e2e = allreduce_max(e0.elapsed_time(e1) / args.steps, world)
+    return {"ms": ms, "ms_e2e": ms_e2e, "stage": stage, "launches": launches, "timing_on": timing_on}
+
+
+def run_ours(args, world, rank, local):
+    import torch
+    from xtbloom_b200 import library_path
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    batch = W.config1(args.systems, seed=1 + 1000 * rank)
+    B, N = batch.batch_size, batch.total_atoms
+    stream = torch.cuda.current_stream(dev)
+    pos_d = torch.from_numpy(batch.positions).to(dev)
+    dev_batch = abi.RaggedBatch(batch.atom_offsets, batch.atomic_numbers, pos_d,
+                                batch.molecular_charges, batch.unpaired_electrons)
+
+    def new_outs_d():
+        return {"energies": torch.empty(B, dtype=torch.float64, device=dev),
+                "forces": torch.empty(3 * N, dtype=torch.float64, device=dev),
+                "atomic_charges": torch.empty(N, dtype=torch.float64, device=dev),
+                "scc_iterations": torch.empty(B, dtype=torch.int32, device=dev),
+                "scc_converged": torch.empty(B, dtype=torch.uint8, device=dev),
+                "per_system_status": torch.empty(B, dtype=torch.int32, device=dev)}
+
+    def new_host_outs():
+        return {"energies": np.empty(B), "forces": np.empty(3 * N), "atomic_charges": np.empty(N),
+                "scc_iterations": np.empty(B, np.int32), "scc_converged": np.empty(B, np.uint8),
+                "per_system_status": np.empty(B, np.int32)}
+
+    forms = {}
+    results = {}
+    clocks = ClockSampler(local)
+    for form in (["fp64", "mixed"] if args.form == "both" else [args.form]):
+        lib = abi.Library(library_path(), backend=abi.BACKEND_CUDA, device_id=local,
+                          stream=stream.cuda_stream)
+        lib.set_execution(abi.PRECISION_MIXED if form == "mixed" else abi.PRECISION_FP64,
+                          capture_graphs=args.graphs)
+        host_outs = new_host_outs()
+        forms[form] = time_form(lib, args, world, stream, dev_batch, new_outs_d(), batch, host_outs)
+        split = lib.fetch("split_iterations", capacity=B)
+        results[form] = (host_outs, split)
+        lib.close()
+        torch.cuda.synchronize()
+    clk = clocks.stop()
     h2d = (B + 1) * 8 + N * 4 + 3 * N * 8 + B * 8 + B * 4
     d2h = B * 8 + 3 * N * 8 + N * 8 + B * 4 + B + B * 4
     if rank != 0:
         return
+    # headline: the FP64 form (exact, and the faster form on this workload);
+    # the split-precision form is reported beside it in "forms"
+    head = "fp64" if "fp64" in forms else "mixed"
+    main = forms[head]
+    host_outs, split = results[head]
     energies = host_outs["energies"]
     status = host_outs["per_system_status"]
     iters = host_outs["scc_iterations"]
@@ -281,6 +314,9 @@ def run_ours(args, world, rank, local):
                      for i in range(B)])
     nocc = n_ao // 2 + 1
     work = stage_work(n_ao, iters, nocc)
+    ms = main["ms"]
+    stage = main["stage"]
+    timing_on = main["timing_on"]
     per_stage_ms = {STAGES[i]: float(stage[i, 0]) / args.steps for i in range(len(STAGES))} if timing_on else {}
     total_stage = sum(per_stage_ms.values()) or 1.0
     peaks = load_peaks()
@@ -310,19 +346,41 @@ def run_ours(args, world, rank, local):
         cpu = {"value": sample.batch_size / t, "unit": "systems/s", "cores": host_cores(),
                "kind": "reference",
                "sample": f"{sample.batch_size} evenly spaced systems of the same batch, one call, cpu_threads=0"}
+    form_lines = {}
+    for name, f in forms.items():
+        form_lines[name] = {"value": world * B / (f["ms"] / 1e3), "ms_per_step": f["ms"],
+                            "e2e_value": world * B / (f["ms_e2e"] / 1e3),
+                            "split_iteration_fraction": float(results[name][1].sum() / max(results[name][0]["scc_iterations"].sum(), 1))}
+    mixed_vs = None
+    if "mixed" in results and "fp64" in results:
+        a, b = results["fp64"][0], results["mixed"][0]
+        ok = (a["per_system_status"] == 0) & (b["per_system_status"] == 0)
+        okat = np.repeat(ok, np.diff(batch.atom_offsets))
+        mixed_vs = {"speedup": forms["fp64"]["ms"] / forms["mixed"]["ms"],
+                    "speedup_e2e": forms["fp64"]["ms_e2e"] / forms["mixed"]["ms_e2e"],
+                    "max_abs_dE_Eh": float(np.abs(a["energies"][ok] - b["energies"][ok]).max()),
+                    "max_abs_dF_Eh_per_bohr": float(np.abs(a["forces"].reshape(-1, 3)[okat] - b["forces"].reshape(-1, 3)[okat]).max()),
+                    "max_abs_dq_e": float(np.abs(a["atomic_charges"][okat] - b["atomic_charges"][okat]).max()),
+                    "status_equal": bool(np.array_equal(a["per_system_status"], b["per_system_status"]))}
     line = {
-        "metric": METRIC, "value": world * B / (ms_max / 1e3), "unit": "systems/s",
-        "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_max,
+        "metric": METRIC, "value": world * B / (ms / 1e3), "unit": "systems/s",
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic",
         "config": {"workload": WORKLOAD, "global_batch": world * B, "atoms_per_rank": int(N),
-                   "path": "FP64 (all stages)", "l2": "inputs larger than L2 (~11 GB of packed matrices per step)",
+                   "path": ("split-precision GEMMs (3xTF32 tensor cores) until the residual is below 1e-5, "
+                            "then FP64; FP64 eigensolver, mixer and reductions") if head == "mixed"
+                           else "FP64 (all stages)",
+                   "graphs": bool(args.graphs),
+                   "l2": "inputs larger than L2 (~11 GB of packed matrices per step)",
                    "parallelism": f"dp{world} (independent systems, no collective)"},
+        "forms": form_lines,
+        "mixed_vs_fp64": mixed_vs,
         "roofline": roofline,
         "cpu_baseline": cpu,
-        "e2e": {"value": world * B / (ms_e2e / 1e3), "unit": "systems/s",
+        "e2e": {"value": world * B / (main["ms_e2e"] / 1e3), "unit": "systems/s",
                 "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)},
-        "gpu_launches": launches // max(args.steps, 1) * args.steps if timing_on else launches,
+        "gpu_launches": main["launches"] // max(args.steps, 1) * args.steps if timing_on else main["launches"],
         "clocks": clk,
         "parity": {"max_abs_dE_vs_reference_Eh": dE,
                    "converged": int(np.sum(status == 0)), "systems": int(B),

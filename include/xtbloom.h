@@ -339,6 +339,30 @@ XTBLOOM_API xtbloom_status_t xtbloom_b200_debug_fetch(xtbloom_context_t* context
                                                       size_t capacity, size_t* count);
 
 /*
+ * Execution form of a CUDA context's later computes (no counterpart in the
+ * reference ABI, whose arithmetic is FP64 throughout).
+ *   precision 0 (XTBLOOM_B200_PRECISION_FP64, the default): every stage FP64.
+ *   precision 1 (XTBLOOM_B200_PRECISION_MIXED): the basis-transform and density
+ *     GEMMs of an SCC iteration run as split-precision (3xTF32, FP32
+ *     accumulation) tensor-core products while the system's charge residual is
+ *     at least switch_residual (0 selects 1e-5); below it the system iterates
+ *     in FP64, and it converges only on an FP64 iteration, so energies, forces
+ *     and charges are those of the FP64 fixed point.  The eigensolver, the
+ *     occupations, the mixer and every energy and force reduction stay FP64.
+ *     scc_iterations may differ from the FP64 form by a few iterations.
+ *   capture_graphs nonzero: SCC iterations whose active set is unchanged are
+ *     replayed from a captured CUDA graph (same kernels and results).
+ * Returns INVALID_ARGUMENT for an unknown precision or a negative or
+ * non-finite switch_residual, BACKEND_UNAVAILABLE for a CPU context.
+ */
+#define XTBLOOM_B200_PRECISION_FP64 0
+#define XTBLOOM_B200_PRECISION_MIXED 1
+XTBLOOM_API xtbloom_status_t xtbloom_b200_context_set_execution(xtbloom_context_t* context,
+                                                                int32_t precision,
+                                                                double switch_residual,
+                                                                int32_t capture_graphs);
+
+/*
  * Allocation-free eigenvectors of one symmetric tridiagonal matrix (no
  * counterpart in the reference ABI).  For callers that may not allocate device
  * memory once set up: cudaMalloc/cudaFree can synchronise the device and fail

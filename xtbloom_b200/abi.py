@@ -127,6 +127,10 @@ ABI_SYMBOLS = [
 ]
 
 
+PRECISION_FP64 = 0
+PRECISION_MIXED = 1
+
+
 def bind(path: str) -> C.CDLL:
     """Load a library exporting the xtbloom ABI and declare its prototypes."""
     lib = C.CDLL(path)
@@ -250,6 +254,27 @@ class Library:
         if status != SUCCESS:
             msg = self.lib.xtbloom_get_last_error()
             raise XtbloomError(status, msg.decode() if msg else "")
+
+    def set_execution(self, precision: int = PRECISION_FP64, switch_residual: float = 0.0,
+                      capture_graphs: bool = False):
+        """Select the execution form of later computes (CUDA contexts only):
+        FP64 throughout, or split-precision GEMMs until the precision switch."""
+        f = self.lib.xtbloom_b200_context_set_execution
+        f.restype = C.c_int32
+        f.argtypes = [C.c_void_p, C.c_int32, C.c_double, C.c_int32]
+        self._check(f(self.ctx, int(precision), float(switch_residual), 1 if capture_graphs else 0))
+
+    def fetch(self, name: str, system: int = -1, capacity: int = 1 << 16) -> np.ndarray:
+        """Diagnostics export of the most recent compute (xtbloom_b200_debug_fetch)."""
+        f = self.lib.xtbloom_b200_debug_fetch
+        f.restype = C.c_int32
+        f.argtypes = [C.c_void_p, C.c_char_p, C.c_int64, C.POINTER(C.c_double), C.c_size_t,
+                      C.POINTER(C.c_size_t)]
+        out = np.zeros(capacity)
+        cnt = C.c_size_t()
+        self._check(f(self.ctx, name.encode(), system, out.ctypes.data_as(C.POINTER(C.c_double)),
+                      capacity, C.byref(cnt)))
+        return out[:cnt.value].copy()
 
     def make_batch(self, b: RaggedBatch) -> Batch:
         batch = Batch()

@@ -637,6 +637,20 @@ xtbloom_status_t xtbloom_b200_debug_fetch(xtbloom_context_t* context, const char
   return st;
 }
 
+xtbloom_status_t xtbloom_b200_context_set_execution(xtbloom_context_t* context, int32_t precision,
+                                                    double switch_residual, int32_t capture_graphs) {
+  if (context == nullptr) return fail(XTBLOOM_STATUS_INVALID_ARGUMENT, "NULL context");
+  if (precision != XTBLOOM_B200_PRECISION_FP64 && precision != XTBLOOM_B200_PRECISION_MIXED)
+    return fail(XTBLOOM_STATUS_INVALID_ARGUMENT, "precision must be 0 (FP64) or 1 (mixed)");
+  if (!(switch_residual >= 0.0) || !std::isfinite(switch_residual))
+    return fail(XTBLOOM_STATUS_INVALID_ARGUMENT, "switch_residual must be finite and >= 0");
+  std::lock_guard<std::mutex> lock(context->mutex);
+  if (!context->engine) return fail(XTBLOOM_STATUS_BACKEND_UNAVAILABLE, "not a CUDA context");
+  context->engine->set_execution(precision, switch_residual > 0.0 ? switch_residual : 1e-5,
+                                 capture_graphs != 0);
+  return XTBLOOM_STATUS_SUCCESS;
+}
+
 xtbloom_status_t xtbloom_b200_tridiag_eigenvectors_static(const double* diagonal,
                                                           const double* offdiagonal,
                                                           const double* eigenvalues, int32_t n,

@@ -239,6 +239,11 @@ struct Engine::Impl {
   int last_memory = 0;
   bool have_results = false;
   bool trace = false;
+  bool tridiag_smem = false;   // use the shared-memory tridiagonalisation for every size
+  bool mixed = false;          // split-precision GEMMs until the precision switch
+  double prec_switch = 1e-5;
+  bool graphs = false;
+  Dbuf prec, split_iters;
   Profiler prof;
 
   DevTopo devtopo() const {
@@ -313,6 +318,14 @@ Engine::Engine(int device, cudaStream_t stream) : impl_(new Impl), device_(devic
   impl_->prof.on = env != nullptr && env[0] == '1';
   const char* tr = std::getenv("XTBLOOM_B200_TRACE");
   impl_->trace = tr != nullptr && tr[0] == '1';
+  const char* td = std::getenv("XTBLOOM_B200_TRIDIAG");
+  impl_->tridiag_smem = td != nullptr && std::strcmp(td, "smem") == 0;
+}
+
+void Engine::set_execution(int precision, double switch_residual, bool graphs) {
+  impl_->mixed = precision == 1;
+  impl_->prec_switch = switch_residual;
+  impl_->graphs = graphs;
 }
 
 Engine::~Engine() {
@@ -501,7 +514,8 @@ xtbloom_status_t build_topology(Engine::Impl& m, const HostBatch& hb, cudaStream
   const size_t mat = (size_t)m.total_mat * d8;
   ok = ok && m.pos.reserve((size_t)N * 3 * d8) && m.list.reserve((size_t)B * 4) &&
        m.count.reserve(16) && m.status.reserve((size_t)B * 4) && m.iterations.reserve((size_t)B * 4) &&
-       m.converged.reserve((size_t)B) && m.nvec.reserve((size_t)B * 4) && m.cn.reserve(N * d8) &&
+       m.converged.reserve((size_t)B) && m.prec.reserve((size_t)B) &&
+       m.split_iters.reserve((size_t)B * 4) && m.nvec.reserve((size_t)B * 4) && m.cn.reserve(N * d8) &&
        m.cn_d4.reserve(N * d8) && m.mrad.reserve(N * d8) && m.dmrad.reserve(N * d8) &&
        m.gam.reserve((size_t)m.total_gam * d8) && m.S.reserve(mat) && m.D.reserve(3 * mat) &&
        m.Q.reserve(6 * mat) && m.H0.reserve(mat) && m.H.reserve(mat) && m.X.reserve(mat) &&
@@ -710,6 +724,8 @@ xtbloom_status_t Engine::compute(const ComputeRequest& req, std::string& error) 
   cudaMemsetAsync(m.iterations.p, 0, B * 4, s);
   cudaMemsetAsync(m.terms.p, 0, kTermCount * B * 8, s);
   cudaMemsetAsync(m.pot_acc.p, 0, 10 * N * 8, s);
+  cudaMemsetAsync(m.prec.p, m.mixed ? 0 : 1, B, s);
+  cudaMemsetAsync(m.split_iters.p, 0, B * 4, s);
   cudaMemcpyAsync(list, order, B * 4, cudaMemcpyDeviceToDevice, s);
 
   // first launch failure of any stage (a launch that fails does not run and
@@ -753,9 +769,11 @@ xtbloom_status_t Engine::compute(const ComputeRequest& req, std::string& error) 
   eg.nel_b = m.nel_b.as<double>();
   const int tiles = ((m.max_n + 63) / 64) * ((m.max_n + 63) / 64);
   auto gemm = [&](const double* A, const double* Bm, double* C, const int32_t* dm, const int32_t* dn,
-                  const int32_t* dk, bool ta, const double* w, int count, bool sym = false) {
+                  const int32_t* dk, bool ta, const double* w, int count, bool sym = false,
+                  const uint8_t* prec = nullptr) {
     GemmArgs g{};
     g.sym = sym ? 1 : 0;
+    g.prec = prec;
     g.list = list;
     g.nao = m.nao.as<int32_t>();
     g.dm = dm;
@@ -824,7 +842,12 @@ xtbloom_status_t Engine::compute(const ComputeRequest& req, std::string& error) 
     };
     XTB_STAGE(stage_base == kStLowdin ? kStLowdin : kStTridiag, (int)bks.size(), for (const Bucket& bk : bks) {
       const EigArgs gb = sub(bk);
-      launch_tridiag_smem(gb, gb.list, bk.count, bk.max_n, s);
+      // few systems: register-resident cluster kernel (latency); many: the
+      // shared-memory kernel, one CTA per system (throughput)
+      if (bk.max_n <= tridiag_reg_max_n() && bk.count * 8 <= sm_count() && !m.tridiag_smem)
+        launch_tridiag_reg(gb, gb.list, bk.count, bk.max_n, s);
+      else
+        launch_tridiag_smem(gb, gb.list, bk.count, bk.max_n, s);
     });
     XTB_STAGE(stage_base == kStLowdin ? kStLowdin : kStEigvals, (int)bks.size(),
               for (const Bucket& bk : bks) launch_eigvals(sub(bk), mode, kt, bk.count, bk.max_n, s));
@@ -896,6 +919,10 @@ xtbloom_status_t Engine::compute(const ComputeRequest& req, std::string& error) 
   a.etol = req.etol;
   a.kt = req.kt;
   a.max_iter = req.max_iter;
+  a.prec = m.mixed ? m.prec.as<uint8_t>() : nullptr;
+  a.prec_switch = m.prec_switch;
+  a.split_iters = m.split_iters.as<int32_t>();
+  const uint8_t* sprec = a.prec;   // split-precision selector of the SCC GEMMs
 
   XTB_STAGE(kStCompact, 1,
             launch_compact(order, nsys, status, a.converged, a.iterations, req.max_iter, list,
@@ -912,15 +939,15 @@ xtbloom_status_t Engine::compute(const ComputeRequest& req, std::string& error) 
     XTB_STAGE(kStFock, 1, launch_fock(a, m.max_n, s));
     XTB_STAGE(kStTransform, 2,
               gemm(m.H.as<double>(), m.X.as<double>(), m.T.as<double>(), dnao, dnao, dnao, false,
-                   nullptr, count);
+                   nullptr, count, false, sprec);
               gemm(m.X.as<double>(), m.T.as<double>(), m.A.as<double>(), dnao, dnao, dnao, false,
-                   nullptr, count, true));
+                   nullptr, count, true, sprec));
     eigensolve(count, 0, req.kt, 2e-7, kStTridiag);
     XTB_STAGE(kStDensity, 2,
               gemm(m.Zv.as<double>(), m.X.as<double>(), m.C.as<double>(), dnvec, dnao, dnao, false,
-                   nullptr, count);
+                   nullptr, count, false, sprec);
               gemm(m.C.as<double>(), m.C.as<double>(), m.P.as<double>(), dnao, dnao, dnvec, true,
-                   m.occ.as<double>(), count, true));
+                   m.occ.as<double>(), count, true, sprec));
     cudaMemsetAsync(m.pop_sh.p, 0, m.nshells * 8, s);
     cudaMemsetAsync(m.pop_dip.p, 0, 3 * m.natoms * 8, s);
     cudaMemsetAsync(m.pop_qp.p, 0, 6 * m.natoms * 8, s);
@@ -1067,6 +1094,26 @@ xtbloom_status_t Engine::debug_fetch(const std::string& name, int64_t system, do
       }
     }
     *count = len;
+    return XTBLOOM_STATUS_SUCCESS;
+  }
+  if (name == "split_iterations" && system == -1) {
+    // the whole batch: SCC iterations each system ran with split-precision GEMMs
+    if (!m.have_results) {
+      error = "no retained results";
+      return XTBLOOM_STATUS_INVALID_ARGUMENT;
+    }
+    if (capacity < (size_t)m.nsys) {
+      error = "capacity too small";
+      return XTBLOOM_STATUS_INVALID_ARGUMENT;
+    }
+    cudaSetDevice(device_);
+    std::vector<int32_t> v(m.nsys);
+    if (cudaMemcpy(v.data(), m.split_iters.p, (size_t)m.nsys * 4, cudaMemcpyDeviceToHost) != cudaSuccess) {
+      error = "device read failed";
+      return XTBLOOM_STATUS_INTERNAL_ERROR;
+    }
+    for (int64_t i = 0; i < m.nsys; ++i) out[i] = (double)v[i];
+    *count = (size_t)m.nsys;
     return XTBLOOM_STATUS_SUCCESS;
   }
   if (name == "point_charge_dq" && system == -1) {

@@ -42,6 +42,10 @@ class Engine {
   xtbloom_status_t compute(const ComputeRequest& req, std::string& error);
   xtbloom_status_t debug_fetch(const std::string& name, int64_t system, double* out,
                                size_t capacity, size_t* count, std::string& error);
+  // Execution form of later computes: precision 0 = FP64 throughout, 1 =
+  // split-precision GEMMs until a system's residual is below switch_residual
+  // (then FP64 to convergence); graphs = replay captured SCC iterations.
+  void set_execution(int precision, double switch_residual, bool graphs);
   int device() const { return device_; }
   cudaStream_t stream() const { return stream_; }
 

@@ -24,35 +24,12 @@
 
 namespace xtb {
 
-// ---------------------------------------------------------------------------
-// Ragged batched GEMM.  C = op(A) * diag(w) * B with op(A) = A or A^T.
-// Every matrix of system s is row-major with leading dimension nao[s].  With
-// g.sym the product is known to be symmetric (M = N): only the tiles on and
-// below the diagonal are computed and each off-diagonal tile is also stored
-// transposed.
-// ---------------------------------------------------------------------------
 constexpr int GB = 64, GK = 16;
 
+// FP64 tile (ti, tj) of system s: 256 threads, 4 x 4 outputs per thread.
 template <bool TA, bool W>
-__global__ void __launch_bounds__(256) k_gemm(GemmArgs g) {
-  const int s = g.list[blockIdx.y];
-  const int M = g.dm[s], N = g.dn[s], K = g.dk[s];
-  const int ld = g.nao[s];
-  const int tn = (N + GB - 1) / GB;
-  const int tm = (M + GB - 1) / GB;
-  int ti, tj;
-  if (g.sym) {
-    const int t = blockIdx.x;
-    if (t >= tm * (tm + 1) / 2) return;
-    ti = (int)((sqrt(8.0 * t + 1.0) - 1.0) * 0.5);   // ti(ti+1)/2 <= t
-    while ((ti + 1) * (ti + 2) / 2 <= t) ++ti;
-    while (ti * (ti + 1) / 2 > t) --ti;
-    tj = t - ti * (ti + 1) / 2;
-  } else {
-    if ((int)blockIdx.x >= tm * tn) return;
-    ti = blockIdx.x / tn;
-    tj = blockIdx.x % tn;
-  }
+__device__ __forceinline__ void gemm_tile_f64(const GemmArgs& g, int s, int M, int N, int K, int ld,
+                                              int ti, int tj) {
   const double* A = g.A + g.offA[s];
   const double* B = g.B + g.offB[s];
   double* C = g.C + g.offC[s];
@@ -116,6 +93,157 @@ __global__ void __launch_bounds__(256) k_gemm(GemmArgs g) {
       }
     }
   }
+}
+
+// x = hi + lo with hi, lo TF32 (10 explicit mantissa bits each): the pair
+// carries about 22 bits of x.
+__device__ __forceinline__ void split_tf32(double x, uint32_t& hi, uint32_t& lo) {
+  const float f = (float)x;
+  asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(hi) : "f"(f));
+  const float r = (float)(x - (double)__uint_as_float(hi));
+  asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(lo) : "f"(r));
+}
+
+__device__ __forceinline__ void mma_tf32(float* c, const uint32_t* a, const uint32_t* b) {
+  asm volatile(
+      "mma.sync.aligned.m16n8k8.row.col.f32.tf32.tf32.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, "
+      "{%8,%9}, {%0,%1,%2,%3};\n"
+      : "+f"(c[0]), "+f"(c[1]), "+f"(c[2]), "+f"(c[3])
+      : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b[0]), "r"(b[1]));
+}
+
+// Split-precision tile: A and B are split into TF32 pairs in shared memory and
+// multiplied on the tensor cores as a_lo b_hi + a_hi b_lo + a_hi b_hi with FP32
+// accumulation (relative error about 1e-6 for the contraction lengths here).
+// Eight warps as 2 x 4, each 32 x 16 of the 64 x 64 tile (2 x 2 m16n8k8).
+template <bool TA, bool W>
+__device__ __forceinline__ void gemm_tile_tf32x3(const GemmArgs& g, int s, int M, int N, int K,
+                                                 int ld, int ti, int tj) {
+  const double* A = g.A + g.offA[s];
+  const double* B = g.B + g.offB[s];
+  double* C = g.C + g.offC[s];
+  const double* w = W ? g.w + g.offW[s] : nullptr;
+  constexpr int AP = GK + 4, BP = GB + 8;   // conflict-free fragment reads
+  __shared__ uint32_t Ah[GB][AP], Al[GB][AP];
+  __shared__ uint32_t Bh[GK][BP], Bl[GK][BP];
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int gq = lane >> 2, tq = lane & 3;
+  const int wm = warp >> 2, wn = warp & 3;
+  float acc[2][2][4];
+#pragma unroll
+  for (int mi = 0; mi < 2; ++mi)
+#pragma unroll
+    for (int ni = 0; ni < 2; ++ni)
+#pragma unroll
+      for (int q = 0; q < 4; ++q) acc[mi][ni][q] = 0.f;
+  const int i0 = ti * GB, j0 = tj * GB;
+  for (int k0 = 0; k0 < K; k0 += GK) {
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      const int e = tid + q * 256;   // 0..1023
+      int ii, kk;
+      double av;
+      if (TA) {
+        kk = e / GB;
+        ii = e % GB;
+        const int gk = k0 + kk, gi = i0 + ii;
+        av = (gk < K && gi < M) ? A[(int64_t)gk * ld + gi] : 0.0;
+      } else {
+        ii = e / GK;
+        kk = e % GK;
+        const int gk = k0 + kk, gi = i0 + ii;
+        av = (gk < K && gi < M) ? A[(int64_t)gi * ld + gk] : 0.0;
+      }
+      split_tf32(av, Ah[ii][kk], Al[ii][kk]);
+      const int kb = e / GB, jj = e % GB;
+      const int gk = k0 + kb, gj = j0 + jj;
+      double bv = (gk < K && gj < N) ? B[(int64_t)gk * ld + gj] : 0.0;
+      if (W && gk < K) bv *= w[gk];
+      split_tf32(bv, Bh[kb][jj], Bl[kb][jj]);
+    }
+    __syncthreads();
+#pragma unroll
+    for (int ks = 0; ks < GK; ks += 8) {
+      uint32_t ah[2][4], al[2][4], bh[2][2], bl[2][2];
+#pragma unroll
+      for (int mi = 0; mi < 2; ++mi) {
+        const int m0 = wm * 32 + mi * 16 + gq;
+        ah[mi][0] = Ah[m0][ks + tq];
+        ah[mi][1] = Ah[m0 + 8][ks + tq];
+        ah[mi][2] = Ah[m0][ks + tq + 4];
+        ah[mi][3] = Ah[m0 + 8][ks + tq + 4];
+        al[mi][0] = Al[m0][ks + tq];
+        al[mi][1] = Al[m0 + 8][ks + tq];
+        al[mi][2] = Al[m0][ks + tq + 4];
+        al[mi][3] = Al[m0 + 8][ks + tq + 4];
+      }
+#pragma unroll
+      for (int ni = 0; ni < 2; ++ni) {
+        const int n0 = wn * 16 + ni * 8 + gq;
+        bh[ni][0] = Bh[ks + tq][n0];
+        bh[ni][1] = Bh[ks + tq + 4][n0];
+        bl[ni][0] = Bl[ks + tq][n0];
+        bl[ni][1] = Bl[ks + tq + 4][n0];
+      }
+#pragma unroll
+      for (int mi = 0; mi < 2; ++mi)
+#pragma unroll
+        for (int ni = 0; ni < 2; ++ni) {
+          mma_tf32(acc[mi][ni], al[mi], bh[ni]);
+          mma_tf32(acc[mi][ni], ah[mi], bl[ni]);
+          mma_tf32(acc[mi][ni], ah[mi], bh[ni]);
+        }
+    }
+    __syncthreads();
+  }
+  const bool mirror = g.sym && ti != tj;
+#pragma unroll
+  for (int mi = 0; mi < 2; ++mi)
+#pragma unroll
+    for (int ni = 0; ni < 2; ++ni)
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        const int gi = i0 + wm * 32 + mi * 16 + gq + (q >= 2 ? 8 : 0);
+        const int gj = j0 + wn * 16 + ni * 8 + 2 * tq + (q & 1);
+        if (gi < M && gj < N) {
+          const double v = (double)acc[mi][ni][q];
+          C[(int64_t)gi * ld + gj] = v;
+          if (mirror) C[(int64_t)gj * ld + gi] = v;
+        }
+      }
+}
+
+// ---------------------------------------------------------------------------
+// Ragged batched GEMM.  C = op(A) * diag(w) * B with op(A) = A or A^T.
+// Every matrix of system s is row-major with leading dimension nao[s].  With
+// g.sym the product is known to be symmetric (M = N): only the tiles on and
+// below the diagonal are computed and each off-diagonal tile is also stored
+// transposed.  g.prec selects, per system, the split-precision tile.
+// ---------------------------------------------------------------------------
+template <bool TA, bool W>
+__global__ void __launch_bounds__(256) k_gemm(GemmArgs g) {
+  const int s = g.list[blockIdx.y];
+  const int M = g.dm[s], N = g.dn[s], K = g.dk[s];
+  const int ld = g.nao[s];
+  const int tn = (N + GB - 1) / GB;
+  const int tm = (M + GB - 1) / GB;
+  int ti, tj;
+  if (g.sym) {
+    const int t = blockIdx.x;
+    if (t >= tm * (tm + 1) / 2) return;
+    ti = (int)((sqrt(8.0 * t + 1.0) - 1.0) * 0.5);   // ti(ti+1)/2 <= t
+    while ((ti + 1) * (ti + 2) / 2 <= t) ++ti;
+    while (ti * (ti + 1) / 2 > t) --ti;
+    tj = t - ti * (ti + 1) / 2;
+  } else {
+    if ((int)blockIdx.x >= tm * tn) return;
+    ti = blockIdx.x / tn;
+    tj = blockIdx.x % tn;
+  }
+  if (g.prec != nullptr && g.prec[s] == 0)
+    gemm_tile_tf32x3<TA, W>(g, s, M, N, K, ld, ti, tj);
+  else
+    gemm_tile_f64<TA, W>(g, s, M, N, K, ld, ti, tj);
 }
 
 void launch_gemm(const GemmArgs& g, bool transA, bool weighted, int max_tiles, int count,

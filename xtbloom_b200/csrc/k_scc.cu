@@ -634,7 +634,8 @@ __global__ void __launch_bounds__(256) k_energy_mixer(SccArgs a) {
   }
   // mixed = cur + damp * res - sum_h omega_h c_h u_h ; shift history
   const double Fold = (it == 0) ? 0.0 : a.free_energy[s];
-  const bool conv = (rms < a.ctol) && (fabs(F - Fold) < a.etol) && hc >= 0;
+  const bool exact = a.prec == nullptr || a.prec[s] != 0;   // this iteration ran in FP64
+  const bool conv = (rms < a.ctol) && (fabs(F - Fold) < a.etol) && hc >= 0 && exact;
   const bool failed = hc < 0 || !isfinite(F) || !isfinite(nrm);
   const int first = it - (hc > 0 ? hc : 0) + 1;
   for (int i = tid; i < dim; i += bs) {
@@ -667,6 +668,10 @@ __global__ void __launch_bounds__(256) k_energy_mixer(SccArgs a) {
     tm[kTermD4] = ed;
     tm[kTermEntropy] = ts;
     tm[kTermPc] = ep;
+    if (!exact) {
+      a.split_iters[s] += 1;
+      if (rms < a.prec_switch) a.prec[s] = 1;
+    }
     if (failed) {
       a.status[s] = kInternal;
     } else if (conv) {

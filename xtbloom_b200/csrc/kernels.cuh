@@ -20,6 +20,7 @@ struct GemmArgs {
   const double* w;         // per-k weight (weighted form)
   const int64_t* offW;
   int32_t sym;             // C is symmetric: compute the lower tiles, mirror them
+  const uint8_t* prec;     // per system: 0 = split-precision (3xTF32) tile, else FP64; NULL = FP64
 };
 
 struct EigArgs {
@@ -90,6 +91,12 @@ struct SccArgs {
   double damping;
   double ctol, etol, kt;
   int32_t max_iter;
+  // precision ladder: prec[s] = 0 while system s iterates with split-precision
+  // GEMMs, 1 once it iterates in FP64 (a system converges only on an FP64
+  // iteration); it switches when its residual falls below prec_switch.
+  uint8_t* prec;
+  double prec_switch;
+  int32_t* split_iters;   // per system: iterations run with split-precision GEMMs
 };
 
 void launch_setup(const DevTopo& t, const int32_t* list, int count, int max_atoms,
@@ -101,6 +108,9 @@ void launch_gemm(const GemmArgs& g, bool transA, bool weighted, int max_tiles, i
                  cudaStream_t stream);
 void launch_tridiag(const EigArgs& g, int count, int max_n, cudaStream_t stream);
 void launch_tridiag_smem(const EigArgs& g, const int32_t* list, int count, int max_n, cudaStream_t stream);
+// Register-resident cluster tridiagonalisation for systems with n <= tridiag_reg_max_n().
+int tridiag_reg_max_n();
+void launch_tridiag_reg(const EigArgs& g, const int32_t* list, int count, int max_n, cudaStream_t stream);
 size_t tridiag_smem_bytes(int nl, int nt);
 int sm_count();   // multiprocessors of the current device (cached)
 void launch_eigvals(const EigArgs& g, int mode, double kt, int count, int max_n, cudaStream_t stream);
