@@ -933,21 +933,23 @@ xtbloom_status_t Engine::compute(const ComputeRequest& req, std::string& error) 
   int count = m.h_count[0];
   a.count = count;
   XTB_STAGE(kStPotential, 1, launch_sad_init(a, s));
-  for (int it = 0; it < req.max_iter && count > 0; ++it) {
-    a.count = count;
+  // One SCC iteration over the current active list (a.count systems): every
+  // launch of it, ending with the compaction of the list and the copies of
+  // the new count and list into pinned host memory.
+  auto iteration = [&](int it) {
     XTB_STAGE(kStPotential, 1, launch_potential(a, a.qsh, a.dip, a.qp, m.max_atoms, m.max_shells, s));
     XTB_STAGE(kStFock, 1, launch_fock(a, m.max_n, s));
     XTB_STAGE(kStTransform, 2,
               gemm(m.H.as<double>(), m.X.as<double>(), m.T.as<double>(), dnao, dnao, dnao, false,
-                   nullptr, count, false, sprec);
+                   nullptr, a.count, false, sprec);
               gemm(m.X.as<double>(), m.T.as<double>(), m.A.as<double>(), dnao, dnao, dnao, false,
-                   nullptr, count, true, sprec));
-    eigensolve(count, 0, req.kt, 2e-7, kStTridiag);
+                   nullptr, a.count, true, sprec));
+    eigensolve(a.count, 0, req.kt, 2e-7, kStTridiag);
     XTB_STAGE(kStDensity, 2,
               gemm(m.Zv.as<double>(), m.X.as<double>(), m.C.as<double>(), dnvec, dnao, dnao, false,
-                   nullptr, count, false, sprec);
+                   nullptr, a.count, false, sprec);
               gemm(m.C.as<double>(), m.C.as<double>(), m.P.as<double>(), dnao, dnao, dnvec, true,
-                   m.occ.as<double>(), count, true, sprec));
+                   m.occ.as<double>(), a.count, true, sprec));
     cudaMemsetAsync(m.pop_sh.p, 0, m.nshells * 8, s);
     cudaMemsetAsync(m.pop_dip.p, 0, 3 * m.natoms * 8, s);
     cudaMemsetAsync(m.pop_qp.p, 0, 6 * m.natoms * 8, s);
@@ -959,15 +961,62 @@ xtbloom_status_t Engine::compute(const ComputeRequest& req, std::string& error) 
                              dcount, s));
     cudaMemcpyAsync(m.h_count, dcount, 4, cudaMemcpyDeviceToHost, s);
     cudaMemcpyAsync(m.h_list, list, B * sizeof(int32_t), cudaMemcpyDeviceToHost, s);
+  };
+  // Graph replay: while the active set is unchanged (same count, hence the
+  // same list), the iteration's launches are identical; the iteration is
+  // captured once into a CUDA graph and replayed.  Not combined with the
+  // per-stage timing events.
+  cudaGraphExec_t gexec = nullptr;
+  int graph_count = -1, prev_count = -1;
+  int64_t graph_launches = 0;
+  bool graphs_ok = m.graphs && !m.prof.on;
+  for (int it = 0; it < req.max_iter && count > 0; ++it) {
+    a.count = count;
+    bool ran = false;
+    if (graphs_ok && count == prev_count) {
+      if (gexec == nullptr || graph_count != count) {
+        if (gexec) cudaGraphExecDestroy(gexec);
+        gexec = nullptr;
+        const int64_t l0 = m.prof.launches;
+        cudaGraph_t graph = nullptr;
+        const cudaError_t le0 = launch_error;
+        if (cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal) == cudaSuccess) {
+          iteration(it);
+          const cudaError_t ce = cudaStreamEndCapture(s, &graph);
+          if (ce == cudaSuccess && graph != nullptr &&
+              cudaGraphInstantiate(&gexec, graph, 0) == cudaSuccess) {
+            graph_count = count;
+            graph_launches = m.prof.launches - l0;
+          } else {
+            gexec = nullptr;
+            graphs_ok = false;   // capture failed: this call continues eagerly
+          }
+          if (graph) cudaGraphDestroy(graph);
+        } else {
+          graphs_ok = false;
+        }
+        m.prof.launches = l0;
+        if (gexec == nullptr) launch_error = le0;   // nothing of the failed capture ran
+        (void)cudaGetLastError();
+      }
+      if (gexec != nullptr && cudaGraphLaunch(gexec, s) == cudaSuccess) {
+        m.prof.launches += graph_launches;
+        ran = true;
+      }
+    }
+    if (!ran) iteration(it);
+    prev_count = count;
     cudaStreamSynchronize(s);
     if (m.trace) {
-      std::fprintf(stderr, "[xtbloom_b200] iteration %d active %d -> %d  t=%.3f ms\n", it, a.count,
+      std::fprintf(stderr, "[xtbloom_b200] iteration %d active %d -> %d  t=%.3f ms%s\n", it, a.count,
                    m.h_count[0],
-                   std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t_start).count());
+                   std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t_start).count(),
+                   ran ? " (graph)" : "");
     }
     count = m.h_count[0];
     if (launch_error) break;
   }
+  if (gexec) cudaGraphExecDestroy(gexec);
   k_finalize_status<<<(nsys + 255) / 256, 256, 0, s>>>(nsys, status, a.converged);
   m.prof.launches += 1;
 
@@ -1068,6 +1117,12 @@ xtbloom_status_t Engine::compute(const ComputeRequest& req, std::string& error) 
 xtbloom_status_t Engine::debug_fetch(const std::string& name, int64_t system, double* out,
                                      size_t capacity, size_t* count, std::string& error) {
   Impl& m = *impl_;
+  if (name == "kernel_timing_on" || name == "kernel_timing_off") {
+    // per-stage CUDA-event timing of later computes (graph replay is off while on)
+    m.prof.on = name == "kernel_timing_on";
+    *count = 0;
+    return XTBLOOM_STATUS_SUCCESS;
+  }
   if (name == "kernel_times" || name == "launch_count" || name == "reset_counters") {
     // Accumulated since the last reset: [ms, calls] per stage, or total launches.
     if (name == "reset_counters") {
