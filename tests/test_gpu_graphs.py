@@ -36,3 +36,18 @@ def test_graph_replay_matches_eager(cuda_lib):
         assert np.isnan(out["energies"][~ok]).all()
         assert np.nanmax(np.abs(out["forces"] - eager["forces"])) < 1e-8
         assert np.nanmax(np.abs(out["atomic_charges"] - eager["atomic_charges"])) < 1e-8
+
+
+def test_repeated_calls_are_reproducible(cuda_lib):
+    """The SCC has no floating-point atomics: repeated calls give bitwise-equal
+    charges, iteration counts and statuses, even for systems that never
+    converge (where any rounding difference would be amplified)."""
+    full = W.config1(4096, seed=1)
+    b = W.subset(full, [1472, 3157, 3349, 3920, 11, 222])
+    one = cuda_lib.compute(b)
+    two = cuda_lib.compute(b)
+    assert np.array_equal(one["per_system_status"], two["per_system_status"])
+    assert np.array_equal(one["scc_iterations"], two["scc_iterations"])
+    assert np.array_equal(one["atomic_charges"], two["atomic_charges"], equal_nan=True)
+    assert np.nanmax(np.abs(one["energies"] - two["energies"])) < 1e-12
+    assert np.nanmax(np.abs(one["forces"] - two["forces"])) < 1e-12

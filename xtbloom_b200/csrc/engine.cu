@@ -150,7 +150,7 @@ enum Stage : int {
   kStBacktransform, kStDensity, kStMulliken, kStEnergyMixer, kStCompact, kStForcePairs,
   kStClassical, kStCnChain, kStPublish, kStageCount
 };
-const char* kStageNames[kStageCount] = {
+[[maybe_unused]] const char* kStageNames[kStageCount] = {
     "setup_integrals", "lowdin", "potential", "fock", "gemm_transform", "tridiag", "eigvals",
     "inverse_iteration", "backtransform", "gemm_density", "mulliken", "energy_mixer", "compact",
     "force_pairs", "classical", "cn_chain", "publish"};
@@ -244,6 +244,7 @@ struct Engine::Impl {
   double prec_switch = 1e-5;
   bool graphs = false;
   Dbuf prec, split_iters;
+  Dbuf fdone;
   Profiler prof;
 
   DevTopo devtopo() const {
@@ -515,6 +516,7 @@ xtbloom_status_t build_topology(Engine::Impl& m, const HostBatch& hb, cudaStream
   ok = ok && m.pos.reserve((size_t)N * 3 * d8) && m.list.reserve((size_t)B * 4) &&
        m.count.reserve(16) && m.status.reserve((size_t)B * 4) && m.iterations.reserve((size_t)B * 4) &&
        m.converged.reserve((size_t)B) && m.prec.reserve((size_t)B) &&
+       m.fdone.reserve((size_t)B) &&
        m.split_iters.reserve((size_t)B * 4) && m.nvec.reserve((size_t)B * 4) && m.cn.reserve(N * d8) &&
        m.cn_d4.reserve(N * d8) && m.mrad.reserve(N * d8) && m.dmrad.reserve(N * d8) &&
        m.gam.reserve((size_t)m.total_gam * d8) && m.S.reserve(mat) && m.D.reserve(3 * mat) &&
@@ -570,24 +572,52 @@ __global__ void k_publish(DevTopo t, const int32_t* status, const double* free_e
   }
 }
 
-__global__ void k_fill_status(const int32_t* order, int nsys, int32_t* status, int32_t value) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i < nsys) status[order[i]] = value;
-}
-
 __global__ void k_finalize_status(int nsys, int32_t* status, const uint8_t* converged) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i < nsys && status[i] == kOk && !converged[i]) status[i] = kNotConverged;
 }
 
-// Converged systems only (status ok), in cost order.
-__global__ void k_list_ok(const int32_t* order, int nsys, const int32_t* status, int32_t* list,
-                          int32_t* count) {
-  if (threadIdx.x != 0 || blockIdx.x != 0) return;
-  int c = 0;
-  for (int i = 0; i < nsys; ++i)
-    if (status[order[i]] == kOk) list[c++] = order[i];
-  count[0] = c;
+// Converged systems (status ok) whose energy and force terms are not yet
+// formed, in cost order; marks them formed.  One block of 1024 threads (an
+// ordered compaction, like the active list).
+__global__ void k_list_ready(const int32_t* order, int nsys, const int32_t* status,
+                             const uint8_t* converged, uint8_t* done, int32_t* list, int32_t* count) {
+  __shared__ int wtot[32];
+  __shared__ int base, chunk_total;
+  if (threadIdx.x == 0) base = 0;
+  __syncthreads();
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  for (int c0 = 0; c0 < nsys; c0 += blockDim.x) {
+    const int i = c0 + threadIdx.x;
+    int sys = -1;
+    bool take = false;
+    if (i < nsys) {
+      sys = order[i];
+      take = status[sys] == kOk && converged[sys] != 0 && done[sys] == 0;
+    }
+    const unsigned b = __ballot_sync(0xffffffffu, take);
+    const int pre = __popc(b & ((1u << lane) - 1u));
+    if (lane == 0) wtot[warp] = __popc(b);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      int acc = 0;
+      for (int w = 0; w < (int)(blockDim.x >> 5); ++w) {
+        const int v = wtot[w];
+        wtot[w] = acc;
+        acc += v;
+      }
+      chunk_total = acc;
+    }
+    __syncthreads();
+    if (take) {
+      list[base + wtot[warp] + pre] = sys;
+      done[sys] = 1;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) base += chunk_total;
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) count[0] = base;
 }
 
 }  // namespace
@@ -726,16 +756,21 @@ xtbloom_status_t Engine::compute(const ComputeRequest& req, std::string& error) 
   cudaMemsetAsync(m.pot_acc.p, 0, 10 * N * 8, s);
   cudaMemsetAsync(m.prec.p, m.mixed ? 0 : 1, B, s);
   cudaMemsetAsync(m.split_iters.p, 0, B * 4, s);
+  cudaMemsetAsync(m.fdone.p, 0, B, s);
+  cudaMemsetAsync(m.grad.p, 0, 3 * N * 8, s);
+  cudaMemsetAsync(m.acn.p, 0, N * 8, s);
+  cudaMemsetAsync(m.acn_d4.p, 0, N * 8, s);
   cudaMemcpyAsync(list, order, B * 4, cudaMemcpyDeviceToDevice, s);
 
   // first launch failure of any stage (a launch that fails does not run and
   // leaves its outputs unwritten, so the call must fail)
   cudaError_t launch_error = cudaSuccess;
-#define XTB_STAGE(id, nk, ...)                                                     \
+#define XTB_STAGE(id, nk, ...) XTB_STAGE_ON(s, id, nk, __VA_ARGS__)
+#define XTB_STAGE_ON(st, id, nk, ...)                                              \
   do {                                                                             \
-    m.prof.begin(id, s);                                                           \
+    m.prof.begin(id, st);                                                          \
     __VA_ARGS__;                                                                   \
-    m.prof.end(s);                                                                 \
+    m.prof.end(st);                                                                \
     m.prof.launches += (nk);                                                       \
     if (const cudaError_t le_ = cudaGetLastError(); le_ != cudaSuccess && !launch_error) \
       launch_error = le_;                                                          \
@@ -933,6 +968,68 @@ xtbloom_status_t Engine::compute(const ComputeRequest& req, std::string& error) 
   int count = m.h_count[0];
   a.count = count;
   XTB_STAGE(kStPotential, 1, launch_sad_init(a, s));
+  // ---- energy and force terms of converged systems ----
+  const bool want_forces = (req.flags & XTBLOOM_COMPUTE_FORCES) != 0;
+  const bool want_pcf = (req.flags & XTBLOOM_COMPUTE_POINT_CHARGE_FORCES) != 0;
+  ForceArgs fbase{};
+  fbase.t = t;
+  fbase.cn = m.cn.as<double>();
+  fbase.cn_d4 = m.cn_d4.as<double>();
+  fbase.mrad = m.mrad.as<double>();
+  fbase.dmrad = m.dmrad.as<double>();
+  fbase.S = m.S.as<double>();
+  fbase.P = m.P.as<double>();
+  fbase.W = m.W.as<double>();
+  fbase.vsh = m.vsh.as<double>();
+  fbase.vd = m.vd.as<double>();
+  fbase.vq = m.vq.as<double>();
+  fbase.qsh = m.qsh.as<double>();
+  fbase.dip = m.dip.as<double>();
+  fbase.qp = m.qp.as<double>();
+  fbase.gam = m.gam.as<double>();
+  fbase.grad = m.grad.as<double>();
+  fbase.acn = m.acn.as<double>();
+  fbase.acn_d4 = m.acn_d4.as<double>();
+  fbase.terms = m.terms.as<double>();
+  fbase.want_grad = want_forces ? 1 : 0;
+  // Every kernel here reads and writes only the listed systems' slices.
+  auto force_terms = [&](const int32_t* flist, int fcount, cudaStream_t st) {
+    if (fcount <= 0) return;
+    ForceArgs f = fbase;
+    f.list = flist;
+    f.count = fcount;
+    SccArgs af = a;
+    af.list = flist;
+    af.count = fcount;
+    if (want_forces) {
+      GemmArgs gw{};
+      gw.sym = 1;
+      gw.list = flist;
+      gw.nao = dnao;
+      gw.dm = dnao;
+      gw.dn = dnao;
+      gw.dk = dnvec;
+      gw.A = m.C.as<double>();
+      gw.offA = m.mat_off.as<int64_t>();
+      gw.B = m.C.as<double>();
+      gw.offB = m.mat_off.as<int64_t>();
+      gw.C = m.W.as<double>();
+      gw.offC = m.mat_off.as<int64_t>();
+      gw.w = m.occ_eps.as<double>();
+      gw.offW = m.ao_off.as<int64_t>();
+      XTB_STAGE_ON(st, kStForcePairs, 3,
+                   launch_potential(af, af.qsh, af.dip, af.qp, m.max_atoms, m.max_shells, st);
+                   launch_gemm(gw, true, true, tiles, fcount, st);
+                   launch_force_pairs(f, m.max_pairs, st));
+    }
+    XTB_STAGE_ON(st, kStClassical, 1, launch_classical(f, m.max_atoms, m.max_shells, st));
+    if (want_forces) XTB_STAGE_ON(st, kStCnChain, 2, launch_cn_chain(f, m.max_atoms, st));
+    if (m.have_pc && (want_forces || want_pcf))
+      XTB_STAGE_ON(st, kStClassical, 1,
+                   launch_pc_forces(t, flist, fcount, m.qsh.as<double>(), m.grad.as<double>(),
+                                    m.pc_grad.as<double>(), m.pc_dq.as<double>(), st));
+  };
+
   // One SCC iteration over the current active list (a.count systems): every
   // launch of it, ending with the compaction of the list and the copies of
   // the new count and list into pinned host memory.
@@ -950,10 +1047,6 @@ xtbloom_status_t Engine::compute(const ComputeRequest& req, std::string& error) 
                    nullptr, a.count, false, sprec);
               gemm(m.C.as<double>(), m.C.as<double>(), m.P.as<double>(), dnao, dnao, dnvec, true,
                    m.occ.as<double>(), a.count, true, sprec));
-    cudaMemsetAsync(m.pop_sh.p, 0, m.nshells * 8, s);
-    cudaMemsetAsync(m.pop_dip.p, 0, 3 * m.natoms * 8, s);
-    cudaMemsetAsync(m.pop_qp.p, 0, 6 * m.natoms * 8, s);
-    cudaMemsetAsync(m.e_core.p, 0, B * 8, s);
     XTB_STAGE(kStMulliken, 1, launch_mulliken(a, m.max_n, s));
     XTB_STAGE(kStEnergyMixer, 1, launch_energy_mixer(a, m.max_atoms, m.max_shells, m.max_dim, it == 0, s));
     XTB_STAGE(kStCompact, 1,
@@ -1020,54 +1113,14 @@ xtbloom_status_t Engine::compute(const ComputeRequest& req, std::string& error) 
   k_finalize_status<<<(nsys + 255) / 256, 256, 0, s>>>(nsys, status, a.converged);
   m.prof.launches += 1;
 
-  // ---- energy/force terms on converged systems ----
-  k_list_ok<<<1, 32, 0, s>>>(order, nsys, status, list, dcount);
+  // ---- energy and force terms of the converged systems ----
+  k_list_ready<<<1, 1024, 0, s>>>(order, nsys, status, a.converged, m.fdone.as<uint8_t>(), list,
+                                  dcount);
   m.prof.launches += 1;
   cudaMemcpyAsync(m.h_count, dcount, 4, cudaMemcpyDeviceToHost, s);
   cudaStreamSynchronize(s);
   count = m.h_count[0];
-  const bool want_forces = (req.flags & XTBLOOM_COMPUTE_FORCES) != 0;
-  cudaMemsetAsync(m.grad.p, 0, 3 * N * 8, s);
-  cudaMemsetAsync(m.acn.p, 0, N * 8, s);
-  cudaMemsetAsync(m.acn_d4.p, 0, N * 8, s);
-  ForceArgs f{};
-  f.t = t;
-  f.list = list;
-  f.count = count;
-  f.cn = m.cn.as<double>();
-  f.cn_d4 = m.cn_d4.as<double>();
-  f.mrad = m.mrad.as<double>();
-  f.dmrad = m.dmrad.as<double>();
-  f.S = m.S.as<double>();
-  f.P = m.P.as<double>();
-  f.W = m.W.as<double>();
-  f.vsh = m.vsh.as<double>();
-  f.vd = m.vd.as<double>();
-  f.vq = m.vq.as<double>();
-  f.qsh = m.qsh.as<double>();
-  f.dip = m.dip.as<double>();
-  f.qp = m.qp.as<double>();
-  f.gam = m.gam.as<double>();
-  f.grad = m.grad.as<double>();
-  f.acn = m.acn.as<double>();
-  f.acn_d4 = m.acn_d4.as<double>();
-  f.terms = m.terms.as<double>();
-  f.want_grad = want_forces ? 1 : 0;
-  if (want_forces && count > 0) {
-    a.count = count;
-    XTB_STAGE(kStForcePairs, 3,
-              launch_potential(a, a.qsh, a.dip, a.qp, m.max_atoms, m.max_shells, s);
-              gemm(m.C.as<double>(), m.C.as<double>(), m.W.as<double>(), dnao, dnao, dnvec, true,
-                   m.occ_eps.as<double>(), count, true);
-              launch_force_pairs(f, m.max_pairs, s));
-  }
-  if (count > 0) XTB_STAGE(kStClassical, 1, launch_classical(f, m.max_atoms, m.max_shells, s));
-  if (want_forces && count > 0) XTB_STAGE(kStCnChain, 2, launch_cn_chain(f, m.max_atoms, s));
-  const bool want_pcf = (req.flags & XTBLOOM_COMPUTE_POINT_CHARGE_FORCES) != 0;
-  if (m.have_pc && (want_forces || want_pcf) && count > 0)
-    XTB_STAGE(kStClassical, 1,
-              launch_pc_forces(t, list, count, m.qsh.as<double>(), m.grad.as<double>(),
-                               m.pc_grad.as<double>(), m.pc_dq.as<double>(), s));
+  force_terms(list, count, s);
   if (m.have_pc && want_pcf)
     XTB_STAGE(kStPublish, 1,
               launch_pc_publish(t, status, nsys, m.pc_grad.as<double>(), m.out_pcf.as<double>(), s));
@@ -1077,6 +1130,7 @@ xtbloom_status_t Engine::compute(const ComputeRequest& req, std::string& error) 
                                            m.qsh.as<double>(), m.out_energy.as<double>(),
                                            m.out_forces.as<double>(), m.out_charges.as<double>()));
 #undef XTB_STAGE
+#undef XTB_STAGE_ON
   if (launch_error == cudaSuccess) launch_error = cudaGetLastError();
   if (launch_error != cudaSuccess) {
     cudaStreamSynchronize(s);

@@ -70,65 +70,43 @@ __device__ __forceinline__ void potential_atoms(const SccArgs& a, const double* 
   }
 }
 
-// Pair (si > fi) contributions to the atomic potential vat, the dipole
-// potential svd and the quadrupole potential svq (shared-memory atomics).
-__device__ __forceinline__ void potential_pair(const SccArgs& a, const double* dip, const double* qp,
-                                               int64_t a0, int64_t p, const double* qat,
-                                               const double* w, const double* dwq, double* vat,
-                                               double* svd, double* svq) {
+// Contribution of partner j to the potentials of atom i (dv = R_i - R_j):
+// acc[0] atomic potential (AES2 + D4 charge response), acc[1..3] dipole
+// potential, acc[4..9] quadrupole potential.  Each atom gathers over all its
+// partners in a fixed order, so the sums are the same in every run and for
+// every launch shape.
+__device__ __forceinline__ void potential_gather_pair(const SccArgs& a, const double* dip,
+                                                      const double* qp, int64_t a0, int i, int j,
+                                                      const double* qat, const double* w,
+                                                      const double* dwq, double* acc) {
   const DevTopo& t = a.t;
-  int64_t si, fi;
-  pair_from_index(p, si, fi);      // si > fi
-  const int f = (int)fi, sc = (int)si;
-  const int64_t gf = a0 + f, gs = a0 + sc;
-  const double d[3] = {t.pos[3 * gf] - t.pos[3 * gs], t.pos[3 * gf + 1] - t.pos[3 * gs + 1],
-                       t.pos[3 * gf + 2] - t.pos[3 * gs + 2]};
+  const int64_t gi = a0 + i, gj = a0 + j;
+  const double d[3] = {t.pos[3 * gi] - t.pos[3 * gj], t.pos[3 * gi + 1] - t.pos[3 * gj + 1],
+                       t.pos[3 * gi + 2] - t.pos[3 * gj + 2]};
   const double r2 = d[0] * d[0] + d[1] * d[1] + d[2] * d[2];
   const double r = sqrt(r2);
-  // AES2
   double k3, k5;
-  aes2_kernels(r, 0.5 * (a.mrad[gf] + a.mrad[gs]), k3, k5);
-  const double* df = dip + 3 * gf;
-  const double* ds = dip + 3 * gs;
-  const double* qf = qp + 6 * gf;
-  const double* qs = qp + 6 * gs;
+  aes2_kernels(r, 0.5 * (a.mrad[gi] + a.mrad[gj]), k3, k5);
+  const double* dj = dip + 3 * gj;
+  const double* qj = qp + 6 * gj;
   const double sqv[6] = {d[0] * d[0] * k5, 2.0 * d[0] * d[1] * k5, d[1] * d[1] * k5,
                          2.0 * d[0] * d[2] * k5, 2.0 * d[1] * d[2] * k5, d[2] * d[2] * k5};
   const double iso = r2 * k5;
-  double pf = 0.0, ps = 0.0, sdf = 0.0, sds = 0.0, tqf = 0.0, tqs = 0.0;
-  for (int c = 0; c < 3; ++c) {
-    pf += d[c] * df[c];
-    ps += d[c] * ds[c];
-    sdf += d[c] * k3 * df[c];
-    sds += d[c] * k3 * ds[c];
-  }
-  for (int c = 0; c < 6; ++c) {
-    tqf += sqv[c] * qf[c];
-    tqs += sqv[c] * qs[c];
-  }
-  double vf = sds + tqs;
-  double vs = -sdf + tqf;
-  for (int c = 0; c < 3; ++c) {
-    atomicAdd(&svd[3 * f + c], -qat[sc] * d[c] * k3 + iso * ds[c] - 3.0 * k5 * d[c] * ps);
-    atomicAdd(&svd[3 * sc + c], qat[f] * d[c] * k3 + iso * df[c] - 3.0 * k5 * d[c] * pf);
-  }
-  for (int c = 0; c < 6; ++c) {
-    atomicAdd(&svq[6 * f + c], qat[sc] * sqv[c]);
-    atomicAdd(&svq[6 * sc + c], qat[f] * sqv[c]);
-  }
-  // D4 charge response
+  const double pj = d[0] * dj[0] + d[1] * dj[1] + d[2] * dj[2];
+  double v = k3 * pj;
+  for (int c = 0; c < 6; ++c) v += sqv[c] * qj[c];
+  for (int c = 0; c < 3; ++c) acc[1 + c] += -qat[j] * d[c] * k3 + iso * dj[c] - 3.0 * k5 * d[c] * pj;
+  for (int c = 0; c < 6; ++c) acc[4 + c] += qat[j] * sqv[c];
   double damp, ddamp;
-  const int zf = t.Z[gf], zs = t.Z[gs];
-  d4_pair_damping(t, zf, zs, r2, damp, ddamp);
+  const int zi = t.Z[gi], zj = t.Z[gj];
+  d4_pair_damping(t, zi, zj, r2, damp, ddamp);
   if (damp != 0.0) {
-    double cf, cs;
-    d4_c6(t, zf, zs, w + kMaxD4Refs * f, w + kMaxD4Refs * sc, dwq + kMaxD4Refs * f,
-          dwq + kMaxD4Refs * sc, &cf, &cs);
-    vf -= cf * damp;
-    vs -= cs * damp;
+    double ci;
+    d4_c6(t, zi, zj, w + kMaxD4Refs * i, w + kMaxD4Refs * j, dwq + kMaxD4Refs * i, nullptr, &ci,
+          nullptr);
+    v -= ci * damp;
   }
-  atomicAdd(&vat[f], vf);
-  atomicAdd(&vat[sc], vs);
+  acc[0] += v;
 }
 
 // Shell potentials of system s from the finished atomic potentials: ES2 (warp
@@ -155,89 +133,47 @@ __device__ __forceinline__ void potential_shells(const SccArgs& a, int s, const 
   }
 }
 
-// One CTA per system.
-__global__ void __launch_bounds__(256) k_potential(SccArgs a, const double* qsh, const double* dip,
-                                                   const double* qp) {
-  extern __shared__ double sm[];
-  const DevTopo& t = a.t;
-  const int s = a.list[blockIdx.x];
-  const int64_t a0 = t.atom_off[s];
-  const int na = (int)(t.atom_off[s + 1] - a0);
-  const int64_t s0 = t.shell_off[s];
-  const int ns = (int)(t.shell_off[s + 1] - s0);
-  double* qat = sm;
-  double* vat = qat + na;
-  double* svd = vat + na;
-  double* svq = svd + 3 * na;
-  double* w = svq + 6 * na;                 // na * 7
-  double* dwq = w + kMaxD4Refs * na;        // na * 7
-  double* sq = dwq + kMaxD4Refs * na;       // ns
-  const int tid = threadIdx.x, bs = blockDim.x;
-  potential_atoms(a, qsh, a0, na, qat, w, dwq);
-  for (int i = tid; i < na; i += bs) {
-    const int64_t g = a0 + i;
-    vat[i] = 0.0;
-    const double dk2 = 2.0 * t.at_dk[g], qk2 = 2.0 * t.at_qk[g];
-    for (int c = 0; c < 3; ++c) svd[3 * i + c] = dk2 * dip[3 * g + c];
-    const double scl[6] = {1.0, 2.0, 1.0, 2.0, 2.0, 1.0};
-    for (int c = 0; c < 6; ++c) svq[6 * i + c] = qk2 * scl[c] * qp[6 * g + c];
-  }
-  for (int i = tid; i < ns; i += bs) sq[i] = qsh[s0 + i];
-  __syncthreads();
-  const int64_t npair = (int64_t)na * (na - 1) / 2;
-  for (int64_t p = tid; p < npair; p += bs)
-    potential_pair(a, dip, qp, a0, p, qat, w, dwq, vat, svd, svq);
-  __syncthreads();
-  potential_shells(a, s, sq, vat);
-  for (int i = tid; i < na; i += bs) {
-    const int64_t g = a0 + i;
-    for (int c = 0; c < 3; ++c) a.vd[3 * g + c] = svd[3 * i + c];
-    for (int c = 0; c < 6; ++c) a.vq[6 * g + c] = svq[6 * i + c];
-  }
-}
-
-// Latency form for few systems: blockIdx.x of gridDim.x CTAs of system
-// blockIdx.y takes a contiguous slice of the atom pairs and adds its partial
-// atomic, dipole and quadrupole potentials to acc (10 per atom, zero on entry).
-__global__ void __launch_bounds__(256) k_potential_pairs(SccArgs a, const double* qsh,
+// Atomic, dipole and quadrupole potentials: CTA blockIdx.x of gridDim.x for
+// system blockIdx.y; warp w of the grid's CTAs of a system gathers atom i for
+// i = w, w + warps, ...  vat goes to vat_out (per atom), vd and vq to a.vd, a.vq.
+__global__ void __launch_bounds__(256) k_potential_atoms(SccArgs a, const double* qsh,
                                                          const double* dip, const double* qp,
-                                                         double* acc) {
+                                                         double* vat_out) {
   extern __shared__ double sm[];
   const DevTopo& t = a.t;
   const int s = a.list[blockIdx.y];
   const int64_t a0 = t.atom_off[s];
   const int na = (int)(t.atom_off[s + 1] - a0);
-  const int64_t npair = (int64_t)na * (na - 1) / 2;
-  const int64_t per = (npair + gridDim.x - 1) / gridDim.x;
-  const int64_t p0 = (int64_t)blockIdx.x * per, p1 = min(npair, p0 + per);
-  if (p0 >= p1) return;   // uniform over the block
+  const int nw = blockDim.x >> 5;
+  const int gw0 = blockIdx.x * nw + (threadIdx.x >> 5), gstride = gridDim.x * nw;
+  if (blockIdx.x * nw >= na) return;   // uniform over the block: no atom for this CTA
   double* qat = sm;
-  double* loc = qat + na;                   // na * 10: vat, svd[3], svq[6] per atom
-  double* w = loc + 10 * na;                // na * 7
+  double* w = qat + na;                     // na * 7
   double* dwq = w + kMaxD4Refs * na;        // na * 7
-  double* vat = loc;
-  double* svd = loc + na;
-  double* svq = loc + 4 * na;
-  const int tid = threadIdx.x, bs = blockDim.x;
   potential_atoms(a, qsh, a0, na, qat, w, dwq);
-  for (int i = tid; i < 10 * na; i += bs) loc[i] = 0.0;
   __syncthreads();
-  for (int64_t p = p0 + tid; p < p1; p += bs)
-    potential_pair(a, dip, qp, a0, p, qat, w, dwq, vat, svd, svq);
-  __syncthreads();
-  for (int i = tid; i < na; i += bs) {
-    double* dst = acc + 10 * (a0 + i);
-    atomicAdd(dst, vat[i]);
-    for (int c = 0; c < 3; ++c) atomicAdd(dst + 1 + c, svd[3 * i + c]);
-    for (int c = 0; c < 6; ++c) atomicAdd(dst + 4 + c, svq[6 * i + c]);
+  const int lane = threadIdx.x & 31;
+  const double scl[6] = {1.0, 2.0, 1.0, 2.0, 2.0, 1.0};
+  for (int i = gw0; i < na; i += gstride) {
+    double acc[10];
+#pragma unroll
+    for (int c = 0; c < 10; ++c) acc[c] = 0.0;
+    for (int j = lane; j < na; j += 32)
+      if (j != i) potential_gather_pair(a, dip, qp, a0, i, j, qat, w, dwq, acc);
+#pragma unroll
+    for (int c = 0; c < 10; ++c) acc[c] = warp_sum(acc[c]);
+    if (lane == 0) {
+      const int64_t g = a0 + i;
+      vat_out[g] = acc[0];
+      const double dk2 = 2.0 * t.at_dk[g], qk2 = 2.0 * t.at_qk[g];
+      for (int c = 0; c < 3; ++c) a.vd[3 * g + c] = dk2 * dip[3 * g + c] + acc[1 + c];
+      for (int c = 0; c < 6; ++c) a.vq[6 * g + c] = qk2 * scl[c] * qp[6 * g + c] + acc[4 + c];
+    }
   }
 }
 
-// Completes the latency form: onsite multipole terms, shell potentials, and
-// clears acc for the next use.
-__global__ void __launch_bounds__(256) k_potential_finish(SccArgs a, const double* qsh,
-                                                          const double* dip, const double* qp,
-                                                          double* acc) {
+__global__ void __launch_bounds__(256) k_potential_shells(SccArgs a, const double* qsh,
+                                                          const double* vat_in) {
   extern __shared__ double sm[];
   const DevTopo& t = a.t;
   const int s = a.list[blockIdx.x];
@@ -247,18 +183,8 @@ __global__ void __launch_bounds__(256) k_potential_finish(SccArgs a, const doubl
   const int ns = (int)(t.shell_off[s + 1] - s0);
   double* vat = sm;
   double* sq = vat + na;
-  const int tid = threadIdx.x, bs = blockDim.x;
-  const double scl[6] = {1.0, 2.0, 1.0, 2.0, 2.0, 1.0};
-  for (int i = tid; i < na; i += bs) {
-    const int64_t g = a0 + i;
-    double* src = acc + 10 * g;
-    vat[i] = src[0];
-    const double dk2 = 2.0 * t.at_dk[g], qk2 = 2.0 * t.at_qk[g];
-    for (int c = 0; c < 3; ++c) a.vd[3 * g + c] = dk2 * dip[3 * g + c] + src[1 + c];
-    for (int c = 0; c < 6; ++c) a.vq[6 * g + c] = qk2 * scl[c] * qp[6 * g + c] + src[4 + c];
-    for (int c = 0; c < 10; ++c) src[c] = 0.0;
-  }
-  for (int i = tid; i < ns; i += bs) sq[i] = qsh[s0 + i];
+  for (int i = threadIdx.x; i < na; i += blockDim.x) vat[i] = vat_in[a0 + i];
+  for (int i = threadIdx.x; i < ns; i += blockDim.x) sq[i] = qsh[s0 + i];
   __syncthreads();
   potential_shells(a, s, sq, vat);
 }
@@ -267,26 +193,18 @@ void launch_potential(const SccArgs& a, const double* qsh, const double* dip, co
                       int max_atoms, int max_shells, cudaStream_t stream) {
   if (a.count == 0) return;
   const int sms = sm_count();
-  const int64_t max_pairs = (int64_t)max_atoms * (max_atoms - 1) / 2;
-  // With fewer systems than SMs, spread each system's pairs over CTAs (at
-  // least 64 pairs each) so that the whole GPU works on the few systems left.
-  const int parts = a.count * 2 > sms || a.pot_acc == nullptr
+  // With fewer systems than SMs, each system's atoms are spread over CTAs
+  // (at least one atom per warp) so that the whole GPU works on the few
+  // systems left; the result does not depend on the split.
+  const int parts = a.count * 2 > sms
                         ? 1
-                        : (int)std::max<int64_t>(1, std::min<int64_t>((max_pairs + 63) / 64,
-                                                                      2 * sms / a.count));
-  if (parts == 1) {
-    const size_t sm = ((size_t)(11 + 2 * kMaxD4Refs) * max_atoms + max_shells + 8) * sizeof(double);
-    static const size_t attr = allow_max_dynamic_smem(k_potential);
-    (void)attr;
-    k_potential<<<a.count, 256, sm, stream>>>(a, qsh, dip, qp);
-    return;
-  }
-  const size_t sm1 = ((size_t)(11 + 2 * kMaxD4Refs) * max_atoms + 8) * sizeof(double);
-  static const size_t attr1 = allow_max_dynamic_smem(k_potential_pairs);
+                        : std::max(1, std::min((max_atoms + 7) / 8, 2 * sms / a.count));
+  const size_t sm1 = ((size_t)(1 + 2 * kMaxD4Refs) * max_atoms + 8) * sizeof(double);
+  static const size_t attr1 = allow_max_dynamic_smem(k_potential_atoms);
   (void)attr1;
-  k_potential_pairs<<<dim3(parts, a.count), 256, sm1, stream>>>(a, qsh, dip, qp, a.pot_acc);
+  k_potential_atoms<<<dim3(parts, a.count), 256, sm1, stream>>>(a, qsh, dip, qp, a.pot_acc);
   const size_t sm2 = ((size_t)max_atoms + max_shells + 8) * sizeof(double);
-  k_potential_finish<<<a.count, 256, sm2, stream>>>(a, qsh, dip, qp, a.pot_acc);
+  k_potential_shells<<<a.count, 256, sm2, stream>>>(a, qsh, a.pot_acc);
 }
 
 // ---------------------------------------------------------------------------
@@ -367,45 +285,85 @@ void launch_fock(const SccArgs& a, int max_n, cudaStream_t stream) {
 // ---------------------------------------------------------------------------
 // Mulliken populations (column reductions) and the band trace Tr(P H0).
 // ---------------------------------------------------------------------------
-constexpr int kMullRows = 64;
+// One CTA per system.  The n rows are cut into RP fixed chunks; thread
+// (chunk, column) sums its column over its chunk, and the chunks, shells,
+// atoms and the trace are then added in a fixed order, so the populations are
+// the same in every run.
+constexpr int kMullThreads = 512;
 
-__global__ void __launch_bounds__(128) k_mulliken(SccArgs a) {
+__global__ void __launch_bounds__(kMullThreads) k_mulliken(SccArgs a) {
+  extern __shared__ double sm[];
   const DevTopo& t = a.t;
-  const int s = a.list[blockIdx.z];
+  const int s = a.list[blockIdx.x];
   const int n = t.nao[s];
-  const int col = blockIdx.x * blockDim.x + threadIdx.x;
-  const int r0 = blockIdx.y * kMullRows;
-  if (r0 >= n) return;
-  const int r1 = min(n, r0 + kMullRows);
   const int64_t mo = t.mat_off[s];
-  double ps = 0.0, ph = 0.0, pd[3] = {0, 0, 0}, pq[6] = {0, 0, 0, 0, 0, 0};
-  if (col < n) {
-    for (int r = r0; r < r1; ++r) {
-      const int64_t idx = mo + (int64_t)r * n + col;
-      const double pv = a.P[idx];
-      ps = fma(pv, a.S[idx], ps);
-      ph = fma(pv, a.H0[idx], ph);
+  const int cw = min(kMullThreads, (n + 31) & ~31);   // threads per row chunk
+  const int rp = kMullThreads / cw;                    // row chunks
+  const int chunk = threadIdx.x / cw, col0 = threadIdx.x - chunk * cw;
+  const int rows = (n + rp - 1) / rp;
+  const int r0 = min(n, chunk * rows), r1 = min(n, r0 + rows);
+  double* part = sm;           // rp x 10 x n: P S, P D (3), P Q (6) per column
+  __shared__ double red[33];
+  double ph = 0.0;
+  if (chunk < rp) {
+    for (int col = col0; col < n; col += cw) {
+      double v[10];
 #pragma unroll
-      for (int c = 0; c < 3; ++c) pd[c] = fma(pv, a.D[c * a.total_mat + idx], pd[c]);
+      for (int c = 0; c < 10; ++c) v[c] = 0.0;
+      for (int r = r0; r < r1; ++r) {
+        const int64_t idx = mo + (int64_t)r * n + col;
+        const double pv = a.P[idx];
+        v[0] = fma(pv, a.S[idx], v[0]);
+        ph = fma(pv, a.H0[idx], ph);
 #pragma unroll
-      for (int c = 0; c < 6; ++c) pq[c] = fma(pv, a.Q[c * a.total_mat + idx], pq[c]);
+        for (int c = 0; c < 3; ++c) v[1 + c] = fma(pv, a.D[c * a.total_mat + idx], v[1 + c]);
+#pragma unroll
+        for (int c = 0; c < 6; ++c) v[4 + c] = fma(pv, a.Q[c * a.total_mat + idx], v[4 + c]);
+      }
+      double* dst = part + (int64_t)chunk * 10 * n;
+#pragma unroll
+      for (int c = 0; c < 10; ++c) dst[c * n + col] = v[c];
     }
-    const int64_t gao = t.ao_off[s] + col;
-    const int sh = t.ao_sh[gao], at = t.ao_at[gao];
-    atomicAdd(&a.pop_sh[sh], ps);
-#pragma unroll
-    for (int c = 0; c < 3; ++c) atomicAdd(&a.pop_dip[3 * at + c], pd[c]);
-#pragma unroll
-    for (int c = 0; c < 6; ++c) atomicAdd(&a.pop_qp[6 * at + c], pq[c]);
   }
-  ph = warp_sum(ph);
-  if ((threadIdx.x & 31) == 0) atomicAdd(&a.e_core[s], ph);
+  const double eb = block_sum(ph, red);   // includes the barrier before the sums below
+  if (threadIdx.x == 0) a.e_core[s] = eb;
+  // column totals over the chunks (in chunk order), into chunk 0's slots
+  for (int idx = threadIdx.x; idx < 10 * n; idx += blockDim.x) {
+    double v = part[idx];
+    for (int q = 1; q < rp; ++q) v += part[(int64_t)q * 10 * n + idx];
+    part[idx] = v;
+  }
+  __syncthreads();
+  const double* cps = part;
+  const int64_t s0 = t.shell_off[s], s1 = t.shell_off[s + 1];
+  for (int64_t sh = s0 + threadIdx.x; sh < s1; sh += blockDim.x) {
+    const int first = t.sh_ao[sh], cnt = 2 * t.sh_l[sh] + 1;
+    double v = 0.0;
+    for (int k = 0; k < cnt; ++k) v += cps[first + k];
+    a.pop_sh[sh] = v;
+  }
+  const int64_t a0 = t.atom_off[s], a1 = t.atom_off[s + 1];
+  for (int64_t at = a0 + threadIdx.x; at < a1; at += blockDim.x) {
+    double pd[3] = {0, 0, 0}, pq[6] = {0, 0, 0, 0, 0, 0};
+    for (int sh = t.atom_sh[at]; sh < t.atom_sh[at + 1]; ++sh) {
+      const int first = t.sh_ao[sh], cnt = 2 * t.sh_l[sh] + 1;
+      for (int k = 0; k < cnt; ++k) {
+        for (int c = 0; c < 3; ++c) pd[c] += part[(1 + c) * n + first + k];
+        for (int c = 0; c < 6; ++c) pq[c] += part[(4 + c) * n + first + k];
+      }
+    }
+    for (int c = 0; c < 3; ++c) a.pop_dip[3 * at + c] = pd[c];
+    for (int c = 0; c < 6; ++c) a.pop_qp[6 * at + c] = pq[c];
+  }
 }
 
 void launch_mulliken(const SccArgs& a, int max_n, cudaStream_t stream) {
   if (a.count == 0) return;
-  dim3 grid((unsigned)((max_n + 127) / 128), (unsigned)((max_n + kMullRows - 1) / kMullRows), a.count);
-  k_mulliken<<<grid, 128, 0, stream>>>(a);
+  // rp(n) * 10 * n doubles: rp * n <= rp * cw = kMullThreads while n <= kMullThreads
+  const size_t words = (size_t)10 * std::max(kMullThreads, max_n);
+  static const size_t attr = allow_max_dynamic_smem(k_mulliken);
+  (void)attr;
+  k_mulliken<<<a.count, kMullThreads, words * sizeof(double), stream>>>(a);
 }
 
 // ---------------------------------------------------------------------------

@@ -19,37 +19,40 @@ __global__ void k_coordination(DevTopo t, const int32_t* list, double* cn, doubl
   const int64_t a0 = t.atom_off[s], na = t.atom_off[s + 1] - a0;
   double* scn = sm;
   double* scn4 = sm + na;
-  for (int64_t i = threadIdx.x; i < na; i += blockDim.x) { scn[i] = 0.0; scn4[i] = 0.0; }
-  __syncthreads();
-  const int64_t npair = na * (na - 1) / 2;
-  for (int64_t p = threadIdx.x; p < npair; p += blockDim.x) {
-    // p -> (i, j), i > j
-    int64_t i = (int64_t)((1.0 + sqrt(1.0 + 8.0 * (double)p)) * 0.5);
-    while (i * (i - 1) / 2 > p) --i;
-    while ((i + 1) * i / 2 <= p) ++i;
-    const int64_t j = p - i * (i - 1) / 2;
-    const int64_t gi = a0 + i, gj = a0 + j;
-    const double dx = t.pos[3 * gi] - t.pos[3 * gj];
-    const double dy = t.pos[3 * gi + 1] - t.pos[3 * gj + 1];
-    const double dz = t.pos[3 * gi + 2] - t.pos[3 * gj + 2];
-    const double r2 = dx * dx + dy * dy + dz * dz;
-    const double r = sqrt(r2);
-    if (r2 <= 625.0) {
-      const double rad = t.at_rcov[gi] + t.at_rcov[gj];
-      const double f1 = logistic(10.0 * (rad / r - 1.0));
-      const double f2 = logistic(20.0 * ((rad + 2.0) / r - 1.0));
-      atomicAdd(&scn[i], f1 * f2);
-      atomicAdd(&scn[j], f1 * f2);
+  // warp per atom, lanes over the partners, fixed-order reduction: the same
+  // coordination numbers in every run
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  for (int64_t i = warp; i < na; i += nw) {
+    const int64_t gi = a0 + i;
+    double c1 = 0.0, c4 = 0.0;
+    for (int64_t j = lane; j < na; j += 32) {
+      if (j == i) continue;
+      const int64_t gj = a0 + j;
+      const double dx = t.pos[3 * gi] - t.pos[3 * gj];
+      const double dy = t.pos[3 * gi + 1] - t.pos[3 * gj + 1];
+      const double dz = t.pos[3 * gi + 2] - t.pos[3 * gj + 2];
+      const double r2 = dx * dx + dy * dy + dz * dz;
+      const double r = sqrt(r2);
+      if (r2 <= 625.0) {
+        const double rad = t.at_rcov[gi] + t.at_rcov[gj];
+        const double f1 = logistic(10.0 * (rad / r - 1.0));
+        const double f2 = logistic(20.0 * ((rad + 2.0) / r - 1.0));
+        c1 += f1 * f2;
+      }
+      if (r2 <= 900.0) {
+        const int zi = t.Z[gi] - 1, zj = t.Z[gj] - 1;
+        const double rc = t.d4_rcov[zi] + t.d4_rcov[zj];
+        const double den = fabs(t.d4_en[zi] - t.d4_en[zj]);
+        const double enf = 4.10451 * exp(-(den + 19.08857) * (den + 19.08857) / (2.0 * 11.28174 * 11.28174));
+        const double x = 7.5 * (r - rc) / rc;
+        c4 += 0.5 * enf * (1.0 + erf(-x));
+      }
     }
-    if (r2 <= 900.0) {
-      const int zi = t.Z[gi] - 1, zj = t.Z[gj] - 1;
-      const double rc = t.d4_rcov[zi] + t.d4_rcov[zj];
-      const double den = fabs(t.d4_en[zi] - t.d4_en[zj]);
-      const double enf = 4.10451 * exp(-(den + 19.08857) * (den + 19.08857) / (2.0 * 11.28174 * 11.28174));
-      const double x = 7.5 * (r - rc) / rc;
-      const double c = 0.5 * enf * (1.0 + erf(-x));
-      atomicAdd(&scn4[i], c);
-      atomicAdd(&scn4[j], c);
+    c1 = warp_sum(c1);
+    c4 = warp_sum(c4);
+    if (lane == 0) {
+      scn[i] = c1;
+      scn4[i] = c4;
     }
   }
   __syncthreads();

@@ -72,7 +72,7 @@ struct SccArgs {
   double* H;
   const double* P;
   int64_t total_mat;
-  double* pot_acc;    // 10 per atom, all zero between uses (pair-split potential)
+  double* pot_acc;    // per atom: atomic potential between the two potential kernels
   // per system energies / status
   const double* entropy;
   double* free_energy;
