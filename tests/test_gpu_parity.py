@@ -95,7 +95,8 @@ def test_stage_intermediates_match_oracle(cuda_lib, fixtures):
     assert np.abs(fetch(cuda_lib, "qsh", 0) - d["qsh"]).max() < 1e-7
     t = fetch(cuda_lib, "energy_terms", 0)
     ref = [r.terms[k] for k in ["core", "es2", "es3", "aes2", "d4", "entropy", "rep", "atm", "pc"]]
-    assert np.abs(t - np.array(ref)).max() < 1e-7
+    assert np.abs(t[:9] - np.array(ref)).max() < 1e-7
+    assert t[9] == 0.0   # spin polarisation: restricted system
 
 
 def test_translation_rotation_invariance(cuda_lib, fixtures):

@@ -104,3 +104,16 @@ def test_oracle_point_charge_derivatives_are_finite_differences(pc_fixtures):
         ep = gfn2.singlepoint(z, x, pc_pos=xp, pc_q=pq, forces=False, **tight).energy
         em = gfn2.singlepoint(z, x, pc_pos=xm, pc_q=pq, forces=False, **tight).energy
         assert abs((ep - em) / (2 * h) - r.pc_gradient[p, c]) < 1e-6
+
+
+def test_unrestricted_goldens_pinned_to_tblite_trace():
+    """The unrestricted goldens come from the reference library; its OH radical
+    (spin_channels = 2) reproduces the reference's tblite UHF SCC trace: same
+    iteration count, final charges within the trace's own residual (1e-5)."""
+    import json
+
+    from conftest import GOLDEN
+    oh = json.loads((GOLDEN / "uhf_fixtures.json").read_text())["oh_radical"]
+    assert oh["status"] == 0
+    assert oh["scc_iterations"] == oh["tblite_iterations"]
+    assert np.abs(np.asarray(oh["charges"]) - np.asarray(oh["tblite_final_charges"])).max() < 2e-5

@@ -335,8 +335,10 @@ class Library:
         return outputs
 
 
-def ragged_from_lists(numbers_list, positions_list, charges=None, uhf=None) -> RaggedBatch:
-    """Pack per-molecule arrays into the ABI's ragged host layout."""
+def ragged_from_lists(numbers_list, positions_list, charges=None, uhf=None,
+                      spin_channels=None) -> RaggedBatch:
+    """Pack per-molecule arrays into the ABI's ragged host layout.  spin_channels
+    (1 restricted, 2 unrestricted per molecule) is omitted when None."""
     counts = [len(z) for z in numbers_list]
     offs = np.zeros(len(counts) + 1, np.int64)
     offs[1:] = np.cumsum(counts)
@@ -347,4 +349,5 @@ def ragged_from_lists(numbers_list, positions_list, charges=None, uhf=None) -> R
         positions=np.ascontiguousarray(np.concatenate([np.asarray(p, float).reshape(-1) for p in positions_list])),
         molecular_charges=np.asarray(charges if charges is not None else np.zeros(nb), float),
         unpaired_electrons=np.asarray(uhf if uhf is not None else np.zeros(nb), np.int32),
+        spin_channels=None if spin_channels is None else np.ascontiguousarray(np.asarray(spin_channels, np.int32)),
     )

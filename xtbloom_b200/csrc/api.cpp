@@ -175,11 +175,8 @@ xtbloom_status_t validate_and_normalise(const xtbloom_batch_t* batch,
         err = "spin_channels values must be one or two";
         return XTBLOOM_STATUS_INVALID_ARGUMENT;
       }
-      if (sc[i] == 2) {
-        err = "unrestricted (two-channel) systems are not supported by this CUDA path";
-        return XTBLOOM_STATUS_NOT_SUPPORTED;
-      }
     }
+    req.spin_channels = true;
   }
   const size_t P = static_cast<size_t>(batch->total_point_charges);
   if (P != 0 || buffer_active(batch->point_charge_offsets)) {

@@ -61,6 +61,8 @@ struct DevTopo {
   const double* nel_a;
   const double* nel_b;
   const double* qmol;
+  const int32_t* nch;         // spin channels (1 restricted, 2 unrestricted)
+  const int32_t* beta_ch;     // channel id of the beta channel (-1 for restricted systems)
   // per atom
   const int32_t* Z;
   const int32_t* atom_sh;     // total_atoms + 1
@@ -94,6 +96,7 @@ struct DevTopo {
   const double* sh_eta;
   const double* sh_g3;
   const double* sh_refocc;
+  const double* sh_spinw;     // 3 per shell: spin coupling W(shell, k-th shell of its atom)
   const double* p_alpha;
   const double* p_coeff;
   // per AO (global)
@@ -116,7 +119,7 @@ struct DevTopo {
 // Per-system energy terms (terms[kTermCount * s + k]).
 enum TermIndex : int {
   kTermCore = 0, kTermEs2 = 1, kTermEs3 = 2, kTermAes2 = 3, kTermD4 = 4, kTermEntropy = 5,
-  kTermRep = 6, kTermAtm = 7, kTermPc = 8, kTermCount = 9
+  kTermRep = 6, kTermAtm = 7, kTermPc = 8, kTermSpin = 9, kTermCount = 10
 };
 
 __device__ __forceinline__ double logistic(double x) {

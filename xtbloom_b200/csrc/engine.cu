@@ -215,6 +215,16 @@ struct Engine::Impl {
 
   // device topology arrays
   Dbuf atom_off, shell_off, ao_off, mat_off, gam_off, vec_off, scr_off, nao, nel_a, nel_b, qmol;
+  // spin channels: id c < nsys is system c's first (restricted or alpha)
+  // channel at the system's own offsets; beta channels have ids nsys + u with
+  // storage after the systems' (matrices at total_mat.., vectors at naos..)
+  int64_t nchan = 0, nuhf = 0, chan_mat = 0, chan_vec = 0, chan_scr = 0;
+  Dbuf nch, beta_ch, sh_spinw, ch_sys, ch_sign, ch_nao, ch_mat, ch_ao, ch_scr, ch_xoff, ch_nel_a,
+      ch_nel_b, clist, ccount;
+  std::vector<int32_t> h_ch_nao, h_ch_sys;
+  std::vector<double> h_ch_nel_a, h_ch_nel_b;
+  int32_t* h_clist = nullptr;   // pinned copy of the active channel list
+  int64_t h_clist_cap = 0;
   Dbuf Z, atom_sh, pos, at_en, at_rad, at_rcov, at_mprad, at_mpvcn, at_dk, at_qk, at_rep_sa, at_rep_z;
   Dbuf sh_atom, sh_l, sh_ao, sh_p0, sh_np, sh_level, sh_kcn, sh_shpoly, sh_zeta, sh_eta, sh_g3,
       sh_refocc, p_alpha, p_coeff, ao_sh, ao_at, order;
@@ -224,6 +234,7 @@ struct Engine::Impl {
   Dbuf S, D, Q, H0, H, X, T, A, Zv, C, P, W;
   Dbuf d, e, tau, eig, occ, occ_eps, entropy, scratch;
   Dbuf qsh, dip, qp, pop_sh, pop_dip, pop_qp, e_core, vsh, vd, vq;
+  Dbuf Pm, qmag, vmag, pop_mag, pop_mdip, pop_mqp;
   Dbuf free_energy, terms;
   Dbuf mx_cur, mx_prev, mx_res, mx_df, mx_u, mx_omega;
   Dbuf grad, acn, acn_d4, pot_acc;
@@ -264,6 +275,9 @@ struct Engine::Impl {
     t.nel_a = nel_a.as<double>();
     t.nel_b = nel_b.as<double>();
     t.qmol = qmol.as<double>();
+    t.nch = nch.as<int32_t>();
+    t.beta_ch = beta_ch.as<int32_t>();
+    t.sh_spinw = sh_spinw.as<double>();
     t.Z = Z.as<int32_t>();
     t.atom_sh = atom_sh.as<int32_t>();
     t.pos = pos.as<double>();
@@ -332,6 +346,7 @@ void Engine::set_execution(int precision, double switch_residual, bool graphs) {
 Engine::~Engine() {
   if (impl_->h_count) cudaFreeHost(impl_->h_count);
   if (impl_->h_list) cudaFreeHost(impl_->h_list);
+  if (impl_->h_clist) cudaFreeHost(impl_->h_clist);
   delete impl_;
 }
 
@@ -359,7 +374,7 @@ bool ensure_tables(Engine::Impl& m, cudaStream_t s) {
 
 bool same_topology(const HostBatch& a, const HostBatch& b) {
   return a.nsys == b.nsys && a.atom_off == b.atom_off && a.Z == b.Z && a.qmol == b.qmol &&
-         a.uhf == b.uhf;
+         a.uhf == b.uhf && a.nch == b.nch;
 }
 
 xtbloom_status_t build_topology(Engine::Impl& m, const HostBatch& hb, cudaStream_t s,
@@ -373,7 +388,8 @@ xtbloom_status_t build_topology(Engine::Impl& m, const HostBatch& hb, cudaStream
   std::vector<double> at_en(N), at_rad(N), at_rcov(N), at_mprad(N), at_mpvcn(N), at_dk(N), at_qk(N),
       at_rep_sa(N), at_rep_z(N);
   std::vector<int32_t> sh_atom, sh_l, sh_ao, sh_p0, sh_np, ao_sh, ao_at;
-  std::vector<double> sh_level, sh_kcn, sh_shpoly, sh_zeta, sh_eta, sh_g3, sh_refocc, p_alpha, p_coeff;
+  std::vector<double> sh_level, sh_kcn, sh_shpoly, sh_zeta, sh_eta, sh_g3, sh_refocc, p_alpha, p_coeff,
+      sh_spinw;
   int64_t shell = 0;
   int max_n = 0, max_atoms = 0, max_shells = 0, max_dim = 0;
   int64_t max_pairs = 0;
@@ -438,6 +454,20 @@ xtbloom_status_t build_topology(Engine::Impl& m, const HostBatch& hb, cudaStream
         ao_local += 2 * l + 1;
         ++shell;
       }
+      // atom-local spin couplings W(l_row, l_col) (tblite element constants,
+      // ss sp pp sd pd dd), 3 per shell
+      for (int64_t r = atom_sh[a]; r < shell; ++r) {
+        for (int k = 0; k < 3; ++k) {
+          double wv = 0.0;
+          if (atom_sh[a] + k < shell) {
+            int l1 = sh_l[r], l2 = sh_l[atom_sh[a] + k];
+            if (l1 > l2) std::swap(l1, l2);
+            const int idx = l1 == 0 ? (l2 == 0 ? 0 : (l2 == 1 ? 1 : 3)) : (l1 == 1 ? (l2 == 1 ? 2 : 4) : 5);
+            wv = kP_spin_constants[6 * zi + idx];
+          }
+          sh_spinw.push_back(wv);
+        }
+      }
     }
     const int na = (int)(atom_off[sy + 1] - atom_off[sy]);
     const int ns = (int)(shell - shell_off[sy]);
@@ -453,7 +483,7 @@ xtbloom_status_t build_topology(Engine::Impl& m, const HostBatch& hb, cudaStream
     max_n = std::max(max_n, ao_local);
     max_atoms = std::max(max_atoms, na);
     max_shells = std::max(max_shells, ns);
-    max_dim = std::max(max_dim, ns + 9 * na);
+    max_dim = std::max(max_dim, hb.nch[sy] * (ns + 9 * na));
     max_pairs = std::max<int64_t>(max_pairs, (int64_t)na * (na + 1) / 2);
   }
   shell_off[B] = shell;
@@ -466,7 +496,7 @@ xtbloom_status_t build_topology(Engine::Impl& m, const HostBatch& hb, cudaStream
     const int64_t na = atom_off[sy + 1] - atom_off[sy];
     mat_off[sy + 1] = mat_off[sy] + n * n;
     gam_off[sy + 1] = gam_off[sy] + k * k;
-    vec_off[sy + 1] = vec_off[sy] + k + 9 * na;
+    vec_off[sy + 1] = vec_off[sy] + hb.nch[sy] * (k + 9 * na);
     scr_off[sy + 1] = scr_off[sy] + 128 * 5 * n;
   }
   // largest systems first
@@ -493,6 +523,75 @@ xtbloom_status_t build_topology(Engine::Impl& m, const HostBatch& hb, cudaStream
   m.h_nel_a = nel_a;
   m.h_nel_b = nel_b;
 
+  // spin channels (see Impl): restricted channel c = s holds both electron
+  // counts (occupation <= 2); unrestricted alpha (c = s) and beta
+  // (c = B + u) hold one count each (occupation <= 1)
+  std::vector<int32_t> nchv(hb.nch.begin(), hb.nch.end()), beta(B, -1);
+  int64_t nU = 0;
+  for (int64_t sy = 0; sy < B; ++sy) nU += nchv[sy] == 2 ? 1 : 0;
+  const int64_t NC = B + nU;
+  std::vector<int32_t> ch_sys(NC), ch_sign(NC), ch_nao(NC);
+  std::vector<int64_t> ch_mat(NC), ch_ao(NC), ch_scr(NC), ch_xoff(NC);
+  std::vector<double> ch_nel_a(NC), ch_nel_b(NC);
+  int64_t xm = 0, xv = 0, xs = 0, u = 0;
+  for (int64_t sy = 0; sy < B; ++sy) {
+    const bool un = nchv[sy] == 2;
+    ch_sys[sy] = (int32_t)sy;
+    ch_sign[sy] = un ? 1 : 0;
+    ch_nao[sy] = nao[sy];
+    ch_mat[sy] = mat_off[sy];
+    ch_ao[sy] = ao_off[sy];
+    ch_scr[sy] = scr_off[sy];
+    ch_xoff[sy] = mat_off[sy];
+    ch_nel_a[sy] = nel_a[sy];
+    ch_nel_b[sy] = un ? 0.0 : nel_b[sy];
+    if (un) {
+      const int64_t c = B + u++;
+      const int64_t n = nao[sy];
+      beta[sy] = (int32_t)c;
+      ch_sys[c] = (int32_t)sy;
+      ch_sign[c] = -1;
+      ch_nao[c] = (int32_t)n;
+      ch_mat[c] = mat_off[B] + xm;
+      ch_ao[c] = ao_off[B] + xv;
+      ch_scr[c] = scr_off[B] + xs;
+      ch_xoff[c] = mat_off[sy];
+      ch_nel_a[c] = nel_b[sy];
+      ch_nel_b[c] = 0.0;
+      xm += n * n;
+      xv += n;
+      xs += 128 * 5 * n;
+    }
+  }
+  m.nchan = NC;
+  m.nuhf = nU;
+  m.chan_mat = xm;
+  m.chan_vec = xv;
+  m.chan_scr = xs;
+  m.h_ch_nao = ch_nao;
+  m.h_ch_sys = ch_sys;
+  m.h_ch_nel_a = ch_nel_a;
+  m.h_ch_nel_b = ch_nel_b;
+  if (m.h_clist_cap < NC) {
+    if (m.h_clist) cudaFreeHost(m.h_clist);
+    m.h_clist = nullptr;
+    if (cudaMallocHost(&m.h_clist, NC * sizeof(int32_t)) != cudaSuccess) {
+      error = "pinned host allocation failed";
+      return XTBLOOM_STATUS_ALLOCATION_FAILED;
+    }
+    m.h_clist_cap = NC;
+  }
+  if (!upload(m.nch, nchv, s) || !upload(m.beta_ch, beta, s) || !upload(m.sh_spinw, sh_spinw, s) ||
+      !upload(m.ch_sys, ch_sys, s) || !upload(m.ch_sign, ch_sign, s) || !upload(m.ch_nao, ch_nao, s) ||
+      !upload(m.ch_mat, ch_mat, s) || !upload(m.ch_ao, ch_ao, s) || !upload(m.ch_scr, ch_scr, s) ||
+      !upload(m.ch_xoff, ch_xoff, s) || !upload(m.ch_nel_a, ch_nel_a, s) ||
+      !upload(m.ch_nel_b, ch_nel_b, s) || !m.clist.reserve((size_t)NC * 4) || !m.ccount.reserve(16)) {
+    error = "device allocation for the spin channels failed";
+    return XTBLOOM_STATUS_ALLOCATION_FAILED;
+  }
+  // the host vectors above must outlive their asynchronous uploads
+  cudaStreamSynchronize(s);
+
   bool ok = upload(m.atom_off, atom_off, s) && upload(m.shell_off, shell_off, s) &&
             upload(m.ao_off, ao_off, s) && upload(m.mat_off, mat_off, s) &&
             upload(m.gam_off, gam_off, s) && upload(m.vec_off, vec_off, s) &&
@@ -513,19 +612,24 @@ xtbloom_status_t build_topology(Engine::Impl& m, const HostBatch& hb, cudaStream
             upload(m.ao_at, ao_at, s) && upload(m.order, order, s);
   const size_t d8 = sizeof(double);
   const size_t mat = (size_t)m.total_mat * d8;
+  const size_t cmat = (size_t)(m.total_mat + m.chan_mat) * d8;     // channel matrices
+  const size_t cvec = (size_t)(m.naos + m.chan_vec) * d8;          // channel vectors
   ok = ok && m.pos.reserve((size_t)N * 3 * d8) && m.list.reserve((size_t)B * 4) &&
        m.count.reserve(16) && m.status.reserve((size_t)B * 4) && m.iterations.reserve((size_t)B * 4) &&
        m.converged.reserve((size_t)B) && m.prec.reserve((size_t)B) &&
        m.fdone.reserve((size_t)B) &&
-       m.split_iters.reserve((size_t)B * 4) && m.nvec.reserve((size_t)B * 4) && m.cn.reserve(N * d8) &&
+       m.split_iters.reserve((size_t)B * 4) && m.nvec.reserve((size_t)NC * 4) && m.cn.reserve(N * d8) &&
        m.cn_d4.reserve(N * d8) && m.mrad.reserve(N * d8) && m.dmrad.reserve(N * d8) &&
        m.gam.reserve((size_t)m.total_gam * d8) && m.S.reserve(mat) && m.D.reserve(3 * mat) &&
-       m.Q.reserve(6 * mat) && m.H0.reserve(mat) && m.H.reserve(mat) && m.X.reserve(mat) &&
-       m.T.reserve(mat) && m.A.reserve(mat) && m.Zv.reserve(mat) && m.C.reserve(mat) &&
-       m.P.reserve(mat) && m.W.reserve(mat) && m.d.reserve(m.naos * d8) && m.e.reserve(m.naos * d8) &&
-       m.tau.reserve(m.naos * d8) && m.eig.reserve(m.naos * d8) && m.occ.reserve(m.naos * d8) &&
-       m.occ_eps.reserve(m.naos * d8) && m.entropy.reserve(B * d8) &&
-       m.scratch.reserve((size_t)m.total_scr * d8) && m.qsh.reserve(shell * d8) &&
+       m.Q.reserve(6 * mat) && m.H0.reserve(mat) && m.H.reserve(cmat) && m.X.reserve(mat) &&
+       m.T.reserve(cmat) && m.A.reserve(cmat) && m.Zv.reserve(cmat) && m.C.reserve(cmat) &&
+       m.P.reserve(cmat) && m.W.reserve(cmat) && m.d.reserve(cvec) && m.e.reserve(cvec) &&
+       m.tau.reserve(cvec) && m.eig.reserve(cvec) && m.occ.reserve(cvec) &&
+       m.occ_eps.reserve(cvec) && m.entropy.reserve(NC * d8) &&
+       m.scratch.reserve((size_t)(m.total_scr + m.chan_scr) * d8) && m.qsh.reserve(shell * d8) &&
+       m.Pm.reserve(nU > 0 ? mat : 8) && m.qmag.reserve(shell * d8) && m.vmag.reserve(shell * d8) &&
+       m.pop_mag.reserve(shell * d8) && m.pop_mdip.reserve(3 * N * d8) &&
+       m.pop_mqp.reserve(6 * N * d8) &&
        m.dip.reserve(3 * N * d8) && m.qp.reserve(6 * N * d8) && m.pop_sh.reserve(shell * d8) &&
        m.pop_dip.reserve(3 * N * d8) && m.pop_qp.reserve(6 * N * d8) && m.e_core.reserve(B * d8) &&
        m.vsh.reserve(shell * d8) && m.vd.reserve(3 * N * d8) && m.vq.reserve(6 * N * d8) &&
@@ -575,6 +679,69 @@ __global__ void k_publish(DevTopo t, const int32_t* status, const double* free_e
 __global__ void k_finalize_status(int nsys, int32_t* status, const uint8_t* converged) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i < nsys && status[i] == kOk && !converged[i]) status[i] = kNotConverged;
+}
+
+// Channel list of a system list: every system's first channel (id = system)
+// followed, for unrestricted systems, by its beta channel; order preserved.
+// One block of 1024 threads; count is read on the device.
+__global__ void k_channels(const int32_t* list, const int32_t* count, const int32_t* beta_ch,
+                           int32_t* clist, int32_t* ccount) {
+  __shared__ int wtot[32];
+  __shared__ int base, chunk_total;
+  if (threadIdx.x == 0) base = 0;
+  __syncthreads();
+  const int n = count[0];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  for (int c0 = 0; c0 < n; c0 += blockDim.x) {
+    const int i = c0 + threadIdx.x;
+    const int sys = i < n ? list[i] : -1;
+    const int bc = sys >= 0 ? beta_ch[sys] : -1;
+    const int w = sys < 0 ? 0 : (bc >= 0 ? 2 : 1);
+    int incl = w;   // inclusive warp scan
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int v = __shfl_up_sync(0xffffffffu, incl, o);
+      if (lane >= o) incl += v;
+    }
+    if (lane == 31) wtot[warp] = incl;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      int acc = 0;
+      for (int q = 0; q < (int)(blockDim.x >> 5); ++q) {
+        const int v = wtot[q];
+        wtot[q] = acc;
+        acc += v;
+      }
+      chunk_total = acc;
+    }
+    __syncthreads();
+    const int pos = base + wtot[warp] + incl - w;
+    if (w >= 1) clist[pos] = sys;
+    if (w == 2) clist[pos + 1] = bc;
+    __syncthreads();
+    if (threadIdx.x == 0) base += chunk_total;
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) ccount[0] = base;
+}
+
+// Unrestricted systems of the list: the alpha-channel matrix (at the system's
+// offset) becomes the total alpha + beta; with Pm, also P_alpha - P_beta.
+__global__ void k_combine_spin(const int32_t* list, const int32_t* beta_ch, const int32_t* nao,
+                               const int64_t* mat_off, const int64_t* ch_mat, double* M,
+                               double* Pm) {
+  const int s = list[blockIdx.y];
+  const int bc = beta_ch[s];
+  if (bc < 0) return;
+  const int64_t n2 = (int64_t)nao[s] * nao[s];
+  double* a = M + mat_off[s];
+  const double* b = M + ch_mat[bc];
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n2;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    const double va = a[i], vb = b[i];
+    a[i] = va + vb;
+    if (Pm != nullptr) Pm[mat_off[s] + i] = va - vb;
+  }
 }
 
 // Converged systems (status ok) whose energy and force terms are not yet
@@ -641,10 +808,13 @@ xtbloom_status_t Engine::compute(const ComputeRequest& req, std::string& error) 
   hb.Z.resize(N);
   hb.qmol.resize(B);
   hb.uhf.resize(B, 0);
+  hb.nch.assign(B, 1);
   if (!read_input(b.atom_offsets, hb.atom_off.data(), (B + 1) * 8, s) ||
       !read_input(b.atomic_numbers, hb.Z.data(), N * 4, s) ||
       !read_input(b.molecular_charges, hb.qmol.data(), B * 8, s) ||
-      (b.unpaired_electrons.data && !read_input(b.unpaired_electrons, hb.uhf.data(), B * 4, s))) {
+      (b.unpaired_electrons.data && !read_input(b.unpaired_electrons, hb.uhf.data(), B * 4, s)) ||
+      (req.spin_channels && b.spin_channels.data &&
+       !read_input(b.spin_channels, hb.nch.data(), B * 4, s))) {
     error = "failed to read the batch descriptors";
     return XTBLOOM_STATUS_INVALID_ARGUMENT;
   }
@@ -663,6 +833,10 @@ xtbloom_status_t Engine::compute(const ComputeRequest& req, std::string& error) 
     }
     if (hb.uhf[i] < 0) {
       error = "unpaired_electrons must be nonnegative";
+      return XTBLOOM_STATUS_INVALID_ARGUMENT;
+    }
+    if (hb.nch[i] != 1 && hb.nch[i] != 2) {
+      error = "spin_channels values must be one or two";
       return XTBLOOM_STATUS_INVALID_ARGUMENT;
     }
   }
@@ -783,11 +957,17 @@ xtbloom_status_t Engine::compute(const ComputeRequest& req, std::string& error) 
                          m.gam.as<double>(), m.total_mat, s);
             if (m.have_pc) launch_pc_potential(t, list, nsys, m.vpc.as<double>(), s));
 
+  // Eigensolver and GEMM arguments are indexed by spin channel; channel c < B
+  // is system c at its own offsets, so system lists work for them as well.
+  const int32_t* dch_nao = m.ch_nao.as<int32_t>();
+  const int64_t* dch_mat = m.ch_mat.as<int64_t>();
+  const int64_t* dch_ao = m.ch_ao.as<int64_t>();
+  const int64_t* dch_xoff = m.ch_xoff.as<int64_t>();
   EigArgs eg{};
   eg.list = list;
-  eg.nao = m.nao.as<int32_t>();
-  eg.mat_off = m.mat_off.as<int64_t>();
-  eg.ao_off = m.ao_off.as<int64_t>();
+  eg.nao = dch_nao;
+  eg.mat_off = dch_mat;
+  eg.ao_off = dch_ao;
   eg.A = m.A.as<double>();
   eg.d = m.d.as<double>();
   eg.e = m.e.as<double>();
@@ -799,32 +979,37 @@ xtbloom_status_t Engine::compute(const ComputeRequest& req, std::string& error) 
   eg.nvec = m.nvec.as<int32_t>();
   eg.Z = m.Zv.as<double>();
   eg.scratch = m.scratch.as<double>();
-  eg.scratch_off = m.scr_off.as<int64_t>();
-  eg.nel_a = m.nel_a.as<double>();
-  eg.nel_b = m.nel_b.as<double>();
+  eg.scratch_off = m.ch_scr.as<int64_t>();
+  eg.nel_a = m.ch_nel_a.as<double>();
+  eg.nel_b = m.ch_nel_b.as<double>();
   const int tiles = ((m.max_n + 63) / 64) * ((m.max_n + 63) / 64);
-  auto gemm = [&](const double* A, const double* Bm, double* C, const int32_t* dm, const int32_t* dn,
+  // C = op(A) diag(w) B over the entries of glist (systems or channels); each
+  // operand has its own offset array (channel matrices at ch_mat, the
+  // system-level orthogonaliser at ch_xoff).
+  auto gemm = [&](const int32_t* glist, const double* A, const int64_t* offA, const double* Bm,
+                  const int64_t* offB, double* C, const int32_t* dm, const int32_t* dn,
                   const int32_t* dk, bool ta, const double* w, int count, bool sym = false,
-                  const uint8_t* prec = nullptr) {
+                  const uint8_t* prec = nullptr, cudaStream_t st = nullptr) {
     GemmArgs g{};
     g.sym = sym ? 1 : 0;
     g.prec = prec;
-    g.list = list;
-    g.nao = m.nao.as<int32_t>();
+    g.prec_of = m.ch_sys.as<int32_t>();
+    g.list = glist;
+    g.nao = dch_nao;
     g.dm = dm;
     g.dn = dn;
     g.dk = dk;
     g.A = A;
-    g.offA = m.mat_off.as<int64_t>();
+    g.offA = offA;
     g.B = Bm;
-    g.offB = m.mat_off.as<int64_t>();
+    g.offB = offB;
     g.C = C;
-    g.offC = m.mat_off.as<int64_t>();
+    g.offC = dch_mat;
     g.w = w;
-    g.offW = m.ao_off.as<int64_t>();
-    launch_gemm(g, ta, w != nullptr, tiles, count, s);
+    g.offW = dch_ao;
+    launch_gemm(g, ta, w != nullptr, tiles, count, st != nullptr ? st : s);
   };
-  const int32_t* dnao = m.nao.as<int32_t>();
+  const int32_t* dnao = dch_nao;
   const int32_t* dnvec = m.nvec.as<int32_t>();
 
   // AO-count buckets of the (n-descending) active list: each bucket gets its
@@ -837,29 +1022,29 @@ xtbloom_status_t Engine::compute(const ComputeRequest& req, std::string& error) 
   struct Bucket {
     int start, count, max_n, max_m;
   };
-  auto buckets = [&](int count) {
+  auto buckets = [&](const int32_t* hl, int count) {
     static const int kEdges[] = {230, 192, 160, 128, 96, 64, 0};
     std::vector<Bucket> out;
     int i = 0;
     if (count <= 296) {
       // at most two waves: one launch, so few large systems run concurrently
-      Bucket bk{0, count, count > 0 ? m.h_nao[m.h_list[0]] : 0, 0};
+      Bucket bk{0, count, count > 0 ? m.h_ch_nao[hl[0]] : 0, 0};
       for (int k = 0; k < count; ++k) {
-        const int sy = m.h_list[k];
-        bk.max_m = std::max(bk.max_m, (int)std::ceil(std::max(m.h_nel_a[sy], m.h_nel_b[sy])) + 4);
+        const int c = hl[k];
+        bk.max_m = std::max(bk.max_m, (int)std::ceil(std::max(m.h_ch_nel_a[c], m.h_ch_nel_b[c])) + 4);
       }
       if (count > 0) out.push_back(bk);
       return out;
     }
     while (i < count) {
-      const int n0 = m.h_nao[m.h_list[i]];
+      const int n0 = m.h_ch_nao[hl[i]];
       int lo_edge = 0;
       for (int e : kEdges)
         if (n0 > e) { lo_edge = e; break; }
       Bucket bk{i, 0, n0, 0};
-      while (i < count && m.h_nao[m.h_list[i]] > lo_edge) {
-        const int sy = m.h_list[i];
-        bk.max_m = std::max(bk.max_m, (int)std::ceil(std::max(m.h_nel_a[sy], m.h_nel_b[sy])) + 4);
+      while (i < count && m.h_ch_nao[hl[i]] > lo_edge) {
+        const int c = hl[i];
+        bk.max_m = std::max(bk.max_m, (int)std::ceil(std::max(m.h_ch_nel_a[c], m.h_ch_nel_b[c])) + 4);
         ++bk.count;
         ++i;
       }
@@ -868,11 +1053,13 @@ xtbloom_status_t Engine::compute(const ComputeRequest& req, std::string& error) 
     return out;
   };
   // tridiagonalise, eigenvalues (+ occupations), eigenvectors, back-transform
-  auto eigensolve = [&](int count, int mode, double kt, double ortol_rel, int stage_base) {
-    const std::vector<Bucket> bks = buckets(count);
+  // over the entries of dl (device) / hl (its host copy), systems or channels
+  auto eigensolve = [&](const int32_t* dl, const int32_t* hl, int count, int mode, double kt,
+                        double ortol_rel, int stage_base) {
+    const std::vector<Bucket> bks = buckets(hl, count);
     auto sub = [&](const Bucket& bk) {
       EigArgs gb = eg;
-      gb.list = list + bk.start;
+      gb.list = dl + bk.start;
       return gb;
     };
     XTB_STAGE(stage_base == kStLowdin ? kStLowdin : kStTridiag, (int)bks.size(), for (const Bucket& bk : bks) {
@@ -906,10 +1093,10 @@ xtbloom_status_t Engine::compute(const ComputeRequest& req, std::string& error) 
   // ---- Loewdin orthogonaliser X = U s^-1/2 U^T ----
   cudaMemcpyAsync(m.A.p, m.S.p, (size_t)m.total_mat * 8, cudaMemcpyDeviceToDevice, s);
   std::memcpy(m.h_list, m.h_order.data(), B * sizeof(int32_t));
-  eigensolve(nsys, 1, 0.0, 2e-6, kStLowdin);
+  eigensolve(list, m.h_list, nsys, 1, 0.0, 2e-6, kStLowdin);
   XTB_STAGE(kStLowdin, 2, launch_lowdin_weights(eg, status, nsys, s);
-            gemm(m.Zv.as<double>(), m.Zv.as<double>(), m.X.as<double>(), dnao, dnao, dnao, true,
-                 m.occ.as<double>(), nsys, true));
+            gemm(list, m.Zv.as<double>(), dch_mat, m.Zv.as<double>(), dch_mat, m.X.as<double>(),
+                 dnao, dnao, dnao, true, m.occ.as<double>(), nsys, true));
 
   // ---- SCC ----
   SccArgs a{};
@@ -958,15 +1145,50 @@ xtbloom_status_t Engine::compute(const ComputeRequest& req, std::string& error) 
   a.prec_switch = m.prec_switch;
   a.split_iters = m.split_iters.as<int32_t>();
   const uint8_t* sprec = a.prec;   // split-precision selector of the SCC GEMMs
+  a.qmag = m.qmag.as<double>();
+  a.vmag = m.vmag.as<double>();
+  a.pop_mag = m.pop_mag.as<double>();
+  a.pop_mdip = m.pop_mdip.as<double>();
+  a.pop_mqp = m.pop_mqp.as<double>();
+  a.Pm = m.Pm.as<double>();
+  a.ch_sys = m.ch_sys.as<int32_t>();
+  a.ch_sign = m.ch_sign.as<int32_t>();
+  a.ch_mat = dch_mat;
+  // Spin channels of the active list: without unrestricted systems the channel
+  // list is the system list itself.
+  const bool have_uhf = m.nuhf > 0;
+  int32_t* clist = have_uhf ? m.clist.as<int32_t>() : list;
+  int32_t* dccount = have_uhf ? m.ccount.as<int32_t>() : dcount;
+  int32_t* h_cl = have_uhf ? m.h_clist : m.h_list;
+  a.clist = clist;
+  auto channels = [&](cudaStream_t st) {
+    if (!have_uhf) return;
+    k_channels<<<1, 1024, 0, st>>>(list, dcount, m.beta_ch.as<int32_t>(), clist, dccount);
+    m.prof.launches += 1;
+    cudaMemcpyAsync(m.h_count + 2, dccount, 4, cudaMemcpyDeviceToHost, st);
+    cudaMemcpyAsync(h_cl, clist, (size_t)m.nchan * sizeof(int32_t), cudaMemcpyDeviceToHost, st);
+  };
+  auto channel_count = [&]() { return have_uhf ? m.h_count[2] : m.h_count[0]; };
+  // totals alpha + beta (and P_alpha - P_beta) of the unrestricted systems
+  auto combine = [&](double* M, double* Pm, int cnt, cudaStream_t st) {
+    if (!have_uhf || cnt == 0) return;
+    const int per = std::max(1, std::min(64, (m.max_n * m.max_n + 255) / 256));
+    k_combine_spin<<<dim3(per, cnt), 256, 0, st>>>(list, m.beta_ch.as<int32_t>(), m.nao.as<int32_t>(),
+                                                    m.mat_off.as<int64_t>(), dch_mat, M, Pm);
+    m.prof.launches += 1;
+  };
 
   XTB_STAGE(kStCompact, 1,
             launch_compact(order, nsys, status, a.converged, a.iterations, req.max_iter, list,
                            dcount, s));
   cudaMemcpyAsync(m.h_count, dcount, 4, cudaMemcpyDeviceToHost, s);
   cudaMemcpyAsync(m.h_list, list, B * sizeof(int32_t), cudaMemcpyDeviceToHost, s);
+  channels(s);
   cudaStreamSynchronize(s);
   int count = m.h_count[0];
+  int ccount = channel_count();
   a.count = count;
+  a.ccount = ccount;
   XTB_STAGE(kStPotential, 1, launch_sad_init(a, s));
   // ---- energy and force terms of converged systems ----
   const bool want_forces = (req.flags & XTBLOOM_COMPUTE_FORCES) != 0;
@@ -983,6 +1205,8 @@ xtbloom_status_t Engine::compute(const ComputeRequest& req, std::string& error) 
   fbase.vsh = m.vsh.as<double>();
   fbase.vd = m.vd.as<double>();
   fbase.vq = m.vq.as<double>();
+  fbase.vmag = m.vmag.as<double>();
+  fbase.Pm = m.Pm.as<double>();
   fbase.qsh = m.qsh.as<double>();
   fbase.dip = m.dip.as<double>();
   fbase.qp = m.qp.as<double>();
@@ -1002,24 +1226,18 @@ xtbloom_status_t Engine::compute(const ComputeRequest& req, std::string& error) 
     af.list = flist;
     af.count = fcount;
     if (want_forces) {
-      GemmArgs gw{};
-      gw.sym = 1;
-      gw.list = flist;
-      gw.nao = dnao;
-      gw.dm = dnao;
-      gw.dn = dnao;
-      gw.dk = dnvec;
-      gw.A = m.C.as<double>();
-      gw.offA = m.mat_off.as<int64_t>();
-      gw.B = m.C.as<double>();
-      gw.offB = m.mat_off.as<int64_t>();
-      gw.C = m.W.as<double>();
-      gw.offC = m.mat_off.as<int64_t>();
-      gw.w = m.occ_eps.as<double>();
-      gw.offW = m.ao_off.as<int64_t>();
+      // energy-weighted density per spin channel, then the alpha + beta totals
+      int fcc = fcount;
+      if (have_uhf) {
+        channels(st);
+        cudaStreamSynchronize(st);
+        fcc = channel_count();
+      }
       XTB_STAGE_ON(st, kStForcePairs, 3,
                    launch_potential(af, af.qsh, af.dip, af.qp, m.max_atoms, m.max_shells, st);
-                   launch_gemm(gw, true, true, tiles, fcount, st);
+                   gemm(clist, m.C.as<double>(), dch_mat, m.C.as<double>(), dch_mat, m.W.as<double>(),
+                        dnao, dnao, dnvec, true, m.occ_eps.as<double>(), fcc, true, nullptr, st);
+                   combine(m.W.as<double>(), nullptr, fcount, st);
                    launch_force_pairs(f, m.max_pairs, st));
     }
     XTB_STAGE_ON(st, kStClassical, 1, launch_classical(f, m.max_atoms, m.max_shells, st));
@@ -1030,6 +1248,7 @@ xtbloom_status_t Engine::compute(const ComputeRequest& req, std::string& error) 
                                     m.pc_grad.as<double>(), m.pc_dq.as<double>(), st));
   };
 
+
   // One SCC iteration over the current active list (a.count systems): every
   // launch of it, ending with the compaction of the list and the copies of
   // the new count and list into pinned host memory.
@@ -1037,16 +1256,17 @@ xtbloom_status_t Engine::compute(const ComputeRequest& req, std::string& error) 
     XTB_STAGE(kStPotential, 1, launch_potential(a, a.qsh, a.dip, a.qp, m.max_atoms, m.max_shells, s));
     XTB_STAGE(kStFock, 1, launch_fock(a, m.max_n, s));
     XTB_STAGE(kStTransform, 2,
-              gemm(m.H.as<double>(), m.X.as<double>(), m.T.as<double>(), dnao, dnao, dnao, false,
-                   nullptr, a.count, false, sprec);
-              gemm(m.X.as<double>(), m.T.as<double>(), m.A.as<double>(), dnao, dnao, dnao, false,
-                   nullptr, a.count, true, sprec));
-    eigensolve(a.count, 0, req.kt, 2e-7, kStTridiag);
+              gemm(clist, m.H.as<double>(), dch_mat, m.X.as<double>(), dch_xoff, m.T.as<double>(),
+                   dnao, dnao, dnao, false, nullptr, a.ccount, false, sprec);
+              gemm(clist, m.X.as<double>(), dch_xoff, m.T.as<double>(), dch_mat, m.A.as<double>(),
+                   dnao, dnao, dnao, false, nullptr, a.ccount, true, sprec));
+    eigensolve(clist, h_cl, a.ccount, 0, req.kt, 2e-7, kStTridiag);
     XTB_STAGE(kStDensity, 2,
-              gemm(m.Zv.as<double>(), m.X.as<double>(), m.C.as<double>(), dnvec, dnao, dnao, false,
-                   nullptr, a.count, false, sprec);
-              gemm(m.C.as<double>(), m.C.as<double>(), m.P.as<double>(), dnao, dnao, dnvec, true,
-                   m.occ.as<double>(), a.count, true, sprec));
+              gemm(clist, m.Zv.as<double>(), dch_mat, m.X.as<double>(), dch_xoff, m.C.as<double>(),
+                   dnvec, dnao, dnao, false, nullptr, a.ccount, false, sprec);
+              gemm(clist, m.C.as<double>(), dch_mat, m.C.as<double>(), dch_mat, m.P.as<double>(),
+                   dnao, dnao, dnvec, true, m.occ.as<double>(), a.ccount, true, sprec);
+              combine(m.P.as<double>(), m.Pm.as<double>(), a.count, s));
     XTB_STAGE(kStMulliken, 1, launch_mulliken(a, m.max_n, s));
     XTB_STAGE(kStEnergyMixer, 1, launch_energy_mixer(a, m.max_atoms, m.max_shells, m.max_dim, it == 0, s));
     XTB_STAGE(kStCompact, 1,
@@ -1054,6 +1274,7 @@ xtbloom_status_t Engine::compute(const ComputeRequest& req, std::string& error) 
                              dcount, s));
     cudaMemcpyAsync(m.h_count, dcount, 4, cudaMemcpyDeviceToHost, s);
     cudaMemcpyAsync(m.h_list, list, B * sizeof(int32_t), cudaMemcpyDeviceToHost, s);
+    channels(s);
   };
   // Graph replay: while the active set is unchanged (same count, hence the
   // same list), the iteration's launches are identical; the iteration is
@@ -1065,6 +1286,7 @@ xtbloom_status_t Engine::compute(const ComputeRequest& req, std::string& error) 
   bool graphs_ok = m.graphs && !m.prof.on;
   for (int it = 0; it < req.max_iter && count > 0; ++it) {
     a.count = count;
+    a.ccount = ccount;
     bool ran = false;
     if (graphs_ok && count == prev_count) {
       if (gexec == nullptr || graph_count != count) {
@@ -1107,6 +1329,7 @@ xtbloom_status_t Engine::compute(const ComputeRequest& req, std::string& error) 
                    ran ? " (graph)" : "");
     }
     count = m.h_count[0];
+    ccount = channel_count();
     if (launch_error) break;
   }
   if (gexec) cudaGraphExecDestroy(gexec);

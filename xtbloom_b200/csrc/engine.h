@@ -17,6 +17,7 @@ struct HostBatch {
   std::vector<int32_t> Z;
   std::vector<double> qmol;
   std::vector<int32_t> uhf;
+  std::vector<int32_t> nch;   // spin channels per system (1 or 2)
 };
 
 struct ComputeRequest {
@@ -29,6 +30,7 @@ struct ComputeRequest {
   double ctol = 1e-6, etol = 1e-8, kt = 0.0;
   int32_t memory = 8;
   double damping = 0.4;
+  bool spin_channels = false;   // the batch carries a spin_channels field
 };
 
 class Engine {

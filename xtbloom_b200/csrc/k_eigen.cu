@@ -240,7 +240,7 @@ __global__ void __launch_bounds__(256) k_gemm(GemmArgs g) {
     ti = blockIdx.x / tn;
     tj = blockIdx.x % tn;
   }
-  if (g.prec != nullptr && g.prec[s] == 0)
+  if (g.prec != nullptr && g.prec[g.prec_of != nullptr ? g.prec_of[s] : s] == 0)
     gemm_tile_tf32x3<TA, W>(g, s, M, N, K, ld, ti, tj);
   else
     gemm_tile_f64<TA, W>(g, s, M, N, K, ld, ti, tj);

@@ -36,6 +36,10 @@ __global__ void __launch_bounds__(128) k_force_pairs(ForceArgs f) {
   const int64_t mo = t.mat_off[s];
   const double* P = f.P + mo;
   const double* W = f.W + mo;
+  // unrestricted: the magnetisation is an overlap population too, so
+  // P_alpha - P_beta with the spin potential enters the overlap adjoint
+  const bool uhf = t.nch[s] == 2;
+  const double* Pm = uhf ? f.Pm + mo : nullptr;
   if (A == B) return;   // onsite blocks: k_force_onsite
   const double v[3] = {t.pos[3 * gA] - t.pos[3 * gB], t.pos[3 * gA + 1] - t.pos[3 * gB + 1],
                        t.pos[3 * gA + 2] - t.pos[3 * gB + 2]};
@@ -52,12 +56,14 @@ __global__ void __launch_bounds__(128) k_force_pairs(ForceArgs f) {
     const double* ak = t.p_alpha + t.sh_p0[ks];
     const double* ck = t.p_coeff + t.sh_p0[ks];
     const double vk = f.vsh[ks];
+    const double vmk = uhf ? f.vmag[ks] : 0.0;
     for (int bs = t.atom_sh[gB]; bs < t.atom_sh[gB + 1]; ++bs) {
       const int lb = t.sh_l[bs];
       const int npb = t.sh_np[bs];
       const double* ab = t.p_alpha + t.sh_p0[bs];
       const double* cb = t.p_coeff + t.sh_p0[bs];
       const double vb = f.vsh[bs];
+      const double vmb = uhf ? f.vmag[bs] : 0.0;
       // H0 factor pieces
       const double avg = 0.5 * (lev(t, bs, f.cn) + lev(t, ks, f.cn));
       const double zi = t.sh_zeta[bs], zj = t.sh_zeta[ks];
@@ -81,7 +87,8 @@ __global__ void __launch_bounds__(128) k_force_pairs(ForceArgs f) {
           sph_pair<true>(lb, ib, lk, ik, ab, cb, npb, ak, ck, npk, v, val, dv);
           const double S = val[0];
           bw += Pv * S;
-          const double sA = 2.0 * (Pv * fac - Wv) - Pv * (vb + vk);
+          double sA = 2.0 * (Pv * fac - Wv) - Pv * (vb + vk);
+          if (uhf) sA -= Pm[row * n + col] * (vmb + vmk);
           double fD[3], rD[3], qadj[6], rQ[6];
 #pragma unroll
           for (int c = 0; c < 3; ++c) {

@@ -40,6 +40,12 @@ __global__ void k_sad_init(SccArgs a) {
       a.mx_cur[v0 + ns + 3 * na + 6 * i + c] = 0.0;
     }
   }
+  if (t.nch[s] == 2) {
+    // the magnetisation block of the mixed vector starts at zero
+    const int64_t d1 = ns + 9 * na;
+    for (int64_t i = threadIdx.x; i < d1; i += blockDim.x) a.mx_cur[v0 + d1 + i] = 0.0;
+    for (int64_t i = threadIdx.x; i < ns; i += blockDim.x) a.qmag[s0 + i] = 0.0;
+  }
   if (threadIdx.x == 0) {
     a.iterations[s] = 0;
     a.converged[s] = 0;
@@ -187,6 +193,17 @@ __global__ void __launch_bounds__(256) k_potential_shells(SccArgs a, const doubl
   for (int i = threadIdx.x; i < ns; i += blockDim.x) sq[i] = qsh[s0 + i];
   __syncthreads();
   potential_shells(a, s, sq, vat);
+  // spin potential v_mag = W m of the atom-local couplings (unrestricted systems)
+  if (t.nch[s] == 2) {
+    for (int i = threadIdx.x; i < ns; i += blockDim.x) {
+      const int64_t sh = s0 + i;
+      const int at = t.sh_atom[sh];
+      const int f0 = t.atom_sh[at], cnt = t.atom_sh[at + 1] - f0;
+      double v = 0.0;
+      for (int k = 0; k < cnt; ++k) v = fma(t.sh_spinw[3 * sh + k], a.qmag[f0 + k], v);
+      a.vmag[sh] = v;
+    }
+  }
 }
 
 void launch_potential(const SccArgs& a, const double* qsh, const double* dip, const double* qp,
@@ -221,10 +238,15 @@ __device__ __forceinline__ double g_element(const SccArgs& a, int64_t idx, int a
   return g;
 }
 
+// One spin channel per grid row: the restricted channel (or alpha/beta of an
+// unrestricted system, with the spin potential added with sign +1 / -1:
+// H_sigma = H0 - S (v + sigma v_mag)_mu,nu / 2 - ...).
 __global__ void __launch_bounds__(256) k_fock(SccArgs a) {
   __shared__ double sg[32][33];
   const DevTopo& t = a.t;
-  const int s = a.list[blockIdx.y];
+  const int ch = a.clist[blockIdx.y];
+  const int s = a.ch_sys[ch];
+  const double sgn = (double)a.ch_sign[ch];
   const int n = t.nao[s];
   const int T = (n + 31) / 32;
   const int64_t p = blockIdx.x;
@@ -237,6 +259,7 @@ __global__ void __launch_bounds__(256) k_fock(SccArgs a) {
   const int row0 = ti * 32, col0 = tj * 32;
   const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
   const int64_t mo = t.mat_off[s];
+  const int64_t ho = a.ch_mat[ch];   // this channel's Hamiltonian
   const int64_t ao0 = t.ao_off[s];
   // transposed tile: G(col0 + r, row0 + c) -> sg[r][c]
   for (int r = ty; r < 32; r += 8) {
@@ -249,7 +272,8 @@ __global__ void __launch_bounds__(256) k_fock(SccArgs a) {
   double h[4];
   const int y = col0 + tx;
   const bool yin = y < n;
-  const double vy = yin ? a.vsh[t.ao_sh[ao0 + y]] : 0.0;
+  const double vy =
+      yin ? a.vsh[t.ao_sh[ao0 + y]] + (sgn != 0.0 ? sgn * a.vmag[t.ao_sh[ao0 + y]] : 0.0) : 0.0;
   const int aty = yin ? t.ao_at[ao0 + y] : 0;
 #pragma unroll
   for (int k = 0; k < 4; ++k) {
@@ -259,9 +283,10 @@ __global__ void __launch_bounds__(256) k_fock(SccArgs a) {
     if (x < n && yin) {
       const int64_t idx = mo + (int64_t)x * n + y;
       const double g1 = g_element(a, idx, aty);
-      const double vx = a.vsh[t.ao_sh[ao0 + x]];
+      const int shx = t.ao_sh[ao0 + x];
+      const double vx = a.vsh[shx] + (sgn != 0.0 ? sgn * a.vmag[shx] : 0.0);
       h[k] = a.H0[idx] - 0.5 * a.S[idx] * (vx + vy) - 0.5 * (g1 + sg[tx][r]);
-      a.H[idx] = h[k];
+      a.H[ho + (int64_t)x * n + y] = h[k];
     }
   }
   if (ti == tj) return;
@@ -271,14 +296,14 @@ __global__ void __launch_bounds__(256) k_fock(SccArgs a) {
   __syncthreads();
   for (int r = ty; r < 32; r += 8) {
     const int x = col0 + r, yy = row0 + tx;
-    if (x < n && yy < n) a.H[mo + (int64_t)x * n + yy] = sg[r][tx];
+    if (x < n && yy < n) a.H[ho + (int64_t)x * n + yy] = sg[r][tx];
   }
 }
 
 void launch_fock(const SccArgs& a, int max_n, cudaStream_t stream) {
-  if (a.count == 0) return;
+  if (a.ccount == 0) return;
   const int T = (max_n + 31) / 32;
-  dim3 grid((unsigned)(T * (T + 1) / 2), a.count);
+  dim3 grid((unsigned)(T * (T + 1) / 2), a.ccount);
   k_fock<<<grid, 256, 0, stream>>>(a);
 }
 
@@ -291,10 +316,13 @@ void launch_fock(const SccArgs& a, int max_n, cudaStream_t stream) {
 // the same in every run.
 constexpr int kMullThreads = 512;
 
-__global__ void __launch_bounds__(kMullThreads) k_mulliken(SccArgs a) {
-  extern __shared__ double sm[];
+// Populations of density P (at the system's matrix offset) into the shell,
+// dipole and quadrupole arrays; with want_trace, also returns Tr(P H0)
+// (block-wide).  part: shared memory of kMullThreads / cw * 10 * n doubles.
+__device__ __forceinline__ double mulliken_pass(const SccArgs& a, int s, const double* Pbase,
+                                                bool want_trace, double* part, double* red,
+                                                double* out_sh, double* out_dip, double* out_qp) {
   const DevTopo& t = a.t;
-  const int s = a.list[blockIdx.x];
   const int n = t.nao[s];
   const int64_t mo = t.mat_off[s];
   const int cw = min(kMullThreads, (n + 31) & ~31);   // threads per row chunk
@@ -302,8 +330,6 @@ __global__ void __launch_bounds__(kMullThreads) k_mulliken(SccArgs a) {
   const int chunk = threadIdx.x / cw, col0 = threadIdx.x - chunk * cw;
   const int rows = (n + rp - 1) / rp;
   const int r0 = min(n, chunk * rows), r1 = min(n, r0 + rows);
-  double* part = sm;           // rp x 10 x n: P S, P D (3), P Q (6) per column
-  __shared__ double red[33];
   double ph = 0.0;
   if (chunk < rp) {
     for (int col = col0; col < n; col += cw) {
@@ -312,9 +338,9 @@ __global__ void __launch_bounds__(kMullThreads) k_mulliken(SccArgs a) {
       for (int c = 0; c < 10; ++c) v[c] = 0.0;
       for (int r = r0; r < r1; ++r) {
         const int64_t idx = mo + (int64_t)r * n + col;
-        const double pv = a.P[idx];
+        const double pv = Pbase[idx];
         v[0] = fma(pv, a.S[idx], v[0]);
-        ph = fma(pv, a.H0[idx], ph);
+        if (want_trace) ph = fma(pv, a.H0[idx], ph);
 #pragma unroll
         for (int c = 0; c < 3; ++c) v[1 + c] = fma(pv, a.D[c * a.total_mat + idx], v[1 + c]);
 #pragma unroll
@@ -326,7 +352,6 @@ __global__ void __launch_bounds__(kMullThreads) k_mulliken(SccArgs a) {
     }
   }
   const double eb = block_sum(ph, red);   // includes the barrier before the sums below
-  if (threadIdx.x == 0) a.e_core[s] = eb;
   // column totals over the chunks (in chunk order), into chunk 0's slots
   for (int idx = threadIdx.x; idx < 10 * n; idx += blockDim.x) {
     double v = part[idx];
@@ -334,13 +359,12 @@ __global__ void __launch_bounds__(kMullThreads) k_mulliken(SccArgs a) {
     part[idx] = v;
   }
   __syncthreads();
-  const double* cps = part;
   const int64_t s0 = t.shell_off[s], s1 = t.shell_off[s + 1];
   for (int64_t sh = s0 + threadIdx.x; sh < s1; sh += blockDim.x) {
     const int first = t.sh_ao[sh], cnt = 2 * t.sh_l[sh] + 1;
     double v = 0.0;
-    for (int k = 0; k < cnt; ++k) v += cps[first + k];
-    a.pop_sh[sh] = v;
+    for (int k = 0; k < cnt; ++k) v += part[first + k];
+    out_sh[sh] = v;
   }
   const int64_t a0 = t.atom_off[s], a1 = t.atom_off[s + 1];
   for (int64_t at = a0 + threadIdx.x; at < a1; at += blockDim.x) {
@@ -352,9 +376,26 @@ __global__ void __launch_bounds__(kMullThreads) k_mulliken(SccArgs a) {
         for (int c = 0; c < 6; ++c) pq[c] += part[(4 + c) * n + first + k];
       }
     }
-    for (int c = 0; c < 3; ++c) a.pop_dip[3 * at + c] = pd[c];
-    for (int c = 0; c < 6; ++c) a.pop_qp[6 * at + c] = pq[c];
+    for (int c = 0; c < 3; ++c) out_dip[3 * at + c] = pd[c];
+    for (int c = 0; c < 6; ++c) out_qp[6 * at + c] = pq[c];
   }
+  __syncthreads();   // part is reused by a second pass
+  return eb;
+}
+
+// One CTA per system.  The n rows are cut into fixed chunks; thread
+// (chunk, column) sums its column over its chunk, and the chunks, shells,
+// atoms and the trace are then added in a fixed order, so the populations are
+// the same in every run.  Unrestricted systems also get the magnetisation
+// populations of P_alpha - P_beta.
+__global__ void __launch_bounds__(kMullThreads) k_mulliken(SccArgs a) {
+  extern __shared__ double sm[];
+  __shared__ double red[33];
+  const int s = a.list[blockIdx.x];
+  const double eb = mulliken_pass(a, s, a.P, true, sm, red, a.pop_sh, a.pop_dip, a.pop_qp);
+  if (threadIdx.x == 0) a.e_core[s] = eb;
+  if (a.t.nch[s] == 2)
+    mulliken_pass(a, s, a.Pm, false, sm, red, a.pop_mag, a.pop_mdip, a.pop_mqp);
 }
 
 void launch_mulliken(const SccArgs& a, int max_n, cudaStream_t stream) {
@@ -403,8 +444,10 @@ __global__ void __launch_bounds__(256) k_energy_mixer(SccArgs a) {
   const int na = (int)(t.atom_off[s + 1] - a0);
   const int64_t s0 = t.shell_off[s];
   const int ns = (int)(t.shell_off[s + 1] - s0);
-  const int dim = ns + 9 * na;
-  double* raw = sm;                       // dim: [qsh, dip (3na), qp (6na)]
+  const int d1 = ns + 9 * na;              // charge block
+  const bool uhf = t.nch[s] == 2;
+  const int dim = uhf ? 2 * d1 : d1;
+  double* raw = sm;                       // dim: [qsh, dip (3na), qp (6na)] (+ the same for m)
   double* qat = raw + dim;                // na
   double* w = qat + na;                   // 7 na
   double* red = w + kMaxD4Refs * na;      // 64 + 8*64
@@ -413,6 +456,12 @@ __global__ void __launch_bounds__(256) k_energy_mixer(SccArgs a) {
   for (int i = tid; i < ns; i += bs) raw[i] = t.sh_refocc[s0 + i] - a.pop_sh[s0 + i];
   for (int i = tid; i < 3 * na; i += bs) raw[ns + i] = -a.pop_dip[3 * a0 + i];
   for (int i = tid; i < 6 * na; i += bs) raw[ns + 3 * na + i] = -a.pop_qp[6 * a0 + i];
+  if (uhf) {
+    // magnetisation m = pop_beta - pop_alpha (the charge-like sign of the populations)
+    for (int i = tid; i < ns; i += bs) raw[d1 + i] = -a.pop_mag[s0 + i];
+    for (int i = tid; i < 3 * na; i += bs) raw[d1 + ns + i] = -a.pop_mdip[3 * a0 + i];
+    for (int i = tid; i < 6 * na; i += bs) raw[d1 + ns + 3 * na + i] = -a.pop_mqp[6 * a0 + i];
+  }
   __syncthreads();
   for (int i = tid; i < na; i += bs) {
     const int64_t g = a0 + i;
@@ -482,6 +531,18 @@ __global__ void __launch_bounds__(256) k_energy_mixer(SccArgs a) {
                   nullptr) * damp;
     }
   }
+  // spin polarisation: E_spin = 1/2 sum_A m_A^T W_A m_A (raw magnetisation)
+  double es = 0.0;
+  if (uhf) {
+    for (int i = tid; i < ns; i += bs) {
+      const int64_t sh = s0 + i;
+      const int at = t.sh_atom[sh];
+      const int f0 = t.atom_sh[at] - (int)s0, cnt = t.atom_sh[at + 1] - t.atom_sh[at];
+      double v = 0.0;
+      for (int k = 0; k < cnt; ++k) v = fma(t.sh_spinw[3 * sh + k], raw[d1 + f0 + k], v);
+      es = fma(0.5 * raw[d1 + i], v, es);
+    }
+  }
   // external point charges: E_pc = sum_s q_s V_s (potential fixed by the geometry)
   double ep = 0.0;
   if (t.vpc != nullptr)
@@ -491,9 +552,11 @@ __global__ void __launch_bounds__(256) k_energy_mixer(SccArgs a) {
   ea = block_sum(ea, red);
   ed = block_sum(ed, red);
   ep = block_sum(ep, red);
+  es = block_sum(es, red);
   const double ecore = a.e_core[s];
-  const double ts = -a.kt * a.entropy[s];
-  const double F = ecore + e2 + e3 + ea + ed + ep + ts;
+  const int bch = t.beta_ch[s];
+  const double ts = -a.kt * (a.entropy[s] + (bch >= 0 ? a.entropy[bch] : 0.0));
+  const double F = ecore + e2 + e3 + ea + ed + ep + es + ts;
 
   // ---- modified Broyden (Johnson) ----
   const int64_t v0 = t.vec_off[s];
@@ -611,8 +674,10 @@ __global__ void __launch_bounds__(256) k_energy_mixer(SccArgs a) {
       a.qsh[s0 + i] = out;
     } else if (i < ns + 3 * na) {
       a.dip[3 * a0 + (i - ns)] = out;
-    } else {
+    } else if (i < d1) {
       a.qp[6 * a0 + (i - ns - 3 * na)] = out;
+    } else if (i < d1 + ns) {
+      a.qmag[s0 + (i - d1)] = out;   // magnetisation multipoles live only in the mixer state
     }
   }
   if (tid == 0) {
@@ -626,6 +691,7 @@ __global__ void __launch_bounds__(256) k_energy_mixer(SccArgs a) {
     tm[kTermD4] = ed;
     tm[kTermEntropy] = ts;
     tm[kTermPc] = ep;
+    tm[kTermSpin] = es;
     if (!exact) {
       a.split_iters[s] += 1;
       if (rms < a.prec_switch) a.prec[s] = 1;

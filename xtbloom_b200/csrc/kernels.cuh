@@ -21,6 +21,7 @@ struct GemmArgs {
   const int64_t* offW;
   int32_t sym;             // C is symmetric: compute the lower tiles, mirror them
   const uint8_t* prec;     // per system: 0 = split-precision (3xTF32) tile, else FP64; NULL = FP64
+  const int32_t* prec_of;  // list entry (channel) -> index into prec; NULL = the entry itself
 };
 
 struct EigArgs {
@@ -60,6 +61,22 @@ struct SccArgs {
   double* vsh;        // per shell (scalar shell + atomic potential)
   double* vd;
   double* vq;
+  // spin polarisation (unrestricted systems): magnetisation m = pop_beta -
+  // pop_alpha per shell (mixed input), its potential W m, and the raw
+  // magnetisation populations of P_alpha - P_beta
+  double* qmag;
+  double* vmag;
+  double* pop_mag;    // per shell: sum (P_a - P_b) S
+  double* pop_mdip;   // 3 per atom
+  double* pop_mqp;    // 6 per atom
+  const double* Pm;   // P_alpha - P_beta at the system's matrix offset
+  // spin channels: channel c of an active list -> system, sign (0 restricted,
+  // +1 alpha, -1 beta), matrix offset of its Hamiltonian
+  const int32_t* clist;
+  int32_t ccount;
+  const int32_t* ch_sys;
+  const int32_t* ch_sign;
+  const int64_t* ch_mat;
   // geometry caches
   const double* gam;
   const double* mrad;
@@ -148,6 +165,8 @@ struct ForceArgs {
   const double* vsh;
   const double* vd;
   const double* vq;
+  const double* vmag;     // spin potential per shell (unrestricted systems)
+  const double* Pm;       // P_alpha - P_beta (unrestricted systems)
   const double* qsh;
   const double* dip;
   const double* qp;

@@ -3,7 +3,8 @@
 The GFN2-xTB element/shell parameters (tblite 0.7.0 export), the Stewart
 STO-nG expansion tables, the D4 reference tables (dftd4) and the two mctc-lib
 radius tables are read from the reference checkout's published data files
-(``data/parameters/gfn2.json``, ``tblite_sto.hpp``, ``d4.hpp``) and from the
+(``data/parameters/gfn2.json``, ``tblite_sto.hpp``, ``d4.hpp``,
+``tblite_spin.hpp``) and from the
 two small radius tables in ``src/model/gfn2/h0.cpp`` and
 ``src/model/gfn2/coordination.cpp``.  Nothing is typed in by hand: every
 number is parsed from those files and written to ``params.npz`` beside this
@@ -145,12 +146,23 @@ def d4_tables(ref: Path) -> dict[str, np.ndarray]:
     }
 
 
+def spin_tables(ref: Path) -> dict[str, np.ndarray]:
+    """Element spin constants W_ll' (ss, sp, pp, sd, pd, dd; Hartree) of tblite,
+    parsed from ``data/parameters/tblite_spin.hpp``."""
+    text = (ref / "data" / "parameters" / "tblite_spin.hpp").read_text()
+    start = text.index("kSpinConstants{{")
+    body = text[start + len("kSpinConstants{{"):text.index("}};", start)]
+    vals = np.array(_numbers(body), float)
+    return {"spin_constants": vals.reshape(86, 6)}
+
+
 def generate(ref: Path, out: Path) -> None:
     tables: dict[str, np.ndarray] = {}
     tables.update(gfn2_tables(ref))
     tables.update(sto_tables(ref))
     tables.update(radius_tables(ref))
     tables.update(d4_tables(ref))
+    tables.update(spin_tables(ref))
     np.savez_compressed(out, **tables)
 
 

@@ -180,6 +180,24 @@ def config2(count: int = 1024, seed: int = 2, npc: int = 200):
     return b
 
 
+def config4(count: int = 2048, seed: int = 4):
+    """Open-shell radicals (doublets, two spin channels): alkane chains C_nH_(2n+2)
+    with n uniform in 4..45 and one H removed at a uniform random carbon; 15 % of
+    them carry 1-3 H -> Cl or Br substitutions (C-Cl 3.33, C-Br 3.65 bohr), seed 4."""
+    rng = np.random.default_rng(seed)
+    mols = []
+    for _ in range(count):
+        c = int(rng.integers(4, 46))
+        rm = int(rng.integers(0, c))
+        hal: dict = {}
+        if rng.random() < 0.15:
+            for _ in range(int(rng.integers(1, 4))):
+                hal.setdefault(int(rng.integers(0, c)), []).append("Cl" if rng.random() < 0.5 else "Br")
+        mols.append(chain(["C"] * c, rng, remove_h_at=rm, halogens=hal))
+    return ragged_from_lists([m[0] for m in mols], [m[1] for m in mols], np.zeros(count),
+                             np.ones(count, np.int32), np.full(count, 2, np.int32))
+
+
 def subset(b: RaggedBatch, idx) -> RaggedBatch:
     idx = list(idx)
     nums, poss = [], []
@@ -187,7 +205,8 @@ def subset(b: RaggedBatch, idx) -> RaggedBatch:
         a0, a1 = int(b.atom_offsets[i]), int(b.atom_offsets[i + 1])
         nums.append(b.atomic_numbers[a0:a1])
         poss.append(b.positions[3 * a0:3 * a1])
-    return ragged_from_lists(nums, poss, b.molecular_charges[idx], b.unpaired_electrons[idx])
+    sc = None if b.spin_channels is None else np.asarray(b.spin_channels)[idx]
+    return ragged_from_lists(nums, poss, b.molecular_charges[idx], b.unpaired_electrons[idx], sc)
 
 
 def molecule(b: RaggedBatch, i: int):
