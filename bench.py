@@ -61,6 +61,8 @@ def parse():
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--form", default="both", choices=["both", "mixed", "fp64"])
     p.add_argument("--graphs", type=int, default=1)
+    p.add_argument("--once", action="store_true",
+                   help="one device-resident call of the chosen form and exit (profiler runs)")
     return p.parse_args()
 
 
@@ -300,6 +302,15 @@ def run_ours(args, world, rank, local):
                 "scc_iterations": np.empty(B, np.int32), "scc_converged": np.empty(B, np.uint8),
                 "per_system_status": np.empty(B, np.int32)}
 
+    if args.once:
+        lib = abi.Library(library_path(), backend=abi.BACKEND_CUDA, device_id=local,
+                          stream=stream.cuda_stream)
+        lib.set_execution(abi.PRECISION_MIXED if args.form == "mixed" else abi.PRECISION_FP64,
+                          capture_graphs=args.graphs)
+        lib.compute(dev_batch, lib.make_options(), new_outs_d())
+        torch.cuda.synchronize()
+        lib.close()
+        return
     forms = {}
     results = {}
     clocks = ClockSampler(local)
