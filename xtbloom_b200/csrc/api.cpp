@@ -241,15 +241,14 @@ xtbloom_status_t validate_and_normalise(const xtbloom_batch_t* batch,
   req.memory = 8;
   req.damping = 0.4;
   if (has_field(options->struct_size, XTBLOOM_COMPUTE_OPTIONS_V2_SIZE)) {
-    if (options->scc_start_mode == XTBLOOM_SCC_START_WARM) {
-      err = "WARM start requires a converged compatible checkpoint; none is retained";
-      return XTBLOOM_STATUS_INVALID_ARGUMENT;
-    }
-    if (options->scc_start_mode != XTBLOOM_SCC_START_FRESH && options->scc_start_mode != 0) {
+    if (options->scc_start_mode != XTBLOOM_SCC_START_FRESH &&
+        options->scc_start_mode != XTBLOOM_SCC_START_WARM && options->scc_start_mode != 0) {
       err = "unknown SCC start mode";
       return XTBLOOM_STATUS_INVALID_ARGUMENT;
     }
   }
+  req.warm = has_field(options->struct_size, XTBLOOM_COMPUTE_OPTIONS_V2_SIZE) &&
+             options->scc_start_mode == XTBLOOM_SCC_START_WARM;
   if (has_field(options->struct_size, XTBLOOM_COMPUTE_OPTIONS_V3_SIZE)) {
     if (options->scc_mixer != XTBLOOM_SCC_MIXER_MODIFIED_BROYDEN || options->scc_mixer_history < 1 ||
         options->scc_mixer_history > 64 || !(options->scc_mixer_damping > 0.0) ||

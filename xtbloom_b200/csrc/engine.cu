@@ -255,6 +255,24 @@ struct Engine::Impl {
   double prec_switch = 1e-5;
   bool graphs = false;
   Dbuf prec, split_iters;
+  // strict WARM start: the converged state of the latest fully converged call
+  // and that call's identity (topology, charges, spin, point-charge layout,
+  // requested properties and SCC settings)
+  Dbuf ck_qsh, ck_dip, ck_qp, ck_qmag, ck_mdip, ck_mqp;
+  bool ck_valid = false;
+  struct CallIdentity {
+    HostBatch topo;
+    uint32_t flags = 0;
+    int32_t max_iter = 0, memory = 0;
+    double ctol = 0, etol = 0, kt = 0, damping = 0;
+    std::vector<int64_t> pc_off;
+    bool operator==(const CallIdentity& o) const {
+      return topo.nsys == o.topo.nsys && topo.atom_off == o.topo.atom_off && topo.Z == o.topo.Z &&
+             topo.qmol == o.topo.qmol && topo.uhf == o.topo.uhf && topo.nch == o.topo.nch &&
+             flags == o.flags && max_iter == o.max_iter && memory == o.memory && ctol == o.ctol &&
+             etol == o.etol && kt == o.kt && damping == o.damping && pc_off == o.pc_off;
+    }
+  } ck_id;
   Dbuf fdone;
   Profiler prof;
 
@@ -910,6 +928,26 @@ xtbloom_status_t Engine::compute(const ComputeRequest& req, std::string& error) 
       cudaStreamSynchronize(s);
     }
   }
+  // ---- strict WARM policy (reference include/xtbloom/xtbloom.h:502-523): a
+  // WARM call needs the checkpoint of the latest fully converged call with the
+  // same identity; every accepted call consumes the checkpoint ----
+  Impl::CallIdentity ident;
+  ident.topo = hb;
+  ident.flags = req.flags;
+  ident.max_iter = req.max_iter;
+  ident.memory = req.memory;
+  ident.ctol = req.ctol;
+  ident.etol = req.etol;
+  ident.kt = req.kt;
+  ident.damping = req.damping;
+  if (m.have_pc) ident.pc_off = m.h_pc_off;
+  if (req.warm && !(m.ck_valid && ident == m.ck_id)) {
+    error = "WARM start requires the checkpoint of a fully converged call with the same topology, "
+            "charges, spin settings, point-charge layout, requested properties and SCC settings";
+    return XTBLOOM_STATUS_INVALID_ARGUMENT;
+  }
+  const bool warm = req.warm;
+  m.ck_valid = false;
   // Broyden history sized by the requested memory
   const int M = req.memory;
   if (!m.mx_df.reserve((size_t)m.total_vec * M * 8) || !m.mx_u.reserve((size_t)m.total_vec * M * 8) ||
@@ -1189,7 +1227,16 @@ xtbloom_status_t Engine::compute(const ComputeRequest& req, std::string& error) 
   int ccount = channel_count();
   a.count = count;
   a.ccount = ccount;
-  XTB_STAGE(kStPotential, 1, launch_sad_init(a, s));
+  a.ck_qsh = m.ck_qsh.as<double>();
+  a.ck_dip = m.ck_dip.as<double>();
+  a.ck_qp = m.ck_qp.as<double>();
+  a.ck_qmag = m.ck_qmag.as<double>();
+  a.ck_mdip = m.ck_mdip.as<double>();
+  a.ck_mqp = m.ck_mqp.as<double>();
+  if (warm)
+    XTB_STAGE(kStPotential, 1, launch_warm_init(a, s));
+  else
+    XTB_STAGE(kStPotential, 1, launch_sad_init(a, s));
   // ---- energy and force terms of converged systems ----
   const bool want_forces = (req.flags & XTBLOOM_COMPUTE_FORCES) != 0;
   const bool want_pcf = (req.flags & XTBLOOM_COMPUTE_POINT_CHARGE_FORCES) != 0;
@@ -1376,13 +1423,32 @@ xtbloom_status_t Engine::compute(const ComputeRequest& req, std::string& error) 
   put(r.scc_iterations, m.iterations.p, B * 4);
   put(r.scc_converged, m.converged.p, B);
   put(r.per_system_status, status, B * 4);
+  // a fully converged call leaves its converged state as the WARM checkpoint
+  const bool fully_converged = count == nsys;
+  if (fully_converged) {
+    const size_t sh = (size_t)m.nshells * 8, at = (size_t)N * 8;
+    const bool ok = m.ck_qsh.reserve(sh) && m.ck_dip.reserve(3 * at) && m.ck_qp.reserve(6 * at) &&
+                    m.ck_qmag.reserve(sh) && m.ck_mdip.reserve(3 * at) && m.ck_mqp.reserve(6 * at) &&
+                    cudaMemcpyAsync(m.ck_qsh.p, m.qsh.p, sh, cudaMemcpyDeviceToDevice, s) == cudaSuccess &&
+                    cudaMemcpyAsync(m.ck_dip.p, m.dip.p, 3 * at, cudaMemcpyDeviceToDevice, s) == cudaSuccess &&
+                    cudaMemcpyAsync(m.ck_qp.p, m.qp.p, 6 * at, cudaMemcpyDeviceToDevice, s) == cudaSuccess &&
+                    (m.nuhf == 0 ||
+                     (cudaMemcpyAsync(m.ck_qmag.p, m.qmag.p, sh, cudaMemcpyDeviceToDevice, s) == cudaSuccess &&
+                      cudaMemcpyAsync(m.ck_mdip.p, m.pop_mdip.p, 3 * at, cudaMemcpyDeviceToDevice, s) == cudaSuccess &&
+                      cudaMemcpyAsync(m.ck_mqp.p, m.pop_mqp.p, 6 * at, cudaMemcpyDeviceToDevice, s) == cudaSuccess));
+    if (!ok) (void)cudaGetLastError();
+    m.ck_valid = ok;
+    if (ok) m.ck_id = ident;
+  }
   const cudaError_t ce = cudaStreamSynchronize(s);
   if (ce != cudaSuccess) {
+    m.ck_valid = false;
     error = std::string("CUDA failure: ") + cudaGetErrorString(ce);
     return XTBLOOM_STATUS_INTERNAL_ERROR;
   }
   const cudaError_t le = cudaGetLastError();
   if (le != cudaSuccess) {
+    m.ck_valid = false;
     error = std::string("CUDA launch failure: ") + cudaGetErrorString(le);
     return XTBLOOM_STATUS_INTERNAL_ERROR;
   }

@@ -31,6 +31,7 @@ struct ComputeRequest {
   int32_t memory = 8;
   double damping = 0.4;
   bool spin_channels = false;   // the batch carries a spin_channels field
+  bool warm = false;            // strict WARM start from the retained checkpoint
 };
 
 class Engine {

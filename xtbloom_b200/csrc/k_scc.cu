@@ -53,6 +53,55 @@ __global__ void k_sad_init(SccArgs a) {
   }
 }
 
+// WARM start (src/runtime/gfn2_cpu_execution.cpp:1261-1266,1313-1325 of the
+// reference): the previous converged state is the first mixed input, the
+// mixer starts a new history from it.
+__global__ void k_warm_init(SccArgs a) {
+  const int s = a.list[blockIdx.x];
+  const DevTopo& t = a.t;
+  const int64_t a0 = t.atom_off[s], na = t.atom_off[s + 1] - a0;
+  const int64_t s0 = t.shell_off[s], ns = t.shell_off[s + 1] - s0;
+  const int64_t v0 = t.vec_off[s];
+  const int64_t d1 = ns + 9 * na;
+  for (int64_t i = threadIdx.x; i < ns; i += blockDim.x) {
+    const double q = a.ck_qsh[s0 + i];
+    a.qsh[s0 + i] = q;
+    a.mx_cur[v0 + i] = q;
+  }
+  for (int64_t i = threadIdx.x; i < 3 * na; i += blockDim.x) {
+    const double v = a.ck_dip[3 * a0 + i];
+    a.dip[3 * a0 + i] = v;
+    a.mx_cur[v0 + ns + i] = v;
+  }
+  for (int64_t i = threadIdx.x; i < 6 * na; i += blockDim.x) {
+    const double v = a.ck_qp[6 * a0 + i];
+    a.qp[6 * a0 + i] = v;
+    a.mx_cur[v0 + ns + 3 * na + i] = v;
+  }
+  if (t.nch[s] == 2) {
+    for (int64_t i = threadIdx.x; i < ns; i += blockDim.x) {
+      const double m = a.ck_qmag[s0 + i];
+      a.qmag[s0 + i] = m;
+      a.mx_cur[v0 + d1 + i] = m;
+    }
+    // magnetisation multipoles: the raw values -pop of the converged iteration
+    for (int64_t i = threadIdx.x; i < 3 * na; i += blockDim.x)
+      a.mx_cur[v0 + d1 + ns + i] = -a.ck_mdip[3 * a0 + i];
+    for (int64_t i = threadIdx.x; i < 6 * na; i += blockDim.x)
+      a.mx_cur[v0 + d1 + ns + 3 * na + i] = -a.ck_mqp[6 * a0 + i];
+  }
+  if (threadIdx.x == 0) {
+    a.iterations[s] = 0;
+    a.converged[s] = 0;
+    a.free_energy[s] = 0.0;
+  }
+}
+
+void launch_warm_init(const SccArgs& a, cudaStream_t stream) {
+  if (a.count == 0) return;
+  k_warm_init<<<a.count, 128, 0, stream>>>(a);
+}
+
 void launch_sad_init(const SccArgs& a, cudaStream_t stream) {
   if (a.count == 0) return;
   k_sad_init<<<a.count, 128, 0, stream>>>(a);

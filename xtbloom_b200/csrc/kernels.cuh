@@ -111,6 +111,14 @@ struct SccArgs {
   // precision ladder: prec[s] = 0 while system s iterates with split-precision
   // GEMMs, 1 once it iterates in FP64 (a system converges only on an FP64
   // iteration); it switches when its residual falls below prec_switch.
+  // WARM start: the retained converged state (shell charges, dipoles,
+  // quadrupoles; magnetisation, its dipoles and quadrupoles) seeds the SCC
+  const double* ck_qsh;
+  const double* ck_dip;
+  const double* ck_qp;
+  const double* ck_qmag;
+  const double* ck_mdip;
+  const double* ck_mqp;
   uint8_t* prec;
   double prec_switch;
   int32_t* split_iters;   // per system: iterations run with split-precision GEMMs
@@ -141,6 +149,7 @@ size_t backtransform_wy_bytes(int n, int m);
 void launch_lowdin_weights(const EigArgs& g, int32_t* status, int count, cudaStream_t stream);
 
 void launch_sad_init(const SccArgs& a, cudaStream_t stream);
+void launch_warm_init(const SccArgs& a, cudaStream_t stream);
 void launch_potential(const SccArgs& a, const double* qsh, const double* dip, const double* qp,
                       int max_atoms, int max_shells, cudaStream_t stream);
 void launch_fock(const SccArgs& a, int max_n, cudaStream_t stream);
