@@ -117,3 +117,16 @@ def test_unrestricted_goldens_pinned_to_tblite_trace():
     assert oh["status"] == 0
     assert oh["scc_iterations"] == oh["tblite_iterations"]
     assert np.abs(np.asarray(oh["charges"]) - np.asarray(oh["tblite_final_charges"])).max() < 2e-5
+
+
+def test_field_goldens_pinned_to_tblite():
+    """The electric-field goldens come from the reference library, whose water
+    energy in the field (0.003, -0.004, 0.005) equals the reference's committed
+    tblite value of its water_efield conformance case."""
+    import json
+
+    from conftest import GOLDEN
+    g = json.loads((GOLDEN / "field_fixtures.json").read_text())
+    w = next(s for s in g["systems"] if s["name"] == "water_efield" and s["case"] == "field")
+    assert w["status"] == 0
+    assert abs(w["energy"] - g["tblite_water_efield_energy"]) < 1e-9

@@ -181,6 +181,31 @@ class XtbloomError(RuntimeError):
         self.status = status
 
 
+INTERACTION_ELECTRIC_FIELD = 0x0101
+
+
+class Interaction(C.Structure):
+    _fields_ = [("type", C.c_int32), ("flags", C.c_uint32), ("system_index", C.c_int64),
+                ("payload_offset", C.c_uint64), ("payload_size", C.c_uint64)]
+
+
+def pack_efields(efields):
+    """Descriptors and payload of electric-field attachments (block_version 1:
+    int32 version, int32 reserved, three doubles) for every row without NaN."""
+    rows = [i for i, e in enumerate(np.asarray(efields, float)) if np.all(np.isfinite(e))]
+    desc = (Interaction * max(len(rows), 1))()
+    payload = np.zeros(32 * max(len(rows), 1), np.uint8)
+    for k, i in enumerate(rows):
+        desc[k] = Interaction(INTERACTION_ELECTRIC_FIELD, 0, i, 32 * k, 32)
+        block = np.zeros(4, np.float64)
+        block[1:] = np.asarray(efields, float)[i]
+        raw = block.view(np.uint8).copy()
+        raw[0:4] = np.frombuffer(np.int32(1).tobytes(), np.uint8)
+        raw[4:8] = 0
+        payload[32 * k:32 * k + 32] = raw
+    return desc, payload, len(rows)
+
+
 def _cbuf(arr) -> ConstBuffer:
     if arr is None:
         return ConstBuffer(None, 0, MEMORY_HOST, 0)
@@ -212,6 +237,9 @@ class RaggedBatch:
     point_charge_positions: object = None
     point_charge_values: object = None
     point_charge_gammas: object = None
+    # per system uniform electric field (Hartree / (e bohr)), shape (B, 3); a row
+    # of NaN (or None for the whole batch) means no attachment
+    efields: object = None
 
     @property
     def batch_size(self) -> int:
@@ -289,6 +317,14 @@ class Library:
             for name in ("point_charge_offsets", "point_charge_positions",
                          "point_charge_values", "point_charge_gammas"):
                 setattr(batch, name, _cbuf(getattr(b, name)))
+        if b.efields is not None:
+            desc, payload, k = pack_efields(b.efields)
+            if k:
+                batch.total_interactions = k
+                batch.interaction_descriptors = ConstBuffer(C.addressof(desc), C.sizeof(Interaction) * k,
+                                                            MEMORY_HOST, 0)
+                batch.interaction_payload = ConstBuffer(payload.ctypes.data, payload.nbytes, MEMORY_HOST, 0)
+                batch._keep = (desc, payload)   # the buffers must outlive the call
         return batch
 
     def make_options(self, model=MODEL_GFN2, flags=COMPUTE_ENERGY | COMPUTE_FORCES | COMPUTE_CHARGES,

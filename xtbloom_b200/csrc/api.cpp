@@ -193,10 +193,115 @@ xtbloom_status_t validate_and_normalise(const xtbloom_batch_t* batch,
     err = "periodic charge-response embedding is not implemented in this CUDA path";
     return XTBLOOM_STATUS_NOT_IMPLEMENTED;
   }
+  // External interaction attachments (src/runtime/validation.cpp:916-1000,
+  // 1104-1135 of the reference): the uniform electric field is executed, every
+  // other known tag is refused as not implemented.
+  req.field_attached.assign(B, 0);
+  req.field.assign(3 * B, 0.0);
   if (has_field(batch->struct_size, XTBLOOM_BATCH_V3_SIZE) &&
       (batch->total_interactions != 0 || buffer_active(batch->interaction_descriptors))) {
-    err = "external interaction attachments are not implemented in this CUDA path";
-    return XTBLOOM_STATUS_NOT_IMPLEMENTED;
+    if (batch->total_interactions < 0) {
+      err = "total_interactions must be nonnegative";
+      return XTBLOOM_STATUS_INVALID_ARGUMENT;
+    }
+    const size_t K = static_cast<size_t>(batch->total_interactions);
+    if (K > 0) {
+      if (!check_in(batch->interaction_descriptors, K * sizeof(xtbloom_interaction_t),
+                    "interaction_descriptors", err))
+        return XTBLOOM_STATUS_INVALID_ARGUMENT;
+      if (!buffer_active(batch->interaction_payload)) {
+        err = "interaction_payload is required when interactions are present";
+        return XTBLOOM_STATUS_INVALID_ARGUMENT;
+      }
+      auto stage = [&](const xtbloom_const_buffer_t& b, size_t bytes, std::vector<unsigned char>& out) {
+        out.resize(bytes);
+        if (bytes == 0) return true;
+        if (b.memory_space == XTBLOOM_MEMORY_HOST) {
+          std::memcpy(out.data(), b.data, bytes);
+          return true;
+        }
+        return cudaMemcpy(out.data(), b.data, bytes, cudaMemcpyDeviceToHost) == cudaSuccess;
+      };
+      std::vector<unsigned char> desc, payload;
+      const size_t pbytes = batch->interaction_payload.size_bytes;
+      if (!stage(batch->interaction_descriptors, K * sizeof(xtbloom_interaction_t), desc) ||
+          !stage(batch->interaction_payload, pbytes, payload)) {
+        err = "failed to read the interaction attachments";
+        return XTBLOOM_STATUS_INVALID_ARGUMENT;
+      }
+      bool other_tag = false;
+      for (size_t k = 0; k < K; ++k) {
+        xtbloom_interaction_t it;
+        std::memcpy(&it, desc.data() + k * sizeof(xtbloom_interaction_t), sizeof(it));
+        const bool known = (it.type >= 0x0101 && it.type <= 0x0104) ||
+                           (it.type >= 0x0201 && it.type <= 0x0205) || it.type == 0x0301 ||
+                           it.type == 0x0302 || it.type == 0x0401;
+        if (it.flags != 0u) {
+          err = "interaction descriptor flags must be zero";
+          return XTBLOOM_STATUS_INVALID_ARGUMENT;
+        }
+        if (!known) {
+          err = "an interaction descriptor uses an unknown or NONE type tag";
+          return XTBLOOM_STATUS_INVALID_ARGUMENT;
+        }
+        if (it.system_index < 0 || static_cast<size_t>(it.system_index) >= B) {
+          err = "an interaction system_index lies outside the batch";
+          return XTBLOOM_STATUS_INVALID_ARGUMENT;
+        }
+        if (it.payload_offset > pbytes || it.payload_size > pbytes - it.payload_offset) {
+          err = "an interaction payload block extends past interaction_payload";
+          return XTBLOOM_STATUS_INVALID_ARGUMENT;
+        }
+        const uintptr_t addr = reinterpret_cast<uintptr_t>(batch->interaction_payload.data) +
+                               static_cast<uintptr_t>(it.payload_offset);
+        if (it.type != XTBLOOM_INTERACTION_ELECTRIC_FIELD) {
+          if (it.payload_size < sizeof(int32_t) || addr % alignof(int32_t) != 0u) {
+            err = "an interaction payload block must contain an aligned block_version";
+            return XTBLOOM_STATUS_INVALID_ARGUMENT;
+          }
+          other_tag = true;
+          continue;
+        }
+        // block_version 1: int32 version, int32 reserved, three doubles (8-byte aligned)
+        if (it.payload_size < 32u || addr % alignof(double) != 0u) {
+          err = "an electric-field interaction payload block is undersized or misaligned";
+          return XTBLOOM_STATUS_INVALID_ARGUMENT;
+        }
+        if (it.payload_size > 32u) {
+          err = "an electric-field interaction payload block exceeds the released contract";
+          return XTBLOOM_STATUS_INVALID_ARGUMENT;
+        }
+        int32_t version = 0, reserved = 0;
+        double e[3];
+        const unsigned char* blk = payload.data() + it.payload_offset;
+        std::memcpy(&version, blk, 4);
+        std::memcpy(&reserved, blk + 4, 4);
+        std::memcpy(e, blk + 8, 24);
+        if (version != 1) {
+          err = "an electric-field interaction uses an unsupported block_version";
+          return XTBLOOM_STATUS_INVALID_ARGUMENT;
+        }
+        if (reserved != 0) {
+          err = "an electric-field interaction reserved payload field must be zero";
+          return XTBLOOM_STATUS_INVALID_ARGUMENT;
+        }
+        if (!std::isfinite(e[0]) || !std::isfinite(e[1]) || !std::isfinite(e[2])) {
+          err = "an electric-field interaction contains NaN or infinity";
+          return XTBLOOM_STATUS_INVALID_ARGUMENT;
+        }
+        const size_t si = static_cast<size_t>(it.system_index);
+        if (req.field_attached[si]) {
+          err = "a batch item carries more than one electric-field attachment";
+          return XTBLOOM_STATUS_INVALID_ARGUMENT;
+        }
+        req.field_attached[si] = 1;
+        for (int c = 0; c < 3; ++c) req.field[3 * si + c] = e[c];
+      }
+      if (other_tag) {
+        err = "an interaction attachment uses a tag whose execution is not implemented";
+        return XTBLOOM_STATUS_NOT_IMPLEMENTED;
+      }
+    }
   }
   if (has_field(batch->struct_size, XTBLOOM_BATCH_V4_SIZE) &&
       (buffer_active(batch->cell_matrices) || buffer_active(batch->periodic_axes))) {
@@ -218,10 +323,6 @@ xtbloom_status_t validate_and_normalise(const xtbloom_batch_t* batch,
   if ((options->flags & ~known) != 0 || options->reserved != 0) {
     err = "compute flags contain reserved bits";
     return XTBLOOM_STATUS_INVALID_ARGUMENT;
-  }
-  if (options->flags & XTBLOOM_COMPUTE_DIPOLE_MOMENTS) {
-    err = "dipole moments are not implemented in this CUDA path";
-    return XTBLOOM_STATUS_NOT_IMPLEMENTED;
   }
   if (options->max_scc_iterations <= 0) {
     err = "max_scc_iterations must be positive";
@@ -273,6 +374,8 @@ xtbloom_status_t validate_and_normalise(const xtbloom_batch_t* batch,
                  "atomic_charges", err) ||
       !check_out(result->point_charge_forces, P * 24,
                  (f & XTBLOOM_COMPUTE_POINT_CHARGE_FORCES) != 0 && P != 0, "point_charge_forces", err) ||
+      !check_out(result->dipole_moments, B * 24, (f & XTBLOOM_COMPUTE_DIPOLE_MOMENTS) != 0,
+                 "dipole_moments", err) ||
       !check_out(result->scc_iterations, B * 4, true, "scc_iterations", err) ||
       !check_out(result->scc_converged, B, true, "scc_converged", err) ||
       !check_out(result->per_system_status, B * 4, true, "per_system_status", err)) {
@@ -315,7 +418,10 @@ xtbloom_status_t run(xtbloom_context_t* ctx, const xtbloom_batch_t* batch,
     err = "unexpected exception in the CUDA engine";
   }
   cudaSetDevice(prev);
-  if (result_flags) *result_flags = 0;
+  if (result_flags)
+    *result_flags = (st == XTBLOOM_STATUS_SUCCESS && (req.flags & XTBLOOM_COMPUTE_DIPOLE_MOMENTS))
+                        ? XTBLOOM_RESULT_DIPOLE_MOMENTS
+                        : 0u;
   if (st != XTBLOOM_STATUS_SUCCESS) return fail(st, err);
   g_last_error.clear();
   return XTBLOOM_STATUS_SUCCESS;

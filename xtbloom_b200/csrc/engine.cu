@@ -235,6 +235,8 @@ struct Engine::Impl {
   Dbuf d, e, tau, eig, occ, occ_eps, entropy, scratch;
   Dbuf qsh, dip, qp, pop_sh, pop_dip, pop_qp, e_core, vsh, vd, vq;
   Dbuf Pm, qmag, vmag, pop_mag, pop_mdip, pop_mqp;
+  Dbuf efield, out_dipoles;
+  bool have_field = false;
   Dbuf free_energy, terms;
   Dbuf mx_cur, mx_prev, mx_res, mx_df, mx_u, mx_omega;
   Dbuf grad, acn, acn_d4, pot_acc;
@@ -266,11 +268,14 @@ struct Engine::Impl {
     int32_t max_iter = 0, memory = 0;
     double ctol = 0, etol = 0, kt = 0, damping = 0;
     std::vector<int64_t> pc_off;
+    std::vector<uint8_t> field_attached;
+    std::vector<double> field;
     bool operator==(const CallIdentity& o) const {
       return topo.nsys == o.topo.nsys && topo.atom_off == o.topo.atom_off && topo.Z == o.topo.Z &&
              topo.qmol == o.topo.qmol && topo.uhf == o.topo.uhf && topo.nch == o.topo.nch &&
              flags == o.flags && max_iter == o.max_iter && memory == o.memory && ctol == o.ctol &&
-             etol == o.etol && kt == o.kt && damping == o.damping && pc_off == o.pc_off;
+             etol == o.etol && kt == o.kt && damping == o.damping && pc_off == o.pc_off &&
+             field_attached == o.field_attached && field == o.field;
     }
   } ck_id;
   Dbuf fdone;
@@ -296,6 +301,7 @@ struct Engine::Impl {
     t.nch = nch.as<int32_t>();
     t.beta_ch = beta_ch.as<int32_t>();
     t.sh_spinw = sh_spinw.as<double>();
+    t.efield = have_field ? efield.as<double>() : nullptr;
     t.Z = Z.as<int32_t>();
     t.atom_sh = atom_sh.as<int32_t>();
     t.pos = pos.as<double>();
@@ -675,22 +681,36 @@ bool read_input(const xtbloom_const_buffer_t& b, void* dst, size_t bytes, cudaSt
   return cudaMemcpyAsync(dst, b.data, bytes, kind, s) == cudaSuccess && cudaStreamSynchronize(s) == cudaSuccess;
 }
 
+// Per system: energy, forces (with the explicit field force q_A E of a
+// uniform field, gfn2_cpu_execution.cpp:1588-1597 of the reference), charges
+// and the dipole moment sum_A q_A R_A + d_A (gfn2_cpu_execution.cpp:1497-1508).
 __global__ void k_publish(DevTopo t, const int32_t* status, const double* free_energy,
                           const double* terms, const double* grad, const double* qsh,
-                          double* energy, double* forces, double* charges) {
+                          const double* dip, double* energy, double* forces, double* charges,
+                          double* dipoles) {
+  __shared__ double red[33];
   const int s = blockIdx.x;
   const bool ok = status[s] == kOk;
   const double nan = __longlong_as_double(0x7ff8000000000000ll);
   const int64_t a0 = t.atom_off[s], a1 = t.atom_off[s + 1];
+  const double* ef = t.efield != nullptr ? t.efield + 3 * s : nullptr;
   if (threadIdx.x == 0)
     energy[s] = ok ? free_energy[s] + terms[kTermCount * (int64_t)s + kTermRep] +
                          terms[kTermCount * (int64_t)s + kTermAtm]
                : nan;
+  double mu[3] = {0.0, 0.0, 0.0};
   for (int64_t a = a0 + threadIdx.x; a < a1; a += blockDim.x) {
     double q = 0.0;
     for (int sh = t.atom_sh[a]; sh < t.atom_sh[a + 1]; ++sh) q += qsh[sh];
     charges[a] = ok ? q : nan;
-    for (int c = 0; c < 3; ++c) forces[3 * a + c] = ok ? -grad[3 * a + c] : nan;
+    for (int c = 0; c < 3; ++c) {
+      forces[3 * a + c] = ok ? -grad[3 * a + c] + (ef != nullptr ? q * ef[c] : 0.0) : nan;
+      mu[c] += q * t.pos[3 * a + c] + dip[3 * a + c];
+    }
+  }
+  for (int c = 0; c < 3; ++c) {
+    const double m = block_sum(mu[c], red);
+    if (threadIdx.x == 0) dipoles[3 * s + c] = ok ? m : nan;
   }
 }
 
@@ -928,6 +948,20 @@ xtbloom_status_t Engine::compute(const ComputeRequest& req, std::string& error) 
       cudaStreamSynchronize(s);
     }
   }
+  // ---- uniform electric fields of the attachments ----
+  m.have_field = false;
+  for (int64_t i = 0; i < B; ++i) m.have_field = m.have_field || req.field_attached[i] != 0;
+  if (!m.out_dipoles.reserve((size_t)B * 24)) {
+    error = "device allocation for the dipole moments failed";
+    return XTBLOOM_STATUS_ALLOCATION_FAILED;
+  }
+  if (m.have_field) {
+    if (!upload(m.efield, req.field, s)) {
+      error = "device allocation for the electric fields failed";
+      return XTBLOOM_STATUS_ALLOCATION_FAILED;
+    }
+    cudaStreamSynchronize(s);   // req.field outlives the upload either way; keep order simple
+  }
   // ---- strict WARM policy (reference include/xtbloom/xtbloom.h:502-523): a
   // WARM call needs the checkpoint of the latest fully converged call with the
   // same identity; every accepted call consumes the checkpoint ----
@@ -941,6 +975,8 @@ xtbloom_status_t Engine::compute(const ComputeRequest& req, std::string& error) 
   ident.kt = req.kt;
   ident.damping = req.damping;
   if (m.have_pc) ident.pc_off = m.h_pc_off;
+  ident.field_attached = req.field_attached;
+  ident.field = req.field;
   if (req.warm && !(m.ck_valid && ident == m.ck_id)) {
     error = "WARM start requires the checkpoint of a fully converged call with the same topology, "
             "charges, spin settings, point-charge layout, requested properties and SCC settings";
@@ -1397,8 +1433,9 @@ xtbloom_status_t Engine::compute(const ComputeRequest& req, std::string& error) 
   XTB_STAGE(kStPublish, 1,
             k_publish<<<nsys, 128, 0, s>>>(t, status, m.free_energy.as<double>(),
                                            m.terms.as<double>(), m.grad.as<double>(),
-                                           m.qsh.as<double>(), m.out_energy.as<double>(),
-                                           m.out_forces.as<double>(), m.out_charges.as<double>()));
+                                           m.qsh.as<double>(), m.dip.as<double>(),
+                                           m.out_energy.as<double>(), m.out_forces.as<double>(),
+                                           m.out_charges.as<double>(), m.out_dipoles.as<double>()));
 #undef XTB_STAGE
 #undef XTB_STAGE_ON
   if (launch_error == cudaSuccess) launch_error = cudaGetLastError();
@@ -1418,6 +1455,7 @@ xtbloom_status_t Engine::compute(const ComputeRequest& req, std::string& error) 
   if (req.flags & XTBLOOM_COMPUTE_ENERGY) put(r.energies, m.out_energy.p, B * 8);
   if (req.flags & XTBLOOM_COMPUTE_FORCES) put(r.forces, m.out_forces.p, 3 * N * 8);
   if (req.flags & XTBLOOM_COMPUTE_ATOMIC_CHARGES) put(r.atomic_charges, m.out_charges.p, N * 8);
+  if (req.flags & XTBLOOM_COMPUTE_DIPOLE_MOMENTS) put(r.dipole_moments, m.out_dipoles.p, B * 24);
   if ((req.flags & XTBLOOM_COMPUTE_POINT_CHARGE_FORCES) && m.have_pc)
     put(r.point_charge_forces, m.out_pcf.p, (size_t)m.npc * 24);
   put(r.scc_iterations, m.iterations.p, B * 4);

@@ -32,6 +32,9 @@ struct ComputeRequest {
   double damping = 0.4;
   bool spin_channels = false;   // the batch carries a spin_channels field
   bool warm = false;            // strict WARM start from the retained checkpoint
+  // uniform electric field per system (Hartree / (e bohr)), from the attachments
+  std::vector<uint8_t> field_attached;
+  std::vector<double> field;
 };
 
 class Engine {

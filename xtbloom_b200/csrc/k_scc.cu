@@ -219,9 +219,15 @@ __global__ void __launch_bounds__(256) k_potential_atoms(SccArgs a, const double
     for (int c = 0; c < 10; ++c) acc[c] = warp_sum(acc[c]);
     if (lane == 0) {
       const int64_t g = a0 + i;
-      vat_out[g] = acc[0];
+      // uniform field (scc_driver.cpp:2555-2582 of the reference): v_at += -E.R,
+      // dipole potential += -E
+      const double* ef = t.efield != nullptr ? t.efield + 3 * s : nullptr;
+      vat_out[g] = acc[0] - (ef != nullptr ? ef[0] * t.pos[3 * g] + ef[1] * t.pos[3 * g + 1] +
+                                                 ef[2] * t.pos[3 * g + 2]
+                                           : 0.0);
       const double dk2 = 2.0 * t.at_dk[g], qk2 = 2.0 * t.at_qk[g];
-      for (int c = 0; c < 3; ++c) a.vd[3 * g + c] = dk2 * dip[3 * g + c] + acc[1 + c];
+      for (int c = 0; c < 3; ++c)
+        a.vd[3 * g + c] = dk2 * dip[3 * g + c] + acc[1 + c] - (ef != nullptr ? ef[c] : 0.0);
       for (int c = 0; c < 6; ++c) a.vq[6 * g + c] = qk2 * scl[c] * qp[6 * g + c] + acc[4 + c];
     }
   }
@@ -580,6 +586,19 @@ __global__ void __launch_bounds__(256) k_energy_mixer(SccArgs a) {
                   nullptr) * damp;
     }
   }
+  // uniform field: E_field = sum_A q_A (-E.R_A) + (-E).d_A (raw charges and
+  // dipoles; scc_driver.cpp:2212-2232 of the reference)
+  double ef = 0.0;
+  if (t.efield != nullptr) {
+    const double* E = t.efield + 3 * s;
+    for (int i = tid; i < na; i += bs) {
+      const int64_t g = a0 + i;
+      const double vat = -(E[0] * t.pos[3 * g] + E[1] * t.pos[3 * g + 1] + E[2] * t.pos[3 * g + 2]);
+      double c = vat * qat[i];
+      for (int k = 0; k < 3; ++k) c = fma(-E[k], rd[3 * i + k], c);
+      ef += c;
+    }
+  }
   // spin polarisation: E_spin = 1/2 sum_A m_A^T W_A m_A (raw magnetisation)
   double es = 0.0;
   if (uhf) {
@@ -602,10 +621,11 @@ __global__ void __launch_bounds__(256) k_energy_mixer(SccArgs a) {
   ed = block_sum(ed, red);
   ep = block_sum(ep, red);
   es = block_sum(es, red);
+  ef = block_sum(ef, red);
   const double ecore = a.e_core[s];
   const int bch = t.beta_ch[s];
   const double ts = -a.kt * (a.entropy[s] + (bch >= 0 ? a.entropy[bch] : 0.0));
-  const double F = ecore + e2 + e3 + ea + ed + ep + es + ts;
+  const double F = ecore + e2 + e3 + ea + ed + ep + es + ef + ts;
 
   // ---- modified Broyden (Johnson) ----
   const int64_t v0 = t.vec_off[s];
@@ -741,6 +761,7 @@ __global__ void __launch_bounds__(256) k_energy_mixer(SccArgs a) {
     tm[kTermEntropy] = ts;
     tm[kTermPc] = ep;
     tm[kTermSpin] = es;
+    tm[kTermField] = ef;
     if (!exact) {
       a.split_iters[s] += 1;
       if (rms < a.prec_switch) a.prec[s] = 1;
