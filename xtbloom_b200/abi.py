@@ -240,6 +240,11 @@ class RaggedBatch:
     # per system uniform electric field (Hartree / (e bohr)), shape (B, 3); a row
     # of NaN (or None for the whole batch) means no attachment
     efields: object = None
+    # charge response b + A q: per-atom shifts b, per-system symmetric
+    # atoms x atoms blocks A (row-major, packed) at charge_response_offsets
+    atomic_potential_shifts: object = None
+    charge_response_offsets: object = None
+    charge_response_matrix: object = None
 
     @property
     def batch_size(self) -> int:
@@ -316,6 +321,10 @@ class Library:
             batch.total_point_charges = int(len(b.point_charge_values))
             for name in ("point_charge_offsets", "point_charge_positions",
                          "point_charge_values", "point_charge_gammas"):
+                setattr(batch, name, _cbuf(getattr(b, name)))
+        if b.charge_response_matrix is not None:
+            batch.total_charge_response_elements = int(len(b.charge_response_matrix))
+            for name in ("atomic_potential_shifts", "charge_response_offsets", "charge_response_matrix"):
                 setattr(batch, name, _cbuf(getattr(b, name)))
         if b.efields is not None:
             desc, payload, k = pack_efields(b.efields)

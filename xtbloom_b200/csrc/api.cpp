@@ -188,10 +188,72 @@ xtbloom_status_t validate_and_normalise(const xtbloom_batch_t* batch,
                  !check_in(batch->point_charge_gammas, P * 8, "point_charge_gammas", err))) {
     return XTBLOOM_STATUS_INVALID_ARGUMENT;
   }
+  // Charge response b + A q for periodic QM/MM coupling (reference
+  // include/xtbloom/xtbloom.h:429-436): per-atom shifts b, per-system
+  // row-major symmetric A packed at charge_response_offsets.
+  req.have_response = false;
   if (batch->total_charge_response_elements != 0 || buffer_active(batch->atomic_potential_shifts) ||
       buffer_active(batch->charge_response_offsets) || buffer_active(batch->charge_response_matrix)) {
-    err = "periodic charge-response embedding is not implemented in this CUDA path";
-    return XTBLOOM_STATUS_NOT_IMPLEMENTED;
+    const int64_t E = batch->total_charge_response_elements;
+    if (E < 0) {
+      err = "total_charge_response_elements must be nonnegative";
+      return XTBLOOM_STATUS_INVALID_ARGUMENT;
+    }
+    if (!check_in(batch->atomic_potential_shifts, N * 8, "atomic_potential_shifts", err) ||
+        !check_in(batch->charge_response_offsets, (B + 1) * 8, "charge_response_offsets", err) ||
+        !check_in(batch->charge_response_matrix, static_cast<size_t>(E) * 8, "charge_response_matrix", err))
+      return XTBLOOM_STATUS_INVALID_ARGUMENT;
+    req.resp_b.resize(N);
+    req.resp_off.resize(B + 1);
+    req.resp_A.resize(static_cast<size_t>(E));
+    auto fetch_in = [&](const xtbloom_const_buffer_t& b, void* dst, size_t bytes) {
+      if (bytes == 0) return true;
+      if (b.memory_space == XTBLOOM_MEMORY_HOST) {
+        std::memcpy(dst, b.data, bytes);
+        return true;
+      }
+      return cudaMemcpy(dst, b.data, bytes, cudaMemcpyDeviceToHost) == cudaSuccess;
+    };
+    if (!fetch_in(batch->atomic_potential_shifts, req.resp_b.data(), N * 8) ||
+        !fetch_in(batch->charge_response_offsets, req.resp_off.data(), (B + 1) * 8) ||
+        !fetch_in(batch->charge_response_matrix, req.resp_A.data(), static_cast<size_t>(E) * 8)) {
+      err = "failed to read the charge-response inputs";
+      return XTBLOOM_STATUS_INVALID_ARGUMENT;
+    }
+    std::vector<int64_t> aoff(B + 1);
+    if (!fetch_in(batch->atom_offsets, aoff.data(), (B + 1) * 8)) {
+      err = "failed to read atom_offsets";
+      return XTBLOOM_STATUS_INVALID_ARGUMENT;
+    }
+    if (req.resp_off[0] != 0 || req.resp_off[B] != E) {
+      err = "charge_response_offsets must start at zero and end at total_charge_response_elements";
+      return XTBLOOM_STATUS_INVALID_ARGUMENT;
+    }
+    for (size_t i = 0; i < B; ++i) {
+      const int64_t na = aoff[i + 1] - aoff[i];
+      if (na < 0 || req.resp_off[i + 1] - req.resp_off[i] != na * na) {
+        err = "charge_response_offsets must delimit one atoms x atoms block per system";
+        return XTBLOOM_STATUS_INVALID_ARGUMENT;
+      }
+      const double* A = req.resp_A.data() + req.resp_off[i];
+      for (int64_t r = 0; r < na; ++r)
+        for (int64_t c = 0; c < na; ++c) {
+          if (!std::isfinite(A[r * na + c])) {
+            err = "charge_response_matrix contains NaN or infinity";
+            return XTBLOOM_STATUS_INVALID_ARGUMENT;
+          }
+          if (A[r * na + c] != A[c * na + r]) {
+            err = "charge_response_matrix must be exactly symmetric per system";
+            return XTBLOOM_STATUS_INVALID_ARGUMENT;
+          }
+        }
+    }
+    for (size_t a = 0; a < N; ++a)
+      if (!std::isfinite(req.resp_b[a])) {
+        err = "atomic_potential_shifts contains NaN or infinity";
+        return XTBLOOM_STATUS_INVALID_ARGUMENT;
+      }
+    req.have_response = true;
   }
   // External interaction attachments (src/runtime/validation.cpp:916-1000,
   // 1104-1135 of the reference): the uniform electric field is executed, every
@@ -418,10 +480,14 @@ xtbloom_status_t run(xtbloom_context_t* ctx, const xtbloom_batch_t* batch,
     err = "unexpected exception in the CUDA engine";
   }
   cudaSetDevice(prev);
-  if (result_flags)
-    *result_flags = (st == XTBLOOM_STATUS_SUCCESS && (req.flags & XTBLOOM_COMPUTE_DIPOLE_MOMENTS))
-                        ? XTBLOOM_RESULT_DIPOLE_MOMENTS
-                        : 0u;
+  if (result_flags) {
+    uint32_t rf = 0u;
+    if (st == XTBLOOM_STATUS_SUCCESS && (req.flags & XTBLOOM_COMPUTE_DIPOLE_MOMENTS))
+      rf |= XTBLOOM_RESULT_DIPOLE_MOMENTS;
+    if (st == XTBLOOM_STATUS_SUCCESS && req.have_response)
+      rf |= XTBLOOM_RESULT_FORCES_EXCLUDE_EXTERNAL_OPERATOR_DERIVATIVES;
+    *result_flags = rf;
+  }
   if (st != XTBLOOM_STATUS_SUCCESS) return fail(st, err);
   g_last_error.clear();
   return XTBLOOM_STATUS_SUCCESS;

@@ -64,6 +64,9 @@ struct DevTopo {
   const int32_t* nch;         // spin channels (1 restricted, 2 unrestricted)
   const int32_t* beta_ch;     // channel id of the beta channel (-1 for restricted systems)
   const double* efield;       // 3 per system: uniform electric field; NULL when no system has one
+  const double* resp_b;       // per atom: caller potential shift b (charge response); NULL if none
+  const double* resp_A;       // per system: row-major symmetric atoms x atoms block A
+  const int64_t* resp_off;    // nsys + 1 offsets into resp_A
   // per atom
   const int32_t* Z;
   const int32_t* atom_sh;     // total_atoms + 1
@@ -120,7 +123,7 @@ struct DevTopo {
 // Per-system energy terms (terms[kTermCount * s + k]).
 enum TermIndex : int {
   kTermCore = 0, kTermEs2 = 1, kTermEs3 = 2, kTermAes2 = 3, kTermD4 = 4, kTermEntropy = 5,
-  kTermRep = 6, kTermAtm = 7, kTermPc = 8, kTermSpin = 9, kTermField = 10, kTermCount = 11
+  kTermRep = 6, kTermAtm = 7, kTermPc = 8, kTermSpin = 9, kTermField = 10, kTermResp = 11, kTermCount = 12
 };
 
 __device__ __forceinline__ double logistic(double x) {

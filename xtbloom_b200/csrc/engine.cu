@@ -237,6 +237,8 @@ struct Engine::Impl {
   Dbuf Pm, qmag, vmag, pop_mag, pop_mdip, pop_mqp;
   Dbuf efield, out_dipoles;
   bool have_field = false;
+  Dbuf resp_b, resp_A, resp_off;
+  bool have_resp = false;
   Dbuf free_energy, terms;
   Dbuf mx_cur, mx_prev, mx_res, mx_df, mx_u, mx_omega;
   Dbuf grad, acn, acn_d4, pot_acc;
@@ -270,12 +272,13 @@ struct Engine::Impl {
     std::vector<int64_t> pc_off;
     std::vector<uint8_t> field_attached;
     std::vector<double> field;
+    std::vector<int64_t> resp_off;   // charge-response structure (present: nsys + 1 offsets)
     bool operator==(const CallIdentity& o) const {
       return topo.nsys == o.topo.nsys && topo.atom_off == o.topo.atom_off && topo.Z == o.topo.Z &&
              topo.qmol == o.topo.qmol && topo.uhf == o.topo.uhf && topo.nch == o.topo.nch &&
              flags == o.flags && max_iter == o.max_iter && memory == o.memory && ctol == o.ctol &&
              etol == o.etol && kt == o.kt && damping == o.damping && pc_off == o.pc_off &&
-             field_attached == o.field_attached && field == o.field;
+             field_attached == o.field_attached && field == o.field && resp_off == o.resp_off;
     }
   } ck_id;
   Dbuf fdone;
@@ -302,6 +305,9 @@ struct Engine::Impl {
     t.beta_ch = beta_ch.as<int32_t>();
     t.sh_spinw = sh_spinw.as<double>();
     t.efield = have_field ? efield.as<double>() : nullptr;
+    t.resp_b = have_resp ? resp_b.as<double>() : nullptr;
+    t.resp_A = have_resp ? resp_A.as<double>() : nullptr;
+    t.resp_off = have_resp ? resp_off.as<int64_t>() : nullptr;
     t.Z = Z.as<int32_t>();
     t.atom_sh = atom_sh.as<int32_t>();
     t.pos = pos.as<double>();
@@ -962,6 +968,16 @@ xtbloom_status_t Engine::compute(const ComputeRequest& req, std::string& error) 
     }
     cudaStreamSynchronize(s);   // req.field outlives the upload either way; keep order simple
   }
+  // ---- charge response b + A q ----
+  m.have_resp = req.have_response;
+  if (m.have_resp) {
+    if (!upload(m.resp_b, req.resp_b, s) || !upload(m.resp_off, req.resp_off, s) ||
+        !upload(m.resp_A, req.resp_A, s)) {
+      error = "device allocation for the charge response failed";
+      return XTBLOOM_STATUS_ALLOCATION_FAILED;
+    }
+    cudaStreamSynchronize(s);
+  }
   // ---- strict WARM policy (reference include/xtbloom/xtbloom.h:502-523): a
   // WARM call needs the checkpoint of the latest fully converged call with the
   // same identity; every accepted call consumes the checkpoint ----
@@ -977,6 +993,7 @@ xtbloom_status_t Engine::compute(const ComputeRequest& req, std::string& error) 
   if (m.have_pc) ident.pc_off = m.h_pc_off;
   ident.field_attached = req.field_attached;
   ident.field = req.field;
+  if (req.have_response) ident.resp_off = req.resp_off;
   if (req.warm && !(m.ck_valid && ident == m.ck_id)) {
     error = "WARM start requires the checkpoint of a fully converged call with the same topology, "
             "charges, spin settings, point-charge layout, requested properties and SCC settings";

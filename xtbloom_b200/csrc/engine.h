@@ -35,6 +35,10 @@ struct ComputeRequest {
   // uniform electric field per system (Hartree / (e bohr)), from the attachments
   std::vector<uint8_t> field_attached;
   std::vector<double> field;
+  // charge response b + A q (per-atom shifts, per-system symmetric blocks)
+  bool have_response = false;
+  std::vector<double> resp_b, resp_A;
+  std::vector<int64_t> resp_off;
 };
 
 class Engine {

@@ -215,10 +215,17 @@ __global__ void __launch_bounds__(256) k_potential_atoms(SccArgs a, const double
     for (int c = 0; c < 10; ++c) acc[c] = 0.0;
     for (int j = lane; j < na; j += 32)
       if (j != i) potential_gather_pair(a, dip, qp, a0, i, j, qat, w, dwq, acc);
+    // charge response (b + A q)_i of the mixed charges (reference
+    // periodic_embedding.cpp evaluate_system_unchecked)
+    if (t.resp_A != nullptr) {
+      const double* Ar = t.resp_A + t.resp_off[s] + (int64_t)i * na;
+      for (int j = lane; j < na; j += 32) acc[0] = fma(Ar[j], qat[j], acc[0]);
+    }
 #pragma unroll
     for (int c = 0; c < 10; ++c) acc[c] = warp_sum(acc[c]);
     if (lane == 0) {
       const int64_t g = a0 + i;
+      if (t.resp_b != nullptr) acc[0] += t.resp_b[g];
       // uniform field (scc_driver.cpp:2555-2582 of the reference): v_at += -E.R,
       // dipole potential += -E
       const double* ef = t.efield != nullptr ? t.efield + 3 * s : nullptr;
@@ -599,6 +606,16 @@ __global__ void __launch_bounds__(256) k_energy_mixer(SccArgs a) {
       ef += c;
     }
   }
+  // charge response: E = q.b + q^T A q / 2 (raw charges)
+  double er = 0.0;
+  if (t.resp_A != nullptr) {
+    const double* A = t.resp_A + t.resp_off[s];
+    for (int i = tid; i < na; i += bs) {
+      double aq = 0.0;
+      for (int j = 0; j < na; ++j) aq = fma(A[(int64_t)i * na + j], qat[j], aq);
+      er += qat[i] * (t.resp_b[a0 + i] + 0.5 * aq);
+    }
+  }
   // spin polarisation: E_spin = 1/2 sum_A m_A^T W_A m_A (raw magnetisation)
   double es = 0.0;
   if (uhf) {
@@ -622,10 +639,11 @@ __global__ void __launch_bounds__(256) k_energy_mixer(SccArgs a) {
   ep = block_sum(ep, red);
   es = block_sum(es, red);
   ef = block_sum(ef, red);
+  er = block_sum(er, red);
   const double ecore = a.e_core[s];
   const int bch = t.beta_ch[s];
   const double ts = -a.kt * (a.entropy[s] + (bch >= 0 ? a.entropy[bch] : 0.0));
-  const double F = ecore + e2 + e3 + ea + ed + ep + es + ef + ts;
+  const double F = ecore + e2 + e3 + ea + ed + ep + es + ef + er + ts;
 
   // ---- modified Broyden (Johnson) ----
   const int64_t v0 = t.vec_off[s];
@@ -762,6 +780,7 @@ __global__ void __launch_bounds__(256) k_energy_mixer(SccArgs a) {
     tm[kTermPc] = ep;
     tm[kTermSpin] = es;
     tm[kTermField] = ef;
+    tm[kTermResp] = er;
     if (!exact) {
       a.split_iters[s] += 1;
       if (rms < a.prec_switch) a.prec[s] = 1;
