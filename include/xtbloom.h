@@ -290,8 +290,10 @@ XTBLOOM_API xtbloom_status_t xtbloom_plan_compute_enqueue(xtbloom_plan_t* plan,
                                                           const xtbloom_batch_result_t* result,
                                                           xtbloom_request_t* request);
 
-/* Result arenas: xtbloom.h:1011-1150.  Host and CUDA arenas are provided;
- * DLPack export returns NOT_IMPLEMENTED in this release. */
+/* Result arenas: xtbloom.h:1011-1150.  Host and CUDA arenas, reference
+ * counted; a compact row-major slice exports as a DLPack 1.0 managed tensor
+ * (version 1: DLManagedTensorVersioned, version 0: legacy DLManagedTensor)
+ * that holds one arena reference until its deleter runs. */
 typedef struct xtbloom_result_owner xtbloom_result_owner_t;
 typedef struct xtbloom_result_owner_options {
   uint32_t struct_size;
@@ -312,6 +314,9 @@ typedef struct xtbloom_dlpack_view {
   uint32_t reserved;
   const int64_t* shape;
 } xtbloom_dlpack_view_t;
+#define XTBLOOM_DLPACK_MAX_NDIM 8
+#define XTBLOOM_DLPACK_VIEW_V1_SIZE \
+  (offsetof(xtbloom_dlpack_view_t, shape) + sizeof(const int64_t*))
 XTBLOOM_API xtbloom_status_t
 xtbloom_result_owner_options_init(xtbloom_result_owner_options_t* options, size_t struct_size);
 XTBLOOM_API xtbloom_status_t xtbloom_result_owner_create(

@@ -218,6 +218,8 @@ def _cbuf(arr) -> ConstBuffer:
 def _obuf(arr) -> Buffer:
     if arr is None:
         return Buffer(None, 0, MEMORY_HOST, 0)
+    if isinstance(arr, Buffer):           # e.g. a slice of a result arena
+        return arr
     if hasattr(arr, "data_ptr"):
         space = MEMORY_CUDA if arr.is_cuda else MEMORY_HOST
         return Buffer(arr.data_ptr(), arr.numel() * arr.element_size(), space, 0)

@@ -5,6 +5,7 @@
 // call-level failures modify no output; a SUCCESS return means every
 // per-system diagnostic was committed, failed systems carrying quiet-NaN
 // slices.  Exceptions never cross the boundary.
+#include <atomic>
 #include <cmath>
 #include <cstdlib>
 #include <cstring>
@@ -112,7 +113,7 @@ struct xtbloom_plan {
 };
 
 struct xtbloom_result_owner {
-  int refs = 1;
+  std::atomic<int> refs{1};   // exported tensors may be released from any thread
   xtbloom_memory_space_t space = XTBLOOM_MEMORY_HOST;
   int device = -1;
   void* data = nullptr;
@@ -741,9 +742,14 @@ xtbloom_status_t xtbloom_result_owner_options_init(xtbloom_result_owner_options_
 
 xtbloom_status_t xtbloom_result_owner_create(const xtbloom_result_owner_options_t* o,
                                              xtbloom_result_owner_t** owner) {
+  if (owner != nullptr) *owner = nullptr;
   if (owner == nullptr || !valid_header(o, offsetof(xtbloom_result_owner_options_t, reserved) + 4) ||
       o->size_bytes == 0 || o->reserved != 0)
     return fail(XTBLOOM_STATUS_INVALID_ARGUMENT, "invalid result owner options");
+  // host arenas carry the sentinel device -1, CUDA arenas a real ordinal
+  if ((o->memory_space == XTBLOOM_MEMORY_HOST && o->device_id != -1) ||
+      (o->memory_space == XTBLOOM_MEMORY_CUDA_DEVICE && o->device_id < 0))
+    return fail(XTBLOOM_STATUS_INVALID_ARGUMENT, "result owner device id contradicts its memory space");
   auto* r = new (std::nothrow) xtbloom_result_owner;
   if (r == nullptr) return fail(XTBLOOM_STATUS_ALLOCATION_FAILED, "allocation failed");
   r->space = o->memory_space;
@@ -753,8 +759,11 @@ xtbloom_status_t xtbloom_result_owner_create(const xtbloom_result_owner_options_
   } else if (o->memory_space == XTBLOOM_MEMORY_CUDA_DEVICE) {
     int prev = 0;
     cudaGetDevice(&prev);
-    cudaSetDevice(o->device_id < 0 ? 0 : o->device_id);
-    if (cudaMalloc(&r->data, o->size_bytes) != cudaSuccess) r->data = nullptr;
+    if (cudaSetDevice(o->device_id) != cudaSuccess ||
+        cudaMalloc(&r->data, o->size_bytes) != cudaSuccess) {
+      cudaGetLastError();
+      r->data = nullptr;
+    }
     cudaSetDevice(prev);
     r->device = o->device_id;
   } else {
@@ -779,19 +788,169 @@ xtbloom_status_t xtbloom_result_owner_buffer(const xtbloom_result_owner_t* owner
 }
 
 void xtbloom_result_owner_retain(xtbloom_result_owner_t* owner) {
-  if (owner) ++owner->refs;
+  if (owner) owner->refs.fetch_add(1);
 }
 
 void xtbloom_result_owner_release(xtbloom_result_owner_t* owner) {
-  if (owner == nullptr || --owner->refs > 0) return;
-  if (owner->space == XTBLOOM_MEMORY_HOST) std::free(owner->data);
-  else cudaFree(owner->data);
+  if (owner == nullptr || owner->refs.fetch_sub(1) > 1) return;
+  if (owner->space == XTBLOOM_MEMORY_HOST) {
+    std::free(owner->data);
+  } else {
+    int prev = 0;
+    cudaGetDevice(&prev);
+    cudaSetDevice(owner->device);
+    cudaFree(owner->data);
+    cudaSetDevice(prev);
+  }
   delete owner;
 }
 
-xtbloom_status_t xtbloom_result_owner_export_dltensor(const xtbloom_result_owner_t*,
-                                                      const xtbloom_dlpack_view_t*, int, void**) {
-  return fail(XTBLOOM_STATUS_NOT_IMPLEMENTED, "DLPack export is not implemented in this release");
+}  // extern "C"
+
+namespace {
+
+// DLPack 1.0 structures (the public dlpack.h layout, restated; the reference
+// pins the same layout in src/runtime/dlpack_layout.hpp).
+struct DlDevice {
+  int32_t device_type;   // 1 CPU, 2 CUDA
+  int32_t device_id;
+};
+struct DlDataType {
+  uint8_t code;
+  uint8_t bits;
+  uint16_t lanes;
+};
+struct DlTensor {
+  void* data;
+  DlDevice device;
+  int32_t ndim;
+  DlDataType dtype;
+  int64_t* shape;
+  int64_t* strides;
+  uint64_t byte_offset;
+};
+struct DlManagedTensor {
+  DlTensor dl_tensor;
+  void* manager_ctx;
+  void (*deleter)(DlManagedTensor*);
+};
+struct DlPackVersion {
+  uint32_t major;
+  uint32_t minor;
+};
+struct DlManagedTensorVersioned {
+  DlPackVersion version;
+  void* manager_ctx;
+  void (*deleter)(DlManagedTensorVersioned*);
+  uint64_t flags;
+  DlTensor dl_tensor;
+};
+static_assert(sizeof(DlTensor) == 48, "DLTensor layout");
+static_assert(sizeof(DlManagedTensor) == 64, "DLManagedTensor layout");
+static_assert(sizeof(DlManagedTensorVersioned) == 80, "DLManagedTensorVersioned layout");
+
+// One exported tensor: the managed struct first (its address is the exported
+// pointer and the deleter's argument), then the copied shape.  manager_ctx is
+// the arena whose reference the tensor holds.
+template <class M>
+struct Export {
+  M managed;
+  int64_t shape[XTBLOOM_DLPACK_MAX_NDIM];
+};
+
+template <class M>
+void export_deleter(M* self) {
+  if (self == nullptr) return;
+  auto* owner = static_cast<xtbloom_result_owner_t*>(self->manager_ctx);
+  delete reinterpret_cast<Export<M>*>(self);
+  xtbloom_result_owner_release(owner);   // never calls back into the importer
+}
+
+template <class M>
+M* make_export(xtbloom_result_owner_t* owner, const xtbloom_dlpack_view_t* v, uint64_t payload) {
+  auto* e = new (std::nothrow) Export<M>{};
+  if (e == nullptr) return nullptr;
+  DlTensor& t = e->managed.dl_tensor;
+  // the offset is folded into data; an empty slice publishes NULL data
+  t.data = payload == 0 ? nullptr : static_cast<unsigned char*>(owner->data) + v->byte_offset;
+  t.device = owner->space == XTBLOOM_MEMORY_HOST ? DlDevice{1, 0} : DlDevice{2, owner->device};
+  t.ndim = v->ndim;
+  t.dtype = DlDataType{(uint8_t)v->dtype_code, (uint8_t)v->dtype_bits, (uint16_t)v->dtype_lanes};
+  for (int i = 0; i < v->ndim; ++i) e->shape[i] = v->shape[i];
+  t.shape = e->shape;
+  t.strides = nullptr;   // compact row-major
+  t.byte_offset = 0;
+  e->managed.manager_ctx = owner;
+  e->managed.deleter = &export_deleter<M>;
+  return &e->managed;
+}
+
+}  // namespace
+
+extern "C" {
+
+xtbloom_status_t xtbloom_result_owner_export_dltensor(const xtbloom_result_owner_t* owner,
+                                                      const xtbloom_dlpack_view_t* view, int version,
+                                                      void** out_managed) {
+  // Every failure leaves *out_managed NULL and the arena's count untouched.
+  if (out_managed != nullptr) *out_managed = nullptr;
+  if (owner == nullptr) return fail(XTBLOOM_STATUS_INVALID_ARGUMENT, "result owner is NULL");
+  if (version != 0 && version != 1)
+    return fail(XTBLOOM_STATUS_INVALID_ARGUMENT,
+                "DLPack export version must be 0 (legacy) or 1 (versioned)");
+  if (view == nullptr || out_managed == nullptr)
+    return fail(XTBLOOM_STATUS_INVALID_ARGUMENT, "DLPack export view or output pointer is NULL");
+  if (view->struct_size < XTBLOOM_DLPACK_VIEW_V1_SIZE || view->api_version != XTBLOOM_API_VERSION)
+    return fail(XTBLOOM_STATUS_INVALID_ARGUMENT,
+                "DLPack view is too small or uses an unsupported API version");
+  if (view->reserved != 0)
+    return fail(XTBLOOM_STATUS_INVALID_ARGUMENT, "DLPack view reserved field must be zero");
+  if (view->ndim < 0 || view->ndim > XTBLOOM_DLPACK_MAX_NDIM)
+    return fail(XTBLOOM_STATUS_INVALID_ARGUMENT, "DLPack view ndim must lie between 0 and 8");
+  if (view->dtype_lanes != 1)
+    return fail(XTBLOOM_STATUS_INVALID_ARGUMENT, "DLPack view lanes must be 1");
+  // int8/16/32/64, uint8, float32/64: the scalar types the header documents
+  const int code = view->dtype_code, bits = view->dtype_bits;
+  const bool dtype_ok = (code == 0 && (bits == 8 || bits == 16 || bits == 32 || bits == 64)) ||
+                        (code == 1 && bits == 8) || (code == 2 && (bits == 32 || bits == 64));
+  if (!dtype_ok)
+    return fail(XTBLOOM_STATUS_INVALID_ARGUMENT,
+                "DLPack view uses an unsupported dtype code/bits combination");
+  if (view->ndim > 0 && view->shape == nullptr)
+    return fail(XTBLOOM_STATUS_INVALID_ARGUMENT, "DLPack view with ndim > 0 requires a shape");
+  const uint64_t esize = static_cast<uint64_t>(bits / 8);
+  uint64_t count = 1;
+  bool empty = false;
+  for (int i = 0; i < view->ndim; ++i) {
+    if (view->shape[i] < 0)
+      return fail(XTBLOOM_STATUS_INVALID_ARGUMENT, "DLPack view has a negative shape extent");
+    const uint64_t ext = static_cast<uint64_t>(view->shape[i]);
+    if (ext == 0) empty = true;
+    if (empty) continue;   // no elements; keep checking signs only
+    if (ext > UINT64_MAX / esize / count)
+      return fail(XTBLOOM_STATUS_INVALID_ARGUMENT, "DLPack view shape overflows uint64_t");
+    count *= ext;
+  }
+  const uint64_t payload = empty ? 0 : count * esize;
+  if (view->byte_offset > owner->bytes || payload > owner->bytes - view->byte_offset)
+    return fail(XTBLOOM_STATUS_INVALID_ARGUMENT, "DLPack view extends past the arena end");
+  if (payload != 0 &&
+      (reinterpret_cast<uintptr_t>(owner->data) + view->byte_offset) % esize != 0)
+    return fail(XTBLOOM_STATUS_INVALID_ARGUMENT,
+                "DLPack view offset does not preserve the dtype alignment");
+  auto* o = const_cast<xtbloom_result_owner_t*>(owner);
+  void* m = version != 0 ? static_cast<void*>(make_export<DlManagedTensorVersioned>(o, view, payload))
+                         : static_cast<void*>(make_export<DlManagedTensor>(o, view, payload));
+  if (m == nullptr)
+    return fail(XTBLOOM_STATUS_ALLOCATION_FAILED, "failed to allocate a DLPack managed tensor");
+  if (version != 0) {
+    auto* mv = static_cast<DlManagedTensorVersioned*>(m);
+    mv->version = DlPackVersion{1, 0};
+    mv->flags = 0;
+  }
+  o->refs.fetch_add(1);   // the exported tensor's arena reference
+  *out_managed = m;
+  return XTBLOOM_STATUS_SUCCESS;
 }
 
 xtbloom_status_t xtbloom_b200_debug_fetch(xtbloom_context_t* context, const char* name, int64_t system,
