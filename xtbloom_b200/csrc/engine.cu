@@ -1171,7 +1171,7 @@ xtbloom_status_t Engine::compute(const ComputeRequest& req, std::string& error) 
     XTB_STAGE(stage_base == kStLowdin ? kStLowdin : kStBacktransform, (int)bks.size(), for (const Bucket& bk : bks) {
       const EigArgs gb = sub(bk);
       const int want = mode == 1 ? bk.max_n : std::min(bk.max_m, bk.max_n);
-      const long budget = 220L * 1024 / 8 - (long)bk.max_n * 33 - 2 * 32 * 33 - 8;
+      const long budget = 220L * 1024 / 8 - (long)bk.max_n * 33 - 32 * 33 - 8;
       const int wcap = (int)std::min<long>(want, budget / 32);
       if (wcap >= 8) {
         launch_backtransform_wy(gb, bk.count, bk.max_n, wcap, want, s);
@@ -1242,6 +1242,8 @@ xtbloom_status_t Engine::compute(const ComputeRequest& req, std::string& error) 
   a.pop_mdip = m.pop_mdip.as<double>();
   a.pop_mqp = m.pop_mqp.as<double>();
   a.Pm = m.Pm.as<double>();
+  a.work = m.scratch.as<double>();
+  a.work_off = m.ch_scr.as<int64_t>();
   a.ch_sys = m.ch_sys.as<int32_t>();
   a.ch_sign = m.ch_sign.as<int32_t>();
   a.ch_mat = dch_mat;
@@ -1316,6 +1318,10 @@ xtbloom_status_t Engine::compute(const ComputeRequest& req, std::string& error) 
   fbase.acn_d4 = m.acn_d4.as<double>();
   fbase.terms = m.terms.as<double>();
   fbase.want_grad = want_forces ? 1 : 0;
+  fbase.atm_c6 = m.T.as<double>();      // free once the SCC has ended
+  fbase.atm_dc6 = m.A.as<double>();
+  fbase.work = m.scratch.as<double>();
+  fbase.work_off = m.ch_scr.as<int64_t>();
   // Every kernel here reads and writes only the listed systems' slices.
   auto force_terms = [&](const int32_t* flist, int fcount, cudaStream_t st) {
     if (fcount <= 0) return;

@@ -44,7 +44,10 @@ __device__ __forceinline__ void gemm_tile_f64(const GemmArgs& g, int s, int M, i
 #pragma unroll
     for (int j = 0; j < 4; ++j) acc[i][j] = 0.0;
   const int i0 = ti * GB, j0 = tj * GB;
-  for (int k0 = 0; k0 < K; k0 += GK) {
+  // The next chunk's operands are loaded into registers while the current
+  // chunk is multiplied, so global latency overlaps the FMAs.
+  double ra[4], rb[4];
+  auto fetch = [&](int k0) {
 #pragma unroll
     for (int q = 0; q < 4; ++q) {
       const int e = tid + q * 256;   // 0..1023
@@ -52,19 +55,30 @@ __device__ __forceinline__ void gemm_tile_f64(const GemmArgs& g, int s, int M, i
         // A^T tile: element (i, k) = A[k][i]; load row k, cols i (coalesced)
         const int kk = e / GB, ii = e % GB;
         const int gk = k0 + kk, gi = i0 + ii;
-        As[kk][ii] = (gk < K && gi < M) ? A[(int64_t)gk * ld + gi] : 0.0;
+        ra[q] = (gk < K && gi < M) ? A[(int64_t)gk * ld + gi] : 0.0;
       } else {
         const int ii = e / GK, kk = e % GK;
         const int gk = k0 + kk, gi = i0 + ii;
-        As[kk][ii] = (gk < K && gi < M) ? A[(int64_t)gi * ld + gk] : 0.0;
+        ra[q] = (gk < K && gi < M) ? A[(int64_t)gi * ld + gk] : 0.0;
       }
       const int kk = e / GB, jj = e % GB;
       const int gk = k0 + kk, gj = j0 + jj;
       double bv = (gk < K && gj < N) ? B[(int64_t)gk * ld + gj] : 0.0;
       if (W && gk < K) bv *= w[gk];
-      Bs[kk][jj] = bv;
+      rb[q] = bv;
+    }
+  };
+  fetch(0);
+  for (int k0 = 0; k0 < K; k0 += GK) {
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      const int e = tid + q * 256;
+      if (TA) As[e / GB][e % GB] = ra[q];
+      else As[e % GK][e / GK] = ra[q];
+      Bs[e / GB][e % GB] = rb[q];
     }
     __syncthreads();
+    if (k0 + GK < K) fetch(k0 + GK);
 #pragma unroll
     for (int kk = 0; kk < GK; ++kk) {
       double a[4], b[4];
@@ -221,7 +235,7 @@ __device__ __forceinline__ void gemm_tile_tf32x3(const GemmArgs& g, int s, int M
 // transposed.  g.prec selects, per system, the split-precision tile.
 // ---------------------------------------------------------------------------
 template <bool TA, bool W>
-__global__ void __launch_bounds__(256) k_gemm(GemmArgs g) {
+__global__ void __launch_bounds__(256, 3) k_gemm(GemmArgs g) {
   const int s = g.list[blockIdx.y];
   const int M = g.dm[s], N = g.dn[s], K = g.dk[s];
   const int ld = g.nao[s];
@@ -730,22 +744,34 @@ __device__ void warp_fermi(const double* eps, int n, double nel, double kt, doub
       fmax(64.0, -log(target / n) + 8.0) * kt + 64.0 * DBL_EPSILON * fmax(1.0, fabs(span));
   double lo = (eps[0] - ref) - margin, hi = (eps[n - 1] - ref) + margin;
   const double tol = 64.0 * DBL_EPSILON * target;
+  // The root of q(mu) = target to the reference's tolerance |q - target| <=
+  // 64 eps target (it bisects; any mu inside that band gives the same
+  // occupations to rounding).  Newton steps on q' = sum f (1 - f) / kT inside
+  // the bisection bracket: a few iterations where bisection needs ~55, which
+  // matters when few systems are left and this loop is on the critical path.
+  const double ikt = 1.0 / kt;
+  double mu = lo + 0.5 * (hi - lo);
   for (int it = 0; it < 400; ++it) {
-    const double mid = lo + 0.5 * (hi - lo);
-    if (mid == lo || mid == hi) break;
-    double q = 0.0;
+    double q = 0.0, dq = 0.0;
     for (int j = lane; j < n; j += 32) {
-      const double de = (eps[j] - ref) - mid;
-      q += holes ? fermi_f(-de, kt) : fermi_f(de, kt);
+      double x = ((eps[j] - ref) - mu) * ikt;
+      if (holes) x = -x;
+      const double ex = exp(-fabs(x));
+      const double r = 1.0 / (1.0 + ex);
+      const double fj = x > 0.0 ? ex * r : r;
+      q += fj;
+      dq = fma(fj, 1.0 - fj, dq);
     }
     q = warp_sum(q);
-    if (fabs(q - target) <= tol) {
-      lo = hi = mid;
-      break;
-    }
-    if ((!holes && q < target) || (holes && q > target)) lo = mid; else hi = mid;
+    dq = warp_sum(dq) * (holes ? -ikt : ikt);
+    if (fabs(q - target) <= tol) break;
+    if ((!holes && q < target) || (holes && q > target)) lo = mu; else hi = mu;
+    const double mid = lo + 0.5 * (hi - lo);
+    if (mid == lo || mid == hi) break;   // bracket at the resolution limit
+    double nm = dq != 0.0 ? mu - (q - target) / dq : mid;
+    if (!(nm > lo && nm < hi)) nm = mid;
+    mu = nm;
   }
-  const double mu = lo + 0.5 * (hi - lo);
   double sacc = 0.0;
   for (int j = lane; j < n; j += 32) {
     const double fj = fermi_f((eps[j] - ref) - mu, kt);
@@ -1011,14 +1037,94 @@ __global__ void __launch_bounds__(256) k_backtransform(EigArgs g, const int32_t*
 // ---------------------------------------------------------------------------
 constexpr int WB = 32;
 
-size_t backtransform_wy_bytes(int n, int m) {
-  return ((size_t)n * (WB + 1) + 2 * WB * (WB + 1) + (size_t)WB * m + 8) * sizeof(double);
+// Reflectors i0 .. i0+k-1 of one block into V (L x WB, row stride WB + 1):
+// V[r][c] = v_{i0+c}[i0+1+r], unit diagonal, zeros above it and past k.
+// Reflector i is row i of the reduced matrix (columns i+2..n-1), so a warp
+// reads one reflector with consecutive lanes (coalesced) and writes one
+// column of V (stride WB + 1: no bank conflicts).
+__device__ __forceinline__ void load_wy_block(const double* a, int n, int i0, int k, int L, double* V) {
+  constexpr int P = WB + 1;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  for (int c = warp; c < WB; c += nw) {
+    const double* row = a + (int64_t)(i0 + c) * n + i0 + 1;
+    for (int r = lane; r < L; r += 32) {
+      double val = 0.0;
+      if (c < k) {
+        if (r == c) val = 1.0;
+        else if (r > c) val = row[r];
+      }
+      V[r * P + c] = val;
+    }
+  }
 }
 
-// Grid (parts, systems): part blockIdx.x transforms its contiguous slice of
-// the system's eigenvectors (parts > 1 only when few systems are active, so
-// that one system's vectors are spread over several SMs).
-__global__ void __launch_bounds__(256) k_backtransform_wy(EigArgs g, int wcap) {
+size_t wy_factor_bytes(int n) { return ((size_t)n * (WB + 1) + 2 * WB * (WB + 1)) * sizeof(double); }
+
+size_t backtransform_wy_bytes(int n, int m) {
+  return ((size_t)n * (WB + 1) + WB * (WB + 1) + (size_t)WB * m + 8) * sizeof(double);
+}
+
+// T factor of every 32-reflector block (LAPACK larft, forward columnwise):
+// H_i0 ... H_i0+k-1 = I - V T V^T with T upper triangular,
+//   T[j][j] = tau_j,  T[0:j, j] = -tau_j T[0:j, 0:j] (V^T v_j)[0:j].
+// Grid (blocks, systems): the blocks are independent, so the serial
+// triangular recurrence runs once per block and in parallel over blocks, off
+// the back-transform's critical path.  T goes to the system's scratch, block
+// b at b WB^2 (row-major WB x WB, zeros below the diagonal).
+__global__ void __launch_bounds__(256) k_wy_factor(EigArgs g) {
+  extern __shared__ double sm[];
+  const int s = g.list[blockIdx.y];
+  const int n = g.nao[s];
+  const int nr = n - 2;
+  const int b = blockIdx.x;
+  const int i0 = b * WB;
+  if (nr <= 0 || i0 >= nr) return;   // uniform over the block
+  const int k = min(WB, nr - i0);
+  const int L = n - i0 - 1;
+  constexpr int P = WB + 1;
+  double* V = sm;
+  double* G = V + (size_t)n * P;
+  double* T = G + WB * P;
+  const double* tau = g.tau + g.ao_off[s];
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  load_wy_block(g.A + g.mat_off[s], n, i0, k, L, V);
+  __syncthreads();
+  // G[p][q] = v_p . v_q for p < q < k (v_q is zero above row q)
+  for (int idx = tid; idx < WB * WB; idx += blockDim.x) {
+    const int p = idx / WB, q = idx - (idx / WB) * WB;
+    if (p < q && q < k) {
+      double acc = 0.0;
+      for (int r = q; r < L; ++r) acc = fma(V[r * P + p], V[r * P + q], acc);
+      G[p * P + q] = acc;
+    }
+  }
+  __syncthreads();
+  if (warp == 0) {
+    for (int j = 0; j < WB; ++j) {
+      const double tj = j < k ? tau[i0 + j] : 0.0;
+      double t = 0.0;
+      if (lane < j && j < k) {
+        for (int q = lane; q < j; ++q) t = fma(T[lane * P + q], G[q * P + j], t);
+        t *= -tj;
+      }
+      if (lane == j) t = tj;
+      T[lane * P + j] = (lane <= j) ? t : 0.0;
+      __syncwarp();
+    }
+    double* out = g.scratch + g.scratch_off[s] + (int64_t)b * WB * WB;
+    for (int j = 0; j < WB; ++j) out[lane * WB + j] = T[lane * P + j];
+  }
+}
+
+// Blocked back-transform (compact WY form, LAPACK larfb order): each block of
+// 32 reflectors costs one pass over Z: Z <- Z - V (T (V^T Z)), blocks from the
+// last to the first, T from k_wy_factor.  Grid (parts, systems): part
+// blockIdx.x transforms its contiguous slice of the system's eigenvectors
+// (parts > 1 only when few systems are active, so that one system's vectors
+// are spread over several SMs).  STAGED: the slice lives in shared memory for
+// the whole pass (few vectors per CTA), so no block waits on global loads of Z.
+template <bool STAGED>
+__global__ void __launch_bounds__(256) k_backtransform_wy(EigArgs g, int wcap, int per_cap) {
   extern __shared__ double sm[];
   const int s = g.list[blockIdx.y];
   const int n = g.nao[s];
@@ -1027,52 +1133,29 @@ __global__ void __launch_bounds__(256) k_backtransform_wy(EigArgs g, int wcap) {
   const int jbeg = blockIdx.x * per;
   const int m = min(mt - jbeg, per);
   const double* a = g.A + g.mat_off[s];
-  const double* tau = g.tau + g.ao_off[s];
-  double* Z = g.Z + g.mat_off[s] + (int64_t)jbeg * n;
+  const double* tf = g.scratch + g.scratch_off[s];
+  double* gZ = g.Z + g.mat_off[s] + (int64_t)jbeg * n;
   const int nr = n - 2;
   if (nr <= 0 || m <= 0) return;
   const int tid = threadIdx.x, bs = blockDim.x, lane = tid & 31, warp = tid >> 5, nw = bs >> 5;
   constexpr int P = WB + 1;
   double* V = sm;                       // n x P
   double* T = V + (size_t)n * P;        // WB x P
-  double* G = T + WB * P;               // WB x P
-  double* W = G + WB * P;               // WB x m
+  double* W = T + WB * P;               // WB x wcap
+  // per_cap x n staging buffer; a slice larger than planned stays in global memory
+  const bool stage = STAGED && per <= per_cap;
+  double* Z = stage ? W + (size_t)WB * wcap : gZ;
+  if (stage)
+    for (int64_t k = tid; k < (int64_t)m * n; k += bs) Z[k] = gZ[k];
   const int nblk = (nr + WB - 1) / WB;
   for (int b = nblk - 1; b >= 0; --b) {
     const int i0 = b * WB;
     const int k = min(WB, nr - i0);
     const int L = n - i0 - 1;
-    for (int idx = tid; idx < L * WB; idx += bs) {
-      const int r = idx / WB, c = idx - (idx / WB) * WB;
-      double val = 0.0;
-      if (c < k) {
-        if (r == c) val = 1.0;
-        else if (r > c) val = a[(int64_t)(i0 + c) * n + i0 + 1 + r];
-      }
-      V[r * P + c] = val;
-    }
-    __syncthreads();
+    load_wy_block(a, n, i0, k, L, V);
     for (int idx = tid; idx < WB * WB; idx += bs) {
       const int p = idx / WB, q = idx - (idx / WB) * WB;
-      if (p < q && q < k) {
-        double acc = 0.0;
-        for (int r = q; r < L; ++r) acc = fma(V[r * P + p], V[r * P + q], acc);
-        G[p * P + q] = acc;
-      }
-    }
-    __syncthreads();
-    if (warp == 0) {
-      for (int j = 0; j < WB; ++j) {
-        const double tj = j < k ? tau[i0 + j] : 0.0;
-        double t = 0.0;
-        if (lane < j && j < k) {
-          for (int q = lane; q < j; ++q) t = fma(T[lane * P + q], G[q * P + j], t);
-          t *= -tj;
-        }
-        if (lane == j) t = tj;
-        T[lane * P + j] = (lane <= j) ? t : 0.0;
-        __syncwarp();
-      }
+      T[p * P + q] = tf[(int64_t)b * WB * WB + idx];
     }
     __syncthreads();
     // eigenvectors in chunks of at most wcap (the W buffer's capacity)
@@ -1110,17 +1193,33 @@ __global__ void __launch_bounds__(256) k_backtransform_wy(EigArgs g, int wcap) {
     __syncthreads();
     }
   }
+  if (stage)
+    for (int64_t k = tid; k < (int64_t)m * n; k += bs) gZ[k] = Z[k];
 }
 
 void launch_backtransform_wy(const EigArgs& g, int count, int max_n, int max_m, int want_m,
                              cudaStream_t stream) {
   if (count == 0) return;
-  static const size_t cap = allow_max_dynamic_smem(k_backtransform_wy);
-  (void)cap;
-  // Few systems: split each system's vectors over CTAs, at least 8 vectors each.
+  static const size_t cap = allow_max_dynamic_smem(k_backtransform_wy<false>);
+  static const size_t cap_s = allow_max_dynamic_smem(k_backtransform_wy<true>);
+  static const size_t cap_f = allow_max_dynamic_smem(k_wy_factor);
+  (void)cap_f;
+  const int nblk = std::max(1, (max_n - 2 + WB - 1) / WB);
+  k_wy_factor<<<dim3(nblk, count), 256, wy_factor_bytes(max_n), stream>>>(g);
+  // Few systems: split each system's vectors over CTAs, at least 8 vectors
+  // each, and keep each CTA's slice in shared memory when it fits.
   const int sms = sm_count();
   const int parts = count >= sms ? 1 : std::max(1, std::min((want_m + 7) / 8, 2 * sms / count));
-  k_backtransform_wy<<<dim3(parts, count), 256, backtransform_wy_bytes(max_n, max_m), stream>>>(g, max_m);
+  const int per = (want_m + parts - 1) / parts;
+  const int wc = std::min(max_m, per);
+  const size_t staged = backtransform_wy_bytes(max_n, wc) + (size_t)per * max_n * sizeof(double);
+  if (parts > 1 && staged <= cap_s) {
+    k_backtransform_wy<true><<<dim3(parts, count), 256, staged, stream>>>(g, wc, per);
+    return;
+  }
+  (void)cap;
+  k_backtransform_wy<false><<<dim3(parts, count), 256, backtransform_wy_bytes(max_n, max_m), stream>>>(
+      g, max_m, 0);
 }
 
 // Loewdin weights s^-1/2 with the overlap condition guard; failed systems are flagged.

@@ -195,9 +195,7 @@ __global__ void __launch_bounds__(256) k_classical(ForceArgs f) {
   double* qat = acn4 + na;                 // na
   double* w = qat + na;                    // 7 na (charged weights)
   double* wcn = w + kMaxD4Refs * na;       // 7 na (d w / d cn)
-  double* w0 = wcn + kMaxD4Refs * na;      // 7 na (zero-charge weights)
-  double* w0cn = w0 + kMaxD4Refs * na;     // 7 na
-  double* red = w0cn + kMaxD4Refs * na;    // 40
+  double* red = wcn + kMaxD4Refs * na;     // 40
   const int tid = threadIdx.x, bs = blockDim.x;
   const bool grad = f.want_grad != 0;
   for (int i = tid; i < na; i += bs) {
@@ -209,10 +207,9 @@ __global__ void __launch_bounds__(256) k_classical(ForceArgs f) {
     for (int sh = t.atom_sh[g]; sh < t.atom_sh[g + 1]; ++sh) q += f.qsh[sh];
     qat[i] = q;
     d4_weights(t, t.Z[g], f.cn_d4[g], q, w + kMaxD4Refs * i, wcn + kMaxD4Refs * i, nullptr);
-    d4_weights(t, t.Z[g], f.cn_d4[g], 0.0, w0 + kMaxD4Refs * i, w0cn + kMaxD4Refs * i, nullptr);
   }
   __syncthreads();
-  double erep = 0.0, eatm = 0.0;
+  double erep = 0.0;
   const double* gam = f.gam + t.gam_off[s];
   const int64_t npair = (int64_t)na * (na - 1) / 2;
   for (int64_t p = tid; p < npair; p += bs) {
@@ -308,14 +305,98 @@ __global__ void __launch_bounds__(256) k_classical(ForceArgs f) {
         atomicAdd(&gr[3 * j + c], -gs * d[c]);
       }
     }
-    // ATM triples (i > j > k) with all three distances within 25 bohr
-    if (r2 > 625.0) continue;
+  }
+  erep = block_sum(erep, red);
+  if (tid == 0) f.terms[kTermCount * (int64_t)s + kTermRep] = erep;
+  if (!grad) return;
+  for (int i = tid; i < na; i += bs) {
+    const int64_t g = a0 + i;
+    for (int c = 0; c < 3; ++c) atomicAdd(&f.grad[3 * g + c], gr[3 * i + c]);
+    atomicAdd(&f.acn[g], acn[i]);
+    atomicAdd(&f.acn_d4[g], acn4[i]);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// D4 three-body (Axilrod-Teller-Muto) term at zero charges
+// (model/gfn2/d4.cpp of the reference): triples i > j > k with all three
+// distances within 25 bohr.  The pair C6 coefficients and their CN
+// derivatives are tabulated once per system (O(N^2)), so the O(N^3) triple
+// loop only reads them.
+// ---------------------------------------------------------------------------
+// Table of system s (one CTA): C6[i][j] (symmetric) and D[i][j] = dC6_ij /
+// dCN_i, with row stride = atoms, at the system's matrix offset of two work
+// arrays of n^2 >= atoms^2 doubles.  Each pair i > j is evaluated with i as
+// the first partner, the orientation of the triple loop.
+__global__ void __launch_bounds__(256) k_atm_table(ForceArgs f) {
+  extern __shared__ double sm[];
+  const DevTopo& t = f.t;
+  const int s = f.list[blockIdx.x];
+  const int64_t a0 = t.atom_off[s];
+  const int na = (int)(t.atom_off[s + 1] - a0);
+  double* w0 = sm;                         // 7 na zero-charge weights
+  double* w0cn = w0 + kMaxD4Refs * na;     // 7 na, d w / d cn
+  for (int i = threadIdx.x; i < na; i += blockDim.x) {
+    const int64_t g = a0 + i;
+    d4_weights(t, t.Z[g], f.cn_d4[g], 0.0, w0 + kMaxD4Refs * i, w0cn + kMaxD4Refs * i, nullptr);
+  }
+  __syncthreads();
+  double* C6 = f.atm_c6 + t.mat_off[s];
+  double* D = f.atm_dc6 + t.mat_off[s];
+  const int64_t npair = (int64_t)na * (na - 1) / 2;
+  for (int64_t p = threadIdx.x; p < npair; p += blockDim.x) {
+    int64_t ii, jj;
+    pair_from_index(p, ii, jj);
+    const int i = (int)ii, j = (int)jj;
+    double ci, cj;
+    const double c6 = d4_c6(t, t.Z[a0 + i], t.Z[a0 + j], w0 + kMaxD4Refs * i, w0 + kMaxD4Refs * j,
+                            w0cn + kMaxD4Refs * i, w0cn + kMaxD4Refs * j, &ci, &cj);
+    C6[(int64_t)i * na + j] = c6;
+    C6[(int64_t)j * na + i] = c6;
+    D[(int64_t)i * na + j] = ci;
+    D[(int64_t)j * na + i] = cj;
+  }
+}
+
+// Grid (parts, systems): warp w of part p takes pairs i > j (p * 8 + w, step
+// 8 parts), its lanes the third atoms k < j.  Gradients of k go into shared
+// accumulators per triple; those of i and j are reduced over the warp once
+// per pair.  The energy of a part goes to the system's work array (parts >
+// 1; k_atm_combine adds them in part order) or straight into the terms.
+__global__ void __launch_bounds__(256) k_atm(ForceArgs f, int parts) {
+  extern __shared__ double sm[];
+  __shared__ double red[33];
+  const DevTopo& t = f.t;
+  const int s = f.list[blockIdx.y];
+  const int64_t a0 = t.atom_off[s];
+  const int na = (int)(t.atom_off[s + 1] - a0);
+  const bool grad = f.want_grad != 0;
+  double* gr = sm;            // 3 na
+  double* acn4 = gr + 3 * na; // na
+  for (int i = threadIdx.x; i < 4 * na; i += blockDim.x) gr[i] = 0.0;
+  __syncthreads();
+  const double* C6 = f.atm_c6 + t.mat_off[s];
+  const double* D = f.atm_dc6 + t.mat_off[s];
+  const int lane = threadIdx.x & 31;
+  const int nwt = parts * (int)(blockDim.x >> 5);
+  const int64_t npair = (int64_t)na * (na - 1) / 2;
+  double eatm = 0.0;
+  for (int64_t p = (int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); p < npair; p += nwt) {
+    int64_t ii, jj;
+    pair_from_index(p, ii, jj);     // ii > jj
+    const int i = (int)ii, j = (int)jj;
+    if (j == 0) continue;            // uniform over the warp: no third atom
+    const int64_t gi = a0 + i, gj = a0 + j;
+    const double vij[3] = {t.pos[3 * gj] - t.pos[3 * gi], t.pos[3 * gj + 1] - t.pos[3 * gi + 1],
+                           t.pos[3 * gj + 2] - t.pos[3 * gi + 2]};
+    const double r2ij = vij[0] * vij[0] + vij[1] * vij[1] + vij[2] * vij[2];
+    if (r2ij > 625.0) continue;
     const int zi = t.Z[gi], zj = t.Z[gj];
-    double cij_i, cij_j;
-    const double cij = d4_c6(t, zi, zj, w0 + kMaxD4Refs * i, w0 + kMaxD4Refs * j,
-                             w0cn + kMaxD4Refs * i, w0cn + kMaxD4Refs * j, &cij_i, &cij_j);
+    const double cij = C6[(int64_t)i * na + j];
+    const double cij_i = D[(int64_t)i * na + j], cij_j = D[(int64_t)j * na + i];
     const double r0ij = d4_r0(t, zi, zj);
-    for (int k = 0; k < j; ++k) {
+    double g_i[3] = {0.0, 0.0, 0.0}, g_j[3] = {0.0, 0.0, 0.0}, a_i = 0.0, a_j = 0.0;
+    for (int k = lane; k < j; k += 32) {
       const int64_t gk = a0 + k;
       const double vik[3] = {t.pos[3 * gk] - t.pos[3 * gi], t.pos[3 * gk + 1] - t.pos[3 * gi + 1],
                              t.pos[3 * gk + 2] - t.pos[3 * gi + 2]};
@@ -325,13 +406,8 @@ __global__ void __launch_bounds__(256) k_classical(ForceArgs f) {
       const double r2jk = vjk[0] * vjk[0] + vjk[1] * vjk[1] + vjk[2] * vjk[2];
       if (r2ik > 625.0 || r2jk > 625.0) continue;
       const int zk = t.Z[gk];
-      double cik_i, cik_k, cjk_j, cjk_k;
-      const double cik = d4_c6(t, zi, zk, w0 + kMaxD4Refs * i, w0 + kMaxD4Refs * k,
-                               w0cn + kMaxD4Refs * i, w0cn + kMaxD4Refs * k, &cik_i, &cik_k);
-      const double cjk = d4_c6(t, zj, zk, w0 + kMaxD4Refs * j, w0 + kMaxD4Refs * k,
-                               w0cn + kMaxD4Refs * j, w0cn + kMaxD4Refs * k, &cjk_j, &cjk_k);
+      const double cik = C6[(int64_t)i * na + k], cjk = C6[(int64_t)j * na + k];
       const double r0ik = d4_r0(t, zi, zk), r0jk = d4_r0(t, zj, zk);
-      const double r2ij = r2;
       const double r2p = r2ij * r2ik * r2jk;
       const double r1p = sqrt(r2p);
       const double r3p = r2p * r1p;
@@ -352,46 +428,80 @@ __global__ void __launch_bounds__(256) k_classical(ForceArgs f) {
                              5.0 * (o1 - o2) * (o1 - o2) * (o1 + o2)) / r5p;
         return c9 * (-dang * damp + ang * ddmp) / tt;
       };
-      // vij = R_i - R_j in the reference's pair cache (first = j, second = i)
-      const double vij[3] = {t.pos[3 * gj] - t.pos[3 * gi], t.pos[3 * gj + 1] - t.pos[3 * gi + 1],
-                             t.pos[3 * gj + 2] - t.pos[3 * gi + 2]};
+      // vij = R_j - R_i as in the reference's pair cache (first = j, second = i)
       const double sij = dg(r2ij, r2jk, r2ik);
       const double sik = dg(r2ik, r2jk, r2ij);
       const double sjk = dg(r2jk, r2ik, r2ij);
       for (int c = 0; c < 3; ++c) {
         const double gij = sij * vij[c], gik = sik * vik[c], gjk = sjk * vjk[c];
-        atomicAdd(&gr[3 * i + c], -(gij + gik));
-        atomicAdd(&gr[3 * j + c], gij - gjk);
+        g_i[c] -= gij + gik;
+        g_j[c] += gij - gjk;
         atomicAdd(&gr[3 * k + c], gik + gjk);
       }
       const double de = ang * damp * c9;
-      atomicAdd(&acn4[i], -0.5 * de * (cij_i / cij + cik_i / cik));
-      atomicAdd(&acn4[j], -0.5 * de * (cij_j / cij + cjk_j / cjk));
+      const double cik_i = D[(int64_t)i * na + k], cik_k = D[(int64_t)k * na + i];
+      const double cjk_j = D[(int64_t)j * na + k], cjk_k = D[(int64_t)k * na + j];
+      a_i -= 0.5 * de * (cij_i / cij + cik_i / cik);
+      a_j -= 0.5 * de * (cij_j / cij + cjk_j / cjk);
       atomicAdd(&acn4[k], -0.5 * de * (cik_k / cik + cjk_k / cjk));
     }
+    if (grad) {
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        g_i[c] = warp_sum(g_i[c]);
+        g_j[c] = warp_sum(g_j[c]);
+      }
+      a_i = warp_sum(a_i);
+      a_j = warp_sum(a_j);
+      if (lane == 0) {
+        for (int c = 0; c < 3; ++c) {
+          atomicAdd(&gr[3 * i + c], g_i[c]);
+          atomicAdd(&gr[3 * j + c], g_j[c]);
+        }
+        atomicAdd(&acn4[i], a_i);
+        atomicAdd(&acn4[j], a_j);
+      }
+    }
   }
-  erep = block_sum(erep, red);
   eatm = block_sum(eatm, red);
-  if (tid == 0) {
-    f.terms[kTermCount * (int64_t)s + kTermRep] = erep;
-    f.terms[kTermCount * (int64_t)s + kTermAtm] = eatm;
+  if (threadIdx.x == 0) {
+    if (parts == 1) f.terms[kTermCount * (int64_t)s + kTermAtm] = eatm;
+    else f.work[f.work_off[s] + blockIdx.x] = eatm;
   }
   if (!grad) return;
-  for (int i = tid; i < na; i += bs) {
+  __syncthreads();
+  for (int i = threadIdx.x; i < na; i += blockDim.x) {
     const int64_t g = a0 + i;
     for (int c = 0; c < 3; ++c) atomicAdd(&f.grad[3 * g + c], gr[3 * i + c]);
-    atomicAdd(&f.acn[g], acn[i]);
     atomicAdd(&f.acn_d4[g], acn4[i]);
   }
+}
+
+__global__ void k_atm_combine(ForceArgs f, int parts) {
+  const int idx = blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= f.count) return;
+  const int s = f.list[idx];
+  double e = 0.0;
+  for (int q = 0; q < parts; ++q) e += f.work[f.work_off[s] + q];
+  f.terms[kTermCount * (int64_t)s + kTermAtm] = e;
 }
 
 void launch_classical(const ForceArgs& f, int max_atoms, int max_shells, cudaStream_t stream) {
   (void)max_shells;
   if (f.count == 0) return;
-  const size_t sm = ((size_t)(7 + 4 * kMaxD4Refs) * max_atoms + 48) * sizeof(double);
+  const size_t sm = ((size_t)(7 + 2 * kMaxD4Refs) * max_atoms + 48) * sizeof(double);
   static const size_t attr = allow_max_dynamic_smem(k_classical);
+  static const size_t attr_t = allow_max_dynamic_smem(k_atm_table);
+  static const size_t attr_a = allow_max_dynamic_smem(k_atm);
   (void)attr;
+  (void)attr_t;
+  (void)attr_a;
   k_classical<<<f.count, 256, sm, stream>>>(f);
+  k_atm_table<<<f.count, 256, (size_t)2 * kMaxD4Refs * max_atoms * sizeof(double), stream>>>(f);
+  // few systems: each system's pairs over several CTAs
+  const int parts = std::max(1, std::min(16, 2 * sm_count() / f.count));
+  k_atm<<<dim3(parts, f.count), 256, (size_t)4 * max_atoms * sizeof(double), stream>>>(f, parts);
+  if (parts > 1) k_atm_combine<<<(f.count + 127) / 128, 128, 0, stream>>>(f, parts);
 }
 
 // Chain rule through the double-exponential CN (acn) and the D4 CN (acn_d4).

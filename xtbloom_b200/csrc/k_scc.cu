@@ -378,6 +378,9 @@ void launch_fock(const SccArgs& a, int max_n, cudaStream_t stream) {
 // the same in every run.
 constexpr int kMullThreads = 512;
 
+__device__ void mulliken_reduce(const SccArgs& a, int s, const double* part, double* out_sh,
+                                double* out_dip, double* out_qp);
+
 // Populations of density P (at the system's matrix offset) into the shell,
 // dipole and quadrupole arrays; with want_trace, also returns Tr(P H0)
 // (block-wide).  part: shared memory of kMullThreads / cw * 10 * n doubles.
@@ -421,6 +424,82 @@ __device__ __forceinline__ double mulliken_pass(const SccArgs& a, int s, const d
     part[idx] = v;
   }
   __syncthreads();
+  mulliken_reduce(a, s, part, out_sh, out_dip, out_qp);
+  return eb;
+}
+
+// Latency form for few systems: CTA (p, i) sums rows [p rows, (p+1) rows) of
+// system i's P S, P D and P Q columns (and of P_alpha - P_beta for
+// unrestricted systems) plus its share of Tr(P H0) into the system's
+// workspace; k_mulliken_combine adds the parts in part order.
+__global__ void __launch_bounds__(256) k_mulliken_part(SccArgs a, int parts) {
+  __shared__ double red[33];
+  const DevTopo& t = a.t;
+  const int s = a.list[blockIdx.y];
+  const int p = blockIdx.x;
+  const int n = t.nao[s];
+  const int64_t mo = t.mat_off[s];
+  const int rows = (n + parts - 1) / parts;
+  const int r0 = min(n, p * rows), r1 = min(n, r0 + rows);
+  const int npass = t.nch[s] == 2 ? 2 : 1;
+  for (int pass = 0; pass < npass; ++pass) {
+    const double* Pb = pass == 0 ? a.P : a.Pm;
+    double* out = a.work + a.work_off[s] + (int64_t)pass * (parts * 10 * (int64_t)n + parts);
+    double ph = 0.0;
+    for (int col = threadIdx.x; col < n; col += blockDim.x) {
+      double v[10];
+#pragma unroll
+      for (int c = 0; c < 10; ++c) v[c] = 0.0;
+      for (int r = r0; r < r1; ++r) {
+        const int64_t idx = mo + (int64_t)r * n + col;
+        const double pv = Pb[idx];
+        v[0] = fma(pv, a.S[idx], v[0]);
+        if (pass == 0) ph = fma(pv, a.H0[idx], ph);
+#pragma unroll
+        for (int c = 0; c < 3; ++c) v[1 + c] = fma(pv, a.D[c * a.total_mat + idx], v[1 + c]);
+#pragma unroll
+        for (int c = 0; c < 6; ++c) v[4 + c] = fma(pv, a.Q[c * a.total_mat + idx], v[4 + c]);
+      }
+#pragma unroll
+      for (int c = 0; c < 10; ++c) out[((int64_t)p * 10 + c) * n + col] = v[c];
+    }
+    if (pass == 0) {
+      ph = block_sum(ph, red);
+      if (threadIdx.x == 0) out[(int64_t)parts * 10 * n + p] = ph;
+    }
+  }
+}
+
+__global__ void __launch_bounds__(kMullThreads) k_mulliken_combine(SccArgs a, int parts) {
+  extern __shared__ double sm[];   // 10 n
+  const DevTopo& t = a.t;
+  const int s = a.list[blockIdx.x];
+  const int n = t.nao[s];
+  const int npass = t.nch[s] == 2 ? 2 : 1;
+  for (int pass = 0; pass < npass; ++pass) {
+    const double* in = a.work + a.work_off[s] + (int64_t)pass * (parts * 10 * (int64_t)n + parts);
+    for (int idx = threadIdx.x; idx < 10 * n; idx += blockDim.x) {
+      double v = in[idx];
+      for (int q = 1; q < parts; ++q) v += in[(int64_t)q * 10 * n + idx];
+      sm[idx] = v;
+    }
+    if (pass == 0 && threadIdx.x == 0) {
+      double eb = 0.0;
+      for (int q = 0; q < parts; ++q) eb += in[(int64_t)parts * 10 * n + q];
+      a.e_core[s] = eb;
+    }
+    __syncthreads();
+    if (pass == 0) mulliken_reduce(a, s, sm, a.pop_sh, a.pop_dip, a.pop_qp);
+    else mulliken_reduce(a, s, sm, a.pop_mag, a.pop_mdip, a.pop_mqp);
+    __syncthreads();
+  }
+}
+
+// Shell, dipole and quadrupole populations from the column totals part[c n + col].
+__device__ void mulliken_reduce(const SccArgs& a, int s, const double* part, double* out_sh,
+                                double* out_dip, double* out_qp) {
+  const DevTopo& t = a.t;
+  const int n = t.nao[s];
   const int64_t s0 = t.shell_off[s], s1 = t.shell_off[s + 1];
   for (int64_t sh = s0 + threadIdx.x; sh < s1; sh += blockDim.x) {
     const int first = t.sh_ao[sh], cnt = 2 * t.sh_l[sh] + 1;
@@ -442,7 +521,6 @@ __device__ __forceinline__ double mulliken_pass(const SccArgs& a, int s, const d
     for (int c = 0; c < 6; ++c) out_qp[6 * at + c] = pq[c];
   }
   __syncthreads();   // part is reused by a second pass
-  return eb;
 }
 
 // One CTA per system.  The n rows are cut into fixed chunks; thread
@@ -462,6 +540,17 @@ __global__ void __launch_bounds__(kMullThreads) k_mulliken(SccArgs a) {
 
 void launch_mulliken(const SccArgs& a, int max_n, cudaStream_t stream) {
   if (a.count == 0) return;
+  // Few systems: each system's rows over several CTAs (one SM alone cannot
+  // stream the 11 n^2 doubles fast enough); the workspace holds 16 parts of
+  // two passes (2 (160 n + 16) doubles, within its 640 n).
+  const int parts = std::min(16, 2 * sm_count() / a.count);
+  if (parts >= 2 && a.work != nullptr) {
+    static const size_t attr_c = allow_max_dynamic_smem(k_mulliken_combine);
+    (void)attr_c;
+    k_mulliken_part<<<dim3(parts, a.count), 256, 0, stream>>>(a, parts);
+    k_mulliken_combine<<<a.count, kMullThreads, (size_t)10 * max_n * sizeof(double), stream>>>(a, parts);
+    return;
+  }
   // rp(n) * 10 * n doubles: rp * n <= rp * cw = kMullThreads while n <= kMullThreads
   const size_t words = (size_t)10 * std::max(kMullThreads, max_n);
   static const size_t attr = allow_max_dynamic_smem(k_mulliken);
@@ -533,19 +622,16 @@ __global__ void __launch_bounds__(256) k_energy_mixer(SccArgs a) {
     d4_weights(t, t.Z[g], a.cn_d4[g], q, w + kMaxD4Refs * i, nullptr, nullptr);
   }
   __syncthreads();
-  // ES2 and ES3
+  // ES2 and ES3: thread j forms (gamma q)_j down column j of the symmetric
+  // gamma (coalesced rows, independent loads)
   double e2 = 0.0, e3 = 0.0, ea = 0.0, ed = 0.0;
   const double* gam = a.gam + t.gam_off[s];
-  for (int i = warp; i < ns; i += nw) {
-    const double* row = gam + (int64_t)i * ns;
+  for (int j = tid; j < ns; j += bs) {
     double acc = 0.0;
-    for (int j = lane; j < ns; j += 32) acc = fma(row[j], raw[j], acc);
-    acc = warp_sum(acc);
-    if (lane == 0) {
-      const double q = raw[i];
-      e2 += 0.5 * q * acc;
-      e3 += t.sh_g3[s0 + i] * q * q * q / 3.0;
-    }
+    for (int i = 0; i < ns; ++i) acc = fma(gam[(int64_t)i * ns + j], raw[i], acc);
+    const double q = raw[j];
+    e2 += 0.5 * q * acc;
+    e3 += t.sh_g3[s0 + j] * q * q * q / 3.0;
   }
   // AES2 onsite
   const double* rd = raw + ns;
@@ -704,20 +790,23 @@ __global__ void __launch_bounds__(256) k_energy_mixer(SccArgs a) {
         for (int k = 0; k <= h; ++k) part[q++] += dv[h] * dv[k];
       }
     }
-    double* wsum = red + 64;   // [nw][44]
+    double* wsum = red + 64;   // [nw][44], then the 44 totals
 #pragma unroll
     for (int q = 0; q < 44; ++q) {
       const double v = warp_sum(part[q]);
       if (lane == 0) wsum[warp * 44 + q] = v;
     }
     __syncthreads();
+    double* totals = red;      // the block sums above are done with red[0..32]
+    if (tid < 44) {
+      double v = 0.0;
+      for (int ww = 0; ww < nw; ++ww) v += wsum[ww * 44 + tid];
+      totals[tid] = v;
+    }
+    __syncthreads();
     if (tid == 0) {
       double tot[44];
-      for (int q = 0; q < 44; ++q) {
-        double v = 0.0;
-        for (int ww = 0; ww < nw; ++ww) v += wsum[ww * 44 + q];
-        tot[q] = v;
-      }
+      for (int q = 0; q < 44; ++q) tot[q] = totals[q];
       double B[64], c[8];
       int q = 8;
       for (int h = 0; h < 8; ++h) {

@@ -70,6 +70,10 @@ struct SccArgs {
   double* pop_mdip;   // 3 per atom
   double* pop_mqp;    // 6 per atom
   const double* Pm;   // P_alpha - P_beta at the system's matrix offset
+  // per-channel workspace (the eigensolver's scratch, free after the
+  // back-transform): partial column sums of the split Mulliken reduction
+  double* work;
+  const int64_t* work_off;
   // spin channels: channel c of an active list -> system, sign (0 restricted,
   // +1 alpha, -1 beta), matrix offset of its Hamiltonian
   const int32_t* clist;
@@ -185,6 +189,12 @@ struct ForceArgs {
   double* acn_d4;     // dE/dCN (D4) per atom, accumulated
   double* terms;      // per-system energy terms (rep, atm written)
   int32_t want_grad;
+  // work arrays free once the SCC has ended: the D4 three-body pair tables
+  // (n^2 per system at the matrix offsets) and per-system scratch
+  double* atm_c6;
+  double* atm_dc6;
+  double* work;
+  const int64_t* work_off;
 };
 
 void launch_force_pairs(const ForceArgs& f, int64_t max_pairs, cudaStream_t stream);
