@@ -237,6 +237,22 @@ struct Engine::Impl {
   Dbuf Pm, qmag, vmag, pop_mag, pop_mdip, pop_mqp;
   Dbuf efield, out_dipoles;
   bool have_field = false;
+  // side streams for the size buckets of the eigensolver, which run
+  // concurrently (small systems fill the SMs that large ones leave free)
+  static constexpr int kBucketStreams = 8;
+  cudaStream_t bst[kBucketStreams] = {};
+  cudaEvent_t bfork = nullptr, bjoin[kBucketStreams] = {};
+  bool bstreams = false;
+  bool ensure_bucket_streams() {
+    if (bstreams) return true;
+    if (cudaEventCreateWithFlags(&bfork, cudaEventDisableTiming) != cudaSuccess) return false;
+    for (int i = 0; i < kBucketStreams; ++i)
+      if (cudaStreamCreateWithFlags(&bst[i], cudaStreamNonBlocking) != cudaSuccess ||
+          cudaEventCreateWithFlags(&bjoin[i], cudaEventDisableTiming) != cudaSuccess)
+        return false;
+    bstreams = true;
+    return true;
+  }
   Dbuf resp_b, resp_A, resp_off;
   bool have_resp = false;
   Dbuf free_energy, terms;
@@ -374,6 +390,11 @@ void Engine::set_execution(int precision, double switch_residual, bool graphs) {
 }
 
 Engine::~Engine() {
+  for (int i = 0; i < Impl::kBucketStreams; ++i) {
+    if (impl_->bst[i]) cudaStreamDestroy(impl_->bst[i]);
+    if (impl_->bjoin[i]) cudaEventDestroy(impl_->bjoin[i]);
+  }
+  if (impl_->bfork) cudaEventDestroy(impl_->bfork);
   if (impl_->h_count) cudaFreeHost(impl_->h_count);
   if (impl_->h_list) cudaFreeHost(impl_->h_list);
   if (impl_->h_clist) cudaFreeHost(impl_->h_clist);
@@ -1153,32 +1174,62 @@ xtbloom_status_t Engine::compute(const ComputeRequest& req, std::string& error) 
       gb.list = dl + bk.start;
       return gb;
     };
-    XTB_STAGE(stage_base == kStLowdin ? kStLowdin : kStTridiag, (int)bks.size(), for (const Bucket& bk : bks) {
+    auto tridiag = [&](const Bucket& bk, cudaStream_t st) {
       const EigArgs gb = sub(bk);
       // few systems: register-resident cluster kernel (latency); many: the
       // shared-memory kernel, one CTA per system (throughput)
       if (bk.max_n <= tridiag_reg_max_n() && bk.count * 8 <= sm_count() && !m.tridiag_smem)
-        launch_tridiag_reg(gb, gb.list, bk.count, bk.max_n, s);
+        launch_tridiag_reg(gb, gb.list, bk.count, bk.max_n, st);
       else
-        launch_tridiag_smem(gb, gb.list, bk.count, bk.max_n, s);
-    });
-    XTB_STAGE(stage_base == kStLowdin ? kStLowdin : kStEigvals, (int)bks.size(),
-              for (const Bucket& bk : bks) launch_eigvals(sub(bk), mode, kt, bk.count, bk.max_n, s));
-    XTB_STAGE(stage_base == kStLowdin ? kStLowdin : kStInvIter, (int)bks.size(),
-              for (const Bucket& bk : bks) launch_inverse_iteration(
-                  sub(bk), bk.count, bk.max_n, mode == 1 ? bk.max_n : std::min(bk.max_m + 4, bk.max_n),
-                  ortol_rel, s));
-    XTB_STAGE(stage_base == kStLowdin ? kStLowdin : kStBacktransform, (int)bks.size(), for (const Bucket& bk : bks) {
+        launch_tridiag_smem(gb, gb.list, bk.count, bk.max_n, st);
+    };
+    auto eigvals = [&](const Bucket& bk, cudaStream_t st) {
+      launch_eigvals(sub(bk), mode, kt, bk.count, bk.max_n, st);
+    };
+    auto invit = [&](const Bucket& bk, cudaStream_t st) {
+      launch_inverse_iteration(sub(bk), bk.count, bk.max_n,
+                               mode == 1 ? bk.max_n : std::min(bk.max_m + 4, bk.max_n), ortol_rel, st);
+    };
+    auto backtransform = [&](const Bucket& bk, cudaStream_t st) {
       const EigArgs gb = sub(bk);
       const int want = mode == 1 ? bk.max_n : std::min(bk.max_m, bk.max_n);
       const long budget = 220L * 1024 / 8 - (long)bk.max_n * 33 - 32 * 33 - 8;
       const int wcap = (int)std::min<long>(want, budget / 32);
       if (wcap >= 8) {
-        launch_backtransform_wy(gb, bk.count, bk.max_n, wcap, want, s);
+        launch_backtransform_wy(gb, bk.count, bk.max_n, wcap, want, st);
       } else {
-        launch_backtransform(gb, gb.list, bk.count, bk.max_n, 0, s);
+        launch_backtransform(gb, gb.list, bk.count, bk.max_n, 0, st);
       }
-    });
+    };
+    if (bks.size() > 1 && !m.prof.on && m.ensure_bucket_streams()) {
+      // Each bucket runs its whole chain on its own side stream, forked from
+      // and joined back into the call's stream (also inside graph capture).
+      cudaEventRecord(m.bfork, s);
+      const int ns = std::min<int>((int)bks.size(), Impl::kBucketStreams);
+      for (int i = 0; i < ns; ++i) cudaStreamWaitEvent(m.bst[i], m.bfork, 0);
+      for (size_t i = 0; i < bks.size(); ++i) {
+        cudaStream_t st = m.bst[i % Impl::kBucketStreams];
+        tridiag(bks[i], st);
+        eigvals(bks[i], st);
+        invit(bks[i], st);
+        backtransform(bks[i], st);
+      }
+      for (int i = 0; i < ns; ++i) {
+        cudaEventRecord(m.bjoin[i], m.bst[i]);
+        cudaStreamWaitEvent(s, m.bjoin[i], 0);
+      }
+      m.prof.launches += 4 * (int)bks.size();
+      if (const cudaError_t le = cudaGetLastError(); le != cudaSuccess && !launch_error) launch_error = le;
+      return;
+    }
+    XTB_STAGE(stage_base == kStLowdin ? kStLowdin : kStTridiag, (int)bks.size(),
+              for (const Bucket& bk : bks) tridiag(bk, s));
+    XTB_STAGE(stage_base == kStLowdin ? kStLowdin : kStEigvals, (int)bks.size(),
+              for (const Bucket& bk : bks) eigvals(bk, s));
+    XTB_STAGE(stage_base == kStLowdin ? kStLowdin : kStInvIter, (int)bks.size(),
+              for (const Bucket& bk : bks) invit(bk, s));
+    XTB_STAGE(stage_base == kStLowdin ? kStLowdin : kStBacktransform, (int)bks.size(),
+              for (const Bucket& bk : bks) backtransform(bk, s));
   };
 
   // ---- Loewdin orthogonaliser X = U s^-1/2 U^T ----

@@ -67,25 +67,31 @@ __device__ __forceinline__ void inverse_iteration_block(const double* d, const d
       xprev = x;
       // LU with partial pivoting of T - xI; U1 holds reciprocal pivots and the
       // sign of LM encodes the row interchange (pivoted rows store -l - 4; both |l| <= 1).
+      // One reciprocal per step on the dependency chain: the multiplier is
+      // the off-pivot element times the reciprocal pivot (within an ulp of
+      // the quotient), and the reciprocal is reused as U1 unless the pivot
+      // is replaced by +-tiny.
       double diag = d[0] - x, sup = n > 1 ? e[0] : 0.0;
       for (int k = 0; k < n - 1; ++k) {
         const double ck = e[k];
         const double nd = d[k + 1] - x;
         const double ns = (k + 1 < n - 1) ? e[k + 1] : 0.0;
-        double u1, l;
-        if (fabs(diag) >= fabs(ck)) {
-          l = diag != 0.0 ? ck / diag : 0.0;
-          u1 = diag; U2(k) = sup; U3(k) = 0.0; LM(k) = l;
+        const bool keep = fabs(diag) >= fabs(ck);
+        const double u1 = keep ? diag : ck;
+        const double r = __drcp_rn(u1);
+        double l;
+        if (keep) {
+          l = diag != 0.0 ? ck * r : 0.0;
+          U2(k) = sup; U3(k) = 0.0; LM(k) = l;
           diag = nd - l * sup;
           sup = ns;
         } else {
-          l = diag / ck;
-          u1 = ck; U2(k) = nd; U3(k) = ns; LM(k) = -l - 4.0;
+          l = diag * r;
+          U2(k) = nd; U3(k) = ns; LM(k) = -l - 4.0;
           diag = sup - l * nd;
           sup = -l * ns;
         }
-        if (fabs(u1) < tiny) u1 = u1 < 0.0 ? -tiny : tiny;
-        U1(k) = 1.0 / u1;
+        U1(k) = fabs(u1) < tiny ? __drcp_rn(u1 < 0.0 ? -tiny : tiny) : r;
       }
       {
         double u1 = diag;

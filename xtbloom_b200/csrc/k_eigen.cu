@@ -1042,9 +1042,37 @@ constexpr int WB = 32;
 // Reflector i is row i of the reduced matrix (columns i+2..n-1), so a warp
 // reads one reflector with consecutive lanes (coalesced) and writes one
 // column of V (stride WB + 1: no bank conflicts).
+// With 256 threads a warp takes columns warp + 8 q (q < 4) and issues the
+// loads of all four columns for 128 rows before storing any (one memory
+// round trip per 128 rows instead of one per 32).
 __device__ __forceinline__ void load_wy_block(const double* a, int n, int i0, int k, int L, double* V) {
   constexpr int P = WB + 1;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  if (nw == 8) {
+    for (int r0 = 0; r0 < L; r0 += 128) {
+      double v[4][4];
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        const int c = warp + 8 * q;
+        const double* row = a + (int64_t)(i0 + c) * n + i0 + 1;
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+          const int r = r0 + lane + 32 * u;
+          v[q][u] = (c < k && r > c && r < L) ? row[r] : 0.0;
+        }
+      }
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        const int c = warp + 8 * q;
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+          const int r = r0 + lane + 32 * u;
+          if (r < L) V[r * P + c] = (c < k && r == c) ? 1.0 : v[q][u];
+        }
+      }
+    }
+    return;
+  }
   for (int c = warp; c < WB; c += nw) {
     const double* row = a + (int64_t)(i0 + c) * n + i0 + 1;
     for (int r = lane; r < L; r += 32) {
@@ -1100,8 +1128,9 @@ __global__ void __launch_bounds__(256) k_wy_factor(EigArgs g) {
   }
   __syncthreads();
   if (warp == 0) {
+    const double tl = lane < k ? tau[i0 + lane] : 0.0;   // one load, not one per column
     for (int j = 0; j < WB; ++j) {
-      const double tj = j < k ? tau[i0 + j] : 0.0;
+      const double tj = __shfl_sync(0xffffffffu, tl, j);
       double t = 0.0;
       if (lane < j && j < k) {
         for (int q = lane; q < j; ++q) t = fma(T[lane * P + q], G[q * P + j], t);
@@ -1114,6 +1143,37 @@ __global__ void __launch_bounds__(256) k_wy_factor(EigArgs g) {
     double* out = g.scratch + g.scratch_off[s] + (int64_t)b * WB * WB;
     for (int j = 0; j < WB; ++j) out[lane * WB + j] = T[lane * P + j];
   }
+}
+
+__device__ __forceinline__ void cp_async8(double* dst, const double* src) {
+  const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(d), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
+}
+
+// load_wy_block and the T factor of block b, issued as asynchronous copies
+// (one commit group) so that they overlap the work on the previous block;
+// the unit diagonal and the zeros above it are plain stores.
+__device__ __forceinline__ void prefetch_wy_block(const double* a, const double* tf, int n, int nr,
+                                                  int b, double* V, double* T) {
+  constexpr int P = WB + 1;
+  const int i0 = b * WB, k = min(WB, nr - i0), L = n - i0 - 1;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  for (int c = warp; c < WB; c += nw) {
+    const double* row = a + (int64_t)(i0 + c) * n + i0 + 1;
+    for (int r = lane; r < L; r += 32) {
+      double* dst = V + r * P + c;
+      if (c < k && r > c) cp_async8(dst, row + r);
+      else *dst = (c < k && r == c) ? 1.0 : 0.0;
+    }
+  }
+  for (int idx = threadIdx.x; idx < WB * WB; idx += blockDim.x)
+    cp_async8(T + (idx / WB) * P + (idx % WB), tf + (int64_t)b * WB * WB + idx);
+  cp_async_commit();
 }
 
 // Blocked back-transform (compact WY form, LAPACK larfb order): each block of
@@ -1139,23 +1199,41 @@ __global__ void __launch_bounds__(256) k_backtransform_wy(EigArgs g, int wcap, i
   if (nr <= 0 || m <= 0) return;
   const int tid = threadIdx.x, bs = blockDim.x, lane = tid & 31, warp = tid >> 5, nw = bs >> 5;
   constexpr int P = WB + 1;
-  double* V = sm;                       // n x P
-  double* T = V + (size_t)n * P;        // WB x P
-  double* W = T + WB * P;               // WB x wcap
+  // V (n x P) and T (WB x P) of one block; STAGED keeps two of each so that
+  // the next block arrives by cp.async while this one is applied
+  double* V0 = sm;
+  double* T0 = V0 + (size_t)n * P;
+  double* V1 = STAGED ? T0 + WB * P : V0;
+  double* T1 = STAGED ? V1 + (size_t)n * P : T0;
+  double* W = T1 + WB * P;               // WB x wcap
   // per_cap x n staging buffer; a slice larger than planned stays in global memory
   const bool stage = STAGED && per <= per_cap;
   double* Z = stage ? W + (size_t)WB * wcap : gZ;
   if (stage)
     for (int64_t k = tid; k < (int64_t)m * n; k += bs) Z[k] = gZ[k];
   const int nblk = (nr + WB - 1) / WB;
-  for (int b = nblk - 1; b >= 0; --b) {
+  if (STAGED) prefetch_wy_block(a, tf, n, nr, nblk - 1, V0, T0);
+  for (int it = 0; it < nblk; ++it) {
+    const int b = nblk - 1 - it;
     const int i0 = b * WB;
     const int k = min(WB, nr - i0);
     const int L = n - i0 - 1;
-    load_wy_block(a, n, i0, k, L, V);
-    for (int idx = tid; idx < WB * WB; idx += bs) {
-      const int p = idx / WB, q = idx - (idx / WB) * WB;
-      T[p * P + q] = tf[(int64_t)b * WB * WB + idx];
+    const bool odd = STAGED && (it & 1);
+    double* V = odd ? V1 : V0;
+    double* T = odd ? T1 : T0;
+    if (STAGED) {
+      if (b > 0) {
+        prefetch_wy_block(a, tf, n, nr, b - 1, odd ? V0 : V1, odd ? T0 : T1);
+        cp_async_wait<1>();   // this block's copies are done, the next one's may fly
+      } else {
+        cp_async_wait<0>();
+      }
+    } else {
+      load_wy_block(a, n, i0, k, L, V);
+      for (int idx = tid; idx < WB * WB; idx += bs) {
+        const int p = idx / WB, q = idx - (idx / WB) * WB;
+        T[p * P + q] = tf[(int64_t)b * WB * WB + idx];
+      }
     }
     __syncthreads();
     // eigenvectors in chunks of at most wcap (the W buffer's capacity)
@@ -1212,7 +1290,8 @@ void launch_backtransform_wy(const EigArgs& g, int count, int max_n, int max_m, 
   const int parts = count >= sms ? 1 : std::max(1, std::min((want_m + 7) / 8, 2 * sms / count));
   const int per = (want_m + parts - 1) / parts;
   const int wc = std::min(max_m, per);
-  const size_t staged = backtransform_wy_bytes(max_n, wc) + (size_t)per * max_n * sizeof(double);
+  const size_t staged = backtransform_wy_bytes(max_n, wc) + (size_t)per * max_n * sizeof(double) +
+                        ((size_t)max_n * (WB + 1) + WB * (WB + 1)) * sizeof(double);
   if (parts > 1 && staged <= cap_s) {
     k_backtransform_wy<true><<<dim3(parts, count), 256, staged, stream>>>(g, wc, per);
     return;
@@ -1272,10 +1351,13 @@ void launch_eigvals(const EigArgs& g, int mode, double kt, int count, int max_n,
     k_tridiag_eigvals<<<count, 256, sm, stream>>>(g, mode, kt, 0, 1);
     return;
   }
+  // Sturm steps are issue-bound: 128-thread parts (a warp per scheduler,
+  // two eigenvalues per warp, 16 threads each) take the fewest cycles per
+  // round for the rounds they need.
   const int need = mode == 0 ? max_n / 2 + 16 : max_n;
   const int parts = std::max(1, std::min((need + 7) / 8, 2 * kNumSMs / count));
   const size_t smp = (2 * (size_t)max_n + 40) * sizeof(double);
-  k_eigvals_part<<<dim3(parts, count), 256, smp, stream>>>(g, mode, parts);
+  k_eigvals_part<<<dim3(parts, count), 128, smp, stream>>>(g, mode, parts);
   k_tridiag_eigvals<<<count, 256, sm, stream>>>(g, mode, kt, 1, 8);
 }
 

@@ -164,8 +164,25 @@ __device__ __forceinline__ void potential_gather_pair(const SccArgs& a, const do
   acc[0] += v;
 }
 
-// Shell potentials of system s from the finished atomic potentials: ES2 (warp
-// per shell row) + ES3 + atomic potential (+ external point charges).
+// (gamma q)_j = sum_i gamma[i][j] q[i] for the symmetric ns x ns gamma: the
+// loads of 16 rows are issued before their products are summed (in row
+// order), so a thread waits for memory once per 16 rows.
+__device__ __forceinline__ double gamma_column_dot(const double* gam, int ns, int j, const double* q) {
+  double acc = 0.0;
+  for (int i0 = 0; i0 < ns; i0 += 16) {
+    double gv[16];
+#pragma unroll
+    for (int u = 0; u < 16; ++u) gv[u] = i0 + u < ns ? gam[(int64_t)(i0 + u) * ns + j] : 0.0;
+#pragma unroll
+    for (int u = 0; u < 16; ++u)
+      if (i0 + u < ns) acc = fma(gv[u], q[i0 + u], acc);
+  }
+  return acc;
+}
+
+// Shell potentials of system s from the finished atomic potentials: ES2
+// (thread per shell, down its column of the symmetric gamma: coalesced rows,
+// independent loads) + ES3 + atomic potential (+ external point charges).
 __device__ __forceinline__ void potential_shells(const SccArgs& a, int s, const double* sq,
                                                  const double* vat) {
   const DevTopo& t = a.t;
@@ -173,18 +190,12 @@ __device__ __forceinline__ void potential_shells(const SccArgs& a, int s, const 
   const int64_t s0 = t.shell_off[s];
   const int ns = (int)(t.shell_off[s + 1] - s0);
   const double* gam = a.gam + t.gam_off[s];
-  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nw = blockDim.x >> 5;
-  for (int i = warp; i < ns; i += nw) {
-    const double* row = gam + (int64_t)i * ns;
-    double acc = 0.0;
-    for (int j = lane; j < ns; j += 32) acc = fma(row[j], sq[j], acc);
-    acc = warp_sum(acc);
-    if (lane == 0) {
-      const int sh = (int)(s0 + i);
-      const double q = sq[i];
-      a.vsh[sh] = acc + t.sh_g3[sh] * q * q + vat[t.sh_atom[sh] - a0] +
-                  (t.vpc != nullptr ? t.vpc[sh] : 0.0);
-    }
+  for (int j = threadIdx.x; j < ns; j += blockDim.x) {
+    const double acc = gamma_column_dot(gam, ns, j, sq);
+    const int sh = (int)(s0 + j);
+    const double q = sq[j];
+    a.vsh[sh] = acc + t.sh_g3[sh] * q * q + vat[t.sh_atom[sh] - a0] +
+                (t.vpc != nullptr ? t.vpc[sh] : 0.0);
   }
 }
 
@@ -627,8 +638,7 @@ __global__ void __launch_bounds__(256) k_energy_mixer(SccArgs a) {
   double e2 = 0.0, e3 = 0.0, ea = 0.0, ed = 0.0;
   const double* gam = a.gam + t.gam_off[s];
   for (int j = tid; j < ns; j += bs) {
-    double acc = 0.0;
-    for (int i = 0; i < ns; ++i) acc = fma(gam[(int64_t)i * ns + j], raw[i], acc);
+    const double acc = gamma_column_dot(gam, ns, j, raw);
     const double q = raw[j];
     e2 += 0.5 * q * acc;
     e3 += t.sh_g3[s0 + j] * q * q * q / 3.0;

@@ -175,29 +175,33 @@ __global__ void __launch_bounds__(NT) k_tridiag_reg(EigArgs g, const int32_t* li
     const bool prev = k >= 1;
     const bool next = k + 2 < n;    // reflector k exists
     // ---- (1) w_{k-1}, column k of A^(k), reflector k (every warp) ----
-    double vp[JC], wp[JC], xk[JC];
+    double wp[JC], xk[JC];
 #pragma unroll
-    for (int j = 0; j < JB; ++j) vp[j] = wp[j] = xk[j] = 0.0;   // finished columns
+    for (int j = 0; j < JB; ++j) wp[j] = xk[j] = 0.0;   // finished columns
+    // v_{k-1} at column slot j (recomputed where needed: fewer live registers)
+    auto vpj = [&](int j) {
+      const int c = lane + 32 * j;
+      return (prev && c >= k && c < n) ? (c == k ? 1.0 : scp * xp[j]) : 0.0;
+    };
     double pv = 0.0;
 #pragma unroll
     for (int j = JB; j < JC; ++j) {
       const int c = lane + 32 * j;
       const bool act = prev && c >= k && c < n;
-      vp[j] = act ? (c == k ? 1.0 : scp * xp[j]) : 0.0;
       wp[j] = act ? P[b][c] : 0.0;
-      pv = fma(wp[j], vp[j], pv);
+      pv = fma(wp[j], vpj(j), pv);
     }
     pv = warp_sum(pv);
     const double kw = 0.5 * taup * pv;
 #pragma unroll
-    for (int j = JB; j < JC; ++j) wp[j] = fma(-kw, vp[j], wp[j]);
+    for (int j = JB; j < JC; ++j) wp[j] = fma(-kw, vpj(j), wp[j]);
     const double wk = __shfl_sync(0xffffffffu, wp[JB], k & 31);
     double nrm = 0.0;
 #pragma unroll
     for (int j = JB; j < JC; ++j) {
       const int c = lane + 32 * j;
       double v = (c >= k && c < n) ? C[b][c] : 0.0;
-      v -= vp[j] * wk + wp[j];    // v_{k-1}[k] = 1; zero where !prev
+      v -= vpj(j) * wk + wp[j];   // v_{k-1}[k] = 1; zero where !prev
       xk[j] = v;
       if (c >= k + 2 && c < n) nrm = fma(v, v, nrm);
     }
@@ -232,7 +236,8 @@ __global__ void __launch_bounds__(NT) k_tridiag_reg(EigArgs g, const int32_t* li
       // [(R i) >> 5, (R i + R - 1) >> 5] whatever the warp
       double v = 0.0, w = 0.0;
       if (act) {
-        v = __shfl_sync(0xffffffffu, pick_row<R, JC>(vp, i, rslot(i)), rlane(i));
+        // v_{k-1}[r] for r > k is sc x[r]
+        v = scp * __shfl_sync(0xffffffffu, pick_row<R, JC>(xp, i, rslot(i)), rlane(i));
         w = __shfl_sync(0xffffffffu, pick_row<R, JC>(wp, i, rslot(i)), rlane(i));
       }
       vr[i] = v;
@@ -243,7 +248,7 @@ __global__ void __launch_bounds__(NT) k_tridiag_reg(EigArgs g, const int32_t* li
     for (int j = JB; j < JC; ++j) {
       const int c = lane + 32 * j;
       const bool cact = c >= k + 1 && c < n;
-      const double vc = cact ? vp[j] : 0.0;
+      const double vc = cact ? vpj(j) : 0.0;
       const double wc = cact ? wp[j] : 0.0;
       const double nc = (next && cact) ? (c == k + 1 ? 1.0 : sc * xk[j]) : 0.0;
 #pragma unroll
