@@ -63,6 +63,9 @@ def parse():
     p.add_argument("--graphs", type=int, default=1)
     p.add_argument("--once", action="store_true",
                    help="one device-resident call of the chosen form and exit (profiler runs)")
+    p.add_argument("--indices", default="",
+                   help="with --once: comma-separated systems of the 4096-system batch to run "
+                        "(e.g. the slowly converging ones, for profiles of the few-system regime)")
     return p.parse_args()
 
 
@@ -283,6 +286,9 @@ def run_ours(args, world, rank, local):
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
     batch = W.config1(args.systems, seed=1 + 1000 * rank)
+    if args.once and args.indices:
+        batch = W.subset(W.config1(4096, seed=1 + 1000 * rank),
+                         np.array([int(x) for x in args.indices.split(",")]))
     B, N = batch.batch_size, batch.total_atoms
     stream = torch.cuda.current_stream(dev)
     pos_d = torch.from_numpy(batch.positions).to(dev)

@@ -26,34 +26,37 @@ namespace xtb {
 
 constexpr int GB = 64, GK = 16;
 
-// FP64 tile (ti, tj) of system s: 256 threads, 4 x 4 outputs per thread.
-template <bool TA, bool W>
+// FP64 tile (ti, tj) of edge TB (64, or 32 when few systems are active) of
+// system s: 256 threads, (TB/16) x (TB/16) outputs per thread.
+template <bool TA, bool W, int TB>
 __device__ __forceinline__ void gemm_tile_f64(const GemmArgs& g, int s, int M, int N, int K, int ld,
-                                              int ti, int tj) {
+                                              int ti, int tj, bool mirror) {
+  constexpr int RT = TB / 16;            // outputs per thread and dimension
+  constexpr int LPT = TB * GK / 256;     // elements of each operand chunk per thread
   const double* A = g.A + g.offA[s];
   const double* B = g.B + g.offB[s];
   double* C = g.C + g.offC[s];
   const double* w = W ? g.w + g.offW[s] : nullptr;
-  __shared__ double As[GK][GB + 1];
-  __shared__ double Bs[GK][GB + 1];
+  __shared__ double As[GK][TB + 1];
+  __shared__ double Bs[GK][TB + 1];
   const int tid = threadIdx.x;
   const int tx = tid & 15, ty = tid >> 4;
-  double acc[4][4];
+  double acc[RT][RT];
 #pragma unroll
-  for (int i = 0; i < 4; ++i)
+  for (int i = 0; i < RT; ++i)
 #pragma unroll
-    for (int j = 0; j < 4; ++j) acc[i][j] = 0.0;
-  const int i0 = ti * GB, j0 = tj * GB;
+    for (int j = 0; j < RT; ++j) acc[i][j] = 0.0;
+  const int i0 = ti * TB, j0 = tj * TB;
   // The next chunk's operands are loaded into registers while the current
   // chunk is multiplied, so global latency overlaps the FMAs.
-  double ra[4], rb[4];
+  double ra[LPT], rb[LPT];
   auto fetch = [&](int k0) {
 #pragma unroll
-    for (int q = 0; q < 4; ++q) {
-      const int e = tid + q * 256;   // 0..1023
+    for (int q = 0; q < LPT; ++q) {
+      const int e = tid + q * 256;
       if (TA) {
         // A^T tile: element (i, k) = A[k][i]; load row k, cols i (coalesced)
-        const int kk = e / GB, ii = e % GB;
+        const int kk = e / TB, ii = e % TB;
         const int gk = k0 + kk, gi = i0 + ii;
         ra[q] = (gk < K && gi < M) ? A[(int64_t)gk * ld + gi] : 0.0;
       } else {
@@ -61,7 +64,7 @@ __device__ __forceinline__ void gemm_tile_f64(const GemmArgs& g, int s, int M, i
         const int gk = k0 + kk, gi = i0 + ii;
         ra[q] = (gk < K && gi < M) ? A[(int64_t)gi * ld + gk] : 0.0;
       }
-      const int kk = e / GB, jj = e % GB;
+      const int kk = e / TB, jj = e % TB;
       const int gk = k0 + kk, gj = j0 + jj;
       double bv = (gk < K && gj < N) ? B[(int64_t)gk * ld + gj] : 0.0;
       if (W && gk < K) bv *= w[gk];
@@ -71,35 +74,34 @@ __device__ __forceinline__ void gemm_tile_f64(const GemmArgs& g, int s, int M, i
   fetch(0);
   for (int k0 = 0; k0 < K; k0 += GK) {
 #pragma unroll
-    for (int q = 0; q < 4; ++q) {
+    for (int q = 0; q < LPT; ++q) {
       const int e = tid + q * 256;
-      if (TA) As[e / GB][e % GB] = ra[q];
+      if (TA) As[e / TB][e % TB] = ra[q];
       else As[e % GK][e / GK] = ra[q];
-      Bs[e / GB][e % GB] = rb[q];
+      Bs[e / TB][e % TB] = rb[q];
     }
     __syncthreads();
     if (k0 + GK < K) fetch(k0 + GK);
 #pragma unroll
     for (int kk = 0; kk < GK; ++kk) {
-      double a[4], b[4];
+      double a[RT], b[RT];
 #pragma unroll
-      for (int i = 0; i < 4; ++i) a[i] = As[kk][ty + 16 * i];
+      for (int i = 0; i < RT; ++i) a[i] = As[kk][ty + 16 * i];
 #pragma unroll
-      for (int j = 0; j < 4; ++j) b[j] = Bs[kk][tx + 16 * j];
+      for (int j = 0; j < RT; ++j) b[j] = Bs[kk][tx + 16 * j];
 #pragma unroll
-      for (int i = 0; i < 4; ++i)
+      for (int i = 0; i < RT; ++i)
 #pragma unroll
-        for (int j = 0; j < 4; ++j) acc[i][j] = fma(a[i], b[j], acc[i][j]);
+        for (int j = 0; j < RT; ++j) acc[i][j] = fma(a[i], b[j], acc[i][j]);
     }
     __syncthreads();
   }
-  const bool mirror = g.sym && ti != tj;
 #pragma unroll
-  for (int i = 0; i < 4; ++i) {
+  for (int i = 0; i < RT; ++i) {
     const int gi = i0 + ty + 16 * i;
     if (gi >= M) continue;
 #pragma unroll
-    for (int j = 0; j < 4; ++j) {
+    for (int j = 0; j < RT; ++j) {
       const int gj = j0 + tx + 16 * j;
       if (gj < N) {
         C[(int64_t)gi * ld + gj] = acc[i][j];
@@ -234,44 +236,68 @@ __device__ __forceinline__ void gemm_tile_tf32x3(const GemmArgs& g, int s, int M
 // below the diagonal are computed and each off-diagonal tile is also stored
 // transposed.  g.prec selects, per system, the split-precision tile.
 // ---------------------------------------------------------------------------
-template <bool TA, bool W>
+template <bool TA, bool W, int TB>
 __global__ void __launch_bounds__(256, 3) k_gemm(GemmArgs g) {
   const int s = g.list[blockIdx.y];
   const int M = g.dm[s], N = g.dn[s], K = g.dk[s];
   const int ld = g.nao[s];
-  const int tn = (N + GB - 1) / GB;
-  const int tm = (M + GB - 1) / GB;
+  const int tn = (N + TB - 1) / TB;
+  const int tm = (M + TB - 1) / TB;
   int ti, tj;
+  bool mirror = false;
   if (g.sym) {
+    // tiles on and below the diagonal, mirrored; 32-wide tiles also compute
+    // the upper tile of each diagonal 64 x 64 block instead of mirroring it,
+    // so that every element is formed exactly as by the 64-wide tiles (the
+    // two orders of a symmetric product differ in rounding)
     const int t = blockIdx.x;
-    if (t >= tm * (tm + 1) / 2) return;
-    ti = (int)((sqrt(8.0 * t + 1.0) - 1.0) * 0.5);   // ti(ti+1)/2 <= t
-    while ((ti + 1) * (ti + 2) / 2 <= t) ++ti;
-    while (ti * (ti + 1) / 2 > t) --ti;
-    tj = t - ti * (ti + 1) / 2;
+    const int lower = tm * (tm + 1) / 2;
+    if (t < lower) {
+      ti = (int)((sqrt(8.0 * t + 1.0) - 1.0) * 0.5);   // ti(ti+1)/2 <= t
+      while ((ti + 1) * (ti + 2) / 2 <= t) ++ti;
+      while (ti * (ti + 1) / 2 > t) --ti;
+      tj = t - ti * (ti + 1) / 2;
+      mirror = TB == GB ? ti != tj : (ti >> 1) != (tj >> 1);
+    } else {
+      const int p = t - lower;
+      if (TB == GB || 2 * p + 1 >= tm) return;
+      ti = 2 * p;
+      tj = 2 * p + 1;
+    }
   } else {
     if ((int)blockIdx.x >= tm * tn) return;
     ti = blockIdx.x / tn;
     tj = blockIdx.x % tn;
   }
-  if (g.prec != nullptr && g.prec[g.prec_of != nullptr ? g.prec_of[s] : s] == 0)
+  // the split-precision tile exists for 64-wide tiles; the few-system
+  // 32-wide launch multiplies every system in FP64
+  if (TB == GB && g.prec != nullptr && g.prec[g.prec_of != nullptr ? g.prec_of[s] : s] == 0)
     gemm_tile_tf32x3<TA, W>(g, s, M, N, K, ld, ti, tj);
   else
-    gemm_tile_f64<TA, W>(g, s, M, N, K, ld, ti, tj);
+    gemm_tile_f64<TA, W, TB>(g, s, M, N, K, ld, ti, tj, mirror);
+}
+
+template <int TB>
+void launch_gemm_tb(const GemmArgs& g, bool transA, bool weighted, int tm, int count, cudaStream_t stream) {
+  const int tiles = g.sym ? tm * (tm + 1) / 2 + (TB == GB ? 0 : tm / 2) : tm * tm;
+  dim3 grid(tiles, count);
+  if (transA && weighted) k_gemm<true, true, TB><<<grid, 256, 0, stream>>>(g);
+  else if (transA) k_gemm<true, false, TB><<<grid, 256, 0, stream>>>(g);
+  else if (weighted) k_gemm<false, true, TB><<<grid, 256, 0, stream>>>(g);
+  else k_gemm<false, false, TB><<<grid, 256, 0, stream>>>(g);
 }
 
 void launch_gemm(const GemmArgs& g, bool transA, bool weighted, int max_tiles, int count,
                  cudaStream_t stream) {
   if (count == 0) return;
-  if (g.sym) {
-    const int tm = (int)std::lround(std::sqrt((double)max_tiles));   // max_tiles = tm * tm
-    max_tiles = tm * (tm + 1) / 2;
-  }
-  dim3 grid(max_tiles, count);
-  if (transA && weighted) k_gemm<true, true><<<grid, 256, 0, stream>>>(g);
-  else if (transA) k_gemm<true, false><<<grid, 256, 0, stream>>>(g);
-  else if (weighted) k_gemm<false, true><<<grid, 256, 0, stream>>>(g);
-  else k_gemm<false, false><<<grid, 256, 0, stream>>>(g);
+  const int tm = (int)std::lround(std::sqrt((double)max_tiles));   // max_tiles = tm * tm (64-wide)
+  // Fewer 64-wide tiles than SMs: 32-wide tiles put four times as many SMs
+  // on each product (a 64 x 64 x 240 FP64 tile alone takes ~8 us on one SM).
+  const int tiles64 = g.sym ? tm * (tm + 1) / 2 : tm * tm;
+  if ((int64_t)tiles64 * count < sm_count())
+    launch_gemm_tb<32>(g, transA, weighted, 2 * tm, count, stream);
+  else
+    launch_gemm_tb<GB>(g, transA, weighted, tm, count, stream);
 }
 
 // ---------------------------------------------------------------------------
