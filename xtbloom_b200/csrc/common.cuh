@@ -13,21 +13,35 @@
 #pragma once
 
 #include <cstdint>
+#include <map>
+#include <mutex>
+#include <utility>
+
 #include <cuda_runtime.h>
 
 namespace xtb {
 
-// Lets `func` use as much dynamic shared memory as the device allows beside
-// its static shared memory; returns that limit in bytes.
+// Lets `func` use as much dynamic shared memory as the current device allows
+// beside its static shared memory; returns that limit in bytes.  The
+// attribute belongs to the device, so it is set once per (kernel, device)
+// and remembered: contexts on several devices of one process each get it.
 template <class F>
 inline size_t allow_max_dynamic_smem(F func) {
-  int dev = 0, optin = 0;
+  static std::mutex mu;
+  static std::map<std::pair<const void*, int>, size_t> done;
+  int dev = 0;
   cudaGetDevice(&dev);
+  const std::pair<const void*, int> key((const void*)func, dev);
+  std::lock_guard<std::mutex> lock(mu);
+  const auto it = done.find(key);
+  if (it != done.end()) return it->second;
+  int optin = 0;
   cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
   cudaFuncAttributes fa{};
   cudaFuncGetAttributes(&fa, func);
   const size_t cap = (size_t)optin > fa.sharedSizeBytes ? (size_t)optin - fa.sharedSizeBytes : 0;
   cudaFuncSetAttribute(func, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)cap);
+  done.emplace(key, cap);
   return cap;
 }
 

@@ -645,8 +645,8 @@ constexpr int kTridiagSmemMax = 228;
 
 void launch_tridiag_smem(const EigArgs& g, const int32_t* list, int count, int max_n, cudaStream_t stream) {
   if (count == 0) return;
-  static const size_t cap256 = allow_max_dynamic_smem(k_tridiag_smem<256>);
-  static const size_t cap512 = allow_max_dynamic_smem(k_tridiag_smem<512>);
+  const size_t cap256 = allow_max_dynamic_smem(k_tridiag_smem<256>);
+  const size_t cap512 = allow_max_dynamic_smem(k_tridiag_smem<512>);
   int nloc = std::min(max_n, kTridiagSmemMax);
   while (nloc > 2 && tridiag_smem_bytes(nloc, 256) > cap256) --nloc;
   if (max_n > nloc) {
@@ -1304,9 +1304,9 @@ __global__ void __launch_bounds__(256) k_backtransform_wy(EigArgs g, int wcap, i
 void launch_backtransform_wy(const EigArgs& g, int count, int max_n, int max_m, int want_m,
                              cudaStream_t stream) {
   if (count == 0) return;
-  static const size_t cap = allow_max_dynamic_smem(k_backtransform_wy<false>);
-  static const size_t cap_s = allow_max_dynamic_smem(k_backtransform_wy<true>);
-  static const size_t cap_f = allow_max_dynamic_smem(k_wy_factor);
+  const size_t cap = allow_max_dynamic_smem(k_backtransform_wy<false>);
+  const size_t cap_s = allow_max_dynamic_smem(k_backtransform_wy<true>);
+  const size_t cap_f = allow_max_dynamic_smem(k_wy_factor);
   (void)cap_f;
   const int nblk = std::max(1, (max_n - 2 + WB - 1) / WB);
   k_wy_factor<<<dim3(nblk, count), 256, wy_factor_bytes(max_n), stream>>>(g);
@@ -1348,7 +1348,7 @@ __global__ void k_lowdin_weights(EigArgs g, int32_t* status) {
 void launch_tridiag(const EigArgs& g, int count, int max_n, cudaStream_t stream) {
   if (count == 0) return;
   const size_t sm = (2 * (size_t)max_n + 40) * sizeof(double);
-  static const size_t cap = allow_max_dynamic_smem(k_tridiag);
+  const size_t cap = allow_max_dynamic_smem(k_tridiag);
   (void)cap;
   k_tridiag<<<count, 512, sm, stream>>>(g, 0);
 }
@@ -1368,7 +1368,7 @@ void launch_eigvals(const EigArgs& g, int mode, double kt, int count, int max_n,
   if (count == 0) return;
   const int kNumSMs = sm_count();
   const size_t sm = (5 * (size_t)max_n + 40) * sizeof(double);
-  static const size_t cap = allow_max_dynamic_smem(k_tridiag_eigvals);
+  const size_t cap = allow_max_dynamic_smem(k_tridiag_eigvals);
   (void)cap;
   // Enough systems to fill the GPU: one CTA each, one thread per eigenvalue
   // (fewest Sturm sequences in total).  Few systems: spread each system's
@@ -1391,7 +1391,7 @@ void launch_inverse_iteration(const EigArgs& g, int count, int max_n, int want_m
                               cudaStream_t stream) {
   if (count == 0) return;
   const size_t smem = (size_t)5 * max_n * kInvSmemThreads * sizeof(double);
-  static const size_t cap = allow_max_dynamic_smem(k_inverse_iteration_smem);
+  const size_t cap = allow_max_dynamic_smem(k_inverse_iteration_smem);
   if (count < sm_count() && smem <= cap) {
     const int parts = std::max(1, (want_m + kInvSmemThreads - 1) / kInvSmemThreads);
     k_inverse_iteration_smem<<<dim3(parts, count), kInvSmemThreads, smem, stream>>>(g, ortol_rel);
@@ -1403,7 +1403,7 @@ void launch_inverse_iteration(const EigArgs& g, int count, int max_n, int want_m
 void launch_backtransform(const EigArgs& g, const int32_t* list, int count, int max_n, int mcap,
                           cudaStream_t stream) {
   if (count == 0) return;
-  static const size_t attr = allow_max_dynamic_smem(k_backtransform);
+  const size_t attr = allow_max_dynamic_smem(k_backtransform);
   (void)attr;
   size_t bytes = ((size_t)max_n + 8) * sizeof(double);
   if (mcap > 0) bytes += (size_t)mcap * max_n * sizeof(double);

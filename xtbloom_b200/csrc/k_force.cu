@@ -490,9 +490,9 @@ void launch_classical(const ForceArgs& f, int max_atoms, int max_shells, cudaStr
   (void)max_shells;
   if (f.count == 0) return;
   const size_t sm = ((size_t)(7 + 2 * kMaxD4Refs) * max_atoms + 48) * sizeof(double);
-  static const size_t attr = allow_max_dynamic_smem(k_classical);
-  static const size_t attr_t = allow_max_dynamic_smem(k_atm_table);
-  static const size_t attr_a = allow_max_dynamic_smem(k_atm);
+  const size_t attr = allow_max_dynamic_smem(k_classical);
+  const size_t attr_t = allow_max_dynamic_smem(k_atm_table);
+  const size_t attr_a = allow_max_dynamic_smem(k_atm);
   (void)attr;
   (void)attr_t;
   (void)attr_a;

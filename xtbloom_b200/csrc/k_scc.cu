@@ -290,7 +290,7 @@ void launch_potential(const SccArgs& a, const double* qsh, const double* dip, co
                         ? 1
                         : std::max(1, std::min((max_atoms + 7) / 8, 2 * sms / a.count));
   const size_t sm1 = ((size_t)(1 + 2 * kMaxD4Refs) * max_atoms + 8) * sizeof(double);
-  static const size_t attr1 = allow_max_dynamic_smem(k_potential_atoms);
+  const size_t attr1 = allow_max_dynamic_smem(k_potential_atoms);
   (void)attr1;
   k_potential_atoms<<<dim3(parts, a.count), 256, sm1, stream>>>(a, qsh, dip, qp, a.pot_acc);
   const size_t sm2 = ((size_t)max_atoms + max_shells + 8) * sizeof(double);
@@ -556,7 +556,7 @@ void launch_mulliken(const SccArgs& a, int max_n, cudaStream_t stream) {
   // two passes (2 (160 n + 16) doubles, within its 640 n).
   const int parts = std::min(16, 2 * sm_count() / a.count);
   if (parts >= 2 && a.work != nullptr) {
-    static const size_t attr_c = allow_max_dynamic_smem(k_mulliken_combine);
+    const size_t attr_c = allow_max_dynamic_smem(k_mulliken_combine);
     (void)attr_c;
     k_mulliken_part<<<dim3(parts, a.count), 256, 0, stream>>>(a, parts);
     k_mulliken_combine<<<a.count, kMullThreads, (size_t)10 * max_n * sizeof(double), stream>>>(a, parts);
@@ -564,7 +564,7 @@ void launch_mulliken(const SccArgs& a, int max_n, cudaStream_t stream) {
   }
   // rp(n) * 10 * n doubles: rp * n <= rp * cw = kMullThreads while n <= kMullThreads
   const size_t words = (size_t)10 * std::max(kMullThreads, max_n);
-  static const size_t attr = allow_max_dynamic_smem(k_mulliken);
+  const size_t attr = allow_max_dynamic_smem(k_mulliken);
   (void)attr;
   k_mulliken<<<a.count, kMullThreads, words * sizeof(double), stream>>>(a);
 }
@@ -899,7 +899,7 @@ void launch_energy_mixer(const SccArgs& a, int max_atoms, int max_shells, int ma
   (void)first_iteration;
   if (a.count == 0) return;
   const size_t sm = ((size_t)max_dim + (1 + kMaxD4Refs) * max_atoms + 64 + 8 * 44 + 8) * sizeof(double);
-  static const size_t attr = allow_max_dynamic_smem(k_energy_mixer);
+  const size_t attr = allow_max_dynamic_smem(k_energy_mixer);
   (void)attr;
   k_energy_mixer<<<a.count, 256, sm, stream>>>(a);
 }

@@ -201,7 +201,7 @@ void launch_setup(const DevTopo& t, const int32_t* list, int count, int max_atom
                   int64_t total_mat, cudaStream_t stream) {
   if (count == 0) return;
   const size_t sm = 2 * sizeof(double) * (size_t)max_atoms;
-  static const size_t attr = allow_max_dynamic_smem(k_coordination);
+  const size_t attr = allow_max_dynamic_smem(k_coordination);
   (void)attr;
   k_coordination<<<count, 256, sm, stream>>>(t, list, cn, cn_d4, mrad, dmrad);
   const int tpb = 64;
