@@ -237,6 +237,9 @@ struct Engine::Impl {
   Dbuf Pm, qmag, vmag, pop_mag, pop_mdip, pop_mqp;
   Dbuf efield, out_dipoles;
   bool have_field = false;
+  // FP64 GEMM tile width chosen by measurement per (product kind, orbital-count
+  // bucket of 32, power-of-two class of the system count)
+  std::map<uint64_t, int> gemm_width;
   // side streams for the size buckets of the eigensolver, which run
   // concurrently (small systems fill the SMs that large ones leave free)
   static constexpr int kBucketStreams = 8;
@@ -402,6 +405,33 @@ Engine::~Engine() {
 }
 
 namespace {
+
+// Times one product at both FP64 tile widths (each twice, best of two) and
+// returns the faster width, or 0 when the events cannot be made.  The product
+// is out of place, so running it several times leaves the same result.
+int tune_gemm_width(const GemmArgs& g, bool ta, bool weighted, int tiles, int count, cudaStream_t st) {
+  cudaEvent_t ev[5] = {};
+  bool ok = true;
+  for (auto& e : ev) ok = ok && cudaEventCreate(&e) == cudaSuccess;
+  int width = 0;
+  if (ok) {
+    const int order[4] = {64, 32, 64, 32};
+    cudaEventRecord(ev[0], st);
+    for (int q = 0; q < 4; ++q) {
+      launch_gemm(g, ta, weighted, tiles, count, st, order[q]);
+      cudaEventRecord(ev[q + 1], st);
+    }
+    float t[4] = {0.f, 0.f, 0.f, 0.f};
+    if (cudaEventSynchronize(ev[4]) == cudaSuccess) {
+      bool timed = true;
+      for (int q = 0; q < 4; ++q) timed = timed && cudaEventElapsedTime(&t[q], ev[q], ev[q + 1]) == cudaSuccess;
+      if (timed) width = std::min(t[1], t[3]) < std::min(t[0], t[2]) ? 32 : 64;
+    }
+  }
+  for (auto& e : ev)
+    if (e) cudaEventDestroy(e);
+  return width;
+}
 
 bool ensure_tables(Engine::Impl& m, cudaStream_t s) {
   if (m.tables_ready) return true;
@@ -1119,7 +1149,32 @@ xtbloom_status_t Engine::compute(const ComputeRequest& req, std::string& error) 
     g.offC = dch_mat;
     g.w = w;
     g.offW = dch_ao;
-    launch_gemm(g, ta, w != nullptr, tiles, count, st != nullptr ? st : s);
+    cudaStream_t gs = st != nullptr ? st : s;
+    // Tile width autotuner (FP64 products only: the two widths form every
+    // element identically, so the choice never changes a result).  The first
+    // product of each kind, size bucket and count class in an eager
+    // iteration runs both widths twice, timed by events, and the faster one
+    // is kept for this context; captured iterations only reuse choices.
+    int width = 0;
+    if (prec == nullptr && count > 0) {
+      const int lg = 31 - __builtin_clz((unsigned)count);
+      const int32_t* nv = m.nvec.as<int32_t>();
+      const uint64_t key = ((uint64_t)((m.max_n + 31) / 32) << 32) | ((uint64_t)lg << 8) |
+                           (uint64_t)(ta ? 1 : 0) | ((uint64_t)(w != nullptr) << 1) |
+                           ((uint64_t)(sym ? 1 : 0) << 2) | ((uint64_t)(dk == nv) << 3) |
+                           ((uint64_t)(dm == nv) << 4);
+      const auto it = m.gemm_width.find(key);
+      if (it != m.gemm_width.end()) {
+        width = it->second;
+      } else {
+        cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+        if (cudaStreamIsCapturing(gs, &cs) == cudaSuccess && cs == cudaStreamCaptureStatusNone) {
+          width = tune_gemm_width(g, ta, w != nullptr, tiles, count, gs);
+          if (width != 0) m.gemm_width.emplace(key, width);
+        }
+      }
+    }
+    launch_gemm(g, ta, w != nullptr, tiles, count, gs, width);
   };
   const int32_t* dnao = dch_nao;
   const int32_t* dnvec = m.nvec.as<int32_t>();

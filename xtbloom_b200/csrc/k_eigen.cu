@@ -288,13 +288,13 @@ void launch_gemm_tb(const GemmArgs& g, bool transA, bool weighted, int tm, int c
 }
 
 void launch_gemm(const GemmArgs& g, bool transA, bool weighted, int max_tiles, int count,
-                 cudaStream_t stream) {
+                 cudaStream_t stream, int width) {
   if (count == 0) return;
   const int tm = (int)std::lround(std::sqrt((double)max_tiles));   // max_tiles = tm * tm (64-wide)
   // Fewer 64-wide tiles than SMs: 32-wide tiles put four times as many SMs
   // on each product (a 64 x 64 x 240 FP64 tile alone takes ~8 us on one SM).
   const int tiles64 = g.sym ? tm * (tm + 1) / 2 : tm * tm;
-  if ((int64_t)tiles64 * count < sm_count())
+  if (width == 32 || (width == 0 && (int64_t)tiles64 * count < sm_count()))
     launch_gemm_tb<32>(g, transA, weighted, 2 * tm, count, stream);
   else
     launch_gemm_tb<GB>(g, transA, weighted, tm, count, stream);

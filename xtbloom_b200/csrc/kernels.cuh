@@ -133,8 +133,10 @@ void launch_setup(const DevTopo& t, const int32_t* list, int count, int max_atom
                   double* dmrad, double* S, double* D, double* Q, double* H0, double* gam,
                   int64_t total_mat, cudaStream_t stream);
 
+// width 32 or 64 forces the FP64 tile edge; 0 picks 32 when fewer 64-wide
+// tiles than SMs.  Both widths form every element identically.
 void launch_gemm(const GemmArgs& g, bool transA, bool weighted, int max_tiles, int count,
-                 cudaStream_t stream);
+                 cudaStream_t stream, int width = 0);
 void launch_tridiag(const EigArgs& g, int count, int max_n, cudaStream_t stream);
 void launch_tridiag_smem(const EigArgs& g, const int32_t* list, int count, int max_n, cudaStream_t stream);
 // Register-resident cluster tridiagonalisation for systems with n <= tridiag_reg_max_n().
