@@ -1,10 +1,17 @@
 # Builds the reference's CPU library (the FP64 oracle and the timed CPU
 # baseline) straight from its sources with g++, without its own build system.
 # Inputs are read in place under REF; every output lands in oracle/_ref/.
-#   make -f oracle/ref.mk -j8 REF=/root/reference
-REF      ?= /root/reference
+#   make -f oracle/ref.mk -j8 REF=<reference checkout>
+# REF comes from the command line or $XTBLOOM_REFERENCE_SRC.  The BLAS/LAPACK
+# the reference's eigensolver loads at run time is the OpenBLAS that ships
+# inside the installed scipy wheel (LP64, scipy_-prefixed symbols), located
+# through the Python interpreter on PATH.
+REF      ?= $(XTBLOOM_REFERENCE_SRC)
 OUT      ?= $(dir $(lastword $(MAKEFILE_LIST)))_ref
-OPENBLAS ?= $(firstword $(wildcard /opt/prime-rl/.venv/lib/python3.12/site-packages/scipy.libs/libscipy_openblas-*.so))
+OPENBLAS ?= $(shell python3 -c 'import glob, os, scipy; d = os.path.join(os.path.dirname(os.path.dirname(scipy.__file__)), "scipy.libs"); print((sorted(glob.glob(os.path.join(d, "libscipy_openblas*.so"))) or [""])[0])')
+ifeq ($(strip $(REF)),)
+$(error set REF=<reference checkout> or XTBLOOM_REFERENCE_SRC)
+endif
 
 SRCS := src/api.cpp src/runtime/backend.cpp src/runtime/gfn2_cpu_execution.cpp \
   src/runtime/gfn2_plan.cpp src/runtime/model_plan.cpp src/runtime/model_registry.cpp \

@@ -12,7 +12,7 @@ electric-field interaction attachments (block_version 1) on
     |E| <= 0.01, and the same molecules without a field,
 storing energies, forces, charges, dipole moments and SCC iteration counts.
 
-Usage:  python tests/golden/make_field.py /root/reference
+Usage:  python tests/golden/make_field.py <reference checkout>  (or set XTBLOOM_REFERENCE_SRC)
 """
 from __future__ import annotations
 
@@ -87,5 +87,15 @@ def main(ref: Path):
         print(s["case"], s["name"], s["status"], s["scc_iterations"], round(s["energy"], 8), np.round(s["dipole"], 4))
 
 
+
+def reference_checkout() -> Path:
+    """The reference checkout: the first argument, else $XTBLOOM_REFERENCE_SRC."""
+    import os
+    arg = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("XTBLOOM_REFERENCE_SRC")
+    if not arg:
+        sys.exit("usage: pass the reference checkout as the first argument "
+                 "or set XTBLOOM_REFERENCE_SRC")
+    return Path(arg)
+
 if __name__ == "__main__":
-    main(Path(sys.argv[1] if len(sys.argv) > 1 else "/root/reference"))
+    main(reference_checkout())

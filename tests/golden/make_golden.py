@@ -16,7 +16,7 @@ Two sources, both produced in the container that holds the reference checkout:
     point-charge forces), together with the reference's xTB 6.7.1 QM/MM
     goldens for the cases that come from its conformance set.
 
-Usage:  python tests/golden/make_golden.py /root/reference
+Usage:  python tests/golden/make_golden.py <reference checkout>  (or set XTBLOOM_REFERENCE_SRC)
 """
 from __future__ import annotations
 
@@ -33,7 +33,7 @@ sys.path.insert(0, str(ROOT))
 from xtbloom_b200 import abi, workloads as W  # noqa: E402
 
 SYM = {"h": 1, "he": 2, "c": 6, "n": 7, "o": 8, "f": 9, "ne": 10, "na": 11, "si": 14, "cl": 17,
-       "zn": 30, "i": 53, "rn": 86}
+       "zn": 30, "br": 35, "i": 53, "rn": 86}
 
 
 def read_coord(path: Path):
@@ -178,6 +178,16 @@ def main_pc(ref: Path):
          "systems": cases}, indent=0))
 
 
+
+def reference_checkout() -> Path:
+    """The reference checkout: the first argument, else $XTBLOOM_REFERENCE_SRC."""
+    import os
+    arg = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("XTBLOOM_REFERENCE_SRC")
+    if not arg:
+        sys.exit("usage: pass the reference checkout as the first argument "
+                 "or set XTBLOOM_REFERENCE_SRC")
+    return Path(arg)
+
 if __name__ == "__main__":
-    main(Path(sys.argv[1] if len(sys.argv) > 1 else "/root/reference"))
-    main_pc(Path(sys.argv[1] if len(sys.argv) > 1 else "/root/reference"))
+    main(reference_checkout())
+    main_pc(reference_checkout())

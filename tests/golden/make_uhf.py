@@ -12,7 +12,7 @@ spin_channels = 2 on
 and stores energies, forces, charges and SCC iteration counts.  The radical
 inputs are regenerated from the seed by the tests.
 
-Usage:  python tests/golden/make_uhf.py /root/reference
+Usage:  python tests/golden/make_uhf.py <reference checkout>  (or set XTBLOOM_REFERENCE_SRC)
 """
 from __future__ import annotations
 
@@ -65,5 +65,15 @@ def main(ref: Path):
     (HERE / "uhf_fixtures.json").write_text(json.dumps(out))
 
 
+
+def reference_checkout() -> Path:
+    """The reference checkout: the first argument, else $XTBLOOM_REFERENCE_SRC."""
+    import os
+    arg = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("XTBLOOM_REFERENCE_SRC")
+    if not arg:
+        sys.exit("usage: pass the reference checkout as the first argument "
+                 "or set XTBLOOM_REFERENCE_SRC")
+    return Path(arg)
+
 if __name__ == "__main__":
-    main(Path(sys.argv[1] if len(sys.argv) > 1 else "/root/reference"))
+    main(reference_checkout())

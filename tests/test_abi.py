@@ -54,6 +54,20 @@ def test_initialisers_set_reference_defaults():
     assert lib.xtbloom_compute_options_init(C.byref(o), 8) == abi.INVALID_ARGUMENT
 
 
+def test_initialisers_record_the_callers_size():
+    """A newer caller's larger structure keeps its size; nothing past the known
+    layout is written; sizes above uint32_t are refused (src/api.cpp:66-80)."""
+    lib = abi.bind(library_path())
+    buf = (C.c_uint8 * 128)(*([0xAB] * 128))
+    assert lib.xtbloom_compute_options_init(C.cast(buf, C.POINTER(abi.ComputeOptions)), 96) == abi.SUCCESS
+    o = abi.ComputeOptions.from_buffer(buf)
+    assert o.struct_size == 96 and o.api_version == 1
+    assert bytes(buf[80:128]) == b"\xab" * 48
+    big = C.c_size_t(1 << 32).value
+    assert lib.xtbloom_compute_options_init(C.byref(abi.ComputeOptions()), big) == abi.INVALID_ARGUMENT
+    assert b"uint32_t" in lib.xtbloom_get_last_error()
+
+
 def test_status_strings_and_version():
     lib = abi.bind(library_path())
     assert lib.xtbloom_status_string(abi.SCC_NOT_CONVERGED) == b"SCC not converged"

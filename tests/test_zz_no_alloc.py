@@ -80,6 +80,14 @@ def test_static_vectors_rebuild_the_existing_loewdin_matrix_twice(cuda_lib, fixt
         Xs = (U * w ** -0.5) @ U.T
         assert np.abs(Xs - X).max() < 1e-10
     assert torch.equal(bufs[0], bufs[1])
+    # after the first call has looked up the scratch, repeated calls leave the
+    # device's free memory unchanged: nothing is allocated per call
+    free0 = torch.cuda.mem_get_info(0)[0]
+    for buf in bufs:
+        assert f(ptr(d_t), ptr(e_t), ptr(w_t), n, n, ptr(buf), 0.0, stream) == abi.SUCCESS
+    torch.cuda.synchronize()
+    assert torch.cuda.mem_get_info(0)[0] == free0
+    assert torch.equal(bufs[0], bufs[1])
     # a leading subset gives the same leading vectors
     part = torch.full((n * n,), float("nan"), dtype=torch.float64, device="cuda:0")
     m = n // 2

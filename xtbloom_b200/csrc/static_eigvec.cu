@@ -63,9 +63,23 @@ int static_eigvec_run(const double* d, const double* e, const double* ev, int n,
   if (m == 0) return 0;
   int dev = 0;
   cudaError_t ce = cudaGetDevice(&dev);
-  if (ce != cudaSuccess || dev < 0 || dev >= kMaxDevices) {
+  if (ce != cudaSuccess) {
     err = std::string("no usable CUDA device: ") + cudaGetErrorString(ce);
     return 2;
+  }
+  if (dev < 0 || dev >= kMaxDevices) {
+    err = "device " + std::to_string(dev) + " is beyond the " + std::to_string(kMaxDevices) +
+          " devices this routine keeps scratch addresses for";
+    return 2;
+  }
+  // An error left by the caller's earlier asynchronous work would otherwise be
+  // read (and cleared) after the launch as if the launch had failed; report it
+  // as what it is and leave it pending for the caller.
+  ce = cudaPeekAtLastError();
+  if (ce != cudaSuccess) {
+    err = std::string("an earlier CUDA error is pending on this thread (nothing was launched): ") +
+          cudaGetErrorString(ce);
+    return 3;
   }
   double* scratch = nullptr;
   {
