@@ -374,11 +374,16 @@ XTBLOOM_API xtbloom_status_t xtbloom_b200_context_set_execution(xtbloom_context_
  * under a committed memory budget.  Inverse iteration for eigenvectors
  * 0..m-1 of T = tridiag(offdiagonal[n-1], diagonal[n], offdiagonal[n-1]) with
  * ascending eigenvalues[m]; vector j goes to vectors[j*n .. j*n+n), largest
- * component positive.  All pointers are CUDA device memory of the current
+ * component positive.  The eigenvalues must be sorted ascending: with
+ * unsorted values every gap looks like a cluster and the vectors returned are
+ * undefined (the call cannot detect this and still returns SUCCESS).  All pointers are CUDA device memory of the current
  * device (offdiagonal may be NULL when n == 1); the work is enqueued on
  * cuda_stream (a cudaStream_t, NULL for the default stream) and the call
- * returns without waiting.  cluster_tolerance (0 selects 2e-7) is relative to
- * ||T||_1: eigenvalues closer than that are re-orthogonalised together.
+ * returns without waiting.  cluster_tolerance (0 selects 2e-7, the value the
+ * SCC uses for Hamiltonians; the overlap factorisation uses 2e-6) is relative
+ * to ||T||_1: eigenvalues closer than that are re-orthogonalised together.
+ * An error already pending from earlier asynchronous work is reported as
+ * INTERNAL_ERROR with its own message, before anything is launched.
  * Work vectors live in a fixed 1.25 MiB array of the library's device memory,
  * so n is limited to 256 (INVALID_ARGUMENT beyond, before anything runs);
  * nothing in it has to start at zero.  Calls that overlap on one device race

@@ -93,3 +93,28 @@ def test_kernels_agree_on_whole_computes(both):
         a0, a1 = offs[i], offs[i + 1]
         assert np.abs(a["forces"][3 * a0:3 * a1] - b["forces"][3 * a0:3 * a1]).max() < tol
         assert np.abs(a["atomic_charges"][a0:a1] - b["atomic_charges"][a0:a1]).max() < tol
+
+
+def test_warm_started_refinement_matches_the_householder_path(cuda_lib, monkeypatch):
+    """The opt-in warm-started eigensolver (Ogita-Aishima refinement of the
+    previous iteration's eigenvectors, k_refine.cu) gives the Householder
+    path's results: same statuses and iteration counts, energies, charges and
+    forces to well inside the public tolerances; it refines most channels
+    after the first iterations and falls back to the Householder path for the
+    rest."""
+    full = W.config1(4096, seed=1)
+    b = W.subset(full, [7, 100, 2048, 4000, 11, 222])
+    ref = cuda_lib.compute(b)
+    monkeypatch.setenv("XTBLOOM_B200_REFINE_STEPS", "5")
+    lib = abi.Library(library_path(), backend=abi.BACKEND_CUDA, device_id=0)
+    try:
+        out = lib.compute(b)
+        stats = lib.fetch("refine_stats", capacity=4096).reshape(256, 8)
+    finally:
+        lib.close()
+    assert np.array_equal(out["per_system_status"], ref["per_system_status"])
+    assert np.abs(out["scc_iterations"] - ref["scc_iterations"]).max() <= 1
+    assert np.abs(out["energies"] - ref["energies"]).max() < 1e-8
+    assert np.abs(out["atomic_charges"] - ref["atomic_charges"]).max() < 1e-6
+    assert np.abs(out["forces"] - ref["forces"]).max() < 1e-6
+    assert stats[:, 0].sum() > 0 and stats[:, 1:4].sum() > 0   # channels were refined

@@ -39,15 +39,49 @@ def test_graph_replay_matches_eager(cuda_lib):
 
 
 def test_repeated_calls_are_reproducible(cuda_lib):
-    """The SCC has no floating-point atomics: repeated calls give bitwise-equal
-    charges, iteration counts and statuses, even for systems that never
-    converge (where any rounding difference would be amplified)."""
+    """The SCC has no floating-point atomics and the force kernels sum their
+    gradient contributions in 64-bit fixed point, whose integer adds do not
+    depend on order: repeated calls give bitwise-equal energies, forces,
+    charges, iteration counts and statuses, also for systems that never
+    converge (where any rounding difference would be amplified).  This is
+    what XTBLOOM_DETERMINISM_REPRODUCIBLE asks for (reference
+    include/xtbloom/xtbloom.h:127-134), and it holds in the default mode too."""
     full = W.config1(4096, seed=1)
     b = W.subset(full, [1472, 3157, 3349, 3920, 11, 222])
     one = cuda_lib.compute(b)
-    two = cuda_lib.compute(b)
-    assert np.array_equal(one["per_system_status"], two["per_system_status"])
-    assert np.array_equal(one["scc_iterations"], two["scc_iterations"])
-    assert np.array_equal(one["atomic_charges"], two["atomic_charges"], equal_nan=True)
-    assert np.nanmax(np.abs(one["energies"] - two["energies"])) < 1e-12
-    assert np.nanmax(np.abs(one["forces"] - two["forces"])) < 1e-12
+    opts = cuda_lib.make_options()
+    opts.determinism = abi.DETERMINISM_REPRODUCIBLE
+    two = cuda_lib.compute(b, opts)
+    for key in ("per_system_status", "scc_iterations", "energies", "forces", "atomic_charges"):
+        assert np.array_equal(one[key], two[key], equal_nan=True), key
+
+
+def _run_at_width(width, batches, monkeypatch):
+    monkeypatch.setenv("XTBLOOM_B200_GEMM_WIDTH", str(width))
+    lib = abi.Library(library_path(), backend=abi.BACKEND_CUDA, device_id=0)
+    try:
+        return [lib.compute(b) for b in batches]
+    finally:
+        lib.close()
+
+
+def test_gemm_tile_widths_form_identical_elements(monkeypatch):
+    """Every FP64 product (plain, transposed, weighted, symmetric with mirrored
+    tiles) at 32-wide and at 64-wide tiles gives bitwise-equal results, so the
+    tile-width autotuner cannot change an outcome.  AO counts here are not
+    multiples of 32; the unrestricted batch adds the spin-channel products and
+    the energy-weighted density of the forces."""
+    import json
+    from conftest import GOLDEN
+    full = W.config1(4096, seed=1)
+    b1 = W.subset(full, [7, 100, 2048, 4000, 11, 222, 1472])
+    uhf = json.loads((GOLDEN / "uhf_fixtures.json").read_text())
+    rad = uhf["radicals"]["systems"][:4]
+    b2 = W.subset(W.config4(2048, seed=4), [c["index"] for c in rad])
+    n_ao = [int(np.sum(np.where(W.molecule(b1, i)[0] == 1, 1, 4))) for i in range(b1.batch_size)]
+    assert any(n % 32 for n in n_ao)
+    r32 = _run_at_width(32, [b1, b2], monkeypatch)
+    r64 = _run_at_width(64, [b1, b2], monkeypatch)
+    for a, b in zip(r32, r64):
+        for key in ("per_system_status", "scc_iterations", "energies", "forces", "atomic_charges"):
+            assert np.array_equal(a[key], b[key], equal_nan=True), key

@@ -1,28 +1,34 @@
-"""Split-precision execution form: the FP64 fixed point, reached on another path.
+"""Split-precision execution form against the reference's FP64 fixed point.
 
-The mixed form runs the SCC basis-transform and density GEMMs as 3xTF32
-tensor-core products until a system's charge residual falls below the
-precision switch, then iterates in FP64; a system converges only on an FP64
-iteration.  Both forms stop anywhere inside the SCC convergence gate (charge
-residual rms < 1e-6, |dF| < 1e-8), on different trajectories.  The energy is
-variational in the density, so it agrees to well inside 1e-6 Eh; charges and
-forces are first order in the residual left at convergence, whose largest
-component can exceed the rms tolerance several times, so they are compared at
-1e-4 (the FP64 form itself is only that close to the fixed point).
+The mixed form runs the SCC products (basis transforms, density, the
+warm-started eigenvector refinement) as 3xTF32 tensor-core products until a
+system's charge residual falls below the precision switch, then iterates in
+FP64; a system converges only on an FP64 iteration, and those iterations go
+on to a gate 100 times tighter than the requested one, so that the result is
+the fixed point itself rather than any point inside the gate.
+
+Why the fixed point is the reference to compare with: the reference itself
+stops anywhere inside its gate (charge residual rms < 1e-6, |dF| < 1e-8), and
+on this workload its charges at the default settings lie up to ~6e-5 e from
+its own fixed point (its result at charge tolerance 1e-10).  A form that
+follows another trajectory can only be held to that fixed point; so the
+outputs are checked (1) against the reference library converged to the fixed
+point, at the public tolerances, and (2) against the reference library at the
+default settings, within the reference's own distance from its fixed point
+plus the public tolerance.
 """
 from __future__ import annotations
+
+import json
 
 import numpy as np
 import pytest
 
-from conftest import TOL_E, TOL_F, TOL_Q, as_molecule
+from conftest import GOLDEN, REF_LIB, TOL_E, TOL_F, TOL_Q, as_molecule
 from xtbloom_b200 import abi, library_path
 from xtbloom_b200 import workloads as W
 
 pytestmark = pytest.mark.gpu
-
-# charge and force agreement of two forms that both stop inside the SCC gate
-TOL_SCC = 1e-4
 
 
 @pytest.fixture(scope="module")
@@ -33,29 +39,59 @@ def mixed_lib():
     lib.close()
 
 
-def test_mixed_matches_fp64_on_workload_sample(cuda_lib, mixed_lib):
-    """96 evenly spaced systems of the 4096-system workload, mixed vs FP64."""
+def per_system_max(b, x, y, width):
+    o = b.atom_offsets
+    return np.array([np.abs(x[width * o[i]:width * o[i + 1]] - y[width * o[i]:width * o[i + 1]]).max()
+                     for i in range(b.batch_size)])
+
+
+@pytest.mark.skipif(not REF_LIB.exists(), reason="reference library not built")
+def test_mixed_reaches_the_reference_fixed_point_on_workload_sample(mixed_lib):
+    """96 evenly spaced systems of the 4096-system workload, against the live reference."""
     full = W.config1(4096, seed=1)
     idx = np.linspace(0, 4095, 96).round().astype(int)
     b = W.subset(full, idx)
-    ref = cuda_lib.compute(b)
     out = mixed_lib.compute(b)
-    split = mixed_lib.fetch("split_iterations")
-    assert np.array_equal(ref["per_system_status"], out["per_system_status"])
-    ok = ref["per_system_status"] == 0
+    split = mixed_lib.fetch("split_iterations", capacity=4096)
+    ref = abi.Library(str(REF_LIB), backend=abi.BACKEND_CPU, cpu_threads=0)
+    tight = ref.compute(b, ref.make_options(ctol=1e-10, etol=1e-13))
+    dflt = ref.compute(b)
+    ok = (tight["per_system_status"] == 0) & (dflt["per_system_status"] == 0)
     assert ok.sum() >= 90
-    assert np.abs(out["energies"][ok] - ref["energies"][ok]).max() < TOL_E
-    for i in np.where(ok)[0]:
-        a0, a1 = b.atom_offsets[i], b.atom_offsets[i + 1]
-        assert np.abs(out["forces"][3 * a0:3 * a1] - ref["forces"][3 * a0:3 * a1]).max() < TOL_SCC
-        assert np.abs(out["atomic_charges"][a0:a1] - ref["atomic_charges"][a0:a1]).max() < TOL_SCC
-    # the split-precision GEMMs ran, and every converged system finished in FP64
+    assert np.array_equal(out["per_system_status"][ok], tight["per_system_status"][ok])
+    # (1) the fixed point, at the public tolerances
+    assert np.abs(out["energies"][ok] - tight["energies"][ok]).max() < TOL_E
+    assert per_system_max(b, out["forces"], tight["forces"], 3)[ok].max() < TOL_F
+    assert per_system_max(b, out["atomic_charges"], tight["atomic_charges"], 1)[ok].max() < TOL_Q
+    # (2) the default-gate reference: no farther than it is from its own fixed point
+    for key, w, tol in (("forces", 3, TOL_F), ("atomic_charges", 1, TOL_Q)):
+        gate = per_system_max(b, dflt[key], tight[key], w)
+        ours = per_system_max(b, out[key], dflt[key], w)
+        assert (ours[ok] <= gate[ok] + 0.1 * tol).all(), key
+    assert np.abs(out["energies"][ok] - dflt["energies"][ok]).max() < TOL_E
+    # the split-precision products ran, and every converged system finished in FP64
     assert (split[ok] >= 1).all()
     assert (split[ok] < out["scc_iterations"][ok]).all()
 
 
+def test_mixed_water_clusters_reach_the_fixed_point(mixed_lib):
+    """Precision stress at 600-1200 AOs: water clusters of the 256-cluster workload
+    against the reference library's fixed point (goldens by tests/golden/make_large.py)."""
+    cases = json.loads((GOLDEN / "large_fixtures.json").read_text())["systems"]
+    assert all("tight_energy" in c for c in cases)
+    full = W.config3(256, seed=3)
+    b = W.subset(full, [c["index"] for c in cases])
+    out = mixed_lib.compute(b)
+    for i, c in enumerate(cases):
+        a0, a1 = b.atom_offsets[i], b.atom_offsets[i + 1]
+        assert out["per_system_status"][i] == c["tight_status"] == 0
+        assert abs(out["energies"][i] - c["tight_energy"]) < TOL_E
+        assert np.abs(out["forces"][3 * a0:3 * a1] - np.asarray(c["tight_forces"])).max() < TOL_F
+        assert np.abs(out["atomic_charges"][a0:a1] - np.asarray(c["tight_charges"])).max() < TOL_Q
+
+
 def test_mixed_reproduces_reference_fixtures(mixed_lib, fixtures):
-    """The committed reference outputs, computed in the mixed form."""
+    """The committed reference outputs (small molecules, ions, atoms), computed in the mixed form."""
     mols = [as_molecule(s) for s in fixtures]
     b = abi.ragged_from_lists([m[0] for m in mols], [m[1] for m in mols],
                               [m[2] for m in mols], [m[3] for m in mols])

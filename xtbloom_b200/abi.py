@@ -22,6 +22,10 @@ KELVIN_TO_HARTREE = 3.166808578545117e-6
 SUCCESS, INVALID_ARGUMENT, BACKEND_UNAVAILABLE, NOT_SUPPORTED = 0, 1, 2, 3
 ALLOCATION_FAILED, NOT_IMPLEMENTED, INTERNAL_ERROR = 4, 5, 6
 SCC_NOT_CONVERGED, EIGENSOLVER_FAILED = 7, 8
+# request states (xtbloom.h:80-90)
+REQUEST_IDLE, REQUEST_PENDING, REQUEST_COMPLETE = 0, 1, 2
+# determinism policies (xtbloom.h:127-134)
+DETERMINISM_DEFAULT, DETERMINISM_REPRODUCIBLE = 0, 1
 STATUS_NAMES = {0: "SUCCESS", 1: "INVALID_ARGUMENT", 2: "BACKEND_UNAVAILABLE",
                 3: "NOT_SUPPORTED", 4: "ALLOCATION_FAILED", 5: "NOT_IMPLEMENTED",
                 6: "INTERNAL_ERROR", 7: "SCC_NOT_CONVERGED", 8: "EIGENSOLVER_FAILED"}
@@ -172,6 +176,17 @@ def bind(path: str) -> C.CDLL:
     lib.xtbloom_request_get_error.argtypes = [C.c_void_p]
     lib.xtbloom_request_destroy.restype = None
     lib.xtbloom_request_destroy.argtypes = [C.c_void_p]
+    lib.xtbloom_plan_create.restype = st
+    lib.xtbloom_plan_create.argtypes = [C.c_void_p, P(Batch), P(ComputeOptions), P(C.c_void_p)]
+    lib.xtbloom_plan_destroy.restype = None
+    lib.xtbloom_plan_destroy.argtypes = [C.c_void_p]
+    lib.xtbloom_plan_query_workspace.restype = st
+    lib.xtbloom_plan_query_workspace.argtypes = [C.c_void_p, P(WorkspaceQuery)]
+    lib.xtbloom_plan_compute.restype = st
+    lib.xtbloom_plan_compute.argtypes = [C.c_void_p, P(Batch), P(ComputeOptions), P(BatchResult)]
+    lib.xtbloom_plan_compute_enqueue.restype = st
+    lib.xtbloom_plan_compute_enqueue.argtypes = [C.c_void_p, P(Batch), P(ComputeOptions),
+                                                 P(BatchResult), C.c_void_p]
     return lib
 
 
@@ -380,6 +395,56 @@ class Library:
         self._check(self.lib.xtbloom_compute(self.ctx, C.byref(batch), C.byref(options), C.byref(res)))
         self.last_result_flags = res.flags
         return outputs
+
+
+def host_outputs(b: RaggedBatch, fill: float = np.nan) -> dict:
+    """Host output buffers of one batch (energies, forces, charges, diagnostics)."""
+    nb, na = b.batch_size, b.total_atoms
+    return {"energies": np.full(nb, fill), "forces": np.full(3 * na, fill),
+            "atomic_charges": np.full(na, fill),
+            "scc_iterations": np.full(nb, -7, np.int32), "scc_converged": np.full(nb, 7, np.uint8),
+            "per_system_status": np.full(nb, -7, np.int32)}
+
+
+class Plan:
+    """A fixed-topology plan (xtbloom_plan_*) of a Library's context."""
+
+    def __init__(self, lib: Library, b: RaggedBatch, options: ComputeOptions | None = None):
+        self.lib = lib
+        self.options = options or lib.make_options()
+        self._batch = lib.make_batch(b)
+        h = C.c_void_p()
+        lib._check(lib.lib.xtbloom_plan_create(lib.ctx, C.byref(self._batch), C.byref(self.options),
+                                               C.byref(h)))
+        self.handle = h
+
+    def workspace(self) -> WorkspaceQuery:
+        q = WorkspaceQuery()
+        self.lib._check(self.lib.lib.xtbloom_workspace_query_init(C.byref(q), C.sizeof(q)))
+        q.compute_flags = self.options.flags
+        self.lib._check(self.lib.lib.xtbloom_plan_query_workspace(self.handle, C.byref(q)))
+        return q
+
+    def compute(self, b: RaggedBatch, outputs: dict | None = None,
+                options: ComputeOptions | None = None) -> dict:
+        outputs = outputs if outputs is not None else host_outputs(b)
+        batch = self.lib.make_batch(b)
+        res = self.lib.make_result({k: v for k, v in outputs.items() if k in RESULT_BUFFERS})
+        self.lib._check(self.lib.lib.xtbloom_plan_compute(self.handle, C.byref(batch),
+                                                          C.byref(options or self.options),
+                                                          C.byref(res)))
+        return outputs
+
+    def close(self):
+        if getattr(self, "handle", None):
+            self.lib.lib.xtbloom_plan_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 def ragged_from_lists(numbers_list, positions_list, charges=None, uhf=None,

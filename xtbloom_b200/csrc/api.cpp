@@ -6,13 +6,17 @@
 // per-system diagnostic was committed, failed systems carrying quiet-NaN
 // slices.  Exceptions never cross the boundary.
 #include <atomic>
+#include <algorithm>
 #include <cmath>
+#include <condition_variable>
 #include <cstdlib>
 #include <cstring>
 #include <memory>
 #include <mutex>
 #include <new>
 #include <string>
+#include <thread>
+#include <vector>
 
 #include <cuda_runtime.h>
 
@@ -32,11 +36,17 @@ xtbloom_status_t fail(xtbloom_status_t st, const std::string& msg) {
 template <class T>
 xtbloom_status_t init_struct(T* p, size_t size, size_t v1) {
   if (p == nullptr) return fail(XTBLOOM_STATUS_INVALID_ARGUMENT, "structure pointer is NULL");
-  if (size < v1) return fail(XTBLOOM_STATUS_INVALID_ARGUMENT, "structure size is smaller than its ABI-v1 prefix");
+  if (size < v1 || size > UINT32_MAX)
+    return fail(XTBLOOM_STATUS_INVALID_ARGUMENT,
+                "structure size is smaller than its ABI-v1 prefix or exceeds uint32_t");
+  // Never write past the layout this library knows; the caller's size is
+  // recorded as given (a newer caller's larger structure keeps its size), as
+  // the reference does (src/api.cpp:66-80).
   const size_t n = size < sizeof(T) ? size : sizeof(T);
   std::memset(static_cast<void*>(p), 0, n);
-  p->struct_size = static_cast<uint32_t>(n);
+  p->struct_size = static_cast<uint32_t>(size);
   p->api_version = XTBLOOM_API_VERSION;
+  g_last_error.clear();
   return XTBLOOM_STATUS_SUCCESS;
 }
 
@@ -90,26 +100,80 @@ bool check_out(const xtbloom_buffer_t& b, size_t need, bool required, const char
 }  // namespace
 
 struct xtbloom_context {
-  std::mutex mutex;
+  std::mutex mutex;   // one transaction at a time (synchronous calls and accepted requests)
   int device = 0;
   cudaStream_t stream = nullptr;
   bool own_stream = false;
   std::unique_ptr<xtb::Engine> engine;
+  // execution form (xtbloom_b200_context_set_execution), applied to the
+  // context engine and to the engines of its plans
+  int precision = 0;
+  double switch_residual = 1e-5;
+  bool graphs = false;
 };
 
+// A reusable asynchronous request (src/runtime/request.cpp semantics): an
+// accepted submission runs on a worker thread that drives the context stream
+// under the context's transaction lock, so enqueue returns at once; query
+// polls the state, wait blocks until the submission has completed.  The
+// descriptors are copied at submission; the buffers they name must stay
+// valid until completion.
 struct xtbloom_request {
   xtbloom_context_t* context = nullptr;
+  std::mutex mu;
+  std::condition_variable cv;
   xtbloom_request_state_t state = XTBLOOM_REQUEST_IDLE;
   xtbloom_status_t completion = XTBLOOM_STATUS_SUCCESS;
   uint32_t result_flags = 0;
   std::string error;
+  std::mutex join_mu;
+  std::thread worker;
+  xtbloom_batch_t batch{};
+  xtbloom_compute_options_t options{};
+  xtbloom_batch_result_t result{};
+  xtb::ComputeRequest req;
+  void join() {
+    std::lock_guard<std::mutex> lock(join_mu);
+    if (worker.joinable()) worker.join();
+  }
+};
+
+// The immutable part of a batch that a fixed-topology plan binds
+// (docs/developer-guide/architecture.md "Fixed-topology plans"): atom
+// offsets, element numbers, molecular charges, unpaired electrons, spin
+// channels, point-charge and charge-response structure.
+struct PlanTopology {
+  int64_t nsys = 0, natoms = 0, npc = 0;
+  std::vector<int64_t> atom_off, pc_off, resp_off;
+  std::vector<int32_t> Z, uhf, nch;
+  std::vector<double> qmol;
+  bool has_nch = false, has_pc = false, has_resp = false;
+  bool operator==(const PlanTopology& o) const {
+    return nsys == o.nsys && natoms == o.natoms && npc == o.npc && atom_off == o.atom_off &&
+           pc_off == o.pc_off && resp_off == o.resp_off && Z == o.Z && uhf == o.uhf && nch == o.nch &&
+           qmol == o.qmol && has_nch == o.has_nch && has_pc == o.has_pc && has_resp == o.has_resp;
+  }
+};
+
+// The compute policy a plan binds: model, requested properties, SCC
+// tolerances, iteration limit, electronic temperature, mixer, determinism
+// (FRESH or WARM stays a per-call choice).
+struct PlanPolicy {
+  int32_t model = 0, max_iter = 0, memory = 0, determinism = 0;
+  uint32_t flags = 0;
+  double ctol = 0, etol = 0, kt = 0, damping = 0;
+  bool operator==(const PlanPolicy& o) const {
+    return model == o.model && max_iter == o.max_iter && memory == o.memory &&
+           determinism == o.determinism && flags == o.flags && ctol == o.ctol && etol == o.etol &&
+           kt == o.kt && damping == o.damping;
+  }
 };
 
 struct xtbloom_plan {
   xtbloom_context_t* context = nullptr;
-  int64_t batch_size = 0;
-  int64_t total_atoms = 0;
-  uint32_t flags = 0;
+  std::unique_ptr<xtb::Engine> engine;   // plan-owned execution cache
+  PlanTopology topo;
+  PlanPolicy policy;
 };
 
 struct xtbloom_result_owner {
@@ -460,19 +524,18 @@ xtbloom_status_t validate_and_normalise(const xtbloom_batch_t* batch,
   return XTBLOOM_STATUS_SUCCESS;
 }
 
-xtbloom_status_t run(xtbloom_context_t* ctx, const xtbloom_batch_t* batch,
-                     const xtbloom_compute_options_t* options, const xtbloom_batch_result_t* result,
-                     uint32_t* result_flags) {
-  if (ctx == nullptr) return fail(XTBLOOM_STATUS_INVALID_ARGUMENT, "context is NULL");
-  xtb::ComputeRequest req;
-  std::string err;
-  xtbloom_status_t st = validate_and_normalise(batch, options, result, req, err);
-  if (st != XTBLOOM_STATUS_SUCCESS) return fail(st, err);
+// One transaction on an engine of the context (its own or a plan's): the
+// caller holds no lock; the context's transaction lock is taken here.  The
+// caller's current device is restored.
+xtbloom_status_t execute(xtbloom_context_t* ctx, xtb::Engine* engine, const xtb::ComputeRequest& req,
+                         uint32_t* result_flags, std::string& err) {
   std::lock_guard<std::mutex> lock(ctx->mutex);
   int prev = 0;
   cudaGetDevice(&prev);
+  xtbloom_status_t st;
   try {
-    st = ctx->engine->compute(req, err);
+    engine->set_execution(ctx->precision, ctx->switch_residual, ctx->graphs);
+    st = engine->compute(req, err);
   } catch (const std::bad_alloc&) {
     st = XTBLOOM_STATUS_ALLOCATION_FAILED;
     err = "host allocation failed";
@@ -489,8 +552,159 @@ xtbloom_status_t run(xtbloom_context_t* ctx, const xtbloom_batch_t* batch,
       rf |= XTBLOOM_RESULT_FORCES_EXCLUDE_EXTERNAL_OPERATOR_DERIVATIVES;
     *result_flags = rf;
   }
+  return st;
+}
+
+xtbloom_status_t run(xtbloom_context_t* ctx, const xtbloom_batch_t* batch,
+                     const xtbloom_compute_options_t* options, const xtbloom_batch_result_t* result,
+                     uint32_t* result_flags) {
+  if (ctx == nullptr) return fail(XTBLOOM_STATUS_INVALID_ARGUMENT, "context is NULL");
+  xtb::ComputeRequest req;
+  std::string err;
+  xtbloom_status_t st = validate_and_normalise(batch, options, result, req, err);
+  if (st != XTBLOOM_STATUS_SUCCESS) return fail(st, err);
+  st = execute(ctx, ctx->engine.get(), req, result_flags, err);
   if (st != XTBLOOM_STATUS_SUCCESS) return fail(st, err);
   g_last_error.clear();
+  return XTBLOOM_STATUS_SUCCESS;
+}
+
+// Copies a caller structure of `struct_size` bytes into the library's own
+// layout (fields past the caller's size stay zero, fields past the library's
+// layout are not read).
+template <class T>
+void copy_struct(T& dst, const T* src) {
+  std::memset(static_cast<void*>(&dst), 0, sizeof(T));
+  std::memcpy(static_cast<void*>(&dst), static_cast<const void*>(src),
+              std::min<size_t>(src->struct_size, sizeof(T)));
+  dst.struct_size = static_cast<uint32_t>(std::min<size_t>(src->struct_size, sizeof(T)));
+}
+
+// Accepts a validated submission on `request`: the descriptors are copied,
+// the request turns PENDING and a worker thread runs the transaction.
+xtbloom_status_t submit(xtbloom_context_t* ctx, xtb::Engine* engine, xtbloom_request_t* r,
+                        const xtbloom_batch_t* batch, const xtbloom_compute_options_t* options,
+                        const xtbloom_batch_result_t* result, xtb::ComputeRequest&& req) {
+  {
+    std::lock_guard<std::mutex> lock(r->mu);
+    if (r->state == XTBLOOM_REQUEST_PENDING)
+      return fail(XTBLOOM_STATUS_INVALID_ARGUMENT, "request already has pending work");
+  }
+  r->join();   // the previous submission's worker has finished; reclaim it
+  copy_struct(r->batch, batch);
+  copy_struct(r->options, options);
+  copy_struct(r->result, result);
+  r->req = std::move(req);
+  r->req.batch = &r->batch;
+  r->req.options = &r->options;
+  r->req.result = &r->result;
+  {
+    std::lock_guard<std::mutex> lock(r->mu);
+    r->state = XTBLOOM_REQUEST_PENDING;
+    r->completion = XTBLOOM_STATUS_SUCCESS;
+    r->result_flags = 0;
+    r->error.clear();
+  }
+  try {
+    r->worker = std::thread([ctx, engine, r] {
+      std::string err;
+      uint32_t flags = 0;
+      const xtbloom_status_t st = execute(ctx, engine, r->req, &flags, err);
+      {
+        std::lock_guard<std::mutex> lock(r->mu);
+        r->completion = st;
+        r->result_flags = st == XTBLOOM_STATUS_SUCCESS ? flags : 0u;
+        r->error = st == XTBLOOM_STATUS_SUCCESS ? std::string() : err;
+        r->state = XTBLOOM_REQUEST_COMPLETE;
+      }
+      r->cv.notify_all();
+    });
+  } catch (...) {
+    std::lock_guard<std::mutex> lock(r->mu);
+    r->state = XTBLOOM_REQUEST_IDLE;
+    return fail(XTBLOOM_STATUS_ALLOCATION_FAILED, "failed to start the request's worker thread");
+  }
+  g_last_error.clear();
+  return XTBLOOM_STATUS_SUCCESS;
+}
+
+bool read_any(const xtbloom_const_buffer_t& b, void* dst, size_t bytes) {
+  if (bytes == 0) return true;
+  if (b.data == nullptr) return false;
+  if (b.memory_space == XTBLOOM_MEMORY_HOST) {
+    std::memcpy(dst, b.data, bytes);
+    return true;
+  }
+  return cudaMemcpy(dst, b.data, bytes, cudaMemcpyDeviceToHost) == cudaSuccess;
+}
+
+// The immutable topology of a validated batch.
+xtbloom_status_t capture_topology(const xtbloom_batch_t* b, const xtb::ComputeRequest& req,
+                                  PlanTopology& t, std::string& err) {
+  t.nsys = b->batch_size;
+  t.natoms = b->total_atoms;
+  t.npc = b->total_point_charges;
+  const size_t B = (size_t)t.nsys, N = (size_t)t.natoms;
+  t.atom_off.resize(B + 1);
+  t.Z.resize(N);
+  t.qmol.resize(B);
+  t.uhf.assign(B, 0);
+  bool ok = read_any(b->atom_offsets, t.atom_off.data(), (B + 1) * 8) &&
+            read_any(b->atomic_numbers, t.Z.data(), N * 4) &&
+            read_any(b->molecular_charges, t.qmol.data(), B * 8) &&
+            (b->unpaired_electrons.data == nullptr || read_any(b->unpaired_electrons, t.uhf.data(), B * 4));
+  t.has_nch = req.spin_channels;
+  t.nch.assign(B, 1);
+  if (ok && t.has_nch && b->spin_channels.data != nullptr) ok = read_any(b->spin_channels, t.nch.data(), B * 4);
+  t.has_pc = t.npc > 0;
+  t.pc_off.clear();
+  if (ok && t.has_pc) {
+    t.pc_off.resize(B + 1);
+    ok = read_any(b->point_charge_offsets, t.pc_off.data(), (B + 1) * 8);
+  }
+  t.has_resp = req.have_response;
+  t.resp_off = req.have_response ? req.resp_off : std::vector<int64_t>();
+  if (!ok) {
+    err = "failed to read the batch topology";
+    return XTBLOOM_STATUS_INVALID_ARGUMENT;
+  }
+  return XTBLOOM_STATUS_SUCCESS;
+}
+
+PlanPolicy capture_policy(const xtbloom_compute_options_t* o, const xtb::ComputeRequest& req) {
+  PlanPolicy p;
+  p.model = o->model;
+  p.flags = req.flags;
+  p.max_iter = req.max_iter;
+  p.ctol = req.ctol;
+  p.etol = req.etol;
+  p.kt = req.kt;
+  p.memory = req.memory;
+  p.damping = req.damping;
+  p.determinism = has_field(o->struct_size, XTBLOOM_COMPUTE_OPTIONS_V3_SIZE) ? o->determinism : 0;
+  return p;
+}
+
+// Validates a plan call: the batch and options on their own, then against
+// the plan's bound topology and policy (before any output is touched).
+xtbloom_status_t plan_request(const xtbloom_plan_t* plan, const xtbloom_batch_t* batch,
+                              const xtbloom_compute_options_t* options,
+                              const xtbloom_batch_result_t* result, xtb::ComputeRequest& req,
+                              std::string& err) {
+  xtbloom_status_t st = validate_and_normalise(batch, options, result, req, err);
+  if (st != XTBLOOM_STATUS_SUCCESS) return st;
+  PlanTopology t;
+  st = capture_topology(batch, req, t, err);
+  if (st != XTBLOOM_STATUS_SUCCESS) return st;
+  if (!(t == plan->topo)) {
+    err = "batch topology (atom offsets, elements, charges, spin, point-charge or charge-response "
+          "structure) differs from the plan";
+    return XTBLOOM_STATUS_INVALID_ARGUMENT;
+  }
+  if (!(capture_policy(options, req) == plan->policy)) {
+    err = "compute policy (model, properties, SCC settings, mixer, determinism) differs from the plan";
+    return XTBLOOM_STATUS_INVALID_ARGUMENT;
+  }
   return XTBLOOM_STATUS_SUCCESS;
 }
 
@@ -612,7 +826,10 @@ void xtbloom_context_destroy(xtbloom_context_t* context) {
   int prev = 0;
   cudaGetDevice(&prev);
   cudaSetDevice(context->device);
-  context->engine.reset();
+  {
+    std::lock_guard<std::mutex> lock(context->mutex);   // no transaction in flight
+    context->engine.reset();
+  }
   if (context->own_stream && context->stream) cudaStreamDestroy(context->stream);
   cudaSetDevice(prev);
   delete context;
@@ -636,102 +853,229 @@ xtbloom_status_t xtbloom_compute(xtbloom_context_t* context, const xtbloom_batch
 }
 
 xtbloom_status_t xtbloom_request_create(xtbloom_context_t* context, xtbloom_request_t** request) {
+  if (request != nullptr) *request = nullptr;
   if (context == nullptr || request == nullptr) return fail(XTBLOOM_STATUS_INVALID_ARGUMENT, "NULL argument");
   auto* r = new (std::nothrow) xtbloom_request;
   if (r == nullptr) return fail(XTBLOOM_STATUS_ALLOCATION_FAILED, "failed to allocate a request");
   r->context = context;
   *request = r;
+  g_last_error.clear();
   return XTBLOOM_STATUS_SUCCESS;
 }
 
-// The submission completes before enqueue returns; the request records the
-// outcome exactly as an asynchronous completion would.
+// Validation happens before admission (a rejected submission changes neither
+// the request nor any output); an accepted one returns at once with the
+// request PENDING, and its transaction runs on the context stream behind any
+// earlier one (src/api.cpp:375).
 xtbloom_status_t xtbloom_compute_enqueue(xtbloom_context_t* context, const xtbloom_batch_t* batch,
                                          const xtbloom_compute_options_t* options,
                                          const xtbloom_batch_result_t* result,
                                          xtbloom_request_t* request) {
-  if (request == nullptr || request->context != context)
-    return fail(XTBLOOM_STATUS_INVALID_ARGUMENT, "request is NULL or bound to another context");
-  if (request->state == XTBLOOM_REQUEST_PENDING)
-    return fail(XTBLOOM_STATUS_INVALID_ARGUMENT, "request already has pending work");
-  uint32_t flags = 0;
-  const xtbloom_status_t st = run(context, batch, options, result, &flags);
-  if (st == XTBLOOM_STATUS_INVALID_ARGUMENT || st == XTBLOOM_STATUS_NOT_IMPLEMENTED ||
-      st == XTBLOOM_STATUS_NOT_SUPPORTED) {
-    return st;   // rejected before acceptance
-  }
-  request->state = XTBLOOM_REQUEST_COMPLETE;
-  request->completion = st;
-  request->result_flags = flags;
-  request->error = st == XTBLOOM_STATUS_SUCCESS ? std::string() : g_last_error;
-  return XTBLOOM_STATUS_SUCCESS;
+  if (context == nullptr) return fail(XTBLOOM_STATUS_INVALID_ARGUMENT, "context is NULL");
+  if (request == nullptr) return fail(XTBLOOM_STATUS_INVALID_ARGUMENT, "request is NULL");
+  if (request->context != context)
+    return fail(XTBLOOM_STATUS_INVALID_ARGUMENT, "request was created by a different context");
+  xtb::ComputeRequest req;
+  std::string err;
+  const xtbloom_status_t st = validate_and_normalise(batch, options, result, req, err);
+  if (st != XTBLOOM_STATUS_SUCCESS) return fail(st, err);
+  return submit(context, context->engine.get(), request, batch, options, result, std::move(req));
 }
 
 xtbloom_status_t xtbloom_request_query(xtbloom_request_t* request, xtbloom_request_info_t* info) {
   if (request == nullptr || !valid_header(info, offsetof(xtbloom_request_info_t, reserved) + sizeof(uint32_t)))
     return fail(XTBLOOM_STATUS_INVALID_ARGUMENT, "invalid request or info");
+  std::lock_guard<std::mutex> lock(request->mu);
   info->state = request->state;
   info->completion_status = request->completion;
   info->result_flags = request->result_flags;
+  g_last_error.clear();
   return XTBLOOM_STATUS_SUCCESS;
 }
 
 xtbloom_status_t xtbloom_request_wait(xtbloom_request_t* request, xtbloom_request_info_t* info) {
-  return xtbloom_request_query(request, info);
-}
-
-const char* xtbloom_request_get_error(const xtbloom_request_t* request) {
-  return request == nullptr ? "" : request->error.c_str();
-}
-
-void xtbloom_request_destroy(xtbloom_request_t* request) { delete request; }
-
-xtbloom_status_t xtbloom_plan_create(xtbloom_context_t* context, const xtbloom_batch_t* batch,
-                                     const xtbloom_compute_options_t* options, xtbloom_plan_t** plan) {
-  if (context == nullptr || plan == nullptr) return fail(XTBLOOM_STATUS_INVALID_ARGUMENT, "NULL argument");
-  if (!valid_header(batch, XTBLOOM_BATCH_V1_SIZE) || !valid_header(options, XTBLOOM_COMPUTE_OPTIONS_V1_SIZE))
-    return fail(XTBLOOM_STATUS_INVALID_ARGUMENT, "invalid batch or options");
-  auto* p = new (std::nothrow) xtbloom_plan;
-  if (p == nullptr) return fail(XTBLOOM_STATUS_ALLOCATION_FAILED, "failed to allocate a plan");
-  p->context = context;
-  p->batch_size = batch->batch_size;
-  p->total_atoms = batch->total_atoms;
-  p->flags = options->flags;
-  *plan = p;
+  if (request == nullptr || !valid_header(info, offsetof(xtbloom_request_info_t, reserved) + sizeof(uint32_t)))
+    return fail(XTBLOOM_STATUS_INVALID_ARGUMENT, "invalid request or info");
+  {
+    std::unique_lock<std::mutex> lock(request->mu);
+    request->cv.wait(lock, [&] { return request->state != XTBLOOM_REQUEST_PENDING; });
+    info->state = request->state;
+    info->completion_status = request->completion;
+    info->result_flags = request->result_flags;
+  }
+  request->join();
+  g_last_error.clear();
   return XTBLOOM_STATUS_SUCCESS;
 }
 
-void xtbloom_plan_destroy(xtbloom_plan_t* plan) { delete plan; }
+const char* xtbloom_request_get_error(const xtbloom_request_t* request) {
+  if (request == nullptr) return "";
+  auto* r = const_cast<xtbloom_request_t*>(request);
+  std::lock_guard<std::mutex> lock(r->mu);
+  return r->error.c_str();
+}
 
+// A pending submission is waited for: its worker must not outlive the request.
+void xtbloom_request_destroy(xtbloom_request_t* request) {
+  if (request == nullptr) return;
+  request->join();
+  delete request;
+}
+
+// A plan binds the batch's immutable topology and the compute policy, and
+// owns its engine (its execution cache): creation validates the request and
+// runs it once (FRESH, into scratch outputs) so that every device buffer,
+// pinned staging buffer and tuned launch choice of the topology exists
+// before the first plan_compute; later plan computes of the same topology
+// allocate nothing.  The set-up run leaves no WARM checkpoint.
+// (docs/developer-guide/architecture.md "Fixed-topology plans", src/api.cpp:636-770.)
+xtbloom_status_t xtbloom_plan_create(xtbloom_context_t* context, const xtbloom_batch_t* batch,
+                                     const xtbloom_compute_options_t* options, xtbloom_plan_t** plan) {
+  if (plan == nullptr) return fail(XTBLOOM_STATUS_INVALID_ARGUMENT, "plan output pointer is NULL");
+  *plan = nullptr;
+  if (context == nullptr) return fail(XTBLOOM_STATUS_INVALID_ARGUMENT, "context is NULL");
+  if (batch == nullptr || options == nullptr)
+    return fail(XTBLOOM_STATUS_INVALID_ARGUMENT, "batch or compute options is NULL");
+  if (!valid_header(batch, XTBLOOM_BATCH_V1_SIZE) || !valid_header(options, XTBLOOM_COMPUTE_OPTIONS_V1_SIZE))
+    return fail(XTBLOOM_STATUS_INVALID_ARGUMENT,
+                "batch or compute options are too small or use an unsupported API version");
+  if (batch->batch_size <= 0 || batch->total_atoms <= 0 || batch->total_point_charges < 0)
+    return fail(XTBLOOM_STATUS_INVALID_ARGUMENT, "batch sizes must be positive");
+  const size_t B = (size_t)batch->batch_size, N = (size_t)batch->total_atoms;
+  const size_t P = (size_t)batch->total_point_charges;
+  // scratch outputs of the set-up run (device memory of the context's device)
+  int prev = 0;
+  cudaGetDevice(&prev);
+  cudaSetDevice(context->device);
+  void* scratch = nullptr;
+  const size_t bytes = B * 8 + N * 24 + N * 8 + P * 24 + B * 24 + B * 4 + B + B * 4 + 64;
+  if (cudaMalloc(&scratch, bytes) != cudaSuccess) {
+    cudaGetLastError();
+    cudaSetDevice(prev);
+    return fail(XTBLOOM_STATUS_ALLOCATION_FAILED, "failed to allocate the plan's set-up outputs");
+  }
+  cudaSetDevice(prev);
+  struct Free {
+    void* p;
+    int dev;
+    ~Free() {
+      int d = 0;
+      cudaGetDevice(&d);
+      cudaSetDevice(dev);
+      cudaFree(p);
+      cudaSetDevice(d);
+    }
+  } free_scratch{scratch, context->device};
+  char* q = static_cast<char*>(scratch);
+  xtbloom_batch_result_t res;
+  xtbloom_batch_result_init(&res, sizeof(res));
+  auto out = [&](xtbloom_buffer_t& b, size_t n) {
+    b.data = n ? q : nullptr;
+    b.size_bytes = n;
+    b.memory_space = XTBLOOM_MEMORY_CUDA_DEVICE;
+    q += (n + 7) & ~size_t(7);
+  };
+  const uint32_t f = options->flags;
+  out(res.energies, (f & XTBLOOM_COMPUTE_ENERGY) ? B * 8 : 0);
+  out(res.forces, (f & XTBLOOM_COMPUTE_FORCES) ? N * 24 : 0);
+  out(res.atomic_charges, (f & XTBLOOM_COMPUTE_ATOMIC_CHARGES) ? N * 8 : 0);
+  out(res.point_charge_forces, (f & XTBLOOM_COMPUTE_POINT_CHARGE_FORCES) ? P * 24 : 0);
+  out(res.dipole_moments, (f & XTBLOOM_COMPUTE_DIPOLE_MOMENTS) ? B * 24 : 0);
+  out(res.scc_iterations, B * 4);
+  out(res.scc_converged, B);
+  out(res.per_system_status, B * 4);
+  xtb::ComputeRequest req;
+  std::string err;
+  xtbloom_status_t st = validate_and_normalise(batch, options, &res, req, err);
+  if (st != XTBLOOM_STATUS_SUCCESS) return fail(st, err);
+  req.warm = false;   // the set-up run starts FRESH whatever the options say
+  std::unique_ptr<xtbloom_plan_t> p(new (std::nothrow) xtbloom_plan);
+  if (!p) return fail(XTBLOOM_STATUS_ALLOCATION_FAILED, "failed to allocate a plan");
+  p->context = context;
+  st = capture_topology(batch, req, p->topo, err);
+  if (st != XTBLOOM_STATUS_SUCCESS) return fail(st, err);
+  p->policy = capture_policy(options, req);
+  try {
+    cudaSetDevice(context->device);
+    p->engine.reset(new xtb::Engine(context->device, context->stream));
+    cudaSetDevice(prev);
+  } catch (...) {
+    cudaSetDevice(prev);
+    return fail(XTBLOOM_STATUS_ALLOCATION_FAILED, "failed to create the plan's engine");
+  }
+  st = execute(context, p->engine.get(), req, nullptr, err);
+  if (st != XTBLOOM_STATUS_SUCCESS) return fail(st, err);
+  p->engine->invalidate_checkpoint();
+  *plan = p.release();
+  g_last_error.clear();
+  return XTBLOOM_STATUS_SUCCESS;
+}
+
+void xtbloom_plan_destroy(xtbloom_plan_t* plan) {
+  if (plan == nullptr) return;
+  if (plan->context != nullptr) {
+    std::lock_guard<std::mutex> lock(plan->context->mutex);   // no transaction of it in flight
+    int prev = 0;
+    cudaGetDevice(&prev);
+    cudaSetDevice(plan->context->device);
+    plan->engine.reset();
+    cudaSetDevice(prev);
+  }
+  delete plan;
+}
+
+// The bytes the plan keeps alive for its property set: device buffers of its
+// engine and its pinned host staging (graph and stream handles are opaque
+// and not counted, as in the reference).
 xtbloom_status_t xtbloom_plan_query_workspace(const xtbloom_plan_t* plan, xtbloom_workspace_query_t* q) {
-  if (plan == nullptr || q == nullptr) return fail(XTBLOOM_STATUS_INVALID_ARGUMENT, "NULL argument");
-  if (q->compute_flags != plan->flags)
+  if (plan == nullptr) return fail(XTBLOOM_STATUS_INVALID_ARGUMENT, "plan is NULL");
+  if (!valid_header(q, offsetof(xtbloom_workspace_query_t, reserved_v2) + sizeof(uint32_t)))
+    return fail(XTBLOOM_STATUS_INVALID_ARGUMENT,
+                "workspace query is NULL, too small, or uses an unsupported API version");
+  if (q->compute_flags != plan->policy.flags)
     return fail(XTBLOOM_STATUS_INVALID_ARGUMENT, "compute_flags must equal the plan's flags");
-  // device workspace is dominated by about 20 packed n x n FP64 matrices
-  q->host_required_bytes = 0;
-  q->host_required_alignment = 1;
-  q->device_required_bytes = 0;
+  std::lock_guard<std::mutex> lock(plan->context->mutex);
+  q->host_required_bytes = plan->engine->host_bytes();
+  q->host_required_alignment = 64;
+  q->device_required_bytes = plan->engine->device_bytes();
   q->device_required_alignment = 256;
+  g_last_error.clear();
   return XTBLOOM_STATUS_SUCCESS;
 }
 
 xtbloom_status_t xtbloom_plan_compute(xtbloom_plan_t* plan, const xtbloom_batch_t* batch,
                                       const xtbloom_compute_options_t* options,
                                       xtbloom_batch_result_t* result) {
-  if (plan == nullptr) return fail(XTBLOOM_STATUS_INVALID_ARGUMENT, "plan is NULL");
-  if (batch == nullptr || batch->batch_size != plan->batch_size || batch->total_atoms != plan->total_atoms)
-    return fail(XTBLOOM_STATUS_INVALID_ARGUMENT, "batch topology differs from the plan");
-  return xtbloom_compute(plan->context, batch, options, result);
+  if (plan == nullptr || !plan->engine) return fail(XTBLOOM_STATUS_INVALID_ARGUMENT, "plan is NULL");
+  if (batch == nullptr || options == nullptr || result == nullptr)
+    return fail(XTBLOOM_STATUS_INVALID_ARGUMENT, "batch, compute options, or batch result is NULL");
+  xtb::ComputeRequest req;
+  std::string err;
+  xtbloom_status_t st = plan_request(plan, batch, options, result, req, err);
+  if (st != XTBLOOM_STATUS_SUCCESS) return fail(st, err);
+  uint32_t flags = 0;
+  st = execute(plan->context, plan->engine.get(), req, &flags, err);
+  if (st != XTBLOOM_STATUS_SUCCESS) return fail(st, err);
+  result->flags = flags;
+  g_last_error.clear();
+  return XTBLOOM_STATUS_SUCCESS;
 }
 
 xtbloom_status_t xtbloom_plan_compute_enqueue(xtbloom_plan_t* plan, const xtbloom_batch_t* batch,
                                               const xtbloom_compute_options_t* options,
                                               const xtbloom_batch_result_t* result,
                                               xtbloom_request_t* request) {
-  if (plan == nullptr) return fail(XTBLOOM_STATUS_INVALID_ARGUMENT, "plan is NULL");
-  if (batch == nullptr || batch->batch_size != plan->batch_size || batch->total_atoms != plan->total_atoms)
-    return fail(XTBLOOM_STATUS_INVALID_ARGUMENT, "batch topology differs from the plan");
-  return xtbloom_compute_enqueue(plan->context, batch, options, result, request);
+  if (plan == nullptr || !plan->engine) return fail(XTBLOOM_STATUS_INVALID_ARGUMENT, "plan is NULL");
+  if (request == nullptr) return fail(XTBLOOM_STATUS_INVALID_ARGUMENT, "request is NULL");
+  if (request->context != plan->context)
+    return fail(XTBLOOM_STATUS_INVALID_ARGUMENT, "request and plan were created by different contexts");
+  if (batch == nullptr || options == nullptr || result == nullptr)
+    return fail(XTBLOOM_STATUS_INVALID_ARGUMENT, "batch, compute options, or batch result is NULL");
+  xtb::ComputeRequest req;
+  std::string err;
+  const xtbloom_status_t st = plan_request(plan, batch, options, result, req, err);
+  if (st != XTBLOOM_STATUS_SUCCESS) return fail(st, err);
+  return submit(plan->context, plan->engine.get(), request, batch, options, result, std::move(req));
 }
 
 xtbloom_status_t xtbloom_result_owner_options_init(xtbloom_result_owner_options_t* o, size_t size) {
@@ -973,8 +1317,10 @@ xtbloom_status_t xtbloom_b200_context_set_execution(xtbloom_context_t* context, 
     return fail(XTBLOOM_STATUS_INVALID_ARGUMENT, "switch_residual must be finite and >= 0");
   std::lock_guard<std::mutex> lock(context->mutex);
   if (!context->engine) return fail(XTBLOOM_STATUS_BACKEND_UNAVAILABLE, "not a CUDA context");
-  context->engine->set_execution(precision, switch_residual > 0.0 ? switch_residual : 1e-5,
-                                 capture_graphs != 0);
+  context->precision = precision;
+  context->switch_residual = switch_residual > 0.0 ? switch_residual : 1e-5;
+  context->graphs = capture_graphs != 0;
+  context->engine->set_execution(context->precision, context->switch_residual, context->graphs);
   return XTBLOOM_STATUS_SUCCESS;
 }
 

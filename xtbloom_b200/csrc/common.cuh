@@ -190,6 +190,26 @@ __device__ __forceinline__ double block_max(double v, double* scratch) {
   return scratch[32];
 }
 
+// Gradient accumulators (dE/dR, dE/dCN and the shared-memory partial sums of
+// the force kernels) are 64-bit two's-complement fixed point with 2^-40
+// units: every contribution is rounded once to the grid, and the integer
+// atomic adds that sum them are associative, so the result does not depend
+// on the order in which threads arrive: forces are bitwise reproducible
+// from run to run.  The grid (9.1e-13) and range (|sum| < 2^23) are far
+// below and above what a gradient needs.
+constexpr double kFixOne = 1099511627776.0;   // 2^40
+__device__ __forceinline__ void fix_add(double* acc, double v) {
+  atomicAdd(reinterpret_cast<unsigned long long*>(acc),
+            static_cast<unsigned long long>(__double2ll_rn(v * kFixOne)));
+}
+// Adds one fixed-point accumulator (a partial sum) to another.
+__device__ __forceinline__ void fix_merge(double* acc, const double& part) {
+  atomicAdd(reinterpret_cast<unsigned long long*>(acc), *reinterpret_cast<const unsigned long long*>(&part));
+}
+__device__ __forceinline__ double fix_value(const double& acc) {
+  return static_cast<double>(*reinterpret_cast<const long long*>(&acc)) * (1.0 / kFixOne);
+}
+
 // Per-system status codes mirror the public per_system_status values.
 enum SysStatus : int32_t { kOk = 0, kNotConverged = 7, kEigenFailed = 8, kInternal = 6 };
 

@@ -31,6 +31,10 @@ constexpr double kEvToHartree = 1.0 / 27.21138505;
 constexpr double kAngstromToBohr = 1.8897261246204404;
 constexpr double kPiH = 3.141592653589793238462643383279502884;
 
+// Device bytes held by the engine whose method runs on this thread (the
+// workspace a fixed-topology plan reports).
+thread_local int64_t* t_ledger = nullptr;
+
 struct Dbuf {
   void* p = nullptr;
   size_t bytes = 0;
@@ -40,11 +44,13 @@ struct Dbuf {
   bool reserve(size_t nbytes) {
     if (nbytes <= bytes && p) return true;
     if (p) cudaFree(p);
+    if (t_ledger) *t_ledger -= (int64_t)bytes;
     p = nullptr;
     bytes = 0;
     const size_t want = std::max<size_t>(nbytes, 256);
     if (cudaMalloc(&p, want) != cudaSuccess) return false;
     bytes = want;
+    if (t_ledger) *t_ledger += (int64_t)bytes;
     return true;
   }
   template <class T>
@@ -148,12 +154,12 @@ ModelConstants make_constants() {
 enum Stage : int {
   kStSetup, kStLowdin, kStPotential, kStFock, kStTransform, kStTridiag, kStEigvals, kStInvIter,
   kStBacktransform, kStDensity, kStMulliken, kStEnergyMixer, kStCompact, kStForcePairs,
-  kStClassical, kStCnChain, kStPublish, kStageCount
+  kStClassical, kStCnChain, kStPublish, kStRefine, kStageCount
 };
 [[maybe_unused]] const char* kStageNames[kStageCount] = {
     "setup_integrals", "lowdin", "potential", "fock", "gemm_transform", "tridiag", "eigvals",
     "inverse_iteration", "backtransform", "gemm_density", "mulliken", "energy_mixer", "compact",
-    "force_pairs", "classical", "cn_chain", "publish"};
+    "force_pairs", "classical", "cn_chain", "publish", "refine"};
 
 struct Profiler {
   bool on = false;
@@ -240,6 +246,7 @@ struct Engine::Impl {
   // FP64 GEMM tile width chosen by measurement per (product kind, orbital-count
   // bucket of 32, power-of-two class of the system count)
   std::map<uint64_t, int> gemm_width;
+  int forced_gemm_width = 0;   // 32 or 64: no timing, every FP64 product at that width
   // side streams for the size buckets of the eigensolver, which run
   // concurrently (small systems fill the SMs that large ones leave free)
   static constexpr int kBucketStreams = 8;
@@ -272,12 +279,33 @@ struct Engine::Impl {
   int64_t h_list_cap = 0;
   int last_memory = 0;
   bool have_results = false;
+  int64_t ledger = 0;          // device bytes of every Dbuf above
   bool trace = false;
   bool tridiag_smem = false;   // use the shared-memory tridiagonalisation for every size
   bool mixed = false;          // split-precision GEMMs until the precision switch
   double prec_switch = 1e-5;
   bool graphs = false;
-  Dbuf prec, split_iters;
+  Dbuf prec, split_iters, gate_hits, last_rms;
+  // warm-started refinement of the SCC eigenvectors (k_refine.cu): the
+  // eigenvector columns V and the product buffer of a step per channel, and
+  // the per-channel phases and masks that route channels between the
+  // refinement and the Householder path
+  Dbuf Vw, Vt, wstate, wphase, m_step, m_apply, m_cold, m_warm, w_emax, w_fail, w_arrive, w_bounds,
+      w_stats;
+  // refinement steps per SCC iteration; 0 (the default) = the Householder path
+  // in every iteration.  The warm-started refinement is an opt-in
+  // (XTBLOOM_B200_REFINE_STEPS): on the hetero-alkane workload too many
+  // channels fall back to the Householder path (near-degenerate levels inside
+  // the occupied and virtual blocks keep the block bounds loose) for it to
+  // pay (1356 vs 1037 ms per 4096-system step, both FP64, same results).
+  int refine_steps = 0;
+  int refine_from = 1;       // first SCC iteration that refines
+  // max |E| that ends a channel's refinement: split-precision iterations,
+  // FP64 iterations, FP64 iterations once the residual is below
+  // refine_final_factor x the charge tolerance (the result must then be as
+  // exact as a direct solve: the gate compares energies to 1e-8 Eh or less)
+  double refine_theta_split = 1e-5, refine_theta = 1e-7, refine_theta_final = 1e-11;
+  double refine_final_factor = 100.0;
   // strict WARM start: the converged state of the latest fully converged call
   // and that call's identity (topology, charges, spin, point-charge layout,
   // requested properties and SCC settings)
@@ -384,6 +412,15 @@ Engine::Engine(int device, cudaStream_t stream) : impl_(new Impl), device_(devic
   impl_->trace = tr != nullptr && tr[0] == '1';
   const char* td = std::getenv("XTBLOOM_B200_TRIDIAG");
   impl_->tridiag_smem = td != nullptr && std::strcmp(td, "smem") == 0;
+  // XTBLOOM_B200_GEMM_WIDTH=32|64 fixes the FP64 tile width of every product
+  // instead of timing both (a check that the widths form identical elements).
+  // XTBLOOM_B200_REFINE_STEPS=k: refinement steps per SCC iteration (k > 0
+  // turns the warm-started eigensolver on; 0 keeps the Householder path).
+  const char* rs = std::getenv("XTBLOOM_B200_REFINE_STEPS");
+  if (rs != nullptr && rs[0] >= '0' && rs[0] <= '9') impl_->refine_steps = std::min(8, std::atoi(rs));
+  const char* gw = std::getenv("XTBLOOM_B200_GEMM_WIDTH");
+  if (gw != nullptr && (std::strcmp(gw, "32") == 0 || std::strcmp(gw, "64") == 0))
+    impl_->forced_gemm_width = std::atoi(gw);
 }
 
 void Engine::set_execution(int precision, double switch_residual, bool graphs) {
@@ -699,12 +736,18 @@ xtbloom_status_t build_topology(Engine::Impl& m, const HostBatch& hb, cudaStream
        m.count.reserve(16) && m.status.reserve((size_t)B * 4) && m.iterations.reserve((size_t)B * 4) &&
        m.converged.reserve((size_t)B) && m.prec.reserve((size_t)B) &&
        m.fdone.reserve((size_t)B) &&
-       m.split_iters.reserve((size_t)B * 4) && m.nvec.reserve((size_t)NC * 4) && m.cn.reserve(N * d8) &&
+       m.split_iters.reserve((size_t)B * 4) && m.gate_hits.reserve((size_t)B * 4) && m.last_rms.reserve((size_t)B * 8) && m.nvec.reserve((size_t)NC * 4) && m.cn.reserve(N * d8) &&
        m.cn_d4.reserve(N * d8) && m.mrad.reserve(N * d8) && m.dmrad.reserve(N * d8) &&
        m.gam.reserve((size_t)m.total_gam * d8) && m.S.reserve(mat) && m.D.reserve(3 * mat) &&
        m.Q.reserve(6 * mat) && m.H0.reserve(mat) && m.H.reserve(cmat) && m.X.reserve(mat) &&
        m.T.reserve(cmat) && m.A.reserve(cmat) && m.Zv.reserve(cmat) && m.C.reserve(cmat) &&
-       m.P.reserve(cmat) && m.W.reserve(cmat) && m.d.reserve(cvec) && m.e.reserve(cvec) &&
+       m.P.reserve(cmat) && m.W.reserve(cmat) && m.Vw.reserve(cmat) && m.Vt.reserve(cmat) &&
+       m.wstate.reserve((size_t)NC) && m.wphase.reserve((size_t)NC) && m.m_step.reserve((size_t)NC) &&
+       m.m_apply.reserve((size_t)NC) && m.m_cold.reserve((size_t)NC) && m.m_warm.reserve((size_t)NC) &&
+       m.w_emax.reserve((size_t)NC * 8) && m.w_fail.reserve((size_t)NC * 4) &&
+       m.w_arrive.reserve((size_t)NC * 4) && m.w_stats.reserve(256 * 8 * 4) &&
+       m.w_bounds.reserve((size_t)NC * kRefineMaxParts * 9 * d8) &&
+       m.d.reserve(cvec) && m.e.reserve(cvec) &&
        m.tau.reserve(cvec) && m.eig.reserve(cvec) && m.occ.reserve(cvec) &&
        m.occ_eps.reserve(cvec) && m.entropy.reserve(NC * d8) &&
        m.scratch.reserve((size_t)(m.total_scr + m.chan_scr) * d8) && m.qsh.reserve(shell * d8) &&
@@ -761,7 +804,7 @@ __global__ void k_publish(DevTopo t, const int32_t* status, const double* free_e
     for (int sh = t.atom_sh[a]; sh < t.atom_sh[a + 1]; ++sh) q += qsh[sh];
     charges[a] = ok ? q : nan;
     for (int c = 0; c < 3; ++c) {
-      forces[3 * a + c] = ok ? -grad[3 * a + c] + (ef != nullptr ? q * ef[c] : 0.0) : nan;
+      forces[3 * a + c] = ok ? -fix_value(grad[3 * a + c]) + (ef != nullptr ? q * ef[c] : 0.0) : nan;
       mu[c] += q * t.pos[3 * a + c] + dip[3 * a + c];
     }
   }
@@ -884,8 +927,23 @@ __global__ void k_list_ready(const int32_t* order, int nsys, const int32_t* stat
 
 }  // namespace
 
+void Engine::invalidate_checkpoint() { impl_->ck_valid = false; }
+
+size_t Engine::device_bytes() const { return (size_t)std::max<int64_t>(0, impl_->ledger); }
+
+size_t Engine::host_bytes() const {
+  return 4 * sizeof(int32_t) + (size_t)impl_->h_list_cap * sizeof(int32_t) +
+         (size_t)impl_->h_clist_cap * sizeof(int32_t);
+}
+
 xtbloom_status_t Engine::compute(const ComputeRequest& req, std::string& error) {
   Impl& m = *impl_;
+  // every device buffer this call grows is counted in the engine's ledger
+  struct LedgerScope {
+    int64_t* prev;
+    explicit LedgerScope(int64_t* l) : prev(t_ledger) { t_ledger = l; }
+    ~LedgerScope() { t_ledger = prev; }
+  } ledger_scope(&m.ledger);
   cudaStream_t s = stream_;
   cudaSetDevice(device_);
   const auto t_start = std::chrono::steady_clock::now();
@@ -1072,6 +1130,11 @@ xtbloom_status_t Engine::compute(const ComputeRequest& req, std::string& error) 
   cudaMemsetAsync(m.pot_acc.p, 0, 10 * N * 8, s);
   cudaMemsetAsync(m.prec.p, m.mixed ? 0 : 1, B, s);
   cudaMemsetAsync(m.split_iters.p, 0, B * 4, s);
+  cudaMemsetAsync(m.gate_hits.p, 0, B * 4, s);
+  cudaMemsetAsync(m.last_rms.p, 0x7f, B * 8, s);   // 1.4e306: no residual yet
+  // no channel has eigenvectors to refine from yet
+  cudaMemsetAsync(m.wstate.p, 0, (size_t)m.nchan, s);
+  cudaMemsetAsync(m.w_stats.p, 0, 256 * 8 * 4, s);
   cudaMemsetAsync(m.fdone.p, 0, B, s);
   cudaMemsetAsync(m.grad.p, 0, 3 * N * 8, s);
   cudaMemsetAsync(m.acn.p, 0, N * 8, s);
@@ -1131,9 +1194,11 @@ xtbloom_status_t Engine::compute(const ComputeRequest& req, std::string& error) 
   auto gemm = [&](const int32_t* glist, const double* A, const int64_t* offA, const double* Bm,
                   const int64_t* offB, double* C, const int32_t* dm, const int32_t* dn,
                   const int32_t* dk, bool ta, const double* w, int count, bool sym = false,
-                  const uint8_t* prec = nullptr, cudaStream_t st = nullptr) {
+                  const uint8_t* prec = nullptr, cudaStream_t st = nullptr,
+                  const uint8_t* only = nullptr) {
     GemmArgs g{};
     g.sym = sym ? 1 : 0;
+    g.only = only;
     g.prec = prec;
     g.prec_of = m.ch_sys.as<int32_t>();
     g.list = glist;
@@ -1156,7 +1221,9 @@ xtbloom_status_t Engine::compute(const ComputeRequest& req, std::string& error) 
     // iteration runs both widths twice, timed by events, and the faster one
     // is kept for this context; captured iterations only reuse choices.
     int width = 0;
-    if (prec == nullptr && count > 0) {
+    if (prec == nullptr && m.forced_gemm_width != 0) {
+      width = m.forced_gemm_width;
+    } else if (prec == nullptr && count > 0) {
       const int lg = 31 - __builtin_clz((unsigned)count);
       const int32_t* nv = m.nvec.as<int32_t>();
       const uint64_t key = ((uint64_t)((m.max_n + 31) / 32) << 32) | ((uint64_t)lg << 8) |
@@ -1221,12 +1288,17 @@ xtbloom_status_t Engine::compute(const ComputeRequest& req, std::string& error) 
   };
   // tridiagonalise, eigenvalues (+ occupations), eigenvectors, back-transform
   // over the entries of dl (device) / hl (its host copy), systems or channels
+  // mode 0: SCC, the occupied vectors; 1: all vectors, no occupations
+  // (overlap); 2: SCC, all vectors (they seed the warm-started refinement).
+  // only: per-channel mask of the entries to solve (NULL: every entry).
   auto eigensolve = [&](const int32_t* dl, const int32_t* hl, int count, int mode, double kt,
-                        double ortol_rel, int stage_base) {
+                        double ortol_rel, int stage_base, const uint8_t* only = nullptr) {
     const std::vector<Bucket> bks = buckets(hl, count);
     auto sub = [&](const Bucket& bk) {
       EigArgs gb = eg;
       gb.list = dl + bk.start;
+      gb.only = only;
+      gb.all_vectors = mode != 0 ? 1 : 0;
       return gb;
     };
     auto tridiag = [&](const Bucket& bk, cudaStream_t st) {
@@ -1243,11 +1315,11 @@ xtbloom_status_t Engine::compute(const ComputeRequest& req, std::string& error) 
     };
     auto invit = [&](const Bucket& bk, cudaStream_t st) {
       launch_inverse_iteration(sub(bk), bk.count, bk.max_n,
-                               mode == 1 ? bk.max_n : std::min(bk.max_m + 4, bk.max_n), ortol_rel, st);
+                               mode != 0 ? bk.max_n : std::min(bk.max_m + 4, bk.max_n), ortol_rel, st);
     };
     auto backtransform = [&](const Bucket& bk, cudaStream_t st) {
       const EigArgs gb = sub(bk);
-      const int want = mode == 1 ? bk.max_n : std::min(bk.max_m, bk.max_n);
+      const int want = mode != 0 ? bk.max_n : std::min(bk.max_m, bk.max_n);
       const long budget = 220L * 1024 / 8 - (long)bk.max_n * 33 - 32 * 33 - 8;
       const int wcap = (int)std::min<long>(want, budget / 32);
       if (wcap >= 8) {
@@ -1341,6 +1413,8 @@ xtbloom_status_t Engine::compute(const ComputeRequest& req, std::string& error) 
   a.prec = m.mixed ? m.prec.as<uint8_t>() : nullptr;
   a.prec_switch = m.prec_switch;
   a.split_iters = m.split_iters.as<int32_t>();
+  a.gate_hits = m.mixed ? m.gate_hits.as<int32_t>() : nullptr;
+  a.last_rms = m.last_rms.as<double>();
   const uint8_t* sprec = a.prec;   // split-precision selector of the SCC GEMMs
   a.qmag = m.qmag.as<double>();
   a.vmag = m.vmag.as<double>();
@@ -1428,6 +1502,59 @@ xtbloom_status_t Engine::compute(const ComputeRequest& req, std::string& error) 
   fbase.atm_dc6 = m.A.as<double>();
   fbase.work = m.scratch.as<double>();
   fbase.work_off = m.ch_scr.as<int64_t>();
+  // Warm-started eigensolver state (k_refine.cu)
+  const bool refine = m.refine_steps > 0;
+  uint8_t* m_step = m.m_step.as<uint8_t>();
+  uint8_t* m_apply = m.m_apply.as<uint8_t>();
+  uint8_t* m_cold = m.m_cold.as<uint8_t>();
+  uint8_t* m_warm = m.m_warm.as<uint8_t>();
+  RefineArgs rbase{};
+  rbase.nao = dch_nao;
+  rbase.mat_off = dch_mat;
+  rbase.ao_off = dch_ao;
+  rbase.ch_sys = m.ch_sys.as<int32_t>();
+  rbase.nel_a = m.ch_nel_a.as<double>();
+  rbase.nel_b = m.ch_nel_b.as<double>();
+  rbase.kt = req.kt;
+  rbase.occ = m.occ.as<double>();
+  rbase.occ_eps = m.occ_eps.as<double>();
+  rbase.nvec = m.nvec.as<int32_t>();
+  rbase.entropy = m.entropy.as<double>();
+  rbase.bounds = m.w_bounds.as<double>();
+  rbase.Sm = m.W.as<double>();
+  rbase.G = m.C.as<double>();
+  rbase.Ep = m.P.as<double>();
+  rbase.V = m.Vw.as<double>();
+  rbase.Vt = m.Vt.as<double>();
+  rbase.Zrows = m.Zv.as<double>();
+  rbase.eig = m.eig.as<double>();
+  rbase.wstate = m.wstate.as<uint8_t>();
+  rbase.phase = m.wphase.as<uint8_t>();
+  rbase.m_step = m_step;
+  rbase.m_apply = m_apply;
+  rbase.m_cold = m_cold;
+  rbase.m_warm = m_warm;
+  rbase.emax = m.w_emax.as<unsigned long long>();
+  rbase.fail = m.w_fail.as<int32_t>();
+  rbase.arrive = m.w_arrive.as<int32_t>();
+  rbase.stats = m.w_stats.as<int32_t>();
+  rbase.iterations = m.iterations.as<int32_t>();
+  rbase.prec = sprec;
+  rbase.warm_from = m.refine_from;
+  rbase.theta = m.refine_theta;
+  rbase.theta_split = m.refine_theta_split;
+  rbase.theta_final = m.refine_theta_final;
+  rbase.final_rms = m.refine_final_factor * req.ctol;
+  rbase.last_rms = m.last_rms.as<double>();
+  // CTAs per channel of the correction kernel: one with many channels, up to
+  // 16 when few are left (the non-converging tail), where it is on the
+  // critical path
+  auto refine_parts = [&](int cnt) {
+    const int sms = sm_count();
+    if (cnt >= sms) return 1;
+    return std::max(1, std::min(16, (2 * sms) / std::max(cnt, 1)));
+  };
+
   // Every kernel here reads and writes only the listed systems' slices.
   auto force_terms = [&](const int32_t* flist, int fcount, cudaStream_t st) {
     if (fcount <= 0) return;
@@ -1444,6 +1571,19 @@ xtbloom_status_t Engine::compute(const ComputeRequest& req, std::string& error) 
         channels(st);
         cudaStreamSynchronize(st);
         fcc = channel_count();
+      } else if (refine) {
+        cudaMemcpyAsync(m.h_list, flist, (size_t)fcount * sizeof(int32_t), cudaMemcpyDeviceToHost, st);
+        cudaStreamSynchronize(st);
+      }
+      if (refine) {
+        // The energy-weighted density needs the eigenpairs of the last
+        // iteration; a channel that ended refined has its occupied subspace
+        // but not the individual levels, so its matrix A (kept) is solved
+        // once more on the Householder path, and C formed from those vectors.
+        eigensolve(clist, h_cl, fcc, 0, req.kt, 2e-7, kStTridiag, m_warm);
+        XTB_STAGE_ON(st, kStDensity, 1,
+                     gemm(clist, m.Zv.as<double>(), dch_mat, m.X.as<double>(), dch_xoff, m.C.as<double>(),
+                          dnvec, dnao, dnao, false, nullptr, fcc, false, nullptr, st, m_warm));
       }
       XTB_STAGE_ON(st, kStForcePairs, 3,
                    launch_potential(af, af.qsh, af.dip, af.qp, m.max_atoms, m.max_shells, st);
@@ -1472,10 +1612,41 @@ xtbloom_status_t Engine::compute(const ComputeRequest& req, std::string& error) 
                    dnao, dnao, dnao, false, nullptr, a.ccount, false, sprec);
               gemm(clist, m.X.as<double>(), dch_xoff, m.T.as<double>(), dch_mat, m.A.as<double>(),
                    dnao, dnao, dnao, false, nullptr, a.ccount, true, sprec));
-    eigensolve(clist, h_cl, a.ccount, 0, req.kt, 2e-7, kStTridiag);
+    if (refine) {
+      // Warm-started refinement first (it reads A, which the Householder path
+      // then overwrites for the channels it solves); U = A V goes to T, the
+      // products V^T U and V^T V to W and C, the correction I + E to P and
+      // V (I + E) to Vt: all free at this point of the iteration.
+      RefineArgs ra = rbase;
+      ra.list = clist;
+      ra.count = a.ccount;
+      XTB_STAGE(kStRefine, 1, launch_warm_begin(ra, s));
+      for (int k = 0; k < m.refine_steps; ++k) {
+        ra.step = k;
+        XTB_STAGE(kStRefine, 6,
+                  gemm(clist, m.A.as<double>(), dch_mat, m.Vw.as<double>(), dch_mat, m.T.as<double>(),
+                       dnao, dnao, dnao, false, nullptr, a.ccount, false, sprec, s, m_step);
+                  gemm(clist, m.Vw.as<double>(), dch_mat, m.T.as<double>(), dch_mat, m.W.as<double>(),
+                       dnao, dnao, dnao, true, nullptr, a.ccount, true, sprec, s, m_step);
+                  gemm(clist, m.Vw.as<double>(), dch_mat, m.Vw.as<double>(), dch_mat, m.C.as<double>(),
+                       dnao, dnao, dnao, true, nullptr, a.ccount, true, sprec, s, m_step);
+                  launch_refine_update(ra, m.max_n, refine_parts(a.ccount), s);
+                  gemm(clist, m.Vw.as<double>(), dch_mat, m.P.as<double>(), dch_mat, m.Vt.as<double>(),
+                       dnao, dnao, dnao, false, nullptr, a.ccount, false, sprec, s, m_apply);
+                  launch_refine_apply(ra, m.max_n, k + 1 == m.refine_steps, s));
+      }
+      eigensolve(clist, h_cl, a.ccount, 2, req.kt, 2e-7, kStTridiag, m_cold);
+      XTB_STAGE(kStRefine, 1, launch_vectors_from_rows(ra, m.max_n, s));
+    } else {
+      eigensolve(clist, h_cl, a.ccount, 0, req.kt, 2e-7, kStTridiag);
+    }
     XTB_STAGE(kStDensity, 2,
-              gemm(clist, m.Zv.as<double>(), dch_mat, m.X.as<double>(), dch_xoff, m.C.as<double>(),
-                   dnvec, dnao, dnao, false, nullptr, a.ccount, false, sprec);
+              if (refine)
+                gemm(clist, m.Vw.as<double>(), dch_mat, m.X.as<double>(), dch_xoff, m.C.as<double>(),
+                     dnvec, dnao, dnao, true, nullptr, a.ccount, false, sprec);
+              else
+                gemm(clist, m.Zv.as<double>(), dch_mat, m.X.as<double>(), dch_xoff, m.C.as<double>(),
+                     dnvec, dnao, dnao, false, nullptr, a.ccount, false, sprec);
               gemm(clist, m.C.as<double>(), dch_mat, m.C.as<double>(), dch_mat, m.P.as<double>(),
                    dnao, dnao, dnvec, true, m.occ.as<double>(), a.ccount, true, sprec);
               combine(m.P.as<double>(), m.Pm.as<double>(), a.count, s));
@@ -1681,6 +1852,24 @@ xtbloom_status_t Engine::debug_fetch(const std::string& name, int64_t system, do
     *count = (size_t)m.nsys;
     return XTBLOOM_STATUS_SUCCESS;
   }
+  if (name == "refine_stats" && system == -1) {
+    // per SCC iteration (256 rows of 8): channels that refined, finished at
+    // step 1, 2, 3 or later, failed, unfinished (went to the Householder path)
+    if (capacity < 256 * 8) {
+      error = "capacity too small";
+      return XTBLOOM_STATUS_INVALID_ARGUMENT;
+    }
+    cudaSetDevice(device_);
+    std::vector<int32_t> v(256 * 8, 0);
+    if (m.w_stats.p != nullptr &&
+        cudaMemcpy(v.data(), m.w_stats.p, v.size() * 4, cudaMemcpyDeviceToHost) != cudaSuccess) {
+      error = "device read failed";
+      return XTBLOOM_STATUS_INTERNAL_ERROR;
+    }
+    for (size_t i = 0; i < v.size(); ++i) out[i] = (double)v[i];
+    *count = v.size();
+    return XTBLOOM_STATUS_SUCCESS;
+  }
   if (name == "point_charge_dq" && system == -1) {
     // the whole batch: dE/dQ for every point charge of the most recent call
     if (!m.have_results || !m.have_pc) {
@@ -1738,7 +1927,15 @@ xtbloom_status_t Engine::debug_fetch(const std::string& name, int64_t system, do
     }
   }
   else if (name == "energy_terms") { src = m.terms.as<double>() + kTermCount * system; len = kTermCount; }
-  else if (name == "gradient") { src = m.grad.as<double>() + 3 * a0; len = 3 * na; }
+  else if (name == "gradient") {
+    // fixed-point accumulator (2^-40 units) to values
+    if (capacity < 3 * (size_t)na) { error = "capacity too small"; return XTBLOOM_STATUS_INVALID_ARGUMENT; }
+    std::vector<long long> raw(3 * na);
+    cudaMemcpy(raw.data(), m.grad.as<double>() + 3 * a0, 3 * na * 8, cudaMemcpyDeviceToHost);
+    for (int64_t k = 0; k < 3 * na; ++k) out[k] = (double)raw[k] / 1099511627776.0;
+    *count = 3 * na;
+    return XTBLOOM_STATUS_SUCCESS;
+  }
   else if (name == "dipole_integrals") {
     if (capacity < 3 * (size_t)(n * n)) { error = "capacity too small"; return XTBLOOM_STATUS_INVALID_ARGUMENT; }
     for (int c = 0; c < 3; ++c)

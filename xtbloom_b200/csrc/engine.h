@@ -56,6 +56,12 @@ class Engine {
   // split-precision GEMMs until a system's residual is below switch_residual
   // (then FP64 to convergence); graphs = replay captured SCC iterations.
   void set_execution(int precision, double switch_residual, bool graphs);
+  // The WARM checkpoint is dropped (a plan's set-up compute must not leave one).
+  void invalidate_checkpoint();
+  // Bytes the engine holds: device buffers (grown by computes, kept for the
+  // next) and pinned host staging.
+  size_t device_bytes() const;
+  size_t host_bytes() const;
   int device() const { return device_; }
   cudaStream_t stream() const { return stream_; }
 

@@ -26,29 +26,44 @@ namespace xtb {
 
 constexpr int GB = 64, GK = 16;
 
+// One FP64 tensor-core product D = A B + D of an 8x8x4 tile (warp-wide):
+// lane l holds A[l/4][l%4], B[l%4][l/4] and D[l/4][2(l%4) .. 2(l%4)+1].
+__device__ __forceinline__ void mma_f64(double* d, double a, double b) {
+  asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
+               : "+d"(d[0]), "+d"(d[1])
+               : "d"(a), "d"(b));
+}
+
 // FP64 tile (ti, tj) of edge TB (64, or 32 when few systems are active) of
-// system s: 256 threads, (TB/16) x (TB/16) outputs per thread.
+// system s on the FP64 tensor cores (mma.m8n8k4.f64, FP64 accumulation):
+// 256 threads as 2 x 4 warps, each warp a (TB/2) x (TB/4) block of 8x8
+// products.  Operand chunks of GK = 16 are staged k-major in shared memory
+// (row stride TB + 4: the fragment reads of a half-warp hit distinct banks);
+// every element is accumulated over k in the same order (chunks, then steps
+// of 4) at either tile width, so both widths give identical results.
 template <bool TA, bool W, int TB>
 __device__ __forceinline__ void gemm_tile_f64(const GemmArgs& g, int s, int M, int N, int K, int ld,
                                               int ti, int tj, bool mirror) {
-  constexpr int RT = TB / 16;            // outputs per thread and dimension
   constexpr int LPT = TB * GK / 256;     // elements of each operand chunk per thread
+  constexpr int MT = TB / 16, NT = TB / 32;   // 8x8 products per warp and dimension
+  constexpr int SP = TB + 4;
   const double* A = g.A + g.offA[s];
   const double* B = g.B + g.offB[s];
   double* C = g.C + g.offC[s];
   const double* w = W ? g.w + g.offW[s] : nullptr;
-  __shared__ double As[GK][TB + 1];
-  __shared__ double Bs[GK][TB + 1];
-  const int tid = threadIdx.x;
-  const int tx = tid & 15, ty = tid >> 4;
-  double acc[RT][RT];
+  __shared__ double As[GK][SP];
+  __shared__ double Bs[GK][SP];
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int wm = warp >> 2, wn = warp & 3;
+  const int gq = lane >> 2, tq = lane & 3;
+  double acc[MT][NT][2];
 #pragma unroll
-  for (int i = 0; i < RT; ++i)
+  for (int i = 0; i < MT; ++i)
 #pragma unroll
-    for (int j = 0; j < RT; ++j) acc[i][j] = 0.0;
+    for (int j = 0; j < NT; ++j) acc[i][j][0] = acc[i][j][1] = 0.0;
   const int i0 = ti * TB, j0 = tj * TB;
   // The next chunk's operands are loaded into registers while the current
-  // chunk is multiplied, so global latency overlaps the FMAs.
+  // chunk is multiplied, so global latency overlaps the products.
   double ra[LPT], rb[LPT];
   auto fetch = [&](int k0) {
 #pragma unroll
@@ -83,29 +98,32 @@ __device__ __forceinline__ void gemm_tile_f64(const GemmArgs& g, int s, int M, i
     __syncthreads();
     if (k0 + GK < K) fetch(k0 + GK);
 #pragma unroll
-    for (int kk = 0; kk < GK; ++kk) {
-      double a[RT], b[RT];
+    for (int ks = 0; ks < GK; ks += 4) {
+      double a[MT], b[NT];
 #pragma unroll
-      for (int i = 0; i < RT; ++i) a[i] = As[kk][ty + 16 * i];
+      for (int i = 0; i < MT; ++i) a[i] = As[ks + tq][wm * (TB / 2) + i * 8 + gq];
 #pragma unroll
-      for (int j = 0; j < RT; ++j) b[j] = Bs[kk][tx + 16 * j];
+      for (int j = 0; j < NT; ++j) b[j] = Bs[ks + tq][wn * (TB / 4) + j * 8 + gq];
 #pragma unroll
-      for (int i = 0; i < RT; ++i)
+      for (int i = 0; i < MT; ++i)
 #pragma unroll
-        for (int j = 0; j < RT; ++j) acc[i][j] = fma(a[i], b[j], acc[i][j]);
+        for (int j = 0; j < NT; ++j) mma_f64(acc[i][j], a[i], b[j]);
     }
     __syncthreads();
   }
 #pragma unroll
-  for (int i = 0; i < RT; ++i) {
-    const int gi = i0 + ty + 16 * i;
+  for (int i = 0; i < MT; ++i) {
+    const int gi = i0 + wm * (TB / 2) + i * 8 + gq;
     if (gi >= M) continue;
 #pragma unroll
-    for (int j = 0; j < RT; ++j) {
-      const int gj = j0 + tx + 16 * j;
-      if (gj < N) {
-        C[(int64_t)gi * ld + gj] = acc[i][j];
-        if (mirror) C[(int64_t)gj * ld + gi] = acc[i][j];
+    for (int j = 0; j < NT; ++j) {
+#pragma unroll
+      for (int h = 0; h < 2; ++h) {
+        const int gj = j0 + wn * (TB / 4) + j * 8 + 2 * tq + h;
+        if (gj < N) {
+          C[(int64_t)gi * ld + gj] = acc[i][j][h];
+          if (mirror) C[(int64_t)gj * ld + gi] = acc[i][j][h];
+        }
       }
     }
   }
@@ -239,6 +257,7 @@ __device__ __forceinline__ void gemm_tile_tf32x3(const GemmArgs& g, int s, int M
 template <bool TA, bool W, int TB>
 __global__ void __launch_bounds__(256, 3) k_gemm(GemmArgs g) {
   const int s = g.list[blockIdx.y];
+  if (g.only != nullptr && g.only[s] == 0) return;
   const int M = g.dm[s], N = g.dn[s], K = g.dk[s];
   const int ld = g.nao[s];
   const int tn = (N + TB - 1) / TB;
@@ -311,6 +330,7 @@ void launch_gemm(const GemmArgs& g, bool transA, bool weighted, int max_tiles, i
 __global__ void __launch_bounds__(512) k_tridiag(EigArgs g, int nloc) {
   extern __shared__ double sm[];
   const int s = g.list[blockIdx.x];
+  if (g.only != nullptr && g.only[s] == 0) return;
   const int n = g.nao[s];
   const int i_end = nloc > 0 ? n - nloc : n - 2;
   if (i_end <= 0 && nloc > 0) return;
@@ -519,6 +539,7 @@ __global__ void __launch_bounds__(NT) k_tridiag_smem(EigArgs g, const int32_t* l
   extern __shared__ double sm[];
   constexpr int nw = NT / 32;
   const int s = list[blockIdx.x];
+  if (g.only != nullptr && g.only[s] == 0) return;
   const int n = g.nao[s];
   const int i0 = n > nloc ? n - nloc : 0;
   const int nl = n - i0;
@@ -812,7 +833,8 @@ __device__ void bisect_range(const double* d, const double* e2, int n, double gl
                              double pivmin, int j0, int j1, double unscale, int tpe_max, double* ev);
 
 // Number of eigenvalues the SCC needs: the occupied levels and eight above
-// them (mode 0); all of them for the overlap (mode 1).
+// them (mode 0); all of them for the overlap (mode 1) and for an SCC
+// iteration that also seeds the warm-started refinement (mode 2).
 __device__ __forceinline__ int levels_needed(const EigArgs& g, int s, int n, int mode) {
   if (mode != 0) return n;
   return min(n, (int)ceil(fmax(g.nel_a[s], g.nel_b[s])) + 8);
@@ -868,6 +890,7 @@ __device__ ScaledTridiag load_scaled_tridiag(const EigArgs& g, int64_t o, int n,
 __global__ void __launch_bounds__(256) k_eigvals_part(EigArgs g, int mode, int parts) {
   extern __shared__ double sm[];
   const int s = g.list[blockIdx.y];
+  if (g.only != nullptr && g.only[s] == 0) return;
   const int n = g.nao[s];
   const int64_t o = g.ao_off[s];
   const int nk = levels_needed(g, s, n, mode);
@@ -881,13 +904,15 @@ __global__ void __launch_bounds__(256) k_eigvals_part(EigArgs g, int mode, int p
   bisect_range(d, e2, n, t.glo, t.ghi, t.pivmin, j0, j1, t.unscale, 32, g.eig + o);
 }
 
-// mode 0: SCC (occupations, needed vectors); mode 1: all vectors, no occupations.
+// mode 0: SCC (occupations, needed vectors); mode 1: all vectors, no
+// occupations; mode 2: SCC occupations from the whole spectrum.
 // have != 0: the needed eigenvalues are already in g.eig (k_eigvals_part).
 // Bisection here uses at most tpe_max threads per eigenvalue.
 __global__ void __launch_bounds__(256) k_tridiag_eigvals(EigArgs g, int mode, double kt, int have,
                                                          int tpe_max) {
   extern __shared__ double sm[];
   const int s = g.list[blockIdx.x];
+  if (g.only != nullptr && g.only[s] == 0) return;
   const int n = g.nao[s];
   const int64_t o = g.ao_off[s];
   double* d = sm;
@@ -994,8 +1019,9 @@ __device__ void bisect_range(const double* d, const double* e2, int n, double gl
 
 __global__ void __launch_bounds__(128) k_inverse_iteration(EigArgs g, double ortol_rel) {
   const int s = g.list[blockIdx.x];
+  if (g.only != nullptr && g.only[s] == 0) return;
   const int64_t o = g.ao_off[s];
-  inverse_iteration_block<128>(g.d + o, g.e + o, g.eig + o, g.nao[s], g.nvec[s],
+  inverse_iteration_block<128>(g.d + o, g.e + o, g.eig + o, g.nao[s], g.all_vectors ? g.nao[s] : g.nvec[s],
                                g.Z + g.mat_off[s], g.scratch + g.scratch_off[s], ortol_rel,
                                (uint32_t)s, 0, 128);
 }
@@ -1007,8 +1033,10 @@ constexpr int kInvSmemThreads = 16;
 __global__ void __launch_bounds__(kInvSmemThreads) k_inverse_iteration_smem(EigArgs g, double ortol_rel) {
   extern __shared__ double sm[];
   const int s = g.list[blockIdx.y];
+  if (g.only != nullptr && g.only[s] == 0) return;
   const int64_t o = g.ao_off[s];
-  inverse_iteration_block<kInvSmemThreads>(g.d + o, g.e + o, g.eig + o, g.nao[s], g.nvec[s],
+  inverse_iteration_block<kInvSmemThreads>(g.d + o, g.e + o, g.eig + o, g.nao[s],
+                                           g.all_vectors ? g.nao[s] : g.nvec[s],
                                            g.Z + g.mat_off[s], sm, ortol_rel, (uint32_t)s,
                                            blockIdx.x * kInvSmemThreads,
                                            gridDim.x * kInvSmemThreads);
@@ -1022,8 +1050,9 @@ __global__ void __launch_bounds__(kInvSmemThreads) k_inverse_iteration_smem(EigA
 __global__ void __launch_bounds__(256) k_backtransform(EigArgs g, const int32_t* list, int mcap) {
   extern __shared__ double sm[];
   const int s = list[blockIdx.x];
+  if (g.only != nullptr && g.only[s] == 0) return;
   const int n = g.nao[s];
-  const int m = g.nvec[s];
+  const int m = g.all_vectors ? n : g.nvec[s];
   const double* a = g.A + g.mat_off[s];
   const double* tau = g.tau + g.ao_off[s];
   double* gZ = g.Z + g.mat_off[s];
@@ -1128,6 +1157,7 @@ size_t backtransform_wy_bytes(int n, int m) {
 __global__ void __launch_bounds__(256) k_wy_factor(EigArgs g) {
   extern __shared__ double sm[];
   const int s = g.list[blockIdx.y];
+  if (g.only != nullptr && g.only[s] == 0) return;
   const int n = g.nao[s];
   const int nr = n - 2;
   const int b = blockIdx.x;
@@ -1213,8 +1243,9 @@ template <bool STAGED>
 __global__ void __launch_bounds__(256) k_backtransform_wy(EigArgs g, int wcap, int per_cap) {
   extern __shared__ double sm[];
   const int s = g.list[blockIdx.y];
+  if (g.only != nullptr && g.only[s] == 0) return;
   const int n = g.nao[s];
-  const int mt = g.nvec[s];
+  const int mt = g.all_vectors ? n : g.nvec[s];
   const int per = (mt + gridDim.x - 1) / gridDim.x;
   const int jbeg = blockIdx.x * per;
   const int m = min(mt - jbeg, per);

@@ -137,12 +137,12 @@ __global__ void __launch_bounds__(128) k_force_pairs(ForceArgs f) {
   if (f.want_grad) {
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
-      atomicAdd(&f.grad[3 * gA + c], g[c]);
-      atomicAdd(&f.grad[3 * gB + c], -g[c]);
+      fix_add(&f.grad[3 * gA + c], g[c]);
+      fix_add(&f.grad[3 * gB + c], -g[c]);
     }
   }
-  atomicAdd(&f.acn[gA], cnA);
-  atomicAdd(&f.acn[gB], cnB);
+  fix_add(&f.acn[gA], cnA);
+  fix_add(&f.acn[gB], cnB);
 }
 
 // Onsite CN adjoint of the shell levels: one thread per atom.
@@ -168,7 +168,7 @@ __global__ void k_force_onsite(ForceArgs f) {
       acc -= 0.5 * bw * (t.sh_kcn[x] + t.sh_kcn[y]);
     }
   }
-  atomicAdd(&f.acn[gA], acc);
+  fix_add(&f.acn[gA], acc);
 }
 
 void launch_force_pairs(const ForceArgs& f, int64_t max_pairs, cudaStream_t stream) {
@@ -250,8 +250,8 @@ __global__ void __launch_bounds__(256) k_classical(ForceArgs f) {
                                 wcn + kMaxD4Refs * j, wcn + kMaxD4Refs * i, &cj, &ci);
         // gradient[first=j] += -c6*ddamp*(R_j - R_i), i.e. gradient[i] += -c6*ddamp*d
         gs -= c6 * ddamp;
-        atomicAdd(&acn4[j], -cj * damp);
-        atomicAdd(&acn4[i], -ci * damp);
+        fix_add(&acn4[j], -cj * damp);
+        fix_add(&acn4[i], -ci * damp);
       }
       // AES2: first = j, second = i, displacement dd = R_j - R_i = -d
       {
@@ -292,17 +292,17 @@ __global__ void __launch_bounds__(256) k_classical(ForceArgs f) {
           const double ddd = 2.0 * ddt * dd[c] - 3.0 * (pf * dps[c] + ps * dpf[c]);
           const double gc = k3 * cdv[c] + k3d * cdn * dd[c] / r + k5 * (ddd + 2.0 * tv[c]) +
                             k5d * k5n * dd[c] / r;
-          atomicAdd(&gr[3 * j + c], gc);
-          atomicAdd(&gr[3 * i + c], -gc);
+          fix_add(&gr[3 * j + c], gc);
+          fix_add(&gr[3 * i + c], -gc);
         }
-        atomicAdd(&acn[j], 0.5 * erd * f.dmrad[gj]);
-        atomicAdd(&acn[i], 0.5 * erd * f.dmrad[gi]);
+        fix_add(&acn[j], 0.5 * erd * f.dmrad[gj]);
+        fix_add(&acn[i], 0.5 * erd * f.dmrad[gi]);
       }
     }
     if (grad) {
       for (int c = 0; c < 3; ++c) {
-        atomicAdd(&gr[3 * i + c], gs * d[c]);
-        atomicAdd(&gr[3 * j + c], -gs * d[c]);
+        fix_add(&gr[3 * i + c], gs * d[c]);
+        fix_add(&gr[3 * j + c], -gs * d[c]);
       }
     }
   }
@@ -311,9 +311,9 @@ __global__ void __launch_bounds__(256) k_classical(ForceArgs f) {
   if (!grad) return;
   for (int i = tid; i < na; i += bs) {
     const int64_t g = a0 + i;
-    for (int c = 0; c < 3; ++c) atomicAdd(&f.grad[3 * g + c], gr[3 * i + c]);
-    atomicAdd(&f.acn[g], acn[i]);
-    atomicAdd(&f.acn_d4[g], acn4[i]);
+    for (int c = 0; c < 3; ++c) fix_merge(&f.grad[3 * g + c], gr[3 * i + c]);
+    fix_merge(&f.acn[g], acn[i]);
+    fix_merge(&f.acn_d4[g], acn4[i]);
   }
 }
 
@@ -436,14 +436,14 @@ __global__ void __launch_bounds__(256) k_atm(ForceArgs f, int parts) {
         const double gij = sij * vij[c], gik = sik * vik[c], gjk = sjk * vjk[c];
         g_i[c] -= gij + gik;
         g_j[c] += gij - gjk;
-        atomicAdd(&gr[3 * k + c], gik + gjk);
+        fix_add(&gr[3 * k + c], gik + gjk);
       }
       const double de = ang * damp * c9;
       const double cik_i = D[(int64_t)i * na + k], cik_k = D[(int64_t)k * na + i];
       const double cjk_j = D[(int64_t)j * na + k], cjk_k = D[(int64_t)k * na + j];
       a_i -= 0.5 * de * (cij_i / cij + cik_i / cik);
       a_j -= 0.5 * de * (cij_j / cij + cjk_j / cjk);
-      atomicAdd(&acn4[k], -0.5 * de * (cik_k / cik + cjk_k / cjk));
+      fix_add(&acn4[k], -0.5 * de * (cik_k / cik + cjk_k / cjk));
     }
     if (grad) {
 #pragma unroll
@@ -455,11 +455,11 @@ __global__ void __launch_bounds__(256) k_atm(ForceArgs f, int parts) {
       a_j = warp_sum(a_j);
       if (lane == 0) {
         for (int c = 0; c < 3; ++c) {
-          atomicAdd(&gr[3 * i + c], g_i[c]);
-          atomicAdd(&gr[3 * j + c], g_j[c]);
+          fix_add(&gr[3 * i + c], g_i[c]);
+          fix_add(&gr[3 * j + c], g_j[c]);
         }
-        atomicAdd(&acn4[i], a_i);
-        atomicAdd(&acn4[j], a_j);
+        fix_add(&acn4[i], a_i);
+        fix_add(&acn4[j], a_j);
       }
     }
   }
@@ -472,8 +472,8 @@ __global__ void __launch_bounds__(256) k_atm(ForceArgs f, int parts) {
   __syncthreads();
   for (int i = threadIdx.x; i < na; i += blockDim.x) {
     const int64_t g = a0 + i;
-    for (int c = 0; c < 3; ++c) atomicAdd(&f.grad[3 * g + c], gr[3 * i + c]);
-    atomicAdd(&f.acn_d4[g], acn4[i]);
+    for (int c = 0; c < 3; ++c) fix_merge(&f.grad[3 * g + c], gr[3 * i + c]);
+    fix_merge(&f.acn_d4[g], acn4[i]);
   }
 }
 
@@ -525,7 +525,7 @@ __global__ void __launch_bounds__(256) k_cn_chain(ForceArgs f) {
       const double f1 = logistic(10.0 * (rad / r - 1.0));
       const double f2 = logistic(20.0 * ((rad + 2.0) / r - 1.0));
       const double dv = -(10.0 * rad * f1 * (1.0 - f1) * f2 + 20.0 * (rad + 2.0) * f2 * (1.0 - f2) * f1) / r2;
-      sc += (f.acn[gi] + f.acn[gj]) * dv / r;
+      sc += (fix_value(f.acn[gi]) + fix_value(f.acn[gj])) * dv / r;
     }
     if (r2 <= 900.0) {
       const int zi = t.Z[gi] - 1, zj = t.Z[gj] - 1;
@@ -534,12 +534,12 @@ __global__ void __launch_bounds__(256) k_cn_chain(ForceArgs f) {
       const double enf = 4.10451 * exp(-(den + 19.08857) * (den + 19.08857) / (2.0 * 11.28174 * 11.28174));
       const double x = 7.5 * (r - rc) / rc;
       const double dv = -enf * 7.5 * exp(-x * x) / sqrt(kPi) / rc;
-      sc += (f.acn_d4[gi] + f.acn_d4[gj]) * dv / r;
+      sc += (fix_value(f.acn_d4[gi]) + fix_value(f.acn_d4[gj])) * dv / r;
     }
     if (sc != 0.0) {
       for (int c = 0; c < 3; ++c) {
-        atomicAdd(&f.grad[3 * gi + c], sc * d[c]);
-        atomicAdd(&f.grad[3 * gj + c], -sc * d[c]);
+        fix_add(&f.grad[3 * gi + c], sc * d[c]);
+        fix_add(&f.grad[3 * gj + c], -sc * d[c]);
       }
     }
   }

@@ -57,9 +57,9 @@ __global__ void __launch_bounds__(128) k_pc_forces(DevTopo t, const int32_t* lis
       gy -= w * dy;
       gz -= w * dz;
     }
-    atomicAdd(&grad[3 * at], gx);
-    atomicAdd(&grad[3 * at + 1], gy);
-    atomicAdd(&grad[3 * at + 2], gz);
+    fix_add(&grad[3 * at], gx);
+    fix_add(&grad[3 * at + 1], gy);
+    fix_add(&grad[3 * at + 2], gz);
   }
   for (int64_t p = p0 + threadIdx.x; p < p1; p += blockDim.x) {
     double fx = 0.0, fy = 0.0, fz = 0.0, dq = 0.0;

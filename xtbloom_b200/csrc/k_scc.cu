@@ -842,7 +842,18 @@ __global__ void __launch_bounds__(256) k_energy_mixer(SccArgs a) {
   // mixed = cur + damp * res - sum_h omega_h c_h u_h ; shift history
   const double Fold = (it == 0) ? 0.0 : a.free_energy[s];
   const bool exact = a.prec == nullptr || a.prec[s] != 0;   // this iteration ran in FP64
-  const bool conv = (rms < a.ctol) && (fabs(F - Fold) < a.etol) && hc >= 0 && exact;
+  // The split-precision form reaches the fixed point on another trajectory
+  // than the FP64 form, so stopping anywhere inside the gate would leave it
+  // as far from the FP64 result as the gate allows (charges ~1e-5 apart):
+  // its FP64 iterations continue to a gate kMixedTighten times tighter, so
+  // that its result is the fixed point itself.  A system that meets the
+  // ordinary gate but not the tighter one within kMixedExtra FP64 iterations
+  // (or by the last iteration) stops on the ordinary gate.
+  const bool gate = (rms < a.ctol) && (fabs(F - Fold) < a.etol) && hc >= 0 && exact;
+  const bool tight = a.prec == nullptr ||
+                     ((rms < a.ctol * kMixedTighten) && (fabs(F - Fold) < a.etol * kMixedTighten));
+  const int hits = (a.gate_hits != nullptr && gate) ? a.gate_hits[s] + 1 : 0;
+  const bool conv = gate && (tight || hits > kMixedExtra || it + 1 >= a.max_iter);
   const bool failed = hc < 0 || !isfinite(F) || !isfinite(nrm);
   const int first = it - (hc > 0 ? hc : 0) + 1;
   for (int i = tid; i < dim; i += bs) {
@@ -882,8 +893,12 @@ __global__ void __launch_bounds__(256) k_energy_mixer(SccArgs a) {
     tm[kTermResp] = er;
     if (!exact) {
       a.split_iters[s] += 1;
-      if (rms < a.prec_switch) a.prec[s] = 1;
+      // switch once the residual is small, or when split-precision
+      // iterations stop making progress (a residual stuck above the switch)
+      if (rms < a.prec_switch || a.split_iters[s] >= kMaxSplitIterations) a.prec[s] = 1;
     }
+    if (a.gate_hits != nullptr && gate) a.gate_hits[s] = hits;
+    if (a.last_rms != nullptr) a.last_rms[s] = rms;
     if (failed) {
       a.status[s] = kInternal;
     } else if (conv) {

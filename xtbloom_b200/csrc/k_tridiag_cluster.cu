@@ -91,6 +91,9 @@ __global__ void __launch_bounds__(NT) k_tridiag_reg(EigArgs g, const int32_t* li
   cg::cluster_group cluster = cg::this_cluster();
   const int crank = (int)cluster.block_rank();
   const int s = list[blockIdx.x / G];
+  // uniform over the cluster (every CTA of it has the same system): all of
+  // them return before any cluster barrier
+  if (g.only != nullptr && g.only[s] == 0) return;
   const int n = g.nao[s];
   double* ga = g.A + g.mat_off[s];
   double* d = g.d + g.ao_off[s];

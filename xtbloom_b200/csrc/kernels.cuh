@@ -22,6 +22,7 @@ struct GemmArgs {
   int32_t sym;             // C is symmetric: compute the lower tiles, mirror them
   const uint8_t* prec;     // per system: 0 = split-precision (3xTF32) tile, else FP64; NULL = FP64
   const int32_t* prec_of;  // list entry (channel) -> index into prec; NULL = the entry itself
+  const uint8_t* only;     // per list entry id: 0 = skip (its CTAs return at once); NULL = all
 };
 
 struct EigArgs {
@@ -43,6 +44,11 @@ struct EigArgs {
   const int64_t* scratch_off;
   const double* nel_a;
   const double* nel_b;
+  // per channel: 0 = skip (every CTA of the channel returns at once); NULL = all
+  const uint8_t* only;
+  // nonzero: inverse iteration and the back-transform form all n eigenvectors
+  // (nvec still counts the occupied ones the density needs)
+  int32_t all_vectors;
 };
 
 struct SccArgs {
@@ -126,7 +132,18 @@ struct SccArgs {
   uint8_t* prec;
   double prec_switch;
   int32_t* split_iters;   // per system: iterations run with split-precision GEMMs
+  int32_t* gate_hits;     // per system: FP64 iterations that met the ordinary gate (split form)
+  double* last_rms;       // per system: charge residual (rms) of the latest iteration
 };
+
+// Split-precision form: FP64 iterations continue until the residual and the
+// energy change are this much below the requested tolerances, for at most
+// kMixedExtra iterations past the ordinary gate.
+constexpr double kMixedTighten = 1e-2;
+constexpr int kMixedExtra = 10;
+// A system whose residual has not fallen below the precision switch after
+// this many split-precision iterations continues in FP64.
+constexpr int kMaxSplitIterations = 40;
 
 void launch_setup(const DevTopo& t, const int32_t* list, int count, int max_atoms,
                   int64_t max_pairs, int64_t max_shells, double* cn, double* cn_d4, double* mrad,
@@ -153,6 +170,65 @@ void launch_backtransform_wy(const EigArgs& g, int count, int max_n, int max_m, 
                              cudaStream_t stream);
 size_t backtransform_wy_bytes(int n, int m);
 void launch_lowdin_weights(const EigArgs& g, int32_t* status, int count, cudaStream_t stream);
+
+// ---------------------------------------------------------------------------
+// Warm-started eigensolver of the SCC (k_refine.cu): from the second SCC
+// iteration on, a channel's eigenvector columns V of the previous iteration
+// are refined for the new matrix A by the matrix-multiplication iteration of
+// Ogita and Aishima, which only needs the products U = A V, S = V^T U and
+// G = V^T V and the update V (I + E); see k_refine.cu.
+// ---------------------------------------------------------------------------
+enum WarmPhase : uint8_t { kWarmCold = 0, kWarmActive = 1, kWarmFinal = 2, kWarmDone = 3, kWarmFailed = 4 };
+
+struct RefineArgs {
+  const int32_t* list;     // active channels
+  int32_t count;
+  const int32_t* nao;
+  const int64_t* mat_off;
+  const int64_t* ao_off;
+  const int32_t* ch_sys;   // channel -> system
+  const double* nel_a;     // per channel: electrons of the two Fermi populations
+  const double* nel_b;
+  double kt;
+  const double* Sm;        // V^T A V
+  const double* G;         // V^T V
+  double* Ep;              // I + E
+  double* V;               // eigenvector columns (valid where wstate == 1)
+  const double* Vt;        // V (I + E) of the step
+  const double* Zrows;     // eigenvector rows of the Householder path
+  double* eig;             // Rayleigh quotients of the columns (ao-indexed)
+  double* occ;             // occupations, occupation * Rayleigh quotient, count of
+  double* occ_eps;         // occupied columns and entropy of refined channels
+  int32_t* nvec;
+  double* entropy;
+  uint8_t* wstate;         // per channel: 1 = V holds the eigenvectors of an earlier iteration
+  uint8_t* phase;          // per channel WarmPhase of this iteration
+  uint8_t* m_step;         // mask: channels whose U, S, G products run in this step
+  uint8_t* m_apply;        // mask: channels whose V (I + E) product runs in this step
+  uint8_t* m_cold;         // mask: channels the Householder path solves in this iteration
+  uint8_t* m_warm;         // mask: channels refined in this iteration
+  unsigned long long* emax;   // per channel: max |E| of the step (bits of a nonnegative double)
+  int32_t* fail;           // per channel: failure flag of the step
+  int32_t* arrive;         // per channel: CTAs of the step that finished
+  double* bounds;          // per channel and part: Gershgorin bounds of the occupation blocks
+  int32_t* stats;          // [iteration][8] counters (attempted, done at step 1..3+, failed, unfinished)
+  const int32_t* iterations;   // per system: SCC iterations done
+  const uint8_t* prec;     // per system split-precision flag (0 = split), NULL = FP64
+  const double* last_rms;  // per system: charge residual of the previous SCC iteration
+  double final_rms;        // below this residual a system is in its final SCC iterations
+  int32_t warm_from;       // first SCC iteration that refines
+  int32_t step;            // 0-based step of this SCC iteration
+  // convergence thresholds of max |E|: split-precision iterations, FP64
+  // iterations on the approach, FP64 iterations near the fixed point
+  double theta_split, theta, theta_final;
+};
+
+constexpr int kRefineMaxParts = 16;
+
+void launch_warm_begin(const RefineArgs& r, cudaStream_t stream);
+void launch_refine_update(const RefineArgs& r, int max_n, int parts, cudaStream_t stream);
+void launch_refine_apply(const RefineArgs& r, int max_n, bool last, cudaStream_t stream);
+void launch_vectors_from_rows(const RefineArgs& r, int max_n, cudaStream_t stream);
 
 void launch_sad_init(const SccArgs& a, cudaStream_t stream);
 void launch_warm_init(const SccArgs& a, cudaStream_t stream);
