@@ -1,9 +1,11 @@
 """Generate the packed parameter tables used by the library and the oracle.
 
-The GFN2-xTB element/shell parameters (tblite 0.7.0 export), the Stewart
-STO-nG expansion tables, the D4 reference tables (dftd4) and the two mctc-lib
-radius tables are read from the reference checkout's published data files
-(``data/parameters/gfn2.json``, ``tblite_sto.hpp``, ``d4.hpp``,
+The GFN2-xTB and GFN1-xTB element/shell parameters (tblite exports), the
+Stewart STO-nG expansion tables (and the legacy STO-6G 4s/4p rows of GFN1),
+the D4 reference tables (dftd4), the D3 reference tables (simple-dftd3) and
+the two mctc-lib radius tables are read from the reference checkout's
+published data files (``data/parameters/gfn2.json``, ``gfn1.json``,
+``gfn1_d3.json``, ``gfn1_legacy_sto.hpp``, ``tblite_sto.hpp``, ``d4.hpp``,
 ``tblite_spin.hpp``) and from the
 two small radius tables in ``src/model/gfn2/h0.cpp`` and
 ``src/model/gfn2/coordination.cpp``.  Nothing is typed in by hand: every
@@ -156,6 +158,105 @@ def spin_tables(ref: Path) -> dict[str, np.ndarray]:
     return {"spin_constants": vals.reshape(86, 6)}
 
 
+def gfn1_tables(ref: Path) -> dict[str, np.ndarray]:
+    """GFN1-xTB element, shell and global parameters (tblite export,
+    ``data/parameters/gfn1.json``); shell levels and CN scales stay in eV."""
+    d = json.loads((ref / "data/parameters/gfn1.json").read_text())
+    els = d["elements"]
+    assert [e["atomic_number"] for e in els] == list(range(1, 87))
+    nz, max_sh = 86, 3
+    out: dict[str, np.ndarray] = {}
+    nsh = np.zeros(nz, np.int32)
+    ints = {k: np.full((nz, max_sh), -1 if k == "l" else 0, np.int32) for k in ("l", "n", "ngauss", "valence")}
+    f = {k: np.zeros((nz, max_sh)) for k in ("level", "kcn", "shpoly", "slater", "refocc", "hubbard_scale")}
+    keymap = {"level": "level", "kcn": "coordination_number_scale", "shpoly": "shell_polynomial",
+              "slater": "slater", "refocc": "reference_occupation", "hubbard_scale": "shell_hubbard_scale"}
+    for zi, e in enumerate(els):
+        nsh[zi] = len(e["shells"])
+        assert nsh[zi] <= max_sh
+        for si, sh in enumerate(e["shells"]):
+            assert sh["index"] == si
+            ints["l"][zi, si] = sh["angular_momentum"]
+            ints["n"][zi, si] = sh["principal_quantum_number"]
+            ints["ngauss"][zi, si] = sh["ngauss"]
+            ints["valence"][zi, si] = 1 if sh["is_valence"] else 0
+            for k, j in keymap.items():
+                f[k][zi, si] = sh[j]
+    out["gfn1_nshell"] = nsh
+    for k, v in ints.items():
+        out["gfn1_shell_" + k] = v
+    for k, v in f.items():
+        out["gfn1_shell_" + k] = v
+    for k, j in (("gam", "gam"), ("gam3", "gam3"), ("arep", "arep"), ("zeff", "zeff"), ("en", "en"),
+                 ("xbond", "xbond"), ("atomic_radius", "atomic_radius_bohr"),
+                 ("covalent_radius", "covalent_radius_bohr")):
+        out["gfn1_" + k] = np.array([e[j] for e in els], float)
+    h = d["hamiltonian"]
+    assert h["coordination_number"] == "exp"
+    sps = np.zeros((3, 3))
+    for item in h["shell_pair_scale"]:
+        a, b = item["angular_momenta"]
+        sps[a, b] = sps[b, a] = item["value"]
+    out["gfn1_shell_pair_scale"] = sps
+    kpair = np.full((nz, nz), h["pair_scale_default"])
+    for item in h["pair_scale_overrides"]:
+        a, b = item["atomic_numbers"]
+        kpair[a - 1, b - 1] = kpair[b - 1, a - 1] = item["value"]
+    out["gfn1_kpair"] = kpair
+    cn = d["coordination_number"]
+    assert cn["model"] == "exp" and d["charge"]["average"] == "harmonic"
+    assert d["thirdorder"]["mode"] == "atom" and d["dispersion"]["model"] == "d3"
+    out["gfn1_globals"] = np.array([
+        h["kpol"], h["enscale"], d["repulsion"]["kexp"], d["repulsion"]["klight"],
+        d["dispersion"]["a1"], d["dispersion"]["a2"], d["dispersion"]["s6"], d["dispersion"]["s8"],
+        d["dispersion"]["s9"], d["halogen"]["damping"], d["halogen"]["radius_scale"],
+        cn["steepness"], cn["cutoff_bohr"], d["charge"]["gexp"],
+    ])
+    return out
+
+
+GFN1_GLOBAL_NAMES = ["kpol", "enscale", "rep_kexp", "rep_klight", "d3_a1", "d3_a2", "d3_s6",
+                     "d3_s8", "d3_s9", "xb_damping", "xb_radius_scale", "cn_steepness",
+                     "cn_cutoff", "es2_gexp"]
+
+
+def gfn1_sto_tables(ref: Path) -> dict[str, np.ndarray]:
+    """The legacy STO-6G 4s/4p rows GFN1 uses (``gfn1_legacy_sto.hpp``)."""
+    t = (ref / "data/parameters/gfn1_legacy_sto.hpp").read_text()
+    out = {}
+    for name, key in (("kLegacyAlpha6_4sp", "alpha"), ("kLegacyCoeff6_4s", "coeff_s"),
+                      ("kLegacyCoeff6_4p", "coeff_p")):
+        v = np.array(_numbers(_std_array_block(t, name)))
+        assert v.size == 6
+        out["gfn1_sto6_4sp_" + key] = v
+    return out
+
+
+def d3_tables(ref: Path) -> dict[str, np.ndarray]:
+    """DFT-D3 reference data of GFN1 (simple-dftd3 export, ``gfn1_d3.json``):
+    per element the reference CNs; the reference C6 of every pair of
+    references, expanded into one symmetric table over all 237 references."""
+    d = json.loads((ref / "data/parameters/gfn1_d3.json").read_text())
+    els = d["elements"]
+    cnt = np.array([e["reference_count"] for e in els], np.int32)
+    off = np.array([e["reference_offset"] for e in els], np.int32)
+    nref = int(cnt.sum())
+    c6 = np.array(d["c6"], float)
+    table = np.zeros((nref, nref))
+    for z2 in range(1, 87):
+        for z1 in range(1, z2 + 1):
+            pr = d["pair_records"][(z1 - 1) + z2 * (z2 - 1) // 2]
+            assert pr["first_reference_count"] == cnt[z1 - 1] and pr["second_reference_count"] == cnt[z2 - 1]
+            for i in range(cnt[z1 - 1]):
+                for j in range(cnt[z2 - 1]):
+                    v = c6[pr["c6_offset"] + j * cnt[z1 - 1] + i]
+                    table[off[z1 - 1] + i, off[z2 - 1] + j] = v
+                    table[off[z2 - 1] + j, off[z1 - 1] + i] = v
+    return {"d3_ref_count": cnt, "d3_ref_offset": off,
+            "d3_ref_cn": np.array(d["coordination_numbers"], float),
+            "d3_r4r2": np.array(d["r4r2"], float), "d3_ref_c6": table}
+
+
 def generate(ref: Path, out: Path) -> None:
     tables: dict[str, np.ndarray] = {}
     tables.update(gfn2_tables(ref))
@@ -163,9 +264,22 @@ def generate(ref: Path, out: Path) -> None:
     tables.update(radius_tables(ref))
     tables.update(d4_tables(ref))
     tables.update(spin_tables(ref))
+    tables.update(gfn1_tables(ref))
+    tables.update(gfn1_sto_tables(ref))
+    tables.update(d3_tables(ref))
     np.savez_compressed(out, **tables)
 
 
+
+def reference_checkout() -> Path:
+    """The reference checkout: the first argument, else $XTBLOOM_REFERENCE_SRC."""
+    import os
+    arg = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("XTBLOOM_REFERENCE_SRC")
+    if not arg:
+        sys.exit("usage: pass the reference checkout as the first argument "
+                 "or set XTBLOOM_REFERENCE_SRC")
+    return Path(arg)
+
 if __name__ == "__main__":
-    reference = Path(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    reference = reference_checkout()
     generate(reference, Path(__file__).with_name("params.npz"))
