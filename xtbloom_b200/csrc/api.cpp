@@ -441,9 +441,17 @@ xtbloom_status_t validate_and_normalise(const xtbloom_batch_t* batch,
     return XTBLOOM_STATUS_INVALID_ARGUMENT;
   }
   if (options->model == XTBLOOM_MODEL_GFN1_XTB) {
-    err = "GFN1-xTB is not implemented in this CUDA path";
-    return XTBLOOM_STATUS_NOT_IMPLEMENTED;
+    // GFN1 runs molecular batches; its external-potential attachments have
+    // their own screening and are not built in this path
+    bool field = false;
+    for (uint8_t v : req.field_attached) field = field || v != 0;
+    if (batch->total_point_charges > 0 || req.have_response || field) {
+      err = "GFN1-xTB with external point charges, charge response or electric fields is not "
+            "implemented in this CUDA path";
+      return XTBLOOM_STATUS_NOT_IMPLEMENTED;
+    }
   }
+  req.model = options->model;
   const uint32_t known = XTBLOOM_COMPUTE_ENERGY | XTBLOOM_COMPUTE_FORCES |
                          XTBLOOM_COMPUTE_ATOMIC_CHARGES | XTBLOOM_COMPUTE_POINT_CHARGE_FORCES |
                          XTBLOOM_COMPUTE_DIPOLE_MOMENTS;

@@ -3,6 +3,8 @@
 // (model/gfn2/aes2.cpp:385-424).
 #pragma once
 
+#include <cfloat>
+
 #include "common.cuh"
 
 namespace xtb {
@@ -118,6 +120,89 @@ __device__ __forceinline__ void pair_from_index(int64_t p, int64_t& i, int64_t& 
   while (i * (i - 1) / 2 > p) --i;
   while ((i + 1) * i / 2 <= p) ++i;
   j = p - i * (i - 1) / 2;
+}
+
+// ---------------------------------------------------------------------------
+// GFN1: DFT-D3(BJ) two-body dispersion at the GFN1 coordination numbers
+// (model/gfn1/d3.cpp:255-410).  Reference weights are Gaussians
+// exp(-4 (CN_ref - CN)^2), normalised (with the reference's fallback to the
+// largest reference CN when the sum underflows); C6 interpolates the
+// reference C6 table; Becke-Johnson damping radius a1 sqrt(3 Q_A Q_B) + a2 and
+// a smooth cutoff over the last 0.05 bohr before 50 bohr.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ void d3_weights(const DevTopo& t, int z, double cn, double* w, double* dw) {
+  const int off = t.d3_roff[z - 1], cnt = t.d3_rcnt[z - 1];
+  double u[kD3MaxRefs];
+  double norm = 0.0, dnorm = 0.0, maxcn = -DBL_MAX;
+  for (int r = 0; r < cnt; ++r) {
+    const double delta = t.d3_ref_cn[off + r] - cn;
+    u[r] = exp(-4.0 * delta * delta);
+    norm += u[r];
+    dnorm += 8.0 * delta * u[r];
+    maxcn = fmax(maxcn, t.d3_ref_cn[off + r]);
+  }
+  const double inv = 1.0 / norm;
+  for (int r = 0; r < kD3MaxRefs; ++r) {
+    if (r >= cnt) {
+      w[r] = dw[r] = 0.0;
+      continue;
+    }
+    const double rcn = t.d3_ref_cn[off + r];
+    const double delta = rcn - cn;
+    double weight = u[r] * inv;
+    if (!isfinite(weight)) weight = rcn == maxcn ? 1.0 : 0.0;
+    double d = 8.0 * delta * u[r] * inv - u[r] * dnorm * inv * inv;
+    if (!isfinite(d)) d = 0.0;
+    w[r] = weight;
+    dw[r] = d;
+  }
+}
+
+// C6 of an atom pair and its derivatives with respect to the two CNs.
+__device__ __forceinline__ double d3_c6(const DevTopo& t, int za, int zb, const double* wa,
+                                        const double* dwa, const double* wb, const double* dwb,
+                                        double& dca, double& dcb) {
+  const int oa = t.d3_roff[za - 1], ca = t.d3_rcnt[za - 1];
+  const int ob = t.d3_roff[zb - 1], cb = t.d3_rcnt[zb - 1];
+  double c6 = 0.0;
+  dca = dcb = 0.0;
+  for (int i = 0; i < ca; ++i) {
+    const double* row = t.d3_c6 + (int64_t)(oa + i) * kD3Refs + ob;
+    for (int j = 0; j < cb; ++j) {
+      const double c = row[j];
+      c6 += wa[i] * wb[j] * c;
+      dca += dwa[i] * wb[j] * c;
+      dcb += wa[i] * dwb[j] * c;
+    }
+  }
+  return c6;
+}
+
+// Damped pair kernel: e = -(s6 t6 + s8 rrij t8) times the cutoff, and
+// de/dr / r; the pair energy is c6 * e.
+__device__ __forceinline__ void d3_pair(const DevTopo& t, int za, int zb, double r2, double& e,
+                                        double& de_over_r) {
+  const double rrij = 3.0 * t.d3_r4r2[za - 1] * t.d3_r4r2[zb - 1];
+  const double r0 = t.m.d3_a1 * sqrt(rrij) + t.m.d3_a2;
+  const double r02 = r0 * r0, r04 = r02 * r02;
+  const double r06 = r04 * r02, r08 = r04 * r04;
+  const double r4 = r2 * r2;
+  const double t6 = 1.0 / (r4 * r2 + r06);
+  const double t8 = 1.0 / (r4 * r4 + r08);
+  const double phi = t.m.d3_s6 * t6 + t.m.d3_s8 * rrij * t8;
+  const double dphi = t.m.d3_s6 * (-6.0 * r4 * t6 * t6) + t.m.d3_s8 * rrij * (-8.0 * r4 * r2 * t8 * t8);
+  const double r = sqrt(r2);
+  constexpr double kCut = 50.0, kWidth = 0.05;
+  double cut = 1.0, dcut = 0.0;
+  if (r >= kCut) {
+    cut = 0.0;
+  } else if (r > kCut - kWidth) {
+    const double x = (kCut - r) / kWidth;
+    cut = x * x * x * (10.0 + x * (-15.0 + 6.0 * x));
+    dcut = -30.0 * x * x * (1.0 - x) * (1.0 - x) / kWidth;
+  }
+  e = -cut * phi;
+  de_over_r = -(cut * dphi + dcut * phi / r);
 }
 
 }  // namespace xtb

@@ -52,13 +52,21 @@ constexpr double kIntegralCutoff = 25.0;          // Gaussian-product screen
 
 // Model constants shared by all kernels (set once per context).
 struct ModelConstants {
+  int32_t gfn1;   // 0: GFN2-xTB, 1: GFN1-xTB (the fields below hold that model's values)
   double wexp, enscale, kpol, pair_scale_default;
   double shell_pair_scale[9];
   double rep_kexp, rep_klight;
   double es3_scale[3];
   double mp_kexp, mp_shift, mp_rmax;
   double d4_a1, d4_a2, d4_s6, d4_s8, d4_s9;
+  // GFN1: D3(BJ) dispersion, halogen-bond correction, exponential CN
+  double d3_a1, d3_a2, d3_s6, d3_s8;
+  double xb_damping, xb_radius_scale;
+  double cn_steepness;
 };
+
+constexpr int kD3MaxRefs = 5;       // D3 reference systems per element
+constexpr int kD3Refs = 237;        // all D3 references
 
 struct DevTopo {
   ModelConstants m;
@@ -101,7 +109,18 @@ struct DevTopo {
   const double* d4_r4r2;
   const int32_t* d4_roff;
   const int32_t* d4_rcnt;
+  // GFN1: halogen-bond strength per atom, pair scaling of H0 (86 x 86),
+  // D3 reference tables (references per element, their offsets and CNs, the
+  // C6 of every pair of references, <r^4>/<r^2> per element)
+  const double* at_xbond;
+  const double* kpair;
+  const int32_t* d3_rcnt;
+  const int32_t* d3_roff;
+  const double* d3_ref_cn;
+  const double* d3_c6;
+  const double* d3_r4r2;
   // per shell
+  const int32_t* sh_val;      // 1 for valence shells (GFN1 H0 pair scaling)
   const int32_t* sh_atom;
   const int32_t* sh_l;
   const int32_t* sh_ao;       // first AO of the shell, system-local
@@ -137,7 +156,8 @@ struct DevTopo {
 // Per-system energy terms (terms[kTermCount * s + k]).
 enum TermIndex : int {
   kTermCore = 0, kTermEs2 = 1, kTermEs3 = 2, kTermAes2 = 3, kTermD4 = 4, kTermEntropy = 5,
-  kTermRep = 6, kTermAtm = 7, kTermPc = 8, kTermSpin = 9, kTermField = 10, kTermResp = 11, kTermCount = 12
+  kTermRep = 6, kTermAtm = 7, kTermPc = 8, kTermSpin = 9, kTermField = 10, kTermResp = 11,
+  kTermDisp3 = 12, kTermXb = 13, kTermCount = 14
 };
 
 __device__ __forceinline__ double logistic(double x) {
@@ -208,6 +228,13 @@ __device__ __forceinline__ void fix_merge(double* acc, const double& part) {
 }
 __device__ __forceinline__ double fix_value(const double& acc) {
   return static_cast<double>(*reinterpret_cast<const long long*>(&acc)) * (1.0 / kFixOne);
+}
+
+// Length of a system's charge block in the Broyden vector: shell charges,
+// atomic dipoles and quadrupoles (GFN2), shell charges only (GFN1).  An
+// unrestricted system carries a magnetisation block of the same length.
+__device__ __forceinline__ int charge_block(const DevTopo& t, int ns, int na) {
+  return t.m.gfn1 ? ns : ns + 9 * na;
 }
 
 // Per-system status codes mirror the public per_system_status values.

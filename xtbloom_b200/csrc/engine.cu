@@ -101,6 +101,23 @@ bool sto_expand(int n, int l, int ng, double zeta, std::vector<double>& alpha,
   return true;
 }
 
+// GFN1 keeps xTB's legacy STO-6G rows for 4s and 4p shells (one exponent
+// row, two coefficient rows; model/gfn1/basis.cpp:64-90); every other shell
+// is the common Stewart expansion.
+bool sto_expand_gfn1(int n, int l, int ng, double zeta, std::vector<double>& alpha,
+                     std::vector<double>& coeff) {
+  if (!(ng == 6 && n == 4 && l <= 1)) return sto_expand(n, l, ng, zeta, alpha, coeff);
+  const double* c0 = l == 0 ? kP_gfn1_sto6_4sp_coeff_s : kP_gfn1_sto6_4sp_coeff_p;
+  alpha.resize(6);
+  coeff.resize(6);
+  for (int i = 0; i < 6; ++i) {
+    alpha[i] = kP_gfn1_sto6_4sp_alpha[i] * zeta * zeta;
+    const double norm = std::pow(2.0 / kPiH * alpha[i], 0.75) * std::pow(std::sqrt(4.0 * alpha[i]), l);
+    coeff[i] = c0[i] * norm;
+  }
+  return true;
+}
+
 void orthogonalize_to_first(const std::vector<double>& a1, const std::vector<double>& c1,
                             std::vector<double>& a, std::vector<double>& c) {
   double ov = 0.0;
@@ -146,6 +163,30 @@ ModelConstants make_constants() {
   m.d4_s8 = g[17];
   m.d4_s9 = g[18];
   (void)kGlobalNames;
+  return m;
+}
+
+// GFN1-xTB constants (tblite export, data/parameters/gfn1.json).
+ModelConstants make_constants_gfn1() {
+  ModelConstants m{};
+  const double* g = kP_gfn1_globals;   // kpol, enscale, rep kexp/klight, d3 a1 a2 s6 s8 s9,
+                                       // xb damping, radius scale, CN steepness, cutoff, gexp
+  m.gfn1 = 1;
+  m.wexp = 0.0;
+  m.kpol = g[0];
+  m.enscale = g[1];
+  m.pair_scale_default = 1.0;
+  for (int i = 0; i < 9; ++i) m.shell_pair_scale[i] = kP_gfn1_shell_pair_scale[i];
+  m.rep_kexp = g[2];
+  m.rep_klight = g[3];
+  m.es3_scale[0] = m.es3_scale[1] = m.es3_scale[2] = 1.0;
+  m.d3_a1 = g[4];
+  m.d3_a2 = g[5];
+  m.d3_s6 = g[6];
+  m.d3_s8 = g[7];
+  m.xb_damping = g[9];
+  m.xb_radius_scale = g[10];
+  m.cn_steepness = g[11];
   return m;
 }
 
@@ -204,7 +245,11 @@ struct Profiler {
 }  // namespace
 
 struct Engine::Impl {
-  ModelConstants model = make_constants();
+  ModelConstants model = make_constants();   // the model of the current topology
+  const ModelConstants model_gfn2 = make_constants();
+  const ModelConstants model_gfn1 = make_constants_gfn1();
+  // GFN1 tables: element-pair H0 scale, D3 references
+  Dbuf kpair, d3_rcnt, d3_roff, d3_ref_cn, d3_c6, d3_r4r2;
   // static parameter tables on the device
   Dbuf d4_rcov, d4_en, d4_zeff, d4_eta, d4_r4r2, d4_roff, d4_rcnt, ref_cn, ref_q, ref_ng, ref_c6;
   bool tables_ready = false;
@@ -231,7 +276,8 @@ struct Engine::Impl {
   std::vector<double> h_ch_nel_a, h_ch_nel_b;
   int32_t* h_clist = nullptr;   // pinned copy of the active channel list
   int64_t h_clist_cap = 0;
-  Dbuf Z, atom_sh, pos, at_en, at_rad, at_rcov, at_mprad, at_mpvcn, at_dk, at_qk, at_rep_sa, at_rep_z;
+  Dbuf Z, atom_sh, pos, at_en, at_rad, at_rcov, at_mprad, at_mpvcn, at_dk, at_qk, at_rep_sa, at_rep_z,
+      at_xbond, sh_val;
   Dbuf sh_atom, sh_l, sh_ao, sh_p0, sh_np, sh_level, sh_kcn, sh_shpoly, sh_zeta, sh_eta, sh_g3,
       sh_refocc, p_alpha, p_coeff, ao_sh, ao_at, order;
   // state
@@ -323,6 +369,7 @@ struct Engine::Impl {
     bool operator==(const CallIdentity& o) const {
       return topo.nsys == o.topo.nsys && topo.atom_off == o.topo.atom_off && topo.Z == o.topo.Z &&
              topo.qmol == o.topo.qmol && topo.uhf == o.topo.uhf && topo.nch == o.topo.nch &&
+             topo.model == o.topo.model &&
              flags == o.flags && max_iter == o.max_iter && memory == o.memory && ctol == o.ctol &&
              etol == o.etol && kt == o.kt && damping == o.damping && pc_off == o.pc_off &&
              field_attached == o.field_attached && field == o.field && resp_off == o.resp_off;
@@ -374,6 +421,14 @@ struct Engine::Impl {
     t.d4_r4r2 = d4_r4r2.as<double>();
     t.d4_roff = d4_roff.as<int32_t>();
     t.d4_rcnt = d4_rcnt.as<int32_t>();
+    t.at_xbond = at_xbond.as<double>();
+    t.kpair = kpair.as<double>();
+    t.d3_rcnt = d3_rcnt.as<int32_t>();
+    t.d3_roff = d3_roff.as<int32_t>();
+    t.d3_ref_cn = d3_ref_cn.as<double>();
+    t.d3_c6 = d3_c6.as<double>();
+    t.d3_r4r2 = d3_r4r2.as<double>();
+    t.sh_val = sh_val.as<int32_t>();
     t.sh_atom = sh_atom.as<int32_t>();
     t.sh_l = sh_l.as<int32_t>();
     t.sh_ao = sh_ao.as<int32_t>();
@@ -485,14 +540,17 @@ bool ensure_tables(Engine::Impl& m, cudaStream_t s) {
             upd(m.d4_r4r2, kP_d4_r4r2, 86) && upi(m.d4_roff, kP_d4_ref_offset, 86) &&
             upi(m.d4_rcnt, kP_d4_ref_count, 86) && upd(m.ref_cn, kP_d4_ref_cn, 262) &&
             upd(m.ref_q, kP_d4_ref_q, 262) && upi(m.ref_ng, kP_d4_ref_ngauss, 262) &&
-            upd(m.ref_c6, kP_d4_ref_c6, 262 * 262);
+            upd(m.ref_c6, kP_d4_ref_c6, 262 * 262) && upd(m.kpair, kP_gfn1_kpair, 86 * 86) &&
+            upi(m.d3_rcnt, kP_d3_ref_count, 86) && upi(m.d3_roff, kP_d3_ref_offset, 86) &&
+            upd(m.d3_ref_cn, kP_d3_ref_cn, kD3Refs) && upd(m.d3_c6, kP_d3_ref_c6, kD3Refs * kD3Refs) &&
+            upd(m.d3_r4r2, kP_d3_r4r2, 86);
   m.tables_ready = ok;
   return ok;
 }
 
 bool same_topology(const HostBatch& a, const HostBatch& b) {
   return a.nsys == b.nsys && a.atom_off == b.atom_off && a.Z == b.Z && a.qmol == b.qmol &&
-         a.uhf == b.uhf && a.nch == b.nch;
+         a.uhf == b.uhf && a.nch == b.nch && a.model == b.model;
 }
 
 xtbloom_status_t build_topology(Engine::Impl& m, const HostBatch& hb, cudaStream_t s,
@@ -504,8 +562,11 @@ xtbloom_status_t build_topology(Engine::Impl& m, const HostBatch& hb, cudaStream
   std::vector<int32_t> nao(B), Zv(hb.Z.begin(), hb.Z.end()), atom_sh(N + 1);
   std::vector<double> nel_a(B), nel_b(B), qmol(hb.qmol.begin(), hb.qmol.end());
   std::vector<double> at_en(N), at_rad(N), at_rcov(N), at_mprad(N), at_mpvcn(N), at_dk(N), at_qk(N),
-      at_rep_sa(N), at_rep_z(N);
-  std::vector<int32_t> sh_atom, sh_l, sh_ao, sh_p0, sh_np, ao_sh, ao_at;
+      at_rep_sa(N), at_rep_z(N), at_xbond(N, 0.0);
+  std::vector<int32_t> sh_atom, sh_l, sh_ao, sh_p0, sh_np, ao_sh, ao_at, sh_val;
+  // GFN1 (model/gfn1/basis.cpp, h0.cpp, es2.cpp, es3.cpp, repulsion.cpp,
+  // coordination.cpp, halogen.cpp) or GFN2 element and shell parameters
+  const bool g1 = hb.model == XTBLOOM_MODEL_GFN1_XTB;
   std::vector<double> sh_level, sh_kcn, sh_shpoly, sh_zeta, sh_eta, sh_g3, sh_refocc, p_alpha, p_coeff,
       sh_spinw;
   int64_t shell = 0;
@@ -520,24 +581,34 @@ xtbloom_status_t build_topology(Engine::Impl& m, const HostBatch& hb, cudaStream
       const int z = Zv[a];
       const int zi = z - 1;
       atom_sh[a] = (int32_t)shell;
-      at_en[a] = kP_gfn2_en[zi];
-      at_rad[a] = kP_atomic_radii_angstrom[zi] * kAngstromToBohr;
-      at_rcov[a] = (4.0 / 3.0) * kAngstromToBohr * kP_covalent_radii_angstrom[zi];
-      at_mprad[a] = kP_gfn2_mprad[zi];
-      at_mpvcn[a] = kP_gfn2_mpvcn[zi];
-      at_dk[a] = kP_gfn2_dkernel[zi];
-      at_qk[a] = kP_gfn2_qkernel[zi];
-      at_rep_sa[a] = std::sqrt(kP_gfn2_arep[zi]);
-      at_rep_z[a] = kP_gfn2_zeff[zi];
-      const int nsh = kP_gfn2_nshell[zi];
+      if (g1) {
+        at_en[a] = kP_gfn1_en[zi];
+        at_rad[a] = kP_gfn1_atomic_radius[zi];
+        at_rcov[a] = kP_gfn1_covalent_radius[zi];
+        at_mprad[a] = at_mpvcn[a] = at_dk[a] = at_qk[a] = 0.0;
+        at_rep_sa[a] = std::sqrt(kP_gfn1_arep[zi]);
+        at_rep_z[a] = kP_gfn1_zeff[zi];
+        at_xbond[a] = kP_gfn1_xbond[zi];
+      } else {
+        at_en[a] = kP_gfn2_en[zi];
+        at_rad[a] = kP_atomic_radii_angstrom[zi] * kAngstromToBohr;
+        at_rcov[a] = (4.0 / 3.0) * kAngstromToBohr * kP_covalent_radii_angstrom[zi];
+        at_mprad[a] = kP_gfn2_mprad[zi];
+        at_mpvcn[a] = kP_gfn2_mpvcn[zi];
+        at_dk[a] = kP_gfn2_dkernel[zi];
+        at_qk[a] = kP_gfn2_qkernel[zi];
+        at_rep_sa[a] = std::sqrt(kP_gfn2_arep[zi]);
+        at_rep_z[a] = kP_gfn2_zeff[zi];
+      }
+      const int nsh = g1 ? kP_gfn1_nshell[zi] : kP_gfn2_nshell[zi];
       int first_of_l[5] = {-1, -1, -1, -1, -1};
       for (int k = 0; k < nsh; ++k) {
-        const int l = kP_gfn2_shell_l[3 * zi + k];
-        const int pn = kP_gfn2_shell_n[3 * zi + k];
-        const int ng = kP_gfn2_shell_ngauss[3 * zi + k];
-        const double zeta = kP_gfn2_shell_slater[3 * zi + k];
+        const int l = g1 ? kP_gfn1_shell_l[3 * zi + k] : kP_gfn2_shell_l[3 * zi + k];
+        const int pn = g1 ? kP_gfn1_shell_n[3 * zi + k] : kP_gfn2_shell_n[3 * zi + k];
+        const int ng = g1 ? kP_gfn1_shell_ngauss[3 * zi + k] : kP_gfn2_shell_ngauss[3 * zi + k];
+        const double zeta = g1 ? kP_gfn1_shell_slater[3 * zi + k] : kP_gfn2_shell_slater[3 * zi + k];
         std::vector<double> al, co;
-        if (!sto_expand(pn, l, ng, zeta, al, co)) {
+        if (!(g1 ? sto_expand_gfn1(pn, l, ng, zeta, al, co) : sto_expand(pn, l, ng, zeta, al, co))) {
           error = "unsupported STO-nG shell in the parameter tables";
           return XTBLOOM_STATUS_INTERNAL_ERROR;
         }
@@ -556,13 +627,25 @@ xtbloom_status_t build_topology(Engine::Impl& m, const HostBatch& hb, cudaStream
         sh_np.push_back((int32_t)al.size());
         p_alpha.insert(p_alpha.end(), al.begin(), al.end());
         p_coeff.insert(p_coeff.end(), co.begin(), co.end());
-        sh_level.push_back(kP_gfn2_shell_level[3 * zi + k] * kEvToHartree);
-        sh_kcn.push_back(kP_gfn2_shell_kcn[3 * zi + k] * kEvToHartree);
-        sh_shpoly.push_back(kP_gfn2_shell_shpoly[3 * zi + k]);
+        if (g1) {
+          // GFN1: levels and CN scales in eV (xTB's 27.21138505 conversion);
+          // third order per atom (no shell scaling)
+          sh_level.push_back(kP_gfn1_shell_level[3 * zi + k] * kEvToHartree);
+          sh_kcn.push_back(kP_gfn1_shell_kcn[3 * zi + k] * kEvToHartree);
+          sh_shpoly.push_back(kP_gfn1_shell_shpoly[3 * zi + k]);
+          sh_eta.push_back(kP_gfn1_gam[zi] * kP_gfn1_shell_hubbard_scale[3 * zi + k]);
+          sh_g3.push_back(kP_gfn1_gam3[zi]);
+          sh_val.push_back(kP_gfn1_shell_valence[3 * zi + k]);
+        } else {
+          sh_level.push_back(kP_gfn2_shell_level[3 * zi + k] * kEvToHartree);
+          sh_kcn.push_back(kP_gfn2_shell_kcn[3 * zi + k] * kEvToHartree);
+          sh_shpoly.push_back(kP_gfn2_shell_shpoly[3 * zi + k]);
+          sh_eta.push_back(kP_gfn2_gam[zi] * kP_gfn2_shell_hubbard_scale[3 * zi + k]);
+          sh_g3.push_back(kP_gfn2_gam3[zi] * m.model_gfn2.es3_scale[l]);
+          sh_val.push_back(1);
+        }
         sh_zeta.push_back(zeta);
-        sh_eta.push_back(kP_gfn2_gam[zi] * kP_gfn2_shell_hubbard_scale[3 * zi + k]);
-        sh_g3.push_back(kP_gfn2_gam3[zi] * m.model.es3_scale[l]);
-        const double ro = kP_gfn2_shell_refocc[3 * zi + k];
+        const double ro = g1 ? kP_gfn1_shell_refocc[3 * zi + k] : kP_gfn2_shell_refocc[3 * zi + k];
         sh_refocc.push_back(ro);
         nel += ro;
         for (int q = 0; q < 2 * l + 1; ++q) {
@@ -601,7 +684,7 @@ xtbloom_status_t build_topology(Engine::Impl& m, const HostBatch& hb, cudaStream
     max_n = std::max(max_n, ao_local);
     max_atoms = std::max(max_atoms, na);
     max_shells = std::max(max_shells, ns);
-    max_dim = std::max(max_dim, hb.nch[sy] * (ns + 9 * na));
+    max_dim = std::max(max_dim, hb.nch[sy] * (g1 ? ns : ns + 9 * na));
     max_pairs = std::max<int64_t>(max_pairs, (int64_t)na * (na + 1) / 2);
   }
   shell_off[B] = shell;
@@ -614,7 +697,7 @@ xtbloom_status_t build_topology(Engine::Impl& m, const HostBatch& hb, cudaStream
     const int64_t na = atom_off[sy + 1] - atom_off[sy];
     mat_off[sy + 1] = mat_off[sy] + n * n;
     gam_off[sy + 1] = gam_off[sy] + k * k;
-    vec_off[sy + 1] = vec_off[sy] + hb.nch[sy] * (k + 9 * na);
+    vec_off[sy + 1] = vec_off[sy] + hb.nch[sy] * (g1 ? k : k + 9 * na);
     scr_off[sy + 1] = scr_off[sy] + 128 * 5 * n;
   }
   // largest systems first
@@ -720,6 +803,7 @@ xtbloom_status_t build_topology(Engine::Impl& m, const HostBatch& hb, cudaStream
             upload(m.at_mprad, at_mprad, s) && upload(m.at_mpvcn, at_mpvcn, s) &&
             upload(m.at_dk, at_dk, s) && upload(m.at_qk, at_qk, s) &&
             upload(m.at_rep_sa, at_rep_sa, s) && upload(m.at_rep_z, at_rep_z, s) &&
+            upload(m.at_xbond, at_xbond, s) && upload(m.sh_val, sh_val, s) &&
             upload(m.sh_atom, sh_atom, s) && upload(m.sh_l, sh_l, s) && upload(m.sh_ao, sh_ao, s) &&
             upload(m.sh_p0, sh_p0, s) && upload(m.sh_np, sh_np, s) &&
             upload(m.sh_level, sh_level, s) && upload(m.sh_kcn, sh_kcn, s) &&
@@ -796,7 +880,9 @@ __global__ void k_publish(DevTopo t, const int32_t* status, const double* free_e
   const double* ef = t.efield != nullptr ? t.efield + 3 * s : nullptr;
   if (threadIdx.x == 0)
     energy[s] = ok ? free_energy[s] + terms[kTermCount * (int64_t)s + kTermRep] +
-                         terms[kTermCount * (int64_t)s + kTermAtm]
+                         terms[kTermCount * (int64_t)s + kTermAtm] +
+                         terms[kTermCount * (int64_t)s + kTermDisp3] +
+                         terms[kTermCount * (int64_t)s + kTermXb]
                : nan;
   double mu[3] = {0.0, 0.0, 0.0};
   for (int64_t a = a0 + threadIdx.x; a < a1; a += blockDim.x) {
@@ -999,6 +1085,8 @@ xtbloom_status_t Engine::compute(const ComputeRequest& req, std::string& error) 
       return XTBLOOM_STATUS_INVALID_ARGUMENT;
     }
   }
+  hb.model = req.model;
+  m.model = hb.model == XTBLOOM_MODEL_GFN1_XTB ? m.model_gfn1 : m.model_gfn2;
   if (!m.topo_valid || !same_topology(m.topo, hb)) {
     m.topo_valid = false;
     xtbloom_status_t st = build_topology(m, hb, s, error);
@@ -1795,6 +1883,28 @@ xtbloom_status_t Engine::compute(const ComputeRequest& req, std::string& error) 
   return XTBLOOM_STATUS_SUCCESS;
 }
 
+namespace {
+
+// FP64 issue-rate probe for the roofline's FP64 bound: every thread runs
+// eight independent FMA chains (2 flops each per step); the sum is written
+// only when it is impossible, so the compiler keeps every FMA.
+__global__ void __launch_bounds__(256) k_fp64_peak(int steps, double seed, double* sink) {
+  double a[8];
+#pragma unroll
+  for (int k = 0; k < 8; ++k) a[k] = seed + 1e-3 * (threadIdx.x + k);
+  const double b = 1.0 - 1e-9, c = 1e-9;
+  for (int i = 0; i < steps; ++i) {
+#pragma unroll
+    for (int k = 0; k < 8; ++k) a[k] = fma(a[k], b, c);
+  }
+  double t = 0.0;
+#pragma unroll
+  for (int k = 0; k < 8; ++k) t += a[k];
+  if (t == -12345.678) sink[0] = t;
+}
+
+}  // namespace
+
 xtbloom_status_t Engine::debug_fetch(const std::string& name, int64_t system, double* out,
                                      size_t capacity, size_t* count, std::string& error) {
   Impl& m = *impl_;
@@ -1850,6 +1960,38 @@ xtbloom_status_t Engine::debug_fetch(const std::string& name, int64_t system, do
     }
     for (int64_t i = 0; i < m.nsys; ++i) out[i] = (double)v[i];
     *count = (size_t)m.nsys;
+    return XTBLOOM_STATUS_SUCCESS;
+  }
+  if (name == "fp64_peak") {
+    // measured FP64 FMA throughput of this device in TFLOP/s (best of 3 runs
+    // of 2 x 8 x steps flops per thread on every SM)
+    if (capacity < 1) {
+      error = "capacity too small";
+      return XTBLOOM_STATUS_INVALID_ARGUMENT;
+    }
+    cudaSetDevice(device_);
+    Dbuf sink;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    if (!sink.reserve(64) || cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess) {
+      error = "failed to set up the FP64 probe";
+      return XTBLOOM_STATUS_ALLOCATION_FAILED;
+    }
+    const int blocks = sm_count() * 8, steps = 1 << 14;
+    double best = 0.0;
+    for (int rep = 0; rep < 4; ++rep) {
+      cudaEventRecord(e0, stream_);
+      k_fp64_peak<<<blocks, 256, 0, stream_>>>(steps, 1.0 + rep, sink.as<double>());
+      cudaEventRecord(e1, stream_);
+      cudaEventSynchronize(e1);
+      float ms = 0.f;
+      cudaEventElapsedTime(&ms, e0, e1);
+      const double tf = 2.0 * 8.0 * steps * (double)blocks * 256.0 / (ms * 1e-3) / 1e12;
+      if (rep > 0) best = std::max(best, tf);   // the first run warms the clocks up
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    out[0] = best;
+    *count = 1;
     return XTBLOOM_STATUS_SUCCESS;
   }
   if (name == "refine_stats" && system == -1) {

@@ -18,6 +18,7 @@ struct HostBatch {
   std::vector<double> qmol;
   std::vector<int32_t> uhf;
   std::vector<int32_t> nch;   // spin channels per system (1 or 2)
+  int32_t model = 2;          // XTBLOOM_MODEL_GFN2_XTB or XTBLOOM_MODEL_GFN1_XTB
 };
 
 struct ComputeRequest {
@@ -25,6 +26,7 @@ struct ComputeRequest {
   const xtbloom_compute_options_t* options = nullptr;
   const xtbloom_batch_result_t* result = nullptr;
   // normalised options
+  int32_t model = 2;   // XTBLOOM_MODEL_GFN2_XTB or XTBLOOM_MODEL_GFN1_XTB
   uint32_t flags = 0;
   int32_t max_iter = 250;
   double ctol = 1e-6, etol = 1e-8, kt = 0.0;

@@ -12,6 +12,7 @@
 //    repulsion.cpp:93-176).
 //  * k_cn_chain: chain rule through both coordination numbers.
 #include "classical.cuh"
+#include "h0.cuh"
 #include "integrals.cuh"
 #include "kernels.cuh"
 
@@ -66,11 +67,7 @@ __global__ void __launch_bounds__(128) k_force_pairs(ForceArgs f) {
       const double vmb = uhf ? f.vmag[bs] : 0.0;
       // H0 factor pieces
       const double avg = 0.5 * (lev(t, bs, f.cn) + lev(t, ks, f.cn));
-      const double zi = t.sh_zeta[bs], zj = t.sh_zeta[ks];
-      const double zs = pow(2.0 * sqrt(zi * zj) / (zi + zj), t.m.wexp);
-      const double den = t.at_en[gB] - t.at_en[gA];
-      const double ps = zs * (1.0 + t.m.enscale * den * den) *
-                        t.m.shell_pair_scale[lb * 3 + lk] * t.m.pair_scale_default;
+      const double ps = h0_pair_scale(t, bs, ks);
       const double rr = sqrt(r / (t.at_rad[gB] + t.at_rad[gA]));
       const double p1 = 1.0 + t.sh_shpoly[bs] * rr, p2 = 1.0 + t.sh_shpoly[ks] * rr;
       const double spat = ps * p1 * p2;
@@ -206,10 +203,13 @@ __global__ void __launch_bounds__(256) k_classical(ForceArgs f) {
     double q = 0.0;
     for (int sh = t.atom_sh[g]; sh < t.atom_sh[g + 1]; ++sh) q += f.qsh[sh];
     qat[i] = q;
-    d4_weights(t, t.Z[g], f.cn_d4[g], q, w + kMaxD4Refs * i, wcn + kMaxD4Refs * i, nullptr);
+    if (t.m.gfn1)   // D3 reference weights at the GFN1 CN, and their CN derivatives
+      d3_weights(t, t.Z[g], f.cn[g], w + kMaxD4Refs * i, wcn + kMaxD4Refs * i);
+    else
+      d4_weights(t, t.Z[g], f.cn_d4[g], q, w + kMaxD4Refs * i, wcn + kMaxD4Refs * i, nullptr);
   }
   __syncthreads();
-  double erep = 0.0;
+  double erep = 0.0, edisp = 0.0;
   const double* gam = f.gam + t.gam_off[s];
   const int64_t npair = (int64_t)na * (na - 1) / 2;
   for (int64_t p = tid; p < npair; p += bs) {
@@ -226,13 +226,27 @@ __global__ void __launch_bounds__(256) k_classical(ForceArgs f) {
     if (r2 <= 625.0) {
       const bool light = t.Z[gi] <= 2 && t.Z[gj] <= 2;
       const double k = light ? t.m.rep_klight : t.m.rep_kexp;
-      const double rp = light ? r : r * sqrt(r);
+      // r^k: k = 1.5 for heavy pairs; GFN2 takes k = 1 for pairs of H/He
+      const double rp = k == 1.0 ? r : (k == 1.5 ? r * sqrt(r) : pow(r, k));
       const double pa = t.at_rep_sa[gi] * t.at_rep_sa[gj];
       const double pe = t.at_rep_z[gi] * t.at_rep_z[gj] * exp(-pa * rp) / r;
       erep += pe;
       gs -= (pa * k * rp + 1.0) * pe / r2;
     }
-    if (grad) {
+    // GFN1: D3(BJ) dispersion (not self-consistent; model/gfn1/d3.cpp:690-735)
+    if (t.m.gfn1 && r2 >= DBL_EPSILON && r2 <= 2500.0) {
+      double dci, dcj, e, der;
+      const double c6 = d3_c6(t, t.Z[gi], t.Z[gj], w + kMaxD4Refs * i, wcn + kMaxD4Refs * i,
+                              w + kMaxD4Refs * j, wcn + kMaxD4Refs * j, dci, dcj);
+      d3_pair(t, t.Z[gi], t.Z[gj], r2, e, der);
+      edisp += c6 * e;
+      if (grad) {
+        gs += c6 * der;
+        fix_add(&acn[i], dci * e);
+        fix_add(&acn[j], dcj * e);
+      }
+    }
+    if (grad && !t.m.gfn1) {
       // ES2 at fixed shell charges
       double wsum = 0.0;
       for (int x = t.atom_sh[gi]; x < t.atom_sh[gi + 1]; ++x)
@@ -299,6 +313,16 @@ __global__ void __launch_bounds__(256) k_classical(ForceArgs f) {
         fix_add(&acn[i], 0.5 * erd * f.dmrad[gi]);
       }
     }
+    if (grad && t.m.gfn1) {
+      // ES2 at fixed shell charges
+      double wsum = 0.0;
+      for (int x = t.atom_sh[gi]; x < t.atom_sh[gi + 1]; ++x)
+        for (int y = t.atom_sh[gj]; y < t.atom_sh[gj + 1]; ++y) {
+          const double gv = gam[(int64_t)(x - s0) * ns + (y - s0)];
+          wsum += f.qsh[x] * f.qsh[y] * gv * gv * gv;
+        }
+      gs -= wsum;
+    }
     if (grad) {
       for (int c = 0; c < 3; ++c) {
         fix_add(&gr[3 * i + c], gs * d[c]);
@@ -307,7 +331,11 @@ __global__ void __launch_bounds__(256) k_classical(ForceArgs f) {
     }
   }
   erep = block_sum(erep, red);
-  if (tid == 0) f.terms[kTermCount * (int64_t)s + kTermRep] = erep;
+  edisp = block_sum(edisp, red);
+  if (tid == 0) {
+    f.terms[kTermCount * (int64_t)s + kTermRep] = erep;
+    if (t.m.gfn1) f.terms[kTermCount * (int64_t)s + kTermDisp3] = edisp;
+  }
   if (!grad) return;
   for (int i = tid; i < na; i += bs) {
     const int64_t g = a0 + i;
@@ -486,6 +514,87 @@ __global__ void k_atm_combine(ForceArgs f, int parts) {
   f.terms[kTermCount * (int64_t)s + kTermAtm] = e;
 }
 
+// GFN1 halogen-bond correction (model/gfn1/halogen.cpp:253-470): every donor
+// (Cl, Br, I, At) with an acceptor (N, O, P, S) within 20 bohr takes its
+// nearest atom as the bond axis; each acceptor within 20 bohr adds
+//   E = xbond_X * ((1 - cos)/2)^6 * (1 - c r^6) / (1 + r^12),
+// cos between donor->acceptor and donor->axis, r = R_XA / (1.3 (R_X + R_A)),
+// c = 0.44.  A thread per donor; not self-consistent (once after the SCC).
+__device__ __forceinline__ bool xb_donor(int z) { return z == 17 || z == 35 || z == 53 || z == 85; }
+__device__ __forceinline__ bool xb_acceptor(int z) { return z == 7 || z == 8 || z == 15 || z == 16; }
+
+__global__ void __launch_bounds__(128) k_halogen(ForceArgs f) {
+  __shared__ double red[33];
+  const DevTopo& t = f.t;
+  const int s = f.list[blockIdx.x];
+  const int64_t a0 = t.atom_off[s];
+  const int na = (int)(t.atom_off[s + 1] - a0);
+  constexpr double kCut = 20.0;
+  double e = 0.0;
+  auto dist = [&](int64_t p, int64_t q, double* d) {
+    for (int c = 0; c < 3; ++c) d[c] = t.pos[3 * q + c] - t.pos[3 * p + c];
+    return sqrt(d[0] * d[0] + d[1] * d[1] + d[2] * d[2]);
+  };
+  for (int x = threadIdx.x; x < na; x += blockDim.x) {
+    const int64_t gx = a0 + x;
+    if (!xb_donor(t.Z[gx])) continue;
+    bool active = false;
+    for (int y = 0; y < na && !active; ++y) {
+      double d[3];
+      if (xb_acceptor(t.Z[a0 + y]) && dist(gx, a0 + y, d) <= kCut) active = true;
+    }
+    if (!active) continue;
+    int nb = -1;
+    double best = DBL_MAX;
+    for (int y = 0; y < na; ++y) {   // nearest atom; the lowest index on ties
+      double d[3];
+      const double r = dist(gx, a0 + y, d);
+      if (r > 0.0 && r < best) {
+        best = r;
+        nb = y;
+      }
+    }
+    if (nb < 0) continue;
+    const int64_t gn = a0 + nb;
+    double un[3];
+    const double rn = dist(gx, gn, un);
+    for (int c = 0; c < 3; ++c) un[c] /= rn;
+    const double rx = t.m.xb_radius_scale * t.at_rad[gx];
+    for (int y = 0; y < na; ++y) {
+      const int64_t ga = a0 + y;
+      if (!xb_acceptor(t.Z[ga]) || ga == gn) continue;
+      double ua[3];
+      const double ra = dist(gx, ga, ua);
+      if (ra > kCut) continue;
+      for (int c = 0; c < 3; ++c) ua[c] /= ra;
+      const double cs = ua[0] * un[0] + ua[1] * un[1] + ua[2] * un[2];
+      const double ab = 0.5 * (1.0 - cs);
+      const double ab2 = ab * ab;
+      const double ang = ab2 * ab2 * ab2;
+      const double rho = ra / (rx + t.m.xb_radius_scale * t.at_rad[ga]);
+      const double rho2 = rho * rho, rho6 = rho2 * rho2 * rho2, rho12 = rho6 * rho6;
+      const double den = 1.0 + rho12;
+      const double rad = (1.0 - t.m.xb_damping * rho6) / den;
+      const double str = t.at_xbond[gx];
+      e += str * ang * rad;
+      if (!f.want_grad) continue;
+      const double drad = 6.0 * rho6 / ra * (t.m.xb_damping * rho12 - 2.0 * rho6 - t.m.xb_damping) / (den * den);
+      const double dang = -3.0 * ab2 * ab2 * ab;
+      for (int c = 0; c < 3; ++c) {
+        const double dca = (un[c] - cs * ua[c]) / ra;
+        const double dcn = (ua[c] - cs * un[c]) / rn;
+        const double ga_c = str * (rad * dang * dca + ang * drad * ua[c]);
+        const double gn_c = str * rad * dang * dcn;
+        fix_add(&f.grad[3 * ga + c], ga_c);
+        fix_add(&f.grad[3 * gn + c], gn_c);
+        fix_add(&f.grad[3 * gx + c], -(ga_c + gn_c));
+      }
+    }
+  }
+  e = block_sum(e, red);
+  if (threadIdx.x == 0) f.terms[kTermCount * (int64_t)s + kTermXb] = e;
+}
+
 void launch_classical(const ForceArgs& f, int max_atoms, int max_shells, cudaStream_t stream) {
   (void)max_shells;
   if (f.count == 0) return;
@@ -497,6 +606,10 @@ void launch_classical(const ForceArgs& f, int max_atoms, int max_shells, cudaStr
   (void)attr_t;
   (void)attr_a;
   k_classical<<<f.count, 256, sm, stream>>>(f);
+  if (f.t.m.gfn1) {   // no three-body dispersion (s9 = 0); the halogen-bond term instead
+    k_halogen<<<f.count, 128, 0, stream>>>(f);
+    return;
+  }
   k_atm_table<<<f.count, 256, (size_t)2 * kMaxD4Refs * max_atoms * sizeof(double), stream>>>(f);
   // few systems: each system's pairs over several CTAs
   const int parts = std::max(1, std::min(16, 2 * sm_count() / f.count));
@@ -520,14 +633,22 @@ __global__ void __launch_bounds__(256) k_cn_chain(ForceArgs f) {
     const double r2 = d[0] * d[0] + d[1] * d[1] + d[2] * d[2];
     const double r = sqrt(r2);
     double sc = 0.0;
-    if (r2 <= 625.0) {
+    if (t.m.gfn1) {
+      // d/dr of 1 / (1 + exp(-k (rad / r - 1))) (model/gfn1/coordination.cpp:230-245)
+      if (r2 <= 625.0 && r2 > 1e-12) {
+        const double rad = t.at_rcov[gi] + t.at_rcov[gj];
+        const double fv = logistic(t.m.cn_steepness * (rad / r - 1.0));
+        const double dv = -t.m.cn_steepness * rad * fv * (1.0 - fv) / r2;
+        sc += (fix_value(f.acn[gi]) + fix_value(f.acn[gj])) * dv / r;
+      }
+    } else if (r2 <= 625.0) {
       const double rad = t.at_rcov[gi] + t.at_rcov[gj];
       const double f1 = logistic(10.0 * (rad / r - 1.0));
       const double f2 = logistic(20.0 * ((rad + 2.0) / r - 1.0));
       const double dv = -(10.0 * rad * f1 * (1.0 - f1) * f2 + 20.0 * (rad + 2.0) * f2 * (1.0 - f2) * f1) / r2;
       sc += (fix_value(f.acn[gi]) + fix_value(f.acn[gj])) * dv / r;
     }
-    if (r2 <= 900.0) {
+    if (!t.m.gfn1 && r2 <= 900.0) {
       const int zi = t.Z[gi] - 1, zj = t.Z[gj] - 1;
       const double rc = t.d4_rcov[zi] + t.d4_rcov[zj];
       const double den = fabs(t.d4_en[zi] - t.d4_en[zj]);

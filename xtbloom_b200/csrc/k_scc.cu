@@ -31,18 +31,16 @@ __global__ void k_sad_init(SccArgs a) {
       a.qsh[sh] = q;
       a.mx_cur[v0 + (sh - s0)] = q;
     }
-    for (int c = 0; c < 3; ++c) {
-      a.dip[3 * g + c] = 0.0;
-      a.mx_cur[v0 + ns + 3 * i + c] = 0.0;
-    }
-    for (int c = 0; c < 6; ++c) {
-      a.qp[6 * g + c] = 0.0;
-      a.mx_cur[v0 + ns + 3 * na + 6 * i + c] = 0.0;
+    for (int c = 0; c < 3; ++c) a.dip[3 * g + c] = 0.0;
+    for (int c = 0; c < 6; ++c) a.qp[6 * g + c] = 0.0;
+    if (!t.m.gfn1) {
+      for (int c = 0; c < 3; ++c) a.mx_cur[v0 + ns + 3 * i + c] = 0.0;
+      for (int c = 0; c < 6; ++c) a.mx_cur[v0 + ns + 3 * na + 6 * i + c] = 0.0;
     }
   }
   if (t.nch[s] == 2) {
     // the magnetisation block of the mixed vector starts at zero
-    const int64_t d1 = ns + 9 * na;
+    const int64_t d1 = charge_block(t, (int)ns, (int)na);
     for (int64_t i = threadIdx.x; i < d1; i += blockDim.x) a.mx_cur[v0 + d1 + i] = 0.0;
     for (int64_t i = threadIdx.x; i < ns; i += blockDim.x) a.qmag[s0 + i] = 0.0;
   }
@@ -62,7 +60,8 @@ __global__ void k_warm_init(SccArgs a) {
   const int64_t a0 = t.atom_off[s], na = t.atom_off[s + 1] - a0;
   const int64_t s0 = t.shell_off[s], ns = t.shell_off[s + 1] - s0;
   const int64_t v0 = t.vec_off[s];
-  const int64_t d1 = ns + 9 * na;
+  const bool mp = !t.m.gfn1;   // the mixed vector carries atomic multipoles (GFN2)
+  const int64_t d1 = charge_block(t, (int)ns, (int)na);
   for (int64_t i = threadIdx.x; i < ns; i += blockDim.x) {
     const double q = a.ck_qsh[s0 + i];
     a.qsh[s0 + i] = q;
@@ -71,12 +70,12 @@ __global__ void k_warm_init(SccArgs a) {
   for (int64_t i = threadIdx.x; i < 3 * na; i += blockDim.x) {
     const double v = a.ck_dip[3 * a0 + i];
     a.dip[3 * a0 + i] = v;
-    a.mx_cur[v0 + ns + i] = v;
+    if (mp) a.mx_cur[v0 + ns + i] = v;
   }
   for (int64_t i = threadIdx.x; i < 6 * na; i += blockDim.x) {
     const double v = a.ck_qp[6 * a0 + i];
     a.qp[6 * a0 + i] = v;
-    a.mx_cur[v0 + ns + 3 * na + i] = v;
+    if (mp) a.mx_cur[v0 + ns + 3 * na + i] = v;
   }
   if (t.nch[s] == 2) {
     for (int64_t i = threadIdx.x; i < ns; i += blockDim.x) {
@@ -85,10 +84,12 @@ __global__ void k_warm_init(SccArgs a) {
       a.mx_cur[v0 + d1 + i] = m;
     }
     // magnetisation multipoles: the raw values -pop of the converged iteration
-    for (int64_t i = threadIdx.x; i < 3 * na; i += blockDim.x)
-      a.mx_cur[v0 + d1 + ns + i] = -a.ck_mdip[3 * a0 + i];
-    for (int64_t i = threadIdx.x; i < 6 * na; i += blockDim.x)
-      a.mx_cur[v0 + d1 + ns + 3 * na + i] = -a.ck_mqp[6 * a0 + i];
+    if (mp) {
+      for (int64_t i = threadIdx.x; i < 3 * na; i += blockDim.x)
+        a.mx_cur[v0 + d1 + ns + i] = -a.ck_mdip[3 * a0 + i];
+      for (int64_t i = threadIdx.x; i < 6 * na; i += blockDim.x)
+        a.mx_cur[v0 + d1 + ns + 3 * na + i] = -a.ck_mqp[6 * a0 + i];
+    }
   }
   if (threadIdx.x == 0) {
     a.iterations[s] = 0;
@@ -121,7 +122,8 @@ __device__ __forceinline__ void potential_atoms(const SccArgs& a, const double* 
     double q = 0.0;
     for (int sh = t.atom_sh[g]; sh < t.atom_sh[g + 1]; ++sh) q += qsh[sh];
     qat[i] = q;
-    d4_weights(t, t.Z[g], a.cn_d4[g], q, w + kMaxD4Refs * i, nullptr, dwq + kMaxD4Refs * i);
+    if (!t.m.gfn1)
+      d4_weights(t, t.Z[g], a.cn_d4[g], q, w + kMaxD4Refs * i, nullptr, dwq + kMaxD4Refs * i);
   }
 }
 
@@ -193,7 +195,14 @@ __device__ __forceinline__ void potential_shells(const SccArgs& a, int s, const 
   for (int j = threadIdx.x; j < ns; j += blockDim.x) {
     const double acc = gamma_column_dot(gam, ns, j, sq);
     const int sh = (int)(s0 + j);
-    const double q = sq[j];
+    // third order: shell-resolved for GFN2; atom-resolved for GFN1, the
+    // potential Gamma_A q_A^2 on every shell of atom A (model/gfn1/es3.cpp:100-125)
+    double q = sq[j];
+    if (t.m.gfn1) {
+      const int at = t.sh_atom[sh];
+      q = 0.0;
+      for (int k = t.atom_sh[at]; k < t.atom_sh[at + 1]; ++k) q += sq[k - s0];
+    }
     a.vsh[sh] = acc + t.sh_g3[sh] * q * q + vat[t.sh_atom[sh] - a0] +
                 (t.vpc != nullptr ? t.vpc[sh] : 0.0);
   }
@@ -224,8 +233,10 @@ __global__ void __launch_bounds__(256) k_potential_atoms(SccArgs a, const double
     double acc[10];
 #pragma unroll
     for (int c = 0; c < 10; ++c) acc[c] = 0.0;
-    for (int j = lane; j < na; j += 32)
-      if (j != i) potential_gather_pair(a, dip, qp, a0, i, j, qat, w, dwq, acc);
+    // GFN1 has neither atomic multipoles nor self-consistent dispersion
+    if (!t.m.gfn1)
+      for (int j = lane; j < na; j += 32)
+        if (j != i) potential_gather_pair(a, dip, qp, a0, i, j, qat, w, dwq, acc);
     // charge response (b + A q)_i of the mixed charges (reference
     // periodic_embedding.cpp evaluate_system_unchecked)
     if (t.resp_A != nullptr) {
@@ -606,7 +617,8 @@ __global__ void __launch_bounds__(256) k_energy_mixer(SccArgs a) {
   const int na = (int)(t.atom_off[s + 1] - a0);
   const int64_t s0 = t.shell_off[s];
   const int ns = (int)(t.shell_off[s + 1] - s0);
-  const int d1 = ns + 9 * na;              // charge block
+  const int d1 = charge_block(t, ns, na);   // charge block
+  const bool mp = !t.m.gfn1;                // atomic multipoles in the mixed vector (GFN2)
   const bool uhf = t.nch[s] == 2;
   const int dim = uhf ? 2 * d1 : d1;
   double* raw = sm;                       // dim: [qsh, dip (3na), qp (6na)] (+ the same for m)
@@ -616,13 +628,17 @@ __global__ void __launch_bounds__(256) k_energy_mixer(SccArgs a) {
   const int tid = threadIdx.x, bs = blockDim.x;
   const int lane = tid & 31, warp = tid >> 5, nw = bs >> 5;
   for (int i = tid; i < ns; i += bs) raw[i] = t.sh_refocc[s0 + i] - a.pop_sh[s0 + i];
-  for (int i = tid; i < 3 * na; i += bs) raw[ns + i] = -a.pop_dip[3 * a0 + i];
-  for (int i = tid; i < 6 * na; i += bs) raw[ns + 3 * na + i] = -a.pop_qp[6 * a0 + i];
+  if (mp) {
+    for (int i = tid; i < 3 * na; i += bs) raw[ns + i] = -a.pop_dip[3 * a0 + i];
+    for (int i = tid; i < 6 * na; i += bs) raw[ns + 3 * na + i] = -a.pop_qp[6 * a0 + i];
+  }
   if (uhf) {
     // magnetisation m = pop_beta - pop_alpha (the charge-like sign of the populations)
     for (int i = tid; i < ns; i += bs) raw[d1 + i] = -a.pop_mag[s0 + i];
-    for (int i = tid; i < 3 * na; i += bs) raw[d1 + ns + i] = -a.pop_mdip[3 * a0 + i];
-    for (int i = tid; i < 6 * na; i += bs) raw[d1 + ns + 3 * na + i] = -a.pop_mqp[6 * a0 + i];
+    if (mp) {
+      for (int i = tid; i < 3 * na; i += bs) raw[d1 + ns + i] = -a.pop_mdip[3 * a0 + i];
+      for (int i = tid; i < 6 * na; i += bs) raw[d1 + ns + 3 * na + i] = -a.pop_mqp[6 * a0 + i];
+    }
   }
   __syncthreads();
   for (int i = tid; i < na; i += bs) {
@@ -630,7 +646,7 @@ __global__ void __launch_bounds__(256) k_energy_mixer(SccArgs a) {
     double q = 0.0;
     for (int sh = t.atom_sh[g]; sh < t.atom_sh[g + 1]; ++sh) q += raw[sh - s0];
     qat[i] = q;
-    d4_weights(t, t.Z[g], a.cn_d4[g], q, w + kMaxD4Refs * i, nullptr, nullptr);
+    if (mp) d4_weights(t, t.Z[g], a.cn_d4[g], q, w + kMaxD4Refs * i, nullptr, nullptr);
   }
   __syncthreads();
   // ES2 and ES3: thread j forms (gamma q)_j down column j of the symmetric
@@ -641,13 +657,19 @@ __global__ void __launch_bounds__(256) k_energy_mixer(SccArgs a) {
     const double acc = gamma_column_dot(gam, ns, j, raw);
     const double q = raw[j];
     e2 += 0.5 * q * acc;
-    e3 += t.sh_g3[s0 + j] * q * q * q / 3.0;
+    if (!t.m.gfn1) e3 += t.sh_g3[s0 + j] * q * q * q / 3.0;
   }
-  // AES2 onsite
+  // GFN1: atom-resolved third order Gamma_A q_A^3 / 3 (model/gfn1/es3.cpp:115-125)
+  if (t.m.gfn1)
+    for (int i = tid; i < na; i += bs) {
+      const double q = qat[i];
+      e3 += t.sh_g3[t.atom_sh[a0 + i]] * q * q * q / 3.0;
+    }
+  // AES2 onsite (GFN2 only: the loops below run for GFN1 with no multipoles)
   const double* rd = raw + ns;
   const double* rq = raw + ns + 3 * na;
   const double scl[6] = {1.0, 2.0, 1.0, 2.0, 2.0, 1.0};
-  for (int i = tid; i < na; i += bs) {
+  for (int i = tid; i < (mp ? na : 0); i += bs) {
     const int64_t g = a0 + i;
     double d2 = 0.0, q2 = 0.0;
     for (int c = 0; c < 3; ++c) d2 += rd[3 * i + c] * rd[3 * i + c];
@@ -655,7 +677,7 @@ __global__ void __launch_bounds__(256) k_energy_mixer(SccArgs a) {
     ea += t.at_dk[g] * d2 + t.at_qk[g] * q2;
   }
   // pairs: AES2 and D4 two-body
-  const int64_t npair = (int64_t)na * (na - 1) / 2;
+  const int64_t npair = mp ? (int64_t)na * (na - 1) / 2 : 0;
   for (int64_t p = tid; p < npair; p += bs) {
     int64_t si, fi;
     pair_from_index(p, si, fi);
@@ -869,10 +891,9 @@ __global__ void __launch_bounds__(256) k_energy_mixer(SccArgs a) {
     const double out = conv ? raw[i] : mixed;
     if (i < ns) {
       a.qsh[s0 + i] = out;
-    } else if (i < ns + 3 * na) {
-      a.dip[3 * a0 + (i - ns)] = out;
-    } else if (i < d1) {
-      a.qp[6 * a0 + (i - ns - 3 * na)] = out;
+    } else if (i < d1) {   // atomic multipoles (GFN2 only: for GFN1 d1 == ns)
+      if (i < ns + 3 * na) a.dip[3 * a0 + (i - ns)] = out;
+      else a.qp[6 * a0 + (i - ns - 3 * na)] = out;
     } else if (i < d1 + ns) {
       a.qmag[s0 + (i - d1)] = out;   // magnetisation multipoles live only in the mixer state
     }

@@ -7,6 +7,7 @@
 // common/integrals.cpp:700-865 and model/gfn2/h0.cpp:248-466 (integrals, H0),
 // model/gfn2/es2.cpp:211-300 (Coulomb kernel).
 #include "kernels.cuh"
+#include "h0.cuh"
 #include "integrals.cuh"
 
 namespace xtb {
@@ -33,6 +34,13 @@ __global__ void k_coordination(DevTopo t, const int32_t* list, double* cn, doubl
       const double dz = t.pos[3 * gi + 2] - t.pos[3 * gj + 2];
       const double r2 = dx * dx + dy * dy + dz * dz;
       const double r = sqrt(r2);
+      if (t.m.gfn1) {
+        // GFN1: exponential counting function, steepness 16, cutoff 25 bohr
+        // (model/gfn1/coordination.cpp:215-265); no D4 CN
+        if (r2 <= 625.0 && r2 > 1e-12)
+          c1 += logistic(t.m.cn_steepness * ((t.at_rcov[gi] + t.at_rcov[gj]) / r - 1.0));
+        continue;
+      }
       if (r2 <= 625.0) {
         const double rad = t.at_rcov[gi] + t.at_rcov[gj];
         const double f1 = logistic(10.0 * (rad / r - 1.0));
@@ -65,38 +73,6 @@ __global__ void k_coordination(DevTopo t, const int32_t* list, double* cn, doubl
     mrad[g] = t.at_mprad[g] + (t.m.mp_rmax - t.at_mprad[g]) * fr;
     dmrad[g] = (t.m.mp_rmax - t.at_mprad[g]) * t.m.mp_kexp * fr * (1.0 - fr);
   }
-}
-
-__device__ __forceinline__ double h0_shell_level(const DevTopo& t, int sh, const double* cn) {
-  return t.sh_level[sh] - t.sh_kcn[sh] * cn[t.sh_atom[sh]];
-}
-
-// zeta, electronegativity and angular-momentum scaling of one shell pair
-__device__ __forceinline__ double h0_pair_scale(const DevTopo& t, int i, int j) {
-  const double zi = t.sh_zeta[i], zj = t.sh_zeta[j];
-  const double zs = pow(2.0 * sqrt(zi * zj) / (zi + zj), t.m.wexp);
-  const double den = t.at_en[t.sh_atom[i]] - t.at_en[t.sh_atom[j]];
-  const double es = 1.0 + t.m.enscale * den * den;
-  return zs * es * t.m.shell_pair_scale[t.sh_l[i] * 3 + t.sh_l[j]] * t.m.pair_scale_default;
-}
-
-// Distance polynomial of a shell pair on different atoms and its radial derivative.
-__device__ __forceinline__ void h0_polynomial(const DevTopo& t, int i, int j, double r, double& poly,
-                                              double& dpoly) {
-  const double rr = sqrt(r / (t.at_rad[t.sh_atom[i]] + t.at_rad[t.sh_atom[j]]));
-  const double p1 = 1.0 + t.sh_shpoly[i] * rr;
-  const double p2 = 1.0 + t.sh_shpoly[j] * rr;
-  poly = p1 * p2;
-  dpoly = (t.sh_shpoly[i] * p2 + t.sh_shpoly[j] * p1) * rr / (2.0 * r);
-}
-
-__device__ __forceinline__ double h0_factor(const DevTopo& t, int i, int j, const double* cn,
-                                            double r, bool same_atom) {
-  const double avg = 0.5 * (h0_shell_level(t, i, cn) + h0_shell_level(t, j, cn));
-  if (same_atom) return avg;
-  double poly, dpoly;
-  h0_polynomial(t, i, j, r, poly, dpoly);
-  return avg * h0_pair_scale(t, i, j) * poly;
 }
 
 // One thread per atom pair (A >= B) of one system; writes every element of
@@ -172,7 +148,8 @@ __global__ void k_integrals(DevTopo t, const int32_t* list, const double* cn, do
 }
 
 // ES2 shell Coulomb matrix gamma_ij = 1/sqrt(r^2 + eta_ij^-2), onsite eta_ij,
-// eta_ij the arithmetic mean of the shell hardnesses (model/gfn2/es2.cpp:211-300).
+// eta_ij the arithmetic mean of the shell hardnesses for GFN2
+// (model/gfn2/es2.cpp:211-300), the harmonic mean for GFN1 (model/gfn1/es2.cpp).
 __global__ void k_es2_gamma(DevTopo t, const int32_t* list, double* gam) {
   const int s = list[blockIdx.y];
   const int64_t s0 = t.shell_off[s], k = t.shell_off[s + 1] - s0;
@@ -180,7 +157,8 @@ __global__ void k_es2_gamma(DevTopo t, const int32_t* list, double* gam) {
   if (e >= k * k) return;
   const int64_t i = e / k, j = e % k;
   const int gi = (int)(s0 + i), gj = (int)(s0 + j);
-  const double avg = 0.5 * (t.sh_eta[gi] + t.sh_eta[gj]);
+  const double ea = t.sh_eta[gi], eb = t.sh_eta[gj];
+  const double avg = t.m.gfn1 ? 2.0 / (1.0 / ea + 1.0 / eb) : 0.5 * (ea + eb);
   const int A = t.sh_atom[gi], B = t.sh_atom[gj];
   double g;
   if (A == B) {
