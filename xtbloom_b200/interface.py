@@ -90,11 +90,18 @@ class _Settings:
 
 
 class BatchCalculator:
-    """Ragged batch of molecules evaluated in one ``xtbloom_compute`` call."""
+    """Ragged batch of molecules evaluated in one ``xtbloom_compute`` call.
+
+    ``device_ids`` (an addition with no reference counterpart) spreads one
+    batch over several GPUs of the node: the systems are partitioned by
+    predicted cost (``sharding.plan_shards``), each GPU's context computes
+    its shard concurrently, and the results come back in system order.  The
+    iteration counts of each call weight the next call's partition."""
 
     def __init__(self, method: str, numbers: Sequence, positions: Sequence,
                  charges: Sequence[float] | None = None, uhf: Sequence[int] | None = None, *,
-                 device_id: int | None = None, max_scc_iterations: int = 250,
+                 device_id: int | None = None, device_ids: Sequence[int] | None = None,
+                 max_scc_iterations: int = 250,
                  charge_tolerance: float = 1.0e-6, energy_tolerance: float = 1.0e-8,
                  electronic_temperature: float = 300.0, scc_mixer_history: int = 8,
                  scc_mixer_damping: float = 0.4):
@@ -113,6 +120,14 @@ class BatchCalculator:
                                    energy_tolerance, electronic_temperature, scc_mixer_history,
                                    scc_mixer_damping)
         self._device_id = device_id
+        if device_ids is not None:
+            device_ids = [int(d) for d in device_ids]
+            if not device_ids or len(set(device_ids)) != len(device_ids):
+                raise ValueError("device_ids must name distinct devices")
+            if device_id is not None:
+                raise ValueError("give device_id or device_ids, not both")
+        self._device_ids = device_ids
+        self._last_iterations = None
 
     def set(self, attribute: str, value) -> None:
         self._settings.set(attribute, value)
@@ -123,11 +138,22 @@ class BatchCalculator:
             raise ValueError("update may change coordinates only")
         self._positions = new
 
+    def _compute(self, batch: abi.RaggedBatch, flags: int) -> dict:
+        if self._device_ids is None or len(self._device_ids) == 1:
+            dev = self._device_id if self._device_ids is None else self._device_ids[0]
+            lib = _library(dev)
+            return lib.compute(batch, self._settings.options(lib, flags))
+        from . import sharding
+        libs = [_library(d) for d in self._device_ids]
+        cost = sharding.predicted_cost(batch, self._model, self._last_iterations)
+        fns = [lambda b, lib=lib: lib.compute(b, self._settings.options(lib, flags)) for lib in libs]
+        return sharding.threaded_compute(batch, fns, cost)
+
     def singlepoint(self) -> Result:
-        lib = _library(self._device_id)
         batch = abi.ragged_from_lists(self._numbers, self._positions, self._charges, self._uhf)
         flags = abi.COMPUTE_ENERGY | abi.COMPUTE_FORCES | abi.COMPUTE_CHARGES
-        out = lib.compute(batch, self._settings.options(lib, flags))
+        out = self._compute(batch, flags)
+        self._last_iterations = np.asarray(out["scc_iterations"]).copy()
         forces = out["forces"].reshape(-1, 3)
         offs = batch.atom_offsets
         split = lambda a: [a[offs[i]:offs[i + 1]] for i in range(len(offs) - 1)]
