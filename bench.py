@@ -44,7 +44,12 @@ from xtbloom_b200 import workloads as W  # noqa: E402
 METRIC = ("GFN2 E+F systems/s on 1 B200: mixed vs FP64 path at |ΔE|≤1e-6 Eh; roofline %")
 STAGES = ["setup_integrals", "lowdin", "potential", "fock", "gemm_transform", "tridiag", "eigvals",
           "inverse_iteration", "backtransform", "gemm_density", "mulliken", "energy_mixer",
-          "compact", "force_pairs", "classical", "cn_chain", "publish"]
+          "compact", "force_pairs", "classical", "cn_chain", "publish", "refine"]
+# DRAM bytes per algorithmic byte of the Householder tridiagonalisation,
+# measured by ncu (dram__bytes_read.sum + dram__bytes_write.sum of
+# k_tridiag_smem on 512 systems of this workload: 6.38 MB read, 0 written,
+# for 6.38 MB of matrices read once): the kernel reads each matrix once.
+TRIDIAG_DRAM_PER_ALG_BYTE = 1.0
 REF_LIB = ROOT / "oracle" / "_ref" / "libxtbloom_ref.so"
 WORKLOAD = ("GFN2-xTB E+F+q, ragged batch of 4096 hetero-alkane chains C_nH_(2n+2), n uniform "
             "in 3..40, 10% interior CH2 -> O/NH, seed 1; SCC 1e-6/1e-8, 300 K, Broyden 8/0.4")
@@ -58,6 +63,9 @@ def parse():
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
     p.add_argument("--systems", type=int, default=4096)
     p.add_argument("--cpu-sample", type=int, default=192)
+    p.add_argument("--cpu-sample-1t", type=int, default=24,
+                   help="systems of the single-thread CPU baseline sample")
+    p.add_argument("--no-gfn1", action="store_true", help="skip the GFN1 radical-batch line")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--form", default="both", choices=["both", "mixed", "fp64"])
     p.add_argument("--graphs", type=int, default=1)
@@ -176,15 +184,18 @@ def reference_sample(batch, count: int):
     return W.subset(batch, idx), idx
 
 
-def cpu_run(sample, threads: int = 0) -> tuple[float, dict]:
+def cpu_run(sample, threads: int = 0, repeats: int = 3) -> tuple[float, dict]:
+    """Median wall time of `repeats` calls on the sample, after one equal
+    warm-up call (the reference arm's protocol)."""
     lib = abi.Library(str(REF_LIB), backend=abi.BACKEND_CPU, cpu_threads=threads)
-    warm = W.subset(sample, range(min(4, sample.batch_size)))
-    lib.compute(warm)
-    t0 = time.perf_counter()
     out = lib.compute(sample)
-    dt = time.perf_counter() - t0
+    times = []
+    for _ in range(repeats):
+        t0 = time.perf_counter()
+        out = lib.compute(sample)
+        times.append(time.perf_counter() - t0)
     lib.close()
-    return dt, out
+    return statistics.median(times), out
 
 
 def host_cores() -> int:
@@ -205,7 +216,7 @@ def run_reference(args, world, rank):
     sample, _ = reference_sample(batch, args.cpu_sample)
     lib = abi.Library(str(REF_LIB), backend=abi.BACKEND_CPU, cpu_threads=0)
     for _ in range(args.warmup):
-        lib.compute(W.subset(sample, range(min(8, sample.batch_size))))
+        lib.compute(sample)
     times = []
     for _ in range(args.steps):
         t0 = time.perf_counter()
@@ -280,6 +291,105 @@ def time_form(lib, args, world, stream, dev_batch, outs_d, host_batch, host_outs
             "timing_on": timing_on}
 
 
+def time_gfn1(args, world, local, stream):
+    """GFN1-xTB, spin-polarised: the 2048-radical workload (doublets, 15 %
+    with Cl/Br), FP64, graph replay, inputs resident in HBM; K timed calls
+    after W warm-up calls (CUDA events on the context stream)."""
+    import torch
+    from xtbloom_b200 import library_path
+    dev = torch.device("cuda", local)
+    b = W.config4(2048, seed=4)
+    B, N = b.batch_size, b.total_atoms
+    pos_d = torch.from_numpy(b.positions).to(dev)
+    db = abi.RaggedBatch(b.atom_offsets, b.atomic_numbers, pos_d, b.molecular_charges,
+                         b.unpaired_electrons, b.spin_channels)
+    outs = {"energies": torch.empty(B, dtype=torch.float64, device=dev),
+            "forces": torch.empty(3 * N, dtype=torch.float64, device=dev),
+            "atomic_charges": torch.empty(N, dtype=torch.float64, device=dev),
+            "scc_iterations": torch.empty(B, dtype=torch.int32, device=dev),
+            "scc_converged": torch.empty(B, dtype=torch.uint8, device=dev),
+            "per_system_status": torch.empty(B, dtype=torch.int32, device=dev)}
+    lib = abi.Library(library_path(), backend=abi.BACKEND_CUDA, device_id=local, stream=stream.cuda_stream)
+    lib.set_execution(abi.PRECISION_FP64, capture_graphs=True)
+    opts = lib.make_options(model=abi.MODEL_GFN1)
+    for _ in range(max(1, min(args.warmup, 2))):
+        lib.compute(db, opts, outs)
+    torch.cuda.synchronize()
+    barrier(world)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    steps = max(1, min(args.steps, 3))
+    e0.record(stream)
+    for _ in range(steps):
+        lib.compute(db, opts, outs)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    barrier(world)
+    ms = allreduce_max(e0.elapsed_time(e1) / steps, world)
+    st = outs["per_system_status"].cpu().numpy()
+    it = outs["scc_iterations"].cpu().numpy()
+    lib.close()
+    return {"workload": "GFN1-xTB E+F+q, 2048 radicals C_nH_(2n+1) (n 4..45, doublets, two spin "
+                        "channels, 15% with 1-3 H -> Cl/Br), seed 4; SCC 1e-6/1e-8, 300 K",
+            "value": world * B / (ms / 1e3), "unit": "systems/s", "ms_per_step": ms, "steps": steps,
+            "converged": int(np.sum(st == 0)), "systems": int(B),
+            "mean_scc_iterations": float(np.mean(it))}
+
+
+def time_strong(args, world, rank, local, stream):
+    """One 4096-system batch over all ranks (strong scaling): the systems are
+    partitioned by predicted cost (n_AO^3 per channel and iteration); one
+    untimed pass over the n^3-only partition gives every system's iteration
+    count, which re-weights the partition that is timed.  K device-resident
+    calls of each rank's shard, CUDA events, max over ranks."""
+    import torch
+    import torch.distributed as dist
+    from xtbloom_b200 import library_path
+    from xtbloom_b200 import sharding as S
+    dev = torch.device("cuda", local)
+    full = W.config1(args.systems, seed=1)
+    lib = abi.Library(library_path(), backend=abi.BACKEND_CUDA, device_id=local, stream=stream.cuda_stream)
+    lib.set_execution(abi.PRECISION_FP64, capture_graphs=args.graphs)
+    first = S.plan_shards(full, world)
+    out = lib.compute(S.shard(full, first[rank]))
+    gathered = [None] * world
+    dist.all_gather_object(gathered, {"scc_iterations": out["scc_iterations"]})
+    iters = S.scatter_back(full, first, gathered)["scc_iterations"]
+    cost = S.predicted_cost(full, iterations=iters)
+    shards = S.plan_shards(full, world, cost)
+    mine = S.shard(full, shards[rank])
+    B, N = mine.batch_size, mine.total_atoms
+    db = abi.RaggedBatch(mine.atom_offsets, mine.atomic_numbers, torch.from_numpy(mine.positions).to(dev),
+                         mine.molecular_charges, mine.unpaired_electrons)
+    outs = {"energies": torch.empty(B, dtype=torch.float64, device=dev),
+            "forces": torch.empty(3 * N, dtype=torch.float64, device=dev),
+            "atomic_charges": torch.empty(N, dtype=torch.float64, device=dev),
+            "scc_iterations": torch.empty(B, dtype=torch.int32, device=dev),
+            "scc_converged": torch.empty(B, dtype=torch.uint8, device=dev),
+            "per_system_status": torch.empty(B, dtype=torch.int32, device=dev)}
+    opts = lib.make_options()
+    for _ in range(max(1, min(args.warmup, 2))):
+        lib.compute(db, opts, outs)
+    torch.cuda.synchronize()
+    barrier(world)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        lib.compute(db, opts, outs)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    mine_ms = e0.elapsed_time(e1) / args.steps
+    barrier(world)
+    ms = allreduce_max(mine_ms, world)
+    lib.close()
+    loads = [float(cost[s].sum()) for s in shards]
+    return {"workload": f"one {args.systems}-system batch over {world} ranks (same batch as the headline, seed 1)",
+            "value": args.systems / (ms / 1e3), "unit": "systems/s", "ms_per_step": ms,
+            "scaling": "strong", "partition": "LPT over n_AO^3 x (channels x iterations + 2), "
+                                              "iterations from one untimed pass",
+            "systems_per_rank": [int(len(s)) for s in shards],
+            "predicted_load_imbalance": max(loads) / (sum(loads) / world)}
+
+
 def run_ours(args, world, rank, local):
     import torch
     from xtbloom_b200 import library_path
@@ -319,6 +429,14 @@ def run_ours(args, world, rank, local):
         return
     forms = {}
     results = {}
+    probe = abi.Library(library_path(), backend=abi.BACKEND_CUDA, device_id=local,
+                        stream=stream.cuda_stream)
+    fp64_peak = float(fetch(probe, "fp64_peak", 4)[0])
+    # the FP64 fixed point of the batch (charge tolerance 1e-10, not timed):
+    # both execution forms are compared with it
+    fixed = new_host_outs()
+    probe.compute(batch, probe.make_options(ctol=1e-10, etol=1e-13), fixed)
+    probe.close()
     clocks = ClockSampler(local)
     for form in (["fp64", "mixed"] if args.form == "both" else [args.form]):
         lib = abi.Library(library_path(), backend=abi.BACKEND_CUDA, device_id=local,
@@ -331,6 +449,10 @@ def run_ours(args, world, rank, local):
         results[form] = (host_outs, split)
         lib.close()
         torch.cuda.synchronize()
+    gfn1_line = None
+    if not args.no_gfn1:
+        gfn1_line = time_gfn1(args, world, local, stream)
+    strong = time_strong(args, world, rank, local, stream) if world > 1 else None
     clk = clocks.stop()
     h2d = (B + 1) * 8 + N * 4 + 3 * N * 8 + B * 8 + B * 4
     d2h = B * 8 + 3 * N * 8 + N * 8 + B * 4 + B + B * 4
@@ -356,18 +478,36 @@ def run_ours(args, world, rank, local):
     peaks = load_peaks()
     roofline = None
     if timing_on:
+        # The stage times come from the profiled pass (per-stage events, size
+        # buckets one after another, no graph replay); they are scaled to the
+        # timed graph pass by the ratio of the two step times.
+        scale = main["ms"] / main["ms_profiled"]
         dom = max(per_stage_ms, key=per_stage_ms.get)
-        dom_ms = per_stage_ms[dom]
+        dom_ms = per_stage_ms[dom] * scale
         calls = float(stage[STAGES.index(dom), 1]) / args.steps
         if dom in work:
-            byts = work[dom]["bytes"]
-            achieved = byts / (dom_ms / 1e3) / 1e9
-            roofline = {"kernel": dom, "bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"],
-                        "unit": "GB/s", "frac": achieved / peaks["hbm_gbs"], "traffic": None,
-                        "peak_source": peaks["source"],
-                        "fp64_tflops": work[dom]["flops"] / (dom_ms / 1e3) / 1e12,
-                        "share_of_step": dom_ms / main["ms_profiled"], "launches_per_step": calls,
-                        "timed_in": "profiled pass (per-stage CUDA events on the context stream)"}
+            byts, flops = work[dom]["bytes"], work[dom]["flops"]
+            gbs = byts / (dom_ms / 1e3) / 1e9
+            tfs = flops / (dom_ms / 1e3) / 1e12
+            f_hbm = gbs / peaks["hbm_gbs"]
+            f_fp64 = tfs / fp64_peak if fp64_peak else 0.0
+            compute = f_fp64 > f_hbm
+            roofline = {"kernel": dom, "bound": "tensor" if compute else "hbm",
+                        "compute_pipe": "fp64" if compute else None,
+                        "achieved": tfs if compute else gbs,
+                        "peak": fp64_peak if compute else peaks["hbm_gbs"],
+                        "unit": "TFLOP/s" if compute else "GB/s",
+                        "frac": max(f_hbm, f_fp64),
+                        "traffic": (byts / calls * TRIDIAG_DRAM_PER_ALG_BYTE) if dom == "tridiag" and calls else None,
+                        "frac_hbm": f_hbm, "frac_fp64": f_fp64,
+                        "achieved_gbs": gbs, "achieved_fp64_tflops": tfs,
+                        "peak_hbm_gbs": peaks["hbm_gbs"], "peak_hbm_source": peaks["source"],
+                        "peak_fp64_tflops": fp64_peak,
+                        "peak_fp64_source": "FP64 FMA probe on this device (xtbloom_b200_debug_fetch fp64_peak)",
+                        "share_of_step": per_stage_ms[dom] / main["ms_profiled"],
+                        "launches_per_step": calls,
+                        "algorithmic_bytes_per_launch": byts / calls if calls else None,
+                        "timed_in": "profiled pass per-stage CUDA events, scaled to the timed graph pass"}
         else:
             roofline = {"kernel": dom, "bound": "hbm", "achieved": None, "peak": peaks["hbm_gbs"],
                         "unit": "GB/s", "frac": None, "traffic": None, "share_of_step": dom_ms / ms}
@@ -380,13 +520,27 @@ def run_ours(args, world, rank, local):
         dE = float(np.max(np.abs(ref["energies"][ok] - energies[idx][ok]))) if ok.any() else None
         cpu = {"value": sample.batch_size / t, "unit": "systems/s", "cores": host_cores(),
                "kind": "reference",
-               "sample": f"{sample.batch_size} evenly spaced systems of the same batch, one call, cpu_threads=0"}
+               "sample": (f"{sample.batch_size} evenly spaced systems of the same batch, "
+                          "median of 3 calls after one warm-up call, cpu_threads=0 (affinity count)")}
+        sample1, _ = reference_sample(batch, args.cpu_sample_1t)
+        t1, _ = cpu_run(sample1, 1)
+        cpu["cpu_threads_1"] = {"value": sample1.batch_size / t1, "unit": "systems/s", "cores": 1,
+                                "sample": f"{sample1.batch_size} evenly spaced systems, median of 3 calls"}
     form_lines = {}
     for name, f in forms.items():
         form_lines[name] = {"value": world * B / (f["ms"] / 1e3), "ms_per_step": f["ms"],
                             "ms_per_step_profiled": f["ms_profiled"],
                             "e2e_value": world * B / (f["ms_e2e"] / 1e3),
                             "split_iteration_fraction": float(results[name][1].sum() / max(results[name][0]["scc_iterations"].sum(), 1))}
+    def vs_fixed(o):
+        ok = (o["per_system_status"] == 0) & (fixed["per_system_status"] == 0)
+        okat = np.repeat(ok, np.diff(batch.atom_offsets))
+        return {"max_abs_dE_Eh": float(np.abs(o["energies"][ok] - fixed["energies"][ok]).max()),
+                "max_abs_dF_Eh_per_bohr": float(np.abs(o["forces"].reshape(-1, 3)[okat]
+                                                       - fixed["forces"].reshape(-1, 3)[okat]).max()),
+                "max_abs_dq_e": float(np.abs(o["atomic_charges"][okat] - fixed["atomic_charges"][okat]).max())}
+    for name in forms:
+        form_lines[name]["vs_fp64_fixed_point"] = vs_fixed(results[name][0])
     mixed_vs = None
     if "mixed" in results and "fp64" in results:
         a, b = results["fp64"][0], results["mixed"][0]
@@ -421,6 +575,8 @@ def run_ours(args, world, rank, local):
         "parity": {"max_abs_dE_vs_reference_Eh": dE,
                    "converged": int(np.sum(status == 0)), "systems": int(B),
                    "mean_scc_iterations": float(np.mean(iters))},
+        "gfn1_radicals": gfn1_line,
+        "one_batch_over_ranks": strong,
         "stage_ms_per_step": per_stage_ms,
         "stage_share": {k: v / total_stage for k, v in per_stage_ms.items()},
     }
