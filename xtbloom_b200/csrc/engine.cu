@@ -1413,7 +1413,8 @@ xtbloom_status_t Engine::compute(const ComputeRequest& req, std::string& error) 
       if (wcap >= 8) {
         launch_backtransform_wy(gb, bk.count, bk.max_n, wcap, want, st);
       } else {
-        launch_backtransform(gb, gb.list, bk.count, bk.max_n, 0, st);
+        // a block of reflectors no longer fits in shared memory: row chunks
+        launch_backtransform_rows(gb, bk.count, bk.max_n, want, st);
       }
     };
     if (bks.size() > 1 && !m.prof.on && m.ensure_bucket_streams()) {

@@ -454,10 +454,14 @@ __device__ __forceinline__ double block_sum1(double v, double* buf) {
 // previous reflector's correction kw is applied here).  The tile's elements
 // are all loaded before any is stored and the row values come from registers
 // by shuffles, so the shared-memory loads issue back to back.
+// SQ: L is a square row-major matrix with leading dimension ld (the lower
+// triangle is used) instead of the packed triangle.
 constexpr int kTileRows = 16;
+template <bool SQ = false>
 __device__ __forceinline__ void fused_tile(double* L, int o, int m, int R0, int C0,
                                            const double* vi, const double* wi, double kw,
-                                           const double* vn, double* pw, int lane, bool want_mv) {
+                                           const double* vn, double* pw, int lane, bool want_mv,
+                                           int ld = 0) {
   const int cj = C0 + lane;
   const bool cok = cj < m;
   const double vn_c = cok ? vn[cj] : 0.0;
@@ -470,14 +474,14 @@ __device__ __forceinline__ void fused_tile(double* L, int o, int m, int R0, int 
   const int rows = min(kTileRows, m - R0);
   const int dcol = cj - R0;            // element (R0+i, cj) is on/below the diagonal iff dcol <= i
   double a[kTileRows];
-  const int base0 = pk32(o + R0, o) + cj;
+  const int base0 = SQ ? (o + R0) * ld + o + cj : pk32(o + R0, o) + cj;
   {
     int base = base0;
 #pragma unroll
     for (int i = 0; i < kTileRows; ++i) {
       const bool ok = i < rows && cok && dcol <= i;
       a[i] = ok ? L[base] : 0.0;
-      base += o + R0 + i + 1;
+      base += SQ ? ld : o + R0 + i + 1;
     }
   }
   double col = 0.0;
@@ -496,7 +500,7 @@ __device__ __forceinline__ void fused_tile(double* L, int o, int m, int R0, int 
     for (int i = 0; i < kTileRows; ++i) {
       const bool ok = i < rows && cok && dcol <= i;
       if (ok) L[base] = a[i];
-      base += o + R0 + i + 1;
+      base += SQ ? ld : o + R0 + i + 1;
     }
   }
   if (!want_mv) return;
@@ -657,6 +661,123 @@ __global__ void __launch_bounds__(NT) k_tridiag_smem(EigArgs g, const int32_t* l
   }
 }
 
+// Global-memory prefix of the same reduction for systems larger than the
+// shared-memory block: the first K = n - nloc reflectors are formed in place
+// on the lower triangle of the square matrix (L2 / HBM resident), with the
+// same four phases per column as the shared-memory kernel, so each column
+// reads and writes the trailing triangle once, in coalesced 16 x 32 tiles.
+// The last step (column K) applies reflector K-1 to the trailing block and
+// forms no reflector: the block from row/column K is then A^(K), which the
+// shared-memory kernel loads and finishes.  Only the vectors and the warps'
+// partial products live in shared memory ((4 + NT/32) n doubles).
+template <int NT>
+__global__ void __launch_bounds__(NT) k_tridiag_prefix(EigArgs g, int nloc) {
+  extern __shared__ double sm[];
+  constexpr int nw = NT / 32;
+  const int s = g.list[blockIdx.x];
+  if (g.only != nullptr && g.only[s] == 0) return;
+  const int n = g.nao[s];
+  const int K = n - nloc;
+  if (K <= 0) return;
+  double* A = g.A + g.mat_off[s];
+  double* d = g.d + g.ao_off[s];
+  double* e = g.e + g.ao_off[s];
+  double* tau = g.tau + g.ao_off[s];
+  const int tid = threadIdx.x;
+  const int lane = tid & 31, warp = tid >> 5;
+  double* vb0 = sm;
+  double* vb1 = vb0 + n;
+  double* wb0 = vb1 + n;
+  double* wb1 = wb0 + n;
+  double* priv = wb1 + n;             // nw x n
+  double* red = priv + nw * n;        // 2 x 32
+  __shared__ double s_alpha;
+  for (int k = tid; k < nw * n; k += NT) priv[k] = 0.0;
+  for (int k = tid; k < n; k += NT) vb0[k] = wb0[k] = vb1[k] = wb1[k] = 0.0;
+  __syncthreads();
+  int cur = 0;
+  double kw = 0.0;
+  for (int i = -1; i < K; ++i) {
+    const int o = i + 1, m = n - o;
+    const double* vi = cur ? vb1 : vb0;
+    const double* wi = cur ? wb1 : wb0;
+    double* vn = cur ? vb0 : vb1;
+    double* wn = cur ? wb0 : wb1;
+    const bool next = o < K && o + 3 <= n;
+    // (A) first column of the block, updated with (v_i, w_i)
+    double part = 0.0;
+    const double vi0 = vi[0], wi0 = fma(-kw, vi0, wi[0]);
+    for (int r = tid; r < m; r += NT) {
+      const int idx = (o + r) * n + o;
+      const double vr = vi[r];
+      const double c = A[idx] - (vr * wi0 + fma(-kw, vr, wi[r]) * vi0);
+      A[idx] = c;
+      if (r == 0) d[o] = c;
+      if (r >= 1) vn[r - 1] = c;
+      if (r == 1) s_alpha = c;
+      if (r >= 2) part += c * c;
+    }
+    const double xn2 = block_sum1<nw>(part, red);
+    // (B) reflector o (row o of the matrix keeps it, columns o+2..)
+    double ti = 0.0;
+    if (next) {
+      const double alpha = s_alpha;
+      double beta = alpha;
+      if (xn2 > 0.0) {
+        beta = -copysign(sqrt(alpha * alpha + xn2), alpha);
+        ti = (beta - alpha) / beta;
+        const double sc = 1.0 / (alpha - beta);
+        for (int k = tid + 1; k < m - 1; k += NT) {
+          const double vk = vn[k] * sc;
+          vn[k] = vk;
+          A[o * n + o + 1 + k] = vk;
+        }
+      } else {
+        for (int k = tid + 1; k < m - 1; k += NT) vn[k] = 0.0;
+      }
+      if (tid == 0) {
+        vn[0] = 1.0;
+        e[o] = beta;
+        tau[o] = ti;
+      }
+    } else {
+      for (int k = tid; k < m; k += NT) vn[k] = 0.0;
+    }
+    __syncthreads();
+    // (C) rank-2 update of the rest of the block, fused with A v_next
+    const int m1 = m - 1;
+    {
+      const int ntiles = tri_tiles(m1);
+      double* pw = priv + warp * n;
+      const bool mv = next && ti != 0.0;
+      for (int tl = warp; tl < ntiles; tl += nw) {
+        int R, C;
+        tri_tile(tl, R, C);
+        fused_tile<true>(A, o + 1, m1, R * kTileRows, C << 5, vi + 1, wi + 1, kw, vn, pw, lane, mv, n);
+      }
+    }
+    __syncthreads();
+    if (!next) break;
+    // (D) w_next = tau p and its correction kw = (tau/2)(tau p . v)
+    double pv = 0.0;
+    for (int k = tid; k < m1; k += NT) {
+      double t = 0.0;
+#pragma unroll
+      for (int w = 0; w < nw; ++w) {
+        t += priv[w * n + k];
+        priv[w * n + k] = 0.0;
+      }
+      t *= ti;
+      wn[k] = t;
+      pv += t * vn[k];
+    }
+    kw = 0.5 * ti * block_sum1<nw>(pv, red + 32);
+    cur ^= 1;
+  }
+}
+
+size_t tridiag_prefix_bytes(int n, int nt) { return ((4 + (size_t)nt / 32) * n + 64) * sizeof(double); }
+
 size_t tridiag_smem_bytes(int nl, int nt) {
   return ((size_t)nl * (nl + 1) / 2 + (4 + nt / 32) * (size_t)nl + 72) * sizeof(double);
 }
@@ -672,8 +793,15 @@ void launch_tridiag_smem(const EigArgs& g, const int32_t* list, int count, int m
   while (nloc > 2 && tridiag_smem_bytes(nloc, 256) > cap256) --nloc;
   if (max_n > nloc) {
     // columns that do not fit: reduced in global memory first
-    const size_t sm = (2 * (size_t)max_n + 40) * sizeof(double);
-    k_tridiag<<<count, 512, sm, stream>>>(g, nloc);
+    const size_t capp = allow_max_dynamic_smem(k_tridiag_prefix<512>);
+    const size_t bp = tridiag_prefix_bytes(max_n, 512);
+    if (bp <= capp) {
+      k_tridiag_prefix<512><<<count, 512, bp, stream>>>(g, nloc);
+    } else {
+      const size_t cap2 = allow_max_dynamic_smem(k_tridiag_prefix<256>);
+      (void)cap2;
+      k_tridiag_prefix<256><<<count, 256, tridiag_prefix_bytes(max_n, 256), stream>>>(g, nloc);
+    }
   }
   // 512 threads shorten one system's critical path (few systems active);
   // with many systems, several 256-thread CTAs per SM give more throughput.
@@ -1356,6 +1484,194 @@ void launch_backtransform_wy(const EigArgs& g, int count, int max_n, int max_m, 
   (void)cap;
   k_backtransform_wy<false><<<dim3(parts, count), 256, backtransform_wy_bytes(max_n, max_m), stream>>>(
       g, max_m, 0);
+}
+
+// ---------------------------------------------------------------------------
+// Large systems (a 32-reflector block of n rows no longer fits in shared
+// memory): the same compact-WY algebra with the reflectors streamed through
+// shared memory in chunks of rows.
+// ---------------------------------------------------------------------------
+constexpr int kWyRows = 128;
+
+// Rows r0 .. r0+rc-1 of the block's V (row stride WB + 1): one warp per
+// reflector, lanes along the reflector's row of the matrix (coalesced).
+__device__ __forceinline__ void load_wy_rows(const double* a, int n, int i0, int k, int r0, int rc,
+                                             double* Vc) {
+  constexpr int P = WB + 1;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  for (int c = warp; c < WB; c += nw) {
+    const double* row = a + (int64_t)(i0 + c) * n + i0 + 1;
+    for (int r = lane; r < rc; r += 32) {
+      const int rr = r0 + r;
+      double val = 0.0;
+      if (c < k) {
+        if (rr == c) val = 1.0;
+        else if (rr > c) val = row[rr];
+      }
+      Vc[r * P + c] = val;
+    }
+  }
+}
+
+// T factors as k_wy_factor, with G = V^T V accumulated over row chunks (each
+// thread sums its pairs in ascending row order, as the one-tile kernel does).
+__global__ void __launch_bounds__(256) k_wy_factor_rows(EigArgs g) {
+  extern __shared__ double sm[];
+  const int s = g.list[blockIdx.y];
+  if (g.only != nullptr && g.only[s] == 0) return;
+  const int n = g.nao[s];
+  const int nr = n - 2;
+  const int b = blockIdx.x;
+  const int i0 = b * WB;
+  if (nr <= 0 || i0 >= nr) return;   // uniform over the block
+  const int k = min(WB, nr - i0);
+  const int L = n - i0 - 1;
+  constexpr int P = WB + 1;
+  constexpr int RC = 2 * kWyRows;
+  double* Vc = sm;
+  double* G = Vc + RC * P;
+  double* T = G + WB * P;
+  const double* tau = g.tau + g.ao_off[s];
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  constexpr int kPer = WB * WB / 256;
+  double acc[kPer];
+#pragma unroll
+  for (int u = 0; u < kPer; ++u) acc[u] = 0.0;
+  for (int r0 = 0; r0 < L; r0 += RC) {
+    const int rc = min(RC, L - r0);
+    load_wy_rows(g.A + g.mat_off[s], n, i0, k, r0, rc, Vc);
+    __syncthreads();
+#pragma unroll
+    for (int u = 0; u < kPer; ++u) {
+      const int idx = tid + 256 * u;
+      const int p = idx / WB, q = idx - (idx / WB) * WB;
+      if (p < q && q < k)
+        for (int r = max(q - r0, 0); r < rc; ++r) acc[u] = fma(Vc[r * P + p], Vc[r * P + q], acc[u]);
+    }
+    __syncthreads();
+  }
+#pragma unroll
+  for (int u = 0; u < kPer; ++u) {
+    const int idx = tid + 256 * u;
+    const int p = idx / WB, q = idx - (idx / WB) * WB;
+    if (p < q && q < k) G[p * P + q] = acc[u];
+  }
+  __syncthreads();
+  if (warp == 0) {
+    const double tl = lane < k ? tau[i0 + lane] : 0.0;
+    for (int j = 0; j < WB; ++j) {
+      const double tj = __shfl_sync(0xffffffffu, tl, j);
+      double t = 0.0;
+      if (lane < j && j < k) {
+        for (int q = lane; q < j; ++q) t = fma(T[lane * P + q], G[q * P + j], t);
+        t *= -tj;
+      }
+      if (lane == j) t = tj;
+      T[lane * P + j] = (lane <= j) ? t : 0.0;
+      __syncwarp();
+    }
+    double* out = g.scratch + g.scratch_off[s] + (int64_t)b * WB * WB;
+    for (int j = 0; j < WB; ++j) out[lane * WB + j] = T[lane * P + j];
+  }
+}
+
+size_t wy_factor_rows_bytes() { return ((size_t)2 * kWyRows * (WB + 1) + 2 * WB * (WB + 1)) * sizeof(double); }
+
+// Back-transform of large systems: grid (vector slices of MC, systems); each
+// CTA keeps its MC eigenvectors in shared memory for the whole pass and, per
+// block (last to first), forms Y = V^T Z over row chunks, W = T Y, and
+// Z -= V W over the same chunks, the reflectors read from the matrix (L2).
+template <int MC>
+__global__ void __launch_bounds__(256) k_backtransform_rows(EigArgs g) {
+  extern __shared__ double sm[];
+  const int s = g.list[blockIdx.y];
+  if (g.only != nullptr && g.only[s] == 0) return;
+  const int n = g.nao[s];
+  const int mt = g.all_vectors ? n : g.nvec[s];
+  const int jbeg = blockIdx.x * MC;
+  const int m = min(mt - jbeg, MC);
+  const int nr = n - 2;
+  if (nr <= 0 || m <= 0) return;
+  const double* a = g.A + g.mat_off[s];
+  const double* tf = g.scratch + g.scratch_off[s];
+  double* gZ = g.Z + g.mat_off[s] + (int64_t)jbeg * n;
+  constexpr int P = WB + 1;
+  double* Z = sm;                          // MC x n
+  double* Vc = Z + (size_t)MC * n;         // kWyRows x P
+  double* T = Vc + kWyRows * P;            // WB x P
+  double* Y = T + WB * P;                  // WB x MC
+  double* W = Y + WB * MC;                 // WB x MC
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nw = blockDim.x >> 5;
+  for (int64_t k = tid; k < (int64_t)m * n; k += blockDim.x) Z[k] = gZ[k];
+  const int nblk = (nr + WB - 1) / WB;
+  for (int it = 0; it < nblk; ++it) {
+    const int b = nblk - 1 - it;
+    const int i0 = b * WB;
+    const int k = min(WB, nr - i0);
+    const int L = n - i0 - 1;
+    for (int idx = tid; idx < WB * WB; idx += blockDim.x)
+      T[(idx / WB) * P + (idx % WB)] = tf[(int64_t)b * WB * WB + idx];
+    for (int idx = tid; idx < WB * MC; idx += blockDim.x) Y[idx] = 0.0;
+    // Y = V^T Z: lane = reflector, warps over this CTA's vectors
+    for (int r0 = 0; r0 < L; r0 += kWyRows) {
+      const int rc = min(kWyRows, L - r0);
+      __syncthreads();
+      load_wy_rows(a, n, i0, k, r0, rc, Vc);
+      __syncthreads();
+      for (int j = warp; j < m; j += nw) {
+        const double* z = Z + (int64_t)j * n + i0 + 1 + r0;
+        double acc = 0.0;
+        for (int r = 0; r < rc; ++r) acc = fma(Vc[r * P + lane], z[r], acc);
+        Y[lane * MC + j] += acc;
+      }
+    }
+    __syncthreads();
+    // W = T Y (T upper triangular)
+    for (int idx = tid; idx < WB * MC; idx += blockDim.x) {
+      const int p = idx / MC, j = idx - (idx / MC) * MC;
+      double acc = 0.0;
+      for (int q = p; q < WB; ++q) acc = fma(T[p * P + q], Y[q * MC + j], acc);
+      W[idx] = acc;
+    }
+    // Z -= V W
+    for (int r0 = 0; r0 < L; r0 += kWyRows) {
+      const int rc = min(kWyRows, L - r0);
+      __syncthreads();
+      load_wy_rows(a, n, i0, k, r0, rc, Vc);
+      __syncthreads();
+      for (int idx = tid; idx < rc * m; idx += blockDim.x) {
+        const int j = idx / rc, r = idx - (idx / rc) * rc;
+        const int qmax = min(k, r0 + r + 1);
+        double acc = 0.0;
+        for (int q = 0; q < qmax; ++q) acc = fma(Vc[r * P + q], W[q * MC + j], acc);
+        Z[(int64_t)j * n + i0 + 1 + r0 + r] -= acc;
+      }
+    }
+    __syncthreads();
+  }
+  for (int64_t k = tid; k < (int64_t)m * n; k += blockDim.x) gZ[k] = Z[k];
+}
+
+template <int MC>
+size_t backtransform_rows_bytes(int n) {
+  return ((size_t)MC * n + kWyRows * (WB + 1) + WB * (WB + 1) + 2 * WB * MC) * sizeof(double);
+}
+
+void launch_backtransform_rows(const EigArgs& g, int count, int max_n, int want_m, cudaStream_t stream) {
+  if (count == 0) return;
+  const int nblk = std::max(1, (max_n - 2 + WB - 1) / WB);
+  const size_t capf = allow_max_dynamic_smem(k_wy_factor_rows);
+  (void)capf;
+  k_wy_factor_rows<<<dim3(nblk, count), 256, wy_factor_rows_bytes(), stream>>>(g);
+  const size_t cap16 = allow_max_dynamic_smem(k_backtransform_rows<16>);
+  if (backtransform_rows_bytes<16>(max_n) <= cap16) {
+    k_backtransform_rows<16><<<dim3((want_m + 15) / 16, count), 256, backtransform_rows_bytes<16>(max_n),
+                               stream>>>(g);
+    return;
+  }
+  const size_t cap4 = allow_max_dynamic_smem(k_backtransform_rows<4>);
+  (void)cap4;
+  k_backtransform_rows<4><<<dim3((want_m + 3) / 4, count), 256, backtransform_rows_bytes<4>(max_n), stream>>>(g);
 }
 
 // Loewdin weights s^-1/2 with the overlap condition guard; failed systems are flagged.

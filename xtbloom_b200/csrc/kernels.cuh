@@ -166,6 +166,7 @@ void launch_inverse_iteration(const EigArgs& g, int count, int max_n, int want_m
                               cudaStream_t stream);
 void launch_backtransform(const EigArgs& g, const int32_t* list, int count, int max_n, int mcap,
                           cudaStream_t stream);
+void launch_backtransform_rows(const EigArgs& g, int count, int max_n, int want_m, cudaStream_t stream);
 void launch_backtransform_wy(const EigArgs& g, int count, int max_n, int max_m, int want_m,
                              cudaStream_t stream);
 size_t backtransform_wy_bytes(int n, int m);
