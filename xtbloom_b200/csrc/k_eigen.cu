@@ -320,98 +320,6 @@ void launch_gemm(const GemmArgs& g, bool transA, bool weighted, int max_tiles, i
 }
 
 // ---------------------------------------------------------------------------
-// Householder tridiagonalisation of the full symmetric matrix (in place).
-// Reflector i (v[0] = 1 at row i+1, v[k] stored in A[i][i+1+k], k >= 1) and
-// tau_i; d, e receive the tridiagonal.
-// ---------------------------------------------------------------------------
-// nloc > 0: only the first n - nloc columns are reduced here (systems with
-// n <= nloc return at once); the shared-memory kernel finishes the trailing
-// nloc x nloc block, which this kernel has updated in place.
-__global__ void __launch_bounds__(512) k_tridiag(EigArgs g, int nloc) {
-  extern __shared__ double sm[];
-  const int s = g.list[blockIdx.x];
-  if (g.only != nullptr && g.only[s] == 0) return;
-  const int n = g.nao[s];
-  const int i_end = nloc > 0 ? n - nloc : n - 2;
-  if (i_end <= 0 && nloc > 0) return;
-  double* a = g.A + g.mat_off[s];
-  double* d = g.d + g.ao_off[s];
-  double* e = g.e + g.ao_off[s];
-  double* tau = g.tau + g.ao_off[s];
-  double* v = sm;
-  double* p = sm + n;
-  double* red = sm + 2 * n;
-  const int tid = threadIdx.x, bs = blockDim.x;
-  const int lane = tid & 31, warp = tid >> 5, nw = bs >> 5;
-  for (int i = 0; i < i_end && i + 2 < n; ++i) {
-    const int m = n - i - 1;
-    double* row = a + (int64_t)i * n + (i + 1);
-    double part = 0.0;
-    for (int k = tid; k < m; k += bs) {
-      const double x = row[k];
-      v[k] = x;
-      if (k >= 1) part += x * x;
-    }
-    const double xn2 = block_sum(part, red);   // includes a sync
-    const double alpha = v[0];
-    double ti = 0.0, beta = alpha;
-    if (xn2 > 0.0) {
-      beta = -copysign(sqrt(alpha * alpha + xn2), alpha);
-      ti = (beta - alpha) / beta;
-      const double sc = 1.0 / (alpha - beta);
-      for (int k = tid; k < m; k += bs) {
-        if (k >= 1) {
-          const double vk = v[k] * sc;
-          v[k] = vk;
-          row[k] = vk;
-        }
-      }
-    }
-    __syncthreads();
-    if (tid == 0) {
-      v[0] = 1.0;
-      d[i] = a[(int64_t)i * n + i];
-      e[i] = beta;
-      tau[i] = ti;
-    }
-    __syncthreads();
-    if (ti == 0.0) continue;
-    // p = tau * A22 v   (A22 = rows/cols i+1..n-1), one warp per row
-    double* a22 = a + (int64_t)(i + 1) * n + (i + 1);
-    for (int r = warp; r < m; r += nw) {
-      const double* ar = a22 + (int64_t)r * n;
-      double acc = 0.0;
-      for (int c = lane; c < m; c += 32) acc = fma(ar[c], v[c], acc);
-      acc = warp_sum(acc);
-      if (lane == 0) p[r] = ti * acc;
-    }
-    __syncthreads();
-    double pv = 0.0;
-    for (int k = tid; k < m; k += bs) pv += p[k] * v[k];
-    const double K = 0.5 * ti * block_sum(pv, red);
-    for (int k = tid; k < m; k += bs) p[k] -= K * v[k];
-    __syncthreads();
-    for (int r = warp; r < m; r += nw) {
-      double* ar = a22 + (int64_t)r * n;
-      const double vr = v[r], wr = p[r];
-      for (int c = lane; c < m; c += 32) ar[c] -= vr * p[c] + wr * v[c];
-    }
-    __syncthreads();
-  }
-  if (nloc > 0) return;
-  if (tid == 0) {
-    if (n >= 2) {
-      d[n - 2] = a[(int64_t)(n - 2) * n + (n - 2)];
-      e[n - 2] = a[(int64_t)(n - 2) * n + (n - 1)];
-      tau[n - 2] = 0.0;
-    }
-    d[n - 1] = a[(int64_t)(n - 1) * n + (n - 1)];
-    e[n - 1] = 0.0;
-    tau[n - 1] = 0.0;
-  }
-}
-
-// ---------------------------------------------------------------------------
 // Shared-memory Householder tridiagonalisation.  The trailing nl x nl block
 // (rows/columns i0..n-1, i0 = max(0, n - nloc)) lives in packed lower storage
 // (local element (r, c), r >= c, at r(r+1)/2 + c) in one CTA's shared memory.
@@ -425,7 +333,7 @@ __global__ void __launch_bounds__(512) k_tridiag(EigArgs g, int nloc) {
 //       (tau/2)(p.v); readers of w apply the correction.
 // Four barriers per column: after (A)'s norm, (B), (C) and (D)'s dot product.
 // Reflectors are stored in the global matrix in the layout the back-transform
-// reads (row i, columns i+2..): the same as the global-memory kernel.
+// reads (row i, columns i+2..), as the global-memory prefix kernel does.
 // ---------------------------------------------------------------------------
 __device__ __forceinline__ int pk32(int r, int c) { return r * (r + 1) / 2 + c; }
 
@@ -1170,47 +1078,6 @@ __global__ void __launch_bounds__(kInvSmemThreads) k_inverse_iteration_smem(EigA
                                            gridDim.x * kInvSmemThreads);
 }
 
-// ---------------------------------------------------------------------------
-// Back-transform Z <- H_0 H_1 ... H_{n-3} Z (eigenvector-major rows of Z).
-// ---------------------------------------------------------------------------
-// mcap > 0: the m formed eigenvectors are staged in shared memory (m <= mcap),
-// applied there and written back once; otherwise they are updated in place.
-__global__ void __launch_bounds__(256) k_backtransform(EigArgs g, const int32_t* list, int mcap) {
-  extern __shared__ double sm[];
-  const int s = list[blockIdx.x];
-  if (g.only != nullptr && g.only[s] == 0) return;
-  const int n = g.nao[s];
-  const int m = g.all_vectors ? n : g.nvec[s];
-  const double* a = g.A + g.mat_off[s];
-  const double* tau = g.tau + g.ao_off[s];
-  double* gZ = g.Z + g.mat_off[s];
-  double* v = sm;
-  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nw = blockDim.x >> 5;
-  const bool staged = mcap > 0 && m <= mcap;
-  double* Z = staged ? sm + n + 8 : gZ;
-  if (staged) {
-    for (int64_t k = tid; k < (int64_t)m * n; k += blockDim.x) Z[k] = gZ[k];
-  }
-  for (int i = n - 3; i >= 0; --i) {
-    const double ti = tau[i];
-    if (ti == 0.0) continue;
-    const int L = n - i - 1;
-    __syncthreads();
-    for (int k = tid; k < L; k += blockDim.x) v[k] = (k == 0) ? 1.0 : a[(int64_t)i * n + i + 1 + k];
-    __syncthreads();
-    for (int j = warp; j < m; j += nw) {
-      double* z = Z + (int64_t)j * n + (i + 1);
-      double acc = 0.0;
-      for (int k = lane; k < L; k += 32) acc = fma(v[k], z[k], acc);
-      acc = ti * warp_sum(acc);
-      for (int k = lane; k < L; k += 32) z[k] -= acc * v[k];
-    }
-  }
-  if (staged) {
-    __syncthreads();
-    for (int64_t k = tid; k < (int64_t)m * n; k += blockDim.x) gZ[k] = Z[k];
-  }
-}
 
 // ---------------------------------------------------------------------------
 // Blocked back-transform (compact WY form, LAPACK larft/larfb order): the
@@ -1692,14 +1559,6 @@ __global__ void k_lowdin_weights(EigArgs g, int32_t* status) {
   if (threadIdx.x == 0 && !ok) status[s] = kEigenFailed;
 }
 
-void launch_tridiag(const EigArgs& g, int count, int max_n, cudaStream_t stream) {
-  if (count == 0) return;
-  const size_t sm = (2 * (size_t)max_n + 40) * sizeof(double);
-  const size_t cap = allow_max_dynamic_smem(k_tridiag);
-  (void)cap;
-  k_tridiag<<<count, 512, sm, stream>>>(g, 0);
-}
-
 int sm_count() {
   static const int n = [] {
     int dev = 0, v = 0;
@@ -1747,15 +1606,6 @@ void launch_inverse_iteration(const EigArgs& g, int count, int max_n, int want_m
   k_inverse_iteration<<<count, 128, 0, stream>>>(g, ortol_rel);
 }
 
-void launch_backtransform(const EigArgs& g, const int32_t* list, int count, int max_n, int mcap,
-                          cudaStream_t stream) {
-  if (count == 0) return;
-  const size_t attr = allow_max_dynamic_smem(k_backtransform);
-  (void)attr;
-  size_t bytes = ((size_t)max_n + 8) * sizeof(double);
-  if (mcap > 0) bytes += (size_t)mcap * max_n * sizeof(double);
-  k_backtransform<<<count, 256, bytes, stream>>>(g, list, mcap);
-}
 
 void launch_lowdin_weights(const EigArgs& g, int32_t* status, int count, cudaStream_t stream) {
   if (count == 0) return;

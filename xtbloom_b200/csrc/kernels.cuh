@@ -154,7 +154,6 @@ void launch_setup(const DevTopo& t, const int32_t* list, int count, int max_atom
 // tiles than SMs.  Both widths form every element identically.
 void launch_gemm(const GemmArgs& g, bool transA, bool weighted, int max_tiles, int count,
                  cudaStream_t stream, int width = 0);
-void launch_tridiag(const EigArgs& g, int count, int max_n, cudaStream_t stream);
 void launch_tridiag_smem(const EigArgs& g, const int32_t* list, int count, int max_n, cudaStream_t stream);
 // Register-resident cluster tridiagonalisation for systems with n <= tridiag_reg_max_n().
 int tridiag_reg_max_n();
@@ -164,8 +163,6 @@ int sm_count();   // multiprocessors of the current device (cached)
 void launch_eigvals(const EigArgs& g, int mode, double kt, int count, int max_n, cudaStream_t stream);
 void launch_inverse_iteration(const EigArgs& g, int count, int max_n, int want_m, double ortol_rel,
                               cudaStream_t stream);
-void launch_backtransform(const EigArgs& g, const int32_t* list, int count, int max_n, int mcap,
-                          cudaStream_t stream);
 void launch_backtransform_rows(const EigArgs& g, int count, int max_n, int want_m, cudaStream_t stream);
 void launch_backtransform_wy(const EigArgs& g, int count, int max_n, int max_m, int want_m,
                              cudaStream_t stream);
