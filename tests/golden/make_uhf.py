@@ -9,8 +9,10 @@ spin_channels = 2 on
   * twelve doublet radicals of ``workloads.config4(2048, seed=4)`` (alkyl
     radicals C4..C45, some with Cl/Br), chosen to span the sizes and to
     include halogens,
-and stores energies, forces, charges and SCC iteration counts.  The radical
-inputs are regenerated from the seed by the tests.
+and stores energies, forces, charges and SCC iteration counts, at the
+default SCC settings and converged to the fixed point (charge tolerance
+1e-10, energy tolerance 1e-13: ``tight_*``).  The radical inputs are
+regenerated from the seed by the tests.
 
 Usage:  python tests/golden/make_uhf.py <reference checkout>  (or set XTBLOOM_REFERENCE_SRC)
 """
@@ -31,9 +33,12 @@ from xtbloom_b200 import abi, workloads as W  # noqa: E402
 
 def run(lib, b):
     r = lib.compute(b)
+    t = lib.compute(b, lib.make_options(ctol=1e-10, etol=1e-13))
     return {"status": int(r["per_system_status"][0]), "scc_iterations": int(r["scc_iterations"][0]),
             "energy": float(r["energies"][0]), "forces": r["forces"].tolist(),
-            "charges": r["atomic_charges"].tolist()}
+            "charges": r["atomic_charges"].tolist(),
+            "tight_status": int(t["per_system_status"][0]), "tight_energy": float(t["energies"][0]),
+            "tight_forces": t["forces"].tolist(), "tight_charges": t["atomic_charges"].tolist()}
 
 
 def main(ref: Path):

@@ -36,7 +36,7 @@ def batch():
     return abi.ragged_from_lists(nums, pos, None, uhf)
 
 
-def run(kernel: str | None):
+def run(kernel: str | None, tight: bool = False):
     if kernel is None:
         os.environ.pop("XTBLOOM_B200_TRIDIAG", None)
     else:
@@ -44,7 +44,7 @@ def run(kernel: str | None):
     lib = abi.Library(library_path(), backend=abi.BACKEND_CUDA, device_id=0)
     try:
         b = batch()
-        out = lib.compute(b)
+        out = lib.compute(b, lib.make_options(ctol=1e-10, etol=1e-13) if tight else None)
         eig = []
         for i in range(b.batch_size):
             h = lib.fetch("hamiltonian", i)
@@ -74,6 +74,20 @@ def test_eigenvalues_match_lapack(both, which):
         assert k >= 1
         scale = max(1.0, np.abs(ref).max())
         assert np.abs(ev[:k] - ref[:k]).max() < 1e-10 * scale
+
+
+def test_kernels_reach_the_same_fixed_point():
+    """Converged to the fixed point (charge tolerance 1e-10), the two kernels
+    agree on every output of every system, the slowly converging one included."""
+    (a, _), (b, _) = run(None, tight=True), run("smem", tight=True)
+    ok = (a["per_system_status"] == 0) & (b["per_system_status"] == 0)
+    assert ok.sum() >= len(ok) - 1
+    assert np.abs(a["energies"][ok] - b["energies"][ok]).max() < 1e-9
+    offs = batch().atom_offsets
+    for i in np.where(ok)[0]:
+        a0, a1 = offs[i], offs[i + 1]
+        assert np.abs(a["forces"][3 * a0:3 * a1] - b["forces"][3 * a0:3 * a1]).max() < 1e-7, i
+        assert np.abs(a["atomic_charges"][a0:a1] - b["atomic_charges"][a0:a1]).max() < 1e-7, i
 
 
 def test_kernels_agree_on_whole_computes(both):

@@ -21,6 +21,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cfloat>
+#include <cstdlib>
 
 namespace xtb {
 
@@ -697,8 +698,23 @@ void launch_tridiag_smem(const EigArgs& g, const int32_t* list, int count, int m
   if (count == 0) return;
   const size_t cap256 = allow_max_dynamic_smem(k_tridiag_smem<256>);
   const size_t cap512 = allow_max_dynamic_smem(k_tridiag_smem<512>);
+  static const int per_sm = [] {
+    int dev = 0, v = 0;
+    cudaGetDevice(&dev);
+    if (cudaDeviceGetAttribute(&v, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev) != cudaSuccess) v = 0;
+    return v;
+  }();
   int nloc = std::min(max_n, kTridiagSmemMax);
   while (nloc > 2 && tridiag_smem_bytes(nloc, 256) > cap256) --nloc;
+  // 512 threads shorten one system's critical path.  They are used when the
+  // SM would hold a single 256-thread CTA anyway (its packed triangle) or
+  // when there are fewer systems than SMs; otherwise two 256-thread CTAs per
+  // SM overlap each other's barrier waits.  The 512-thread block is a few
+  // columns smaller (its per-warp partials); the prefix takes those columns.
+  const bool one_per_sm = per_sm > 0 && 2 * (tridiag_smem_bytes(nloc, 256) + 1024) > (size_t)per_sm;
+  const bool wide = count < sm_count() || one_per_sm;
+  if (wide)
+    while (nloc > 2 && tridiag_smem_bytes(nloc, 512) > cap512) --nloc;
   if (max_n > nloc) {
     // columns that do not fit: reduced in global memory first
     const size_t capp = allow_max_dynamic_smem(k_tridiag_prefix<512>);
@@ -711,9 +727,7 @@ void launch_tridiag_smem(const EigArgs& g, const int32_t* list, int count, int m
       k_tridiag_prefix<256><<<count, 256, tridiag_prefix_bytes(max_n, 256), stream>>>(g, nloc);
     }
   }
-  // 512 threads shorten one system's critical path (few systems active);
-  // with many systems, several 256-thread CTAs per SM give more throughput.
-  if (count < sm_count() && tridiag_smem_bytes(nloc, 512) <= cap512) {
+  if (wide) {
     k_tridiag_smem<512><<<count, 512, tridiag_smem_bytes(nloc, 512), stream>>>(g, list, nloc);
   } else {
     k_tridiag_smem<256><<<count, 256, tridiag_smem_bytes(nloc, 256), stream>>>(g, list, nloc);
