@@ -104,6 +104,36 @@ def test_mixed_reproduces_reference_fixtures(mixed_lib, fixtures):
         assert np.abs(out["atomic_charges"][a0:a1] - np.asarray(s["charges"])).max() < TOL_Q, s["name"]
 
 
+def test_tensor_core_tiles_match_the_mma_sync_tiles(monkeypatch):
+    """The split-precision products run on tcgen05 tiles (TMEM accumulators);
+    the mma.sync tiles (XTBLOOM_B200_SPLIT_TILE=mma) form the same 3xTF32
+    products in another accumulation order.  Both forms iterate to the FP64
+    fixed point, so the two agree far inside the public tolerances, and the
+    split products ran in both.  160 workload systems: enough 64 x 64 tiles
+    for the split-precision launch (fewer systems multiply in FP64)."""
+    b = W.subset(W.config1(4096, seed=1), np.linspace(0, 4095, 160).round().astype(int))
+    mols = list(range(b.batch_size))
+    outs = []
+    for tile in ("tcgen05", "mma"):
+        monkeypatch.setenv("XTBLOOM_B200_SPLIT_TILE", tile)
+        lib = abi.Library(library_path(), backend=abi.BACKEND_CUDA, device_id=0)
+        try:
+            lib.set_execution(abi.PRECISION_MIXED)
+            out = lib.compute(b)
+            split = lib.fetch("split_iterations", capacity=len(mols))
+        finally:
+            lib.close()
+        assert (split >= 1).sum() >= 150, tile
+        outs.append(out)
+    a, c = outs
+    ok = (a["per_system_status"] == 0) & (c["per_system_status"] == 0)
+    assert ok.sum() >= 155
+    okat = np.repeat(ok, np.diff(b.atom_offsets))
+    assert np.abs(a["energies"][ok] - c["energies"][ok]).max() < 1e-8
+    assert np.abs(a["forces"].reshape(-1, 3)[okat] - c["forces"].reshape(-1, 3)[okat]).max() < 1e-6
+    assert np.abs(a["atomic_charges"][okat] - c["atomic_charges"][okat]).max() < 1e-6
+
+
 def test_set_execution_rejects_bad_arguments(mixed_lib):
     with pytest.raises(abi.XtbloomError):
         mixed_lib.set_execution(7)

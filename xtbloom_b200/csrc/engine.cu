@@ -376,6 +376,7 @@ struct Engine::Impl {
     }
   } ck_id;
   Dbuf fdone;
+  Dbuf umma_fault;   // int32: a tensor-core wait of the split-precision tiles ran out
   Profiler prof;
 
   DevTopo devtopo() const {
@@ -819,7 +820,7 @@ xtbloom_status_t build_topology(Engine::Impl& m, const HostBatch& hb, cudaStream
   ok = ok && m.pos.reserve((size_t)N * 3 * d8) && m.list.reserve((size_t)B * 4) &&
        m.count.reserve(16) && m.status.reserve((size_t)B * 4) && m.iterations.reserve((size_t)B * 4) &&
        m.converged.reserve((size_t)B) && m.prec.reserve((size_t)B) &&
-       m.fdone.reserve((size_t)B) &&
+       m.fdone.reserve((size_t)B) && m.umma_fault.reserve(4) &&
        m.split_iters.reserve((size_t)B * 4) && m.gate_hits.reserve((size_t)B * 4) && m.last_rms.reserve((size_t)B * 8) && m.nvec.reserve((size_t)NC * 4) && m.cn.reserve(N * d8) &&
        m.cn_d4.reserve(N * d8) && m.mrad.reserve(N * d8) && m.dmrad.reserve(N * d8) &&
        m.gam.reserve((size_t)m.total_gam * d8) && m.S.reserve(mat) && m.D.reserve(3 * mat) &&
@@ -1224,6 +1225,7 @@ xtbloom_status_t Engine::compute(const ComputeRequest& req, std::string& error) 
   cudaMemsetAsync(m.wstate.p, 0, (size_t)m.nchan, s);
   cudaMemsetAsync(m.w_stats.p, 0, 256 * 8 * 4, s);
   cudaMemsetAsync(m.fdone.p, 0, B, s);
+  cudaMemsetAsync(m.umma_fault.p, 0, 4, s);
   cudaMemsetAsync(m.grad.p, 0, 3 * N * 8, s);
   cudaMemsetAsync(m.acn.p, 0, N * 8, s);
   cudaMemsetAsync(m.acn_d4.p, 0, N * 8, s);
@@ -1285,6 +1287,7 @@ xtbloom_status_t Engine::compute(const ComputeRequest& req, std::string& error) 
                   const uint8_t* prec = nullptr, cudaStream_t st = nullptr,
                   const uint8_t* only = nullptr) {
     GemmArgs g{};
+    g.fault = m.umma_fault.as<int32_t>();
     g.sym = sym ? 1 : 0;
     g.only = only;
     g.prec = prec;
@@ -1832,6 +1835,14 @@ xtbloom_status_t Engine::compute(const ComputeRequest& req, std::string& error) 
     cudaStreamSynchronize(s);
     error = std::string("kernel launch failed: ") + cudaGetErrorString(launch_error);
     return XTBLOOM_STATUS_INTERNAL_ERROR;
+  }
+  if (m.mixed) {
+    cudaMemcpyAsync(m.h_count + 3, m.umma_fault.p, 4, cudaMemcpyDeviceToHost, s);
+    cudaStreamSynchronize(s);
+    if (m.h_count[3] != 0) {
+      error = "a tensor-core product of the split-precision form did not complete in time";
+      return XTBLOOM_STATUS_INTERNAL_ERROR;
+    }
   }
   // ---- copy into caller buffers ----
   const xtbloom_batch_result_t& r = *req.result;

@@ -22,6 +22,7 @@
 #include <cmath>
 #include <cfloat>
 #include <cstdlib>
+#include <cstring>
 
 namespace xtb {
 
@@ -291,9 +292,10 @@ __global__ void __launch_bounds__(256, 3) k_gemm(GemmArgs g) {
   }
   // the split-precision tile exists for 64-wide tiles; the few-system
   // 32-wide launch multiplies every system in FP64
-  if (TB == GB && g.prec != nullptr && g.prec[g.prec_of != nullptr ? g.prec_of[s] : s] == 0)
+  if (TB == GB && g.prec != nullptr && g.prec[g.prec_of != nullptr ? g.prec_of[s] : s] == 0) {
+    if (g.umma) return;   // formed by k_gemm_umma
     gemm_tile_tf32x3<TA, W>(g, s, M, N, K, ld, ti, tj);
-  else
+  } else
     gemm_tile_f64<TA, W, TB>(g, s, M, N, K, ld, ti, tj, mirror);
 }
 
@@ -314,10 +316,18 @@ void launch_gemm(const GemmArgs& g, bool transA, bool weighted, int max_tiles, i
   // Fewer 64-wide tiles than SMs: 32-wide tiles put four times as many SMs
   // on each product (a 64 x 64 x 240 FP64 tile alone takes ~8 us on one SM).
   const int tiles64 = g.sym ? tm * (tm + 1) / 2 : tm * tm;
-  if (width == 32 || (width == 0 && (int64_t)tiles64 * count < sm_count()))
+  if (width == 32 || (width == 0 && (int64_t)tiles64 * count < sm_count())) {
     launch_gemm_tb<32>(g, transA, weighted, 2 * tm, count, stream);
-  else
-    launch_gemm_tb<GB>(g, transA, weighted, tm, count, stream);
+  } else {
+    // split-precision systems on the tcgen05 tiles; XTBLOOM_B200_SPLIT_TILE=mma
+    // selects the mma.sync tiles instead (read per launch: a comparison switch)
+    const char* tile = std::getenv("XTBLOOM_B200_SPLIT_TILE");
+    const bool legacy = tile != nullptr && std::strcmp(tile, "mma") == 0;
+    GemmArgs gu = g;
+    gu.umma = (g.prec != nullptr && !legacy) ? 1 : 0;
+    if (gu.umma) launch_gemm_umma(gu, transA, weighted, tm, count, stream);
+    launch_gemm_tb<GB>(gu, transA, weighted, tm, count, stream);
+  }
 }
 
 // ---------------------------------------------------------------------------

@@ -23,6 +23,8 @@ struct GemmArgs {
   const uint8_t* prec;     // per system: 0 = split-precision (3xTF32) tile, else FP64; NULL = FP64
   const int32_t* prec_of;  // list entry (channel) -> index into prec; NULL = the entry itself
   const uint8_t* only;     // per list entry id: 0 = skip (its CTAs return at once); NULL = all
+  int32_t umma;            // split-precision tiles run in k_gemm_umma: k_gemm skips those systems
+  int32_t* fault;          // set to 1 when a tensor-core wait of k_gemm_umma ran out
 };
 
 struct EigArgs {
@@ -152,6 +154,8 @@ void launch_setup(const DevTopo& t, const int32_t* list, int count, int max_atom
 
 // width 32 or 64 forces the FP64 tile edge; 0 picks 32 when fewer 64-wide
 // tiles than SMs.  Both widths form every element identically.
+void launch_gemm_umma(const GemmArgs& g, bool transA, bool weighted, int tm, int count,
+                      cudaStream_t stream);
 void launch_gemm(const GemmArgs& g, bool transA, bool weighted, int max_tiles, int count,
                  cudaStream_t stream, int width = 0);
 void launch_tridiag_smem(const EigArgs& g, const int32_t* list, int count, int max_n, cudaStream_t stream);
