@@ -66,6 +66,8 @@ def parse():
     p.add_argument("--cpu-sample-1t", type=int, default=24,
                    help="systems of the single-thread CPU baseline sample")
     p.add_argument("--no-gfn1", action="store_true", help="skip the GFN1 radical-batch line")
+    p.add_argument("--no-autograd", action="store_true", help="skip the point-charge autograd line")
+    p.add_argument("--no-water", action="store_true", help="skip the water-cluster line")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--form", default="both", choices=["both", "mixed", "fp64"])
     p.add_argument("--graphs", type=int, default=1)
@@ -335,6 +337,103 @@ def time_gfn1(args, world, local, stream):
             "mean_scc_iterations": float(np.mean(it))}
 
 
+def _device_outs(torch, dev, B, N):
+    return {"energies": torch.empty(B, dtype=torch.float64, device=dev),
+            "forces": torch.empty(3 * N, dtype=torch.float64, device=dev),
+            "atomic_charges": torch.empty(N, dtype=torch.float64, device=dev),
+            "scc_iterations": torch.empty(B, dtype=torch.int32, device=dev),
+            "scc_converged": torch.empty(B, dtype=torch.uint8, device=dev),
+            "per_system_status": torch.empty(B, dtype=torch.int32, device=dev)}
+
+
+def time_autograd(args, world, local, stream):
+    """Energies and their gradients through the torch.autograd function: 1024
+    C20H42 conformers, each in 200 point charges (dE/dR, dE/dR_pc, dE/dQ_pc);
+    one step = forward + backward over the batch, inputs resident in HBM."""
+    import torch
+    from xtbloom_b200.autograd import gfn2_energy
+    dev = torch.device("cuda", local)
+    b = W.config2(1024, seed=2)
+    B = b.batch_size
+    z = torch.from_numpy(b.atomic_numbers).to(dev)
+    off = torch.from_numpy(b.atom_offsets).to(dev)
+    pos = torch.from_numpy(b.positions.reshape(-1, 3)).to(dev).requires_grad_(True)
+    poff = torch.from_numpy(b.point_charge_offsets).to(dev)
+    ppos = torch.from_numpy(b.point_charge_positions.reshape(-1, 3)).to(dev).requires_grad_(True)
+    pq = torch.from_numpy(b.point_charge_values).to(dev).requires_grad_(True)
+    pg = torch.from_numpy(b.point_charge_gammas).to(dev)
+
+    def step():
+        pos.grad = ppos.grad = pq.grad = None
+        e = gfn2_energy(z, off, pos, poff, ppos, pq, pg)
+        e.sum().backward()
+        return e
+
+    for _ in range(max(1, min(args.warmup, 2))):
+        e = step()
+    torch.cuda.synchronize()
+    barrier(world)
+    steps = max(1, min(args.steps, 3))
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(steps):
+        e = step()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    barrier(world)
+    ms = allreduce_max(e0.elapsed_time(e1) / steps, world)
+    ok = int(torch.isfinite(e).sum().item())
+    return {"workload": "GFN2-xTB energy + dE/dR, dE/dR_pc, dE/dQ_pc via torch.autograd.Function; 1024 "
+                        "C20H42 conformers (seed 2), each in 200 point charges (8-20 bohr shell)",
+            "value": world * B / (ms / 1e3), "unit": "systems/s", "ms_per_step": ms, "steps": steps,
+            "converged": ok, "systems": int(B)}
+
+
+def time_water(args, world, local, stream):
+    """Precision stress: 256 water clusters (H2O)_N, N uniform in 100..200
+    (600-1200 AOs), seed 3.  One device-resident call per step in the FP64
+    and split-precision forms, and each form's largest output difference from
+    the FP64 fixed point (charge tolerance 1e-10, untimed)."""
+    import torch
+    from xtbloom_b200 import library_path
+    dev = torch.device("cuda", local)
+    b = W.config3(256, seed=3)
+    B, N = b.batch_size, b.total_atoms
+    db = abi.RaggedBatch(b.atom_offsets, b.atomic_numbers, torch.from_numpy(b.positions).to(dev),
+                         b.molecular_charges, b.unpaired_electrons)
+    lib = abi.Library(library_path(), backend=abi.BACKEND_CUDA, device_id=local, stream=stream.cuda_stream)
+    fixed = lib.compute(b, lib.make_options(ctol=1e-10, etol=1e-13))
+    line = {"workload": "GFN2-xTB E+F+q, 256 water clusters (H2O)_N, N uniform in 100..200 "
+                        "(600-1200 AOs), seed 3; SCC 1e-6/1e-8, 300 K", "unit": "systems/s", "forms": {}}
+    okat_fixed = np.repeat(fixed["per_system_status"] == 0, np.diff(b.atom_offsets))
+    for form, prec in (("fp64", abi.PRECISION_FP64), ("mixed", abi.PRECISION_MIXED)):
+        lib.set_execution(prec, capture_graphs=args.graphs)
+        outs = _device_outs(torch, dev, B, N)
+        lib.compute(db, lib.make_options(), outs)
+        torch.cuda.synchronize()
+        barrier(world)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        lib.compute(db, lib.make_options(), outs)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        barrier(world)
+        ms = allreduce_max(e0.elapsed_time(e1), world)
+        o = {k: v.cpu().numpy() for k, v in outs.items()}
+        ok = (o["per_system_status"] == 0) & (fixed["per_system_status"] == 0)
+        okat = np.repeat(ok, np.diff(b.atom_offsets)) & okat_fixed
+        line["forms"][form] = {
+            "value": world * B / (ms / 1e3), "ms_per_step": ms, "steps": 1,
+            "converged": int(np.sum(o["per_system_status"] == 0)),
+            "vs_fp64_fixed_point": {
+                "max_abs_dE_Eh": float(np.abs(o["energies"][ok] - fixed["energies"][ok]).max()),
+                "max_abs_dF_Eh_per_bohr": float(np.abs(o["forces"].reshape(-1, 3)[okat]
+                                                       - fixed["forces"].reshape(-1, 3)[okat]).max()),
+                "max_abs_dq_e": float(np.abs(o["atomic_charges"][okat] - fixed["atomic_charges"][okat]).max())}}
+    lib.close()
+    return line
+
+
 def time_strong(args, world, rank, local, stream):
     """One 4096-system batch over all ranks (strong scaling): the systems are
     partitioned by predicted cost (n_AO^3 per channel and iteration); one
@@ -452,6 +551,8 @@ def run_ours(args, world, rank, local):
     gfn1_line = None
     if not args.no_gfn1:
         gfn1_line = time_gfn1(args, world, local, stream)
+    autograd_line = None if args.no_autograd else time_autograd(args, world, local, stream)
+    water_line = None if args.no_water else time_water(args, world, local, stream)
     strong = time_strong(args, world, rank, local, stream) if world > 1 else None
     clk = clocks.stop()
     h2d = (B + 1) * 8 + N * 4 + 3 * N * 8 + B * 8 + B * 4
@@ -576,6 +677,8 @@ def run_ours(args, world, rank, local):
                    "converged": int(np.sum(status == 0)), "systems": int(B),
                    "mean_scc_iterations": float(np.mean(iters))},
         "gfn1_radicals": gfn1_line,
+        "point_charges_autograd": autograd_line,
+        "water_clusters": water_line,
         "one_batch_over_ranks": strong,
         "stage_ms_per_step": per_stage_ms,
         "stage_share": {k: v / total_stage for k, v in per_stage_ms.items()},
