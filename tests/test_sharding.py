@@ -191,3 +191,46 @@ def test_two_gloo_ranks_run_one_batch_with_attachments():
     for rank, tmax, ok, computed, owned in got:
         assert tmax == 2.0 and ok
         assert computed == owned < 64     # each rank computed only its own shard
+
+
+class _FakeLibrary:
+    """Stands in for one device's context: records the systems it computed."""
+
+    def __init__(self, device):
+        self.device = device
+        self.seen = []
+
+    def make_options(self, **kw):
+        return kw
+
+    def compute(self, b, options):
+        self.seen.append(b.batch_size)
+        out = fake_compute(b)
+        n = np.diff(np.asarray(b.atom_offsets))
+        out["scc_iterations"] = (10 + (n % 7) * 30).astype(np.int32)   # some slow systems
+        return out
+
+
+def test_batch_calculator_spreads_one_batch_over_devices(monkeypatch):
+    from xtbloom_b200 import interface
+    fakes = {d: _FakeLibrary(d) for d in (0, 1, 2)}
+    monkeypatch.setattr(interface, "_library", lambda d: fakes[d])
+    b = W.config1(50)
+    nums = [W.molecule(b, i)[0] for i in range(50)]
+    pos = [W.molecule(b, i)[1] for i in range(50)]
+    calc = interface.BatchCalculator("GFN2-xTB", nums, pos, device_ids=[0, 1, 2])
+    r1 = calc.singlepoint()
+    assert sum(f.seen[0] for f in fakes.values()) == 50 and all(f.seen[0] > 0 for f in fakes.values())
+    direct = fake_compute(b)
+    assert np.allclose(r1.get("energies"), direct["energies"])
+    for i in range(50):
+        assert np.array_equal(r1.get("charges")[i], direct["atomic_charges"][b.atom_offsets[i]:b.atom_offsets[i + 1]])
+    # the second call is partitioned with the first call's iteration counts
+    first = [f.seen[0] for f in fakes.values()]
+    calc.singlepoint()
+    second = [f.seen[1] for f in fakes.values()]
+    assert sum(second) == 50
+    assert calc._last_iterations is not None and len(calc._last_iterations) == 50
+    assert first != second or len(set(calc._last_iterations)) == 1
+    with pytest.raises(ValueError):
+        interface.BatchCalculator("GFN2-xTB", nums, pos, device_ids=[0, 0])
