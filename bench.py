@@ -76,6 +76,9 @@ def parse():
     p.add_argument("--indices", default="",
                    help="with --once: comma-separated systems of the 4096-system batch to run "
                         "(e.g. the slowly converging ones, for profiles of the few-system regime)")
+    p.add_argument("--workload", default="hetero", choices=["hetero", "water", "radicals"],
+                   help="with --once: the batch to run (hetero: --systems hetero-alkanes; water: "
+                        "--systems water clusters of 600-1200 AOs; radicals: --systems GFN1 radicals)")
     return p.parse_args()
 
 
@@ -522,7 +525,13 @@ def run_ours(args, world, rank, local):
                           stream=stream.cuda_stream)
         lib.set_execution(abi.PRECISION_MIXED if args.form == "mixed" else abi.PRECISION_FP64,
                           capture_graphs=args.graphs)
-        lib.compute(dev_batch, lib.make_options(), new_outs_d())
+        if args.workload == "hetero":
+            lib.compute(dev_batch, lib.make_options(), new_outs_d())
+        else:
+            other = (W.config3(256, seed=3) if args.workload == "water" else W.config4(2048, seed=4))
+            other = W.subset(other, np.arange(min(args.systems, other.batch_size)))
+            model = abi.MODEL_GFN1 if args.workload == "radicals" else abi.MODEL_GFN2
+            lib.compute(other, lib.make_options(model=model))
         torch.cuda.synchronize()
         lib.close()
         return

@@ -127,9 +127,16 @@ def test_gfn1_finite_difference_forces(cuda_lib):
 @pytest.mark.skipif(not REF_LIB.exists(), reason="reference library not built")
 def test_gfn1_live_reference_on_radical_workload(cuda_lib):
     """24 radicals of the 2048-radical workload (12 with Cl/Br), two spin
-    channels, against the reference library run live: at the fixed point
-    (charge tolerance 1e-10) at the public tolerances, and at the default
-    settings within the reference's own distance from its fixed point."""
+    channels, against the reference library run live.
+
+    Radicals that converge within 60 iterations follow the reference's path:
+    every output at the public tolerances at the default settings, and at the
+    fixed point (charge tolerance 1e-10).  Slower ones follow a trajectory
+    that rounding moves, and an open-shell SCC can have more than one
+    solution: such a system is compared at the fixed point when both sides
+    reach the same one; at most one of the sample may settle on another
+    solution, which must then be a converged fixed point of its own (default
+    and tight results agree) with a status equal to the reference's."""
     full = W.config4(2048, seed=4)
     halo = [i for i in range(2048) if np.isin(W.molecule(full, i)[0], (17, 35)).any()]
     plain = [i for i in range(2048) if i not in set(halo)]
@@ -137,29 +144,118 @@ def test_gfn1_live_reference_on_radical_workload(cuda_lib):
     idx = np.sort(np.concatenate([rng.choice(halo, 12, replace=False), rng.choice(plain, 12, replace=False)]))
     b = W.subset(full, idx)
     ref = abi.Library(str(REF_LIB), backend=abi.BACKEND_CPU, cpu_threads=0)
-    tight_o = ref.make_options(model=abi.MODEL_GFN1, ctol=1e-10, etol=1e-13)
-    r_t = ref.compute(b, tight_o)
+    r_t = ref.compute(b, ref.make_options(model=abi.MODEL_GFN1, ctol=1e-10, etol=1e-13))
     r_d = ref.compute(b, ref.make_options(model=abi.MODEL_GFN1))
     out = cuda_lib.compute(b, gfn1_options(cuda_lib))
     out_t = cuda_lib.compute(b, gfn1_options(cuda_lib, ctol=1e-10, etol=1e-13))
     o = b.atom_offsets
-    ok = (r_t["per_system_status"] == 0) & (r_d["per_system_status"] == 0) & (out["per_system_status"] == 0)
-    assert ok.sum() >= 18
-    for i in np.where(ok)[0]:
+    assert np.array_equal(out["per_system_status"] == 0, r_d["per_system_status"] == 0)
+    fast = (r_d["per_system_status"] == 0) & (r_d["scc_iterations"] <= 60)
+    assert fast.sum() >= 12
+    other_solution = 0
+    for i in np.where(r_d["per_system_status"] == 0)[0]:
         sl3, sl = slice(3 * o[i], 3 * o[i + 1]), slice(o[i], o[i + 1])
-        assert abs(out["energies"][i] - r_d["energies"][i]) < TOL_E
-        gate_f = np.abs(r_d["forces"][sl3] - r_t["forces"][sl3]).max()
-        gate_q = np.abs(r_d["atomic_charges"][sl] - r_t["atomic_charges"][sl]).max()
-        assert np.abs(out["forces"][sl3] - r_d["forces"][sl3]).max() < 2 * gate_f + TOL_F
-        assert np.abs(out["atomic_charges"][sl] - r_d["atomic_charges"][sl]).max() < 2 * gate_q + TOL_Q
-        if out_t["per_system_status"][i] == 0:
-            assert abs(out_t["energies"][i] - r_t["energies"][i]) < TOL_E
-            assert np.abs(out_t["forces"][sl3] - r_t["forces"][sl3]).max() < TOL_F
-            assert np.abs(out_t["atomic_charges"][sl] - r_t["atomic_charges"][sl]).max() < TOL_Q
+        if fast[i]:
+            assert abs(out["energies"][i] - r_d["energies"][i]) < TOL_E, i
+            assert np.abs(out["forces"][sl3] - r_d["forces"][sl3]).max() < TOL_F, i
+            assert np.abs(out["atomic_charges"][sl] - r_d["atomic_charges"][sl]).max() < TOL_Q, i
+            assert abs(int(out["scc_iterations"][i]) - int(r_d["scc_iterations"][i])) <= 1, i
+        if out_t["per_system_status"][i] != 0 or r_t["per_system_status"][i] != 0:
+            assert not fast[i], i
+            continue
+        if abs(out_t["energies"][i] - r_t["energies"][i]) < TOL_E:
+            assert np.abs(out_t["forces"][sl3] - r_t["forces"][sl3]).max() < TOL_F, i
+            assert np.abs(out_t["atomic_charges"][sl] - r_t["atomic_charges"][sl]).max() < TOL_Q, i
+        else:
+            assert not fast[i], i
+            other_solution += 1
+            assert abs(out["energies"][i] - out_t["energies"][i]) < TOL_E, i
+    assert other_solution <= 1
 
 
-def test_gfn1_with_point_charges_is_not_implemented(cuda_lib):
-    b = W.config2(2, npc=10)
+def pc_batch(cases):
+    b = batch_of(cases)
+    counts = [len(c["pc_charges"]) for c in cases]
+    b.point_charge_offsets = np.concatenate([[0], np.cumsum(counts)]).astype(np.int64)
+    b.point_charge_positions = np.concatenate([np.asarray(c["pc_positions"], float) for c in cases])
+    b.point_charge_values = np.concatenate([np.asarray(c["pc_charges"], float) for c in cases])
+    b.point_charge_gammas = np.concatenate([np.asarray(c["pc_gammas"], float) for c in cases])
+    return b
+
+
+PC_FLAGS = abi.COMPUTE_ENERGY | abi.COMPUTE_FORCES | abi.COMPUTE_CHARGES | abi.COMPUTE_POINT_CHARGE_FORCES
+
+
+def test_gfn1_qmmm_goldens(cuda_lib, gfn1):
+    """The reference's GFN1 QM/MM goldens (xTB 6.7.1: water dimer in six point
+    charges with GFN1 hardnesses and with gamma = 999; harmonic-mean softening
+    of the shell-charge coupling) at 5e-7, point-charge forces included."""
+    cases = gfn1["tblite_qmmm"]
+    assert len(cases) == 2
+    b = pc_batch(cases)
+    out = cuda_lib.compute(b, gfn1_options(cuda_lib, flags=PC_FLAGS, ctol=1e-10, etol=1e-13))
+    po = b.point_charge_offsets
+    for i, c in enumerate(cases):
+        a0, a1 = b.atom_offsets[i], b.atom_offsets[i + 1]
+        assert out["per_system_status"][i] == 0, c["name"]
+        assert abs(out["energies"][i] - c["energy"]) < 5e-7, (c["name"], out["energies"][i], c["energy"])
+        assert np.abs(out["forces"][3 * a0:3 * a1] - np.asarray(c["forces"]).ravel()).max() < 5e-7, c["name"]
+        pcf = out["point_charge_forces"][3 * po[i]:3 * po[i + 1]]
+        assert np.abs(pcf - np.asarray(c["point_charge_forces"]).ravel()).max() < 5e-7, c["name"]
+        if c["charges"] is not None:
+            assert np.abs(out["atomic_charges"][a0:a1] - np.asarray(c["charges"])).max() < 5e-7, c["name"]
+
+
+def test_gfn1_point_charges_against_reference(cuda_lib, gfn1):
+    """GFN1 chains, radicals and the QM/MM waters in point-charge shells, one
+    ragged batch, against the reference library at the default settings
+    (slow systems: within the reference's own distance from its fixed point)."""
+    cases = [c for c in gfn1["reference_pc"] if c["status"] == 0]
+    assert len(cases) >= 6
+    b = pc_batch(cases)
+    out = cuda_lib.compute(b, gfn1_options(cuda_lib, flags=PC_FLAGS))
+    po = b.point_charge_offsets
+    for i, c in enumerate(cases):
+        a0, a1 = b.atom_offsets[i], b.atom_offsets[i + 1]
+        assert out["per_system_status"][i] == 0, c["name"]
+        assert abs(out["energies"][i] - c["energy"]) < TOL_E, (c["name"], out["energies"][i], c["energy"])
+        slack_f = slack_q = 0.0
+        if c["scc_iterations"] > 60:
+            slack_f = np.abs(np.asarray(c["forces"]) - np.asarray(c["tight_forces"])).max()
+            slack_q = np.abs(np.asarray(c["charges"]) - np.asarray(c["tight_charges"])).max()
+        assert np.abs(out["forces"][3 * a0:3 * a1] - np.asarray(c["forces"])).max() < TOL_F + slack_f, c["name"]
+        assert np.abs(out["atomic_charges"][a0:a1] - np.asarray(c["charges"])).max() < TOL_Q + slack_q, c["name"]
+        pcf = out["point_charge_forces"][3 * po[i]:3 * po[i + 1]]
+        assert np.abs(pcf - np.asarray(c["point_charge_forces"])).max() < TOL_F + slack_f, c["name"]
+
+
+def test_gfn1_charge_response_against_reference(cuda_lib, gfn1):
+    """GFN1 with the charge response b + A q, against the reference library."""
+    cases = [c for c in gfn1["reference_response"] if c["status"] == 0]
+    assert len(cases) >= 4
+    b = batch_of(cases)
+    na = np.diff(b.atom_offsets)
+    b.atomic_potential_shifts = np.concatenate([np.asarray(c["shifts"]) for c in cases])
+    b.charge_response_offsets = np.concatenate([[0], np.cumsum(na * na)]).astype(np.int64)
+    b.charge_response_matrix = np.concatenate([np.asarray(c["response"]) for c in cases])
+    out = cuda_lib.compute(b, gfn1_options(cuda_lib))
+    for i, c in enumerate(cases):
+        a0, a1 = b.atom_offsets[i], b.atom_offsets[i + 1]
+        assert out["per_system_status"][i] == 0, c["name"]
+        assert abs(out["energies"][i] - c["energy"]) < TOL_E, (c["name"], out["energies"][i], c["energy"])
+        assert np.abs(out["forces"][3 * a0:3 * a1] - np.asarray(c["forces"])).max() < TOL_F, c["name"]
+        assert np.abs(out["atomic_charges"][a0:a1] - np.asarray(c["charges"])).max() < TOL_Q, c["name"]
+
+
+def test_gfn1_fields_and_dipoles_are_not_implemented(cuda_lib, gfn1):
+    """As in the reference (src/runtime/validation.cpp:1428-1437): GFN1 refuses
+    interaction attachments and the dipole publication before any output."""
+    cases = gfn1["tblite"][:2]
+    b = batch_of(cases)
+    with pytest.raises(abi.XtbloomError) as e:
+        cuda_lib.compute(b, gfn1_options(cuda_lib, flags=abi.COMPUTE_ENERGY | abi.COMPUTE_DIPOLES))
+    assert e.value.status == abi.NOT_IMPLEMENTED
+    b.efields = np.array([[0.0, 0.0, 1e-3], [np.nan] * 3])
     with pytest.raises(abi.XtbloomError) as e:
         cuda_lib.compute(b, gfn1_options(cuda_lib))
-    assert e.value.args[0].startswith("NOT_IMPLEMENTED")
+    assert e.value.status == abi.NOT_IMPLEMENTED

@@ -137,7 +137,8 @@ def test_gfn1_goldens_pinned_to_tblite():
     point (charge tolerance 1e-10; the committed values were produced with
     xTB's tight SCC accuracy 1e-4) it reproduces the reference's six
     molecular GFN1 conformance cases (xTB 6.7.1 / tblite energies, forces and
-    charges) at their tolerance (5e-7)."""
+    charges) and its two QM/MM cases (energies, forces, point-charge forces)
+    at their tolerance (5e-7)."""
     import json
 
     from conftest import GOLDEN
@@ -151,3 +152,13 @@ def test_gfn1_goldens_pinned_to_tblite():
         assert np.abs(np.asarray(r["tight_forces"]) - np.asarray(c["forces"])).max() < 5e-7, c["name"]
         if c["charges"] is not None:
             assert np.abs(np.asarray(r["tight_charges"]) - np.asarray(c["charges"])).max() < 5e-7, c["name"]
+    # the two QM/MM cases (xTB 6.7.1, water dimer in six point charges)
+    pcref = {c["name"]: c for c in g["reference_pc"]}
+    assert len(g["tblite_qmmm"]) == 2
+    for c in g["tblite_qmmm"]:
+        r = pcref[c["name"]]
+        assert r["tight_status"] == 0, c["name"]
+        assert abs(r["tight_energy"] - c["energy"]) < 5e-7, c["name"]
+        assert np.abs(np.asarray(r["tight_forces"]) - np.asarray(c["forces"]).ravel()).max() < 5e-7, c["name"]
+        assert np.abs(np.asarray(r["tight_point_charge_forces"])
+                      - np.asarray(c["point_charge_forces"]).ravel()).max() < 5e-7, c["name"]

@@ -441,13 +441,17 @@ xtbloom_status_t validate_and_normalise(const xtbloom_batch_t* batch,
     return XTBLOOM_STATUS_INVALID_ARGUMENT;
   }
   if (options->model == XTBLOOM_MODEL_GFN1_XTB) {
-    // GFN1 runs molecular batches; its external-potential attachments have
-    // their own screening and are not built in this path
+    // as the reference (src/runtime/validation.cpp:1425-1437): GFN1 takes
+    // point charges and charge response, but neither interaction attachments
+    // (fields) nor the dipole publication
     bool field = false;
     for (uint8_t v : req.field_attached) field = field || v != 0;
-    if (batch->total_point_charges > 0 || req.have_response || field) {
-      err = "GFN1-xTB with external point charges, charge response or electric fields is not "
-            "implemented in this CUDA path";
+    if ((options->flags & XTBLOOM_COMPUTE_DIPOLE_MOMENTS) != 0u) {
+      err = "GFN1-xTB molecular dipole publication is not implemented";
+      return XTBLOOM_STATUS_NOT_IMPLEMENTED;
+    }
+    if (field || (has_field(batch->struct_size, XTBLOOM_BATCH_V3_SIZE) && batch->total_interactions != 0)) {
+      err = "GFN1-xTB interaction attachments are not implemented";
       return XTBLOOM_STATUS_NOT_IMPLEMENTED;
     }
   }

@@ -1351,6 +1351,105 @@ __global__ void __launch_bounds__(256) k_backtransform_wy(EigArgs g, int wcap, i
     for (int64_t k = tid; k < (int64_t)m * n; k += bs) gZ[k] = Z[k];
 }
 
+// Blocked back-transform on the FP64 tensor cores (many systems, one CTA per
+// system): per 32-reflector block, Y = V^T Z (32 x m) as 8 x 8 x 4 DMMA tiles,
+// each warp a strip of four 8-row blocks for one block of eight eigenvectors
+// (one global load of Z feeds four products), W = T Y in shared memory, and
+// Z <- Z - V W as transposed tiles (eigenvector x row: each lane updates two
+// adjacent rows of one eigenvector).  Z stays in global memory (vector-major
+// rows of n), V and T of the block in shared memory.
+__global__ void __launch_bounds__(256) k_backtransform_dmma(EigArgs g, int mcap) {
+  extern __shared__ double sm[];
+  const int s = g.list[blockIdx.x];
+  if (g.only != nullptr && g.only[s] == 0) return;
+  const int n = g.nao[s];
+  const int m = g.all_vectors ? n : g.nvec[s];
+  const int nr = n - 2;
+  if (nr <= 0 || m <= 0) return;
+  constexpr int P = WB + 1;
+  const double* a = g.A + g.mat_off[s];
+  const double* tf = g.scratch + g.scratch_off[s];
+  double* Z = g.Z + g.mat_off[s];
+  double* V = sm;                        // n x P
+  double* T = V + (size_t)n * P;         // WB x P
+  double* Y = T + WB * P;                // WB x mcap
+  double* Wm = Y + (size_t)WB * mcap;    // WB x mcap
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nw = blockDim.x >> 5;
+  const int gq = lane >> 2, tq = lane & 3;
+  const int nblk = (nr + WB - 1) / WB;
+  const int jb_count = (m + 7) / 8;
+  for (int it = 0; it < nblk; ++it) {
+    const int b = nblk - 1 - it;
+    const int i0 = b * WB;
+    const int k = min(WB, nr - i0);
+    const int L = n - i0 - 1;
+    __syncthreads();
+    load_wy_block(a, n, i0, k, L, V);
+    for (int idx = tid; idx < WB * WB; idx += blockDim.x)
+      T[(idx / WB) * P + (idx % WB)] = tf[(int64_t)b * WB * WB + idx];
+    __syncthreads();
+    // Y = V^T Z over the block's rows
+    for (int jb = warp; jb < jb_count; jb += nw) {
+      double d[4][2];
+#pragma unroll
+      for (int q = 0; q < 4; ++q) d[q][0] = d[q][1] = 0.0;
+      const int j = jb * 8 + gq;
+      const double* z = Z + (int64_t)j * n + i0 + 1;
+      for (int r0 = 0; r0 < L; r0 += 4) {
+        const int r = r0 + tq;
+        const double bz = (j < m && r < L) ? z[r] : 0.0;
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+          const double av = r < L ? V[r * P + q * 8 + gq] : 0.0;
+          mma_f64(d[q], av, bz);
+        }
+      }
+#pragma unroll
+      for (int q = 0; q < 4; ++q)
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+          const int jj = jb * 8 + 2 * tq + h;
+          if (jj < mcap) Y[(q * 8 + gq) * mcap + jj] = d[q][h];
+        }
+    }
+    __syncthreads();
+    // W = T Y (T upper triangular)
+    for (int idx = tid; idx < WB * m; idx += blockDim.x) {
+      const int p = idx / m, jj = idx - (idx / m) * m;
+      double acc = 0.0;
+      for (int q = p; q < WB; ++q) acc = fma(T[p * P + q], Y[q * mcap + jj], acc);
+      Wm[p * mcap + jj] = acc;
+    }
+    __syncthreads();
+    // Z^T tile (eigenvectors jb x rows rb) -= W^T V^T
+    const int rb_count = (L + 7) / 8;
+    for (int t = warp; t < jb_count * rb_count; t += nw) {
+      const int jb = t / rb_count, rb = t - (t / rb_count) * rb_count;
+      double d[2] = {0.0, 0.0};
+#pragma unroll
+      for (int q0 = 0; q0 < WB; q0 += 4) {
+        const int jr = jb * 8 + gq, rr = rb * 8 + gq;
+        const double aw = jr < m ? Wm[(q0 + tq) * mcap + jr] : 0.0;
+        const double bv = rr < L ? V[rr * P + q0 + tq] : 0.0;
+        mma_f64(d, aw, bv);
+      }
+      const int j = jb * 8 + gq;
+      if (j < m) {
+        double* z = Z + (int64_t)j * n + i0 + 1;
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+          const int r = rb * 8 + 2 * tq + h;
+          if (r < L) z[r] -= d[h];
+        }
+      }
+    }
+  }
+}
+
+size_t backtransform_dmma_bytes(int n, int mcap) {
+  return ((size_t)n * (WB + 1) + WB * (WB + 1) + 2 * (size_t)WB * mcap) * sizeof(double);
+}
+
 void launch_backtransform_wy(const EigArgs& g, int count, int max_n, int max_m, int want_m,
                              cudaStream_t stream) {
   if (count == 0) return;
@@ -1370,6 +1469,13 @@ void launch_backtransform_wy(const EigArgs& g, int count, int max_n, int max_m, 
                         ((size_t)max_n * (WB + 1) + WB * (WB + 1)) * sizeof(double);
   if (parts > 1 && staged <= cap_s) {
     k_backtransform_wy<true><<<dim3(parts, count), 256, staged, stream>>>(g, wc, per);
+    return;
+  }
+  // one CTA per system: the block products on the FP64 tensor cores
+  const int mcap = (want_m + 7) / 8 * 8;
+  const size_t capd = allow_max_dynamic_smem(k_backtransform_dmma);
+  if (parts == 1 && backtransform_dmma_bytes(max_n, mcap) <= capd) {
+    k_backtransform_dmma<<<count, 256, backtransform_dmma_bytes(max_n, mcap), stream>>>(g, mcap);
     return;
   }
   (void)cap;

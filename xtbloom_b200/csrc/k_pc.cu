@@ -1,7 +1,10 @@
-// External point charges embedding GFN2 systems (xTB's softened shell
-// monopole coupling, model/gfn2/external_point_charges.cpp:277-490 of the
-// reference): for shell s on atom A and charge p,
-//   K_sp = (|R_A - R_p|^2 + a_sp^2)^-1/2,  a_sp = 2 / (eta_s + gamma_p),
+// External point charges embedding GFN2 and GFN1 systems (xTB's softened
+// shell monopole coupling, model/gfn2/external_point_charges.cpp:277-490 and
+// model/gfn1/external_point_charges.cpp:317-323 of the reference): for shell
+// s on atom A and charge p,
+//   K_sp = (|R_A - R_p|^2 + a_sp^2)^-1/2,
+//   a_sp = 2 / (eta_s + gamma_p) (GFN2: arithmetic mean of the hardnesses),
+//   a_sp = 1 / (2 eta_s) + 1 / (2 gamma_p) (GFN1: harmonic mean),
 //   V_s = sum_p Q_p K_sp (fixed by the geometry, added to the shell potential
 //   every SCC iteration),  E_pc = sum_s q_s V_s,
 //   dE/dR_A = -sum_{s in A, p} q_s Q_p d_Ap K_sp^3,  dE/dR_p = -sum over A of the same,
@@ -16,7 +19,7 @@ __device__ __forceinline__ double pc_kernel(const DevTopo& t, int64_t at, double
   dx = t.pos[3 * at] - t.pc_pos[3 * p];
   dy = t.pos[3 * at + 1] - t.pc_pos[3 * p + 1];
   dz = t.pos[3 * at + 2] - t.pc_pos[3 * p + 2];
-  const double a = 2.0 / (eta + t.pc_gam[p]);
+  const double a = t.m.gfn1 ? 0.5 / eta + 0.5 / t.pc_gam[p] : 2.0 / (eta + t.pc_gam[p]);
   return 1.0 / sqrt(dx * dx + dy * dy + dz * dz + a * a);
 }
 
