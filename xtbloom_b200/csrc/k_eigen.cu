@@ -338,7 +338,7 @@ void launch_gemm(const GemmArgs& g, bool transA, bool weighted, int max_tiles, i
 // reflector with the updated block in the same pass over the packed triangle:
 //   (A) update the block's first column with (v_i, w_i); it gives x_{i+1};
 //   (B) v_{i+1}, tau_{i+1} from x_{i+1};
-//   (C) 16 x 32 tiles of the rest, dealt round-robin to the warps: update with
+//   (C) 8 x 32 tiles of the rest, dealt round-robin to the warps: update with
 //       (v_i, w_i), then accumulate A v_{i+1} (see fused_tile);
 //   (D) w_{i+1} = tau p - (tau/2)(p.v) v, kept as tau p and the scalar
 //       (tau/2)(p.v); readers of w apply the correction.
@@ -363,19 +363,22 @@ __device__ __forceinline__ double block_sum1(double v, double* buf) {
   return t;
 }
 
-// One tile of 16 rows (R0..) and 32 columns (C0..) of the lower triangle of
-// the block that starts at row/column o of the packed storage (size m), for
-// one warp: update every element with (vi, wi), then lane j accumulates the
-// transposed part of A vn for column C0+j directly and keeps 16 row partials,
-// which a butterfly reduce-scatter (15 exchanges, then one across the half
-// warps) leaves with lane i (and i+16) holding row R0+i.  Elements on the
+// One tile of kTileRows rows (R0..) and 32 columns (C0..) of the lower
+// triangle of the block that starts at row/column o of the packed storage
+// (size m), for one warp: update every element with (vi, wi), then lane j
+// accumulates the transposed part of A vn for column C0+j directly and keeps
+// kTileRows row partials, which a butterfly reduce-scatter (over the low lane
+// bits, then exchanges across the remaining lane groups) leaves with lane i
+// (and every lane congruent to it) holding row R0+i.  Eight-row tiles keep
+// the row values and partials in few enough registers that the rows of a
+// tile overlap instead of running one after another.  Elements on the
 // diagonal count once.  Results go to the warp's pw.  wi holds w + kw v (the
 // previous reflector's correction kw is applied here).  The tile's elements
 // are all loaded before any is stored and the row values come from registers
 // by shuffles, so the shared-memory loads issue back to back.
 // SQ: L is a square row-major matrix with leading dimension ld (the lower
 // triangle is used) instead of the packed triangle.
-constexpr int kTileRows = 16;
+constexpr int kTileRows = 8;
 template <bool SQ = false>
 __device__ __forceinline__ void fused_tile(double* L, int o, int m, int R0, int C0,
                                            const double* vi, const double* wi, double kw,
@@ -435,26 +438,29 @@ __device__ __forceinline__ void fused_tile(double* L, int o, int m, int R0, int 
       a[k] = keep + __shfl_xor_sync(0xffffffffu, send, sh);
     }
   }
-  a[0] += __shfl_xor_sync(0xffffffffu, a[0], 16);
+#pragma unroll
+  for (int x = kTileRows; x < 32; x <<= 1) a[0] += __shfl_xor_sync(0xffffffffu, a[0], x);
   if (lane < kTileRows && rl < m) pw[rl] += a[0];
   if (cok) pw[cj] += col;
 }
 
-// Tiles of the lower triangle of an m x m block: row blocks of 16, column
-// blocks of 32; row blocks 2p and 2p+1 hold p+1 tiles each, so the tiles of
-// row blocks below 2p number p(p+1).
+// Tiles of the lower triangle of an m x m block: row blocks of kTileRows,
+// column blocks of 32; with G = 32 / kTileRows, row blocks G p .. G p + G - 1
+// hold p + 1 tiles each, so the tiles of the row blocks below G p number
+// G p (p + 1) / 2.
+constexpr int kTileGroup = 32 / kTileRows;
 __device__ __forceinline__ int tri_tiles(int m) {
   const int nr = (m + kTileRows - 1) / kTileRows;
-  const int p = nr >> 1;
-  return p * (p + 1) + ((nr & 1) ? p + 1 : 0);
+  const int p = nr / kTileGroup;
+  return kTileGroup * p * (p + 1) / 2 + (nr % kTileGroup) * (p + 1);
 }
 __device__ __forceinline__ void tri_tile(int tl, int& R, int& C) {
-  int p = (int)((sqrtf(4.0f * tl + 1.0f) - 1.0f) * 0.5f);
-  while ((p + 1) * (p + 2) <= tl) ++p;
-  while (p * (p + 1) > tl) --p;
-  const int rem = tl - p * (p + 1);
-  R = 2 * p + (rem > p ? 1 : 0);
-  C = rem > p ? rem - (p + 1) : rem;
+  int p = (int)((sqrtf(8.0f * tl / kTileGroup + 1.0f) - 1.0f) * 0.5f);
+  while (kTileGroup * (p + 1) * (p + 2) / 2 <= tl) ++p;
+  while (kTileGroup * p * (p + 1) / 2 > tl) --p;
+  const int rem = tl - kTileGroup * p * (p + 1) / 2;
+  R = kTileGroup * p + rem / (p + 1);
+  C = rem % (p + 1);
 }
 
 template <int NT>
@@ -584,7 +590,7 @@ __global__ void __launch_bounds__(NT) k_tridiag_smem(EigArgs g, const int32_t* l
 // shared-memory block: the first K = n - nloc reflectors are formed in place
 // on the lower triangle of the square matrix (L2 / HBM resident), with the
 // same four phases per column as the shared-memory kernel, so each column
-// reads and writes the trailing triangle once, in coalesced 16 x 32 tiles.
+// reads and writes the trailing triangle once, in coalesced 8 x 32 tiles.
 // The last step (column K) applies reflector K-1 to the trailing block and
 // forms no reflector: the block from row/column K is then A^(K), which the
 // shared-memory kernel loads and finishes.  Only the vectors and the warps'
@@ -1377,7 +1383,6 @@ __global__ void __launch_bounds__(256) k_backtransform_dmma(EigArgs g, int mcap)
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nw = blockDim.x >> 5;
   const int gq = lane >> 2, tq = lane & 3;
   const int nblk = (nr + WB - 1) / WB;
-  const int jb_count = (m + 7) / 8;
   for (int it = 0; it < nblk; ++it) {
     const int b = nblk - 1 - it;
     const int i0 = b * WB;
@@ -1388,60 +1393,64 @@ __global__ void __launch_bounds__(256) k_backtransform_dmma(EigArgs g, int mcap)
     for (int idx = tid; idx < WB * WB; idx += blockDim.x)
       T[(idx / WB) * P + (idx % WB)] = tf[(int64_t)b * WB * WB + idx];
     __syncthreads();
-    // Y = V^T Z over the block's rows
-    for (int jb = warp; jb < jb_count; jb += nw) {
-      double d[4][2];
+    // eigenvectors in chunks of mcap (the Y and W buffers' width): the count
+    // of a system's needed vectors is set on the device and can exceed the
+    // bucket's estimate
+    for (int j0 = 0; j0 < m; j0 += mcap) {
+      const int mc = min(mcap, m - j0);
+      const int jb_count = (mc + 7) / 8;
+      // Y = V^T Z over the block's rows
+      for (int jb = warp; jb < jb_count; jb += nw) {
+        double d[4][2];
 #pragma unroll
-      for (int q = 0; q < 4; ++q) d[q][0] = d[q][1] = 0.0;
-      const int j = jb * 8 + gq;
-      const double* z = Z + (int64_t)j * n + i0 + 1;
-      for (int r0 = 0; r0 < L; r0 += 4) {
-        const int r = r0 + tq;
-        const double bz = (j < m && r < L) ? z[r] : 0.0;
+        for (int q = 0; q < 4; ++q) d[q][0] = d[q][1] = 0.0;
+        const int jl = jb * 8 + gq;
+        const double* z = Z + (int64_t)(j0 + jl) * n + i0 + 1;
+        for (int r0 = 0; r0 < L; r0 += 4) {
+          const int r = r0 + tq;
+          const double bz = (jl < mc && r < L) ? z[r] : 0.0;
 #pragma unroll
-        for (int q = 0; q < 4; ++q) {
-          const double av = r < L ? V[r * P + q * 8 + gq] : 0.0;
-          mma_f64(d[q], av, bz);
+          for (int q = 0; q < 4; ++q) {
+            const double av = r < L ? V[r * P + q * 8 + gq] : 0.0;
+            mma_f64(d[q], av, bz);
+          }
+        }
+#pragma unroll
+        for (int q = 0; q < 4; ++q)
+#pragma unroll
+          for (int h = 0; h < 2; ++h) Y[(q * 8 + gq) * mcap + jb * 8 + 2 * tq + h] = d[q][h];
+      }
+      __syncthreads();
+      // W = T Y (T upper triangular)
+      for (int idx = tid; idx < WB * mc; idx += blockDim.x) {
+        const int p = idx / mc, jj = idx - (idx / mc) * mc;
+        double acc = 0.0;
+        for (int q = p; q < WB; ++q) acc = fma(T[p * P + q], Y[q * mcap + jj], acc);
+        Wm[p * mcap + jj] = acc;
+      }
+      __syncthreads();
+      // Z^T tile (eigenvectors jb x rows rb) -= W^T V^T
+      const int rb_count = (L + 7) / 8;
+      for (int t = warp; t < jb_count * rb_count; t += nw) {
+        const int jb = t / rb_count, rb = t - (t / rb_count) * rb_count;
+        double d[2] = {0.0, 0.0};
+        const int jl = jb * 8 + gq, rr = rb * 8 + gq;
+#pragma unroll
+        for (int q0 = 0; q0 < WB; q0 += 4) {
+          const double aw = jl < mc ? Wm[(q0 + tq) * mcap + jl] : 0.0;
+          const double bv = rr < L ? V[rr * P + q0 + tq] : 0.0;
+          mma_f64(d, aw, bv);
+        }
+        if (jl < mc) {
+          double* z = Z + (int64_t)(j0 + jl) * n + i0 + 1;
+#pragma unroll
+          for (int h = 0; h < 2; ++h) {
+            const int r = rb * 8 + 2 * tq + h;
+            if (r < L) z[r] -= d[h];
+          }
         }
       }
-#pragma unroll
-      for (int q = 0; q < 4; ++q)
-#pragma unroll
-        for (int h = 0; h < 2; ++h) {
-          const int jj = jb * 8 + 2 * tq + h;
-          if (jj < mcap) Y[(q * 8 + gq) * mcap + jj] = d[q][h];
-        }
-    }
-    __syncthreads();
-    // W = T Y (T upper triangular)
-    for (int idx = tid; idx < WB * m; idx += blockDim.x) {
-      const int p = idx / m, jj = idx - (idx / m) * m;
-      double acc = 0.0;
-      for (int q = p; q < WB; ++q) acc = fma(T[p * P + q], Y[q * mcap + jj], acc);
-      Wm[p * mcap + jj] = acc;
-    }
-    __syncthreads();
-    // Z^T tile (eigenvectors jb x rows rb) -= W^T V^T
-    const int rb_count = (L + 7) / 8;
-    for (int t = warp; t < jb_count * rb_count; t += nw) {
-      const int jb = t / rb_count, rb = t - (t / rb_count) * rb_count;
-      double d[2] = {0.0, 0.0};
-#pragma unroll
-      for (int q0 = 0; q0 < WB; q0 += 4) {
-        const int jr = jb * 8 + gq, rr = rb * 8 + gq;
-        const double aw = jr < m ? Wm[(q0 + tq) * mcap + jr] : 0.0;
-        const double bv = rr < L ? V[rr * P + q0 + tq] : 0.0;
-        mma_f64(d, aw, bv);
-      }
-      const int j = jb * 8 + gq;
-      if (j < m) {
-        double* z = Z + (int64_t)j * n + i0 + 1;
-#pragma unroll
-        for (int h = 0; h < 2; ++h) {
-          const int r = rb * 8 + 2 * tq + h;
-          if (r < L) z[r] -= d[h];
-        }
-      }
+      __syncthreads();
     }
   }
 }
@@ -1585,13 +1594,10 @@ __global__ void __launch_bounds__(256) k_backtransform_rows(EigArgs g) {
   if (g.only != nullptr && g.only[s] == 0) return;
   const int n = g.nao[s];
   const int mt = g.all_vectors ? n : g.nvec[s];
-  const int jbeg = blockIdx.x * MC;
-  const int m = min(mt - jbeg, MC);
   const int nr = n - 2;
-  if (nr <= 0 || m <= 0) return;
+  if (nr <= 0) return;
   const double* a = g.A + g.mat_off[s];
   const double* tf = g.scratch + g.scratch_off[s];
-  double* gZ = g.Z + g.mat_off[s] + (int64_t)jbeg * n;
   constexpr int P = WB + 1;
   double* Z = sm;                          // MC x n
   double* Vc = Z + (size_t)MC * n;         // kWyRows x P
@@ -1599,54 +1605,61 @@ __global__ void __launch_bounds__(256) k_backtransform_rows(EigArgs g) {
   double* Y = T + WB * P;                  // WB x MC
   double* W = Y + WB * MC;                 // WB x MC
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nw = blockDim.x >> 5;
-  for (int64_t k = tid; k < (int64_t)m * n; k += blockDim.x) Z[k] = gZ[k];
   const int nblk = (nr + WB - 1) / WB;
-  for (int it = 0; it < nblk; ++it) {
-    const int b = nblk - 1 - it;
-    const int i0 = b * WB;
-    const int k = min(WB, nr - i0);
-    const int L = n - i0 - 1;
-    for (int idx = tid; idx < WB * WB; idx += blockDim.x)
-      T[(idx / WB) * P + (idx % WB)] = tf[(int64_t)b * WB * WB + idx];
-    for (int idx = tid; idx < WB * MC; idx += blockDim.x) Y[idx] = 0.0;
-    // Y = V^T Z: lane = reflector, warps over this CTA's vectors
-    for (int r0 = 0; r0 < L; r0 += kWyRows) {
-      const int rc = min(kWyRows, L - r0);
-      __syncthreads();
-      load_wy_rows(a, n, i0, k, r0, rc, Vc);
-      __syncthreads();
-      for (int j = warp; j < m; j += nw) {
-        const double* z = Z + (int64_t)j * n + i0 + 1 + r0;
-        double acc = 0.0;
-        for (int r = 0; r < rc; ++r) acc = fma(Vc[r * P + lane], z[r], acc);
-        Y[lane * MC + j] += acc;
-      }
-    }
+  // slices of MC eigenvectors; the count of needed vectors is set on the
+  // device, so a CTA takes every gridDim.x-th slice until all are done
+  for (int jbeg = blockIdx.x * MC; jbeg < mt; jbeg += gridDim.x * MC) {
+    const int m = min(mt - jbeg, MC);
+    double* gZ = g.Z + g.mat_off[s] + (int64_t)jbeg * n;
     __syncthreads();
-    // W = T Y (T upper triangular)
-    for (int idx = tid; idx < WB * MC; idx += blockDim.x) {
-      const int p = idx / MC, j = idx - (idx / MC) * MC;
-      double acc = 0.0;
-      for (int q = p; q < WB; ++q) acc = fma(T[p * P + q], Y[q * MC + j], acc);
-      W[idx] = acc;
-    }
-    // Z -= V W
-    for (int r0 = 0; r0 < L; r0 += kWyRows) {
-      const int rc = min(kWyRows, L - r0);
-      __syncthreads();
-      load_wy_rows(a, n, i0, k, r0, rc, Vc);
-      __syncthreads();
-      for (int idx = tid; idx < rc * m; idx += blockDim.x) {
-        const int j = idx / rc, r = idx - (idx / rc) * rc;
-        const int qmax = min(k, r0 + r + 1);
-        double acc = 0.0;
-        for (int q = 0; q < qmax; ++q) acc = fma(Vc[r * P + q], W[q * MC + j], acc);
-        Z[(int64_t)j * n + i0 + 1 + r0 + r] -= acc;
+    for (int64_t k = tid; k < (int64_t)m * n; k += blockDim.x) Z[k] = gZ[k];
+    for (int it = 0; it < nblk; ++it) {
+      const int b = nblk - 1 - it;
+      const int i0 = b * WB;
+      const int k = min(WB, nr - i0);
+      const int L = n - i0 - 1;
+      for (int idx = tid; idx < WB * WB; idx += blockDim.x)
+        T[(idx / WB) * P + (idx % WB)] = tf[(int64_t)b * WB * WB + idx];
+      for (int idx = tid; idx < WB * MC; idx += blockDim.x) Y[idx] = 0.0;
+      // Y = V^T Z: lane = reflector, warps over this CTA's vectors
+      for (int r0 = 0; r0 < L; r0 += kWyRows) {
+        const int rc = min(kWyRows, L - r0);
+        __syncthreads();
+        load_wy_rows(a, n, i0, k, r0, rc, Vc);
+        __syncthreads();
+        for (int j = warp; j < m; j += nw) {
+          const double* z = Z + (int64_t)j * n + i0 + 1 + r0;
+          double acc = 0.0;
+          for (int r = 0; r < rc; ++r) acc = fma(Vc[r * P + lane], z[r], acc);
+          Y[lane * MC + j] += acc;
+        }
       }
+      __syncthreads();
+      // W = T Y (T upper triangular)
+      for (int idx = tid; idx < WB * MC; idx += blockDim.x) {
+        const int p = idx / MC, j = idx - (idx / MC) * MC;
+        double acc = 0.0;
+        for (int q = p; q < WB; ++q) acc = fma(T[p * P + q], Y[q * MC + j], acc);
+        W[idx] = acc;
+      }
+      // Z -= V W
+      for (int r0 = 0; r0 < L; r0 += kWyRows) {
+        const int rc = min(kWyRows, L - r0);
+        __syncthreads();
+        load_wy_rows(a, n, i0, k, r0, rc, Vc);
+        __syncthreads();
+        for (int idx = tid; idx < rc * m; idx += blockDim.x) {
+          const int j = idx / rc, r = idx - (idx / rc) * rc;
+          const int qmax = min(k, r0 + r + 1);
+          double acc = 0.0;
+          for (int q = 0; q < qmax; ++q) acc = fma(Vc[r * P + q], W[q * MC + j], acc);
+          Z[(int64_t)j * n + i0 + 1 + r0 + r] -= acc;
+        }
+      }
+      __syncthreads();
     }
-    __syncthreads();
+    for (int64_t k = tid; k < (int64_t)m * n; k += blockDim.x) gZ[k] = Z[k];
   }
-  for (int64_t k = tid; k < (int64_t)m * n; k += blockDim.x) gZ[k] = Z[k];
 }
 
 template <int MC>
