@@ -557,11 +557,13 @@ def run_ours(args, world, rank, local):
         results[form] = (host_outs, split)
         lib.close()
         torch.cuda.synchronize()
-    gfn1_line = None
-    if not args.no_gfn1:
-        gfn1_line = time_gfn1(args, world, local, stream)
-    autograd_line = None if args.no_autograd else time_autograd(args, world, local, stream)
-    water_line = None if args.no_water else time_water(args, world, local, stream)
+    # the GFN1, autograd and water-cluster lines characterise one GPU; with
+    # several ranks the run times the headline batch per rank and one batch
+    # split over the ranks, and stays short while every GPU is held
+    single = world == 1
+    gfn1_line = time_gfn1(args, world, local, stream) if single and not args.no_gfn1 else None
+    autograd_line = time_autograd(args, world, local, stream) if single and not args.no_autograd else None
+    water_line = time_water(args, world, local, stream) if single and not args.no_water else None
     strong = time_strong(args, world, rank, local, stream) if world > 1 else None
     clk = clocks.stop()
     h2d = (B + 1) * 8 + N * 4 + 3 * N * 8 + B * 8 + B * 4

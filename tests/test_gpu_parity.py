@@ -72,6 +72,21 @@ def test_live_reference_on_random_workload_sample(cuda_lib):
     assert np.abs(out["atomic_charges"] - r["atomic_charges"]).max() < TOL_Q
 
 
+@pytest.mark.skipif(not REF_LIB.exists(), reason="reference library not built")
+def test_all_64_decane_conformers_against_live_reference(cuda_lib):
+    """The whole 64-conformer C10H22 batch (seed 0), every output, against the
+    reference library run live, iteration counts included."""
+    b = W.config0(64, seed=0)
+    out = cuda_lib.compute(b)
+    ref = abi.Library(str(REF_LIB), backend=abi.BACKEND_CPU, cpu_threads=0)
+    r = ref.compute(b)
+    assert (r["per_system_status"] == 0).all() and (out["per_system_status"] == 0).all()
+    assert np.abs(out["energies"] - r["energies"]).max() < TOL_E
+    assert np.abs(out["forces"] - r["forces"]).max() < TOL_F
+    assert np.abs(out["atomic_charges"] - r["atomic_charges"]).max() < TOL_Q
+    assert np.abs(out["scc_iterations"] - r["scc_iterations"]).max() <= 1
+
+
 def test_stage_intermediates_match_oracle(cuda_lib, fixtures):
     """Integer layout and every geometry-stage intermediate against the numpy oracle."""
     from oracle import gfn2
