@@ -331,20 +331,22 @@ void launch_gemm(const GemmArgs& g, bool transA, bool weighted, int max_tiles, i
 }
 
 // ---------------------------------------------------------------------------
-// Shared-memory Householder tridiagonalisation.  The trailing nl x nl block
-// (rows/columns i0..n-1, i0 = max(0, n - nloc)) lives in packed lower storage
-// (local element (r, c), r >= c, at r(r+1)/2 + c) in one CTA's shared memory.
-// Step i applies reflector i's rank-2 update and forms the product of the next
-// reflector with the updated block in the same pass over the packed triangle:
+// Householder tridiagonalisation, one CTA per system.  Step i applies
+// reflector i's rank-2 update and forms the product of the next reflector
+// with the updated block in the same pass over the lower triangle:
 //   (A) update the block's first column with (v_i, w_i); it gives x_{i+1};
 //   (B) v_{i+1}, tau_{i+1} from x_{i+1};
 //   (C) 8 x 32 tiles of the rest, dealt round-robin to the warps: update with
 //       (v_i, w_i), then accumulate A v_{i+1} (see fused_tile);
 //   (D) w_{i+1} = tau p - (tau/2)(p.v) v, kept as tau p and the scalar
 //       (tau/2)(p.v); readers of w apply the correction.
-// Four barriers per column: after (A)'s norm, (B), (C) and (D)'s dot product.
-// Reflectors are stored in the global matrix in the layout the back-transform
-// reads (row i, columns i+2..), as the global-memory prefix kernel does.
+// The global-memory prefix (k_tridiag_prefix, columns above the shared-memory
+// block) runs these four phases with a barrier after each; the
+// shared-memory kernel (k_tridiag_smem) merges (B) and (D) into its other
+// passes and needs two barriers per column.  Both keep the trailing block's
+// lower triangle only: packed ((r, c), r >= c, at r(r+1)/2 + c) in shared
+// memory, or in place in the square matrix.  Reflectors are stored in the
+// global matrix in the layout the back-transform reads (row i, columns i+2..).
 // ---------------------------------------------------------------------------
 __device__ __forceinline__ int pk32(int r, int c) { return r * (r + 1) / 2 + c; }
 
@@ -463,8 +465,97 @@ __device__ __forceinline__ void tri_tile(int tl, int& R, int& C) {
   C = rem % (p + 1);
 }
 
+
+// Shared-memory kernel: the trailing nl x nl block (rows/columns i0..n-1,
+// i0 = max(0, n - nloc)) in packed lower storage in one CTA's shared memory,
+// two barriers per column.  The reflector of a column is kept unscaled (the
+// column's own values) and scaled by 1/(alpha - beta) where it is read, so no
+// pass has to wait for a scaled copy; the warps' partial products
+// A v and their dot products with v are posted by the tile pass and summed by
+// the next column's first pass, where w = tau p - (tau/2)(tau p.v) v is formed.
+// Per column:
+//   (A) row r (one thread): p_r = sum of the warps' partials (row 0's partials
+//       sit in a separate double-buffered array, because every thread reads
+//       them), w_r, the update of the block's first column with (v_i, w_i),
+//       the column's norm -> one barrier;
+//   (C) every thread forms alpha, beta, tau and the scale redundantly; the
+//       8 x 32 tiles of the rest are updated with (v_i, w_i) and multiplied
+//       by v_{i+1}; the warps' partials of p and p.v are posted -> one barrier.
+__device__ __forceinline__ void fused_tile2(double* L, int o, int m, int R0, int C0,
+                                            const double* vi, double sci, const double* wi,
+                                            const double* vn, double scn, double* pw, double* pw0,
+                                            int lane, bool want_mv, double& dot) {
+  const int cj = C0 + lane;
+  const bool cok = cj < m;
+  const double vn_c = cok ? (cj == 0 ? 1.0 : vn[cj] * scn) : 0.0;
+  const double vi_c = cok ? vi[cj] * sci : 0.0;
+  const double wi_c = cok ? wi[cj] : 0.0;
+  const int rl = R0 + (lane & (kTileRows - 1));
+  const bool rok = rl < m;
+  const double vi_r = rok ? vi[rl] * sci : 0.0;
+  const double wi_r = rok ? wi[rl] : 0.0;
+  const double vn_r = rok ? (rl == 0 ? 1.0 : vn[rl] * scn) : 0.0;
+  const int rows = min(kTileRows, m - R0);
+  const int dcol = cj - R0;
+  double a[kTileRows];
+  const int base0 = pk32(o + R0, o) + cj;
+  {
+    int base = base0;
+#pragma unroll
+    for (int i = 0; i < kTileRows; ++i) {
+      const bool ok = i < rows && cok && dcol <= i;
+      a[i] = ok ? L[base] : 0.0;
+      base += o + R0 + i + 1;
+    }
+  }
+  double col = 0.0;
+#pragma unroll
+  for (int i = 0; i < kTileRows; ++i) {
+    const double vr = __shfl_sync(0xffffffffu, vi_r, i);
+    const double wr = __shfl_sync(0xffffffffu, wi_r, i);
+    const double nr = __shfl_sync(0xffffffffu, vn_r, i);
+    const double u = a[i] - (vr * wi_c + wr * vi_c);
+    a[i] = dcol > i ? 0.0 : u;
+    if (dcol < i) col = fma(a[i], nr, col);
+  }
+  {
+    int base = base0;
+#pragma unroll
+    for (int i = 0; i < kTileRows; ++i) {
+      const bool ok = i < rows && cok && dcol <= i;
+      if (ok) L[base] = a[i];
+      base += o + R0 + i + 1;
+    }
+  }
+  if (!want_mv) return;
+#pragma unroll
+  for (int i = 0; i < kTileRows; ++i) a[i] *= vn_c;
+#pragma unroll
+  for (int sh = kTileRows / 2; sh >= 1; sh >>= 1) {
+    const bool up = (lane & sh) != 0;
+#pragma unroll
+    for (int k = 0; k < sh; ++k) {
+      const double send = up ? a[k] : a[k + sh];
+      const double keep = up ? a[k + sh] : a[k];
+      a[k] = keep + __shfl_xor_sync(0xffffffffu, send, sh);
+    }
+  }
+#pragma unroll
+  for (int x = kTileRows; x < 32; x <<= 1) a[0] += __shfl_xor_sync(0xffffffffu, a[0], x);
+  if (lane < kTileRows && rok) {
+    double* dst = rl == 0 ? pw0 : pw + rl;
+    *dst += a[0];
+    dot = fma(a[0], vn_r, dot);
+  }
+  if (cok) {
+    double* dst = cj == 0 ? pw0 : pw + cj;
+    *dst += col;
+    dot = fma(col, vn_c, dot);
+  }
+}
+
 template <int NT>
-__global__ void __launch_bounds__(NT) k_tridiag_smem(EigArgs g, const int32_t* list, int nloc) {
+__global__ void __launch_bounds__(NT, 512 / NT) k_tridiag_smem(EigArgs g, const int32_t* list, int nloc) {
   extern __shared__ double sm[];
   constexpr int nw = NT / 32;
   const int s = list[blockIdx.x];
@@ -481,100 +572,100 @@ __global__ void __launch_bounds__(NT) k_tridiag_smem(EigArgs g, const int32_t* l
   double* L = sm;
   double* vb0 = L + pk32(nl, 0);
   double* vb1 = vb0 + nl;
-  double* wb0 = vb1 + nl;
-  double* wb1 = wb0 + nl;
-  double* priv = wb1 + nl;            // nw x nl
-  double* red = priv + nw * nl;       // 2 x 32 (alternating reduction buffers)
-  __shared__ double s_alpha;
+  double* wb = vb1 + nl;
+  double* priv = wb + nl;             // nw x nl: the warps' partials of p (rows >= 1)
+  double* red = priv + nw * nl;       // 32: norm partials
+  double* dots = red + 32;            // 32: the warps' partials of p.v
+  double* row0 = dots + 32;           // 2 x 32: the warps' partials of p_0
   for (int r = warp; r < nl; r += nw)
     for (int c = lane; c <= r; c += 32) L[pk32(r, c)] = ga[(int64_t)(i0 + r) * n + i0 + c];
   for (int k = tid; k < nw * nl; k += NT) priv[k] = 0.0;
-  for (int k = tid; k < nl; k += NT) vb0[k] = wb0[k] = vb1[k] = wb1[k] = 0.0;
+  for (int k = tid; k < nl; k += NT) vb0[k] = vb1[k] = wb[k] = 0.0;
+  if (tid < 32) { dots[tid] = 0.0; row0[tid] = 0.0; row0[32 + tid] = 0.0; }
   __syncthreads();
   if (nl == 1) {
     if (tid == 0) { d[0] = L[0]; e[0] = 0.0; tau[0] = 0.0; }
     return;
   }
   int cur = 0;
-  // w of the current reflector is stored as tau p; kw = (tau/2)(tau p . v) is
-  // the correction w = tau p - kw v, applied where w is read.
-  double kw = 0.0;
-  // Step i = -1 applies no update; its column gives reflector 0 of the block.
+  double sc_prev = 0.0, tau_prev = 0.0;
   for (int i = -1; i + 2 < nl; ++i) {
     const int o = i + 1, m = nl - o;
     const double* vi = cur ? vb1 : vb0;
-    const double* wi = cur ? wb1 : wb0;
     double* vn = cur ? vb0 : vb1;
-    double* wn = cur ? wb0 : wb1;
-    const bool next = o + 3 <= nl;      // reflector o exists
-    // (A) update the block's first column; its tail gives the next reflector
+    double* r0c = row0 + 32 * cur;
+    double* r0n = row0 + 32 * (cur ^ 1);
+    const bool next = o + 3 <= nl;
+    // (A) w_i from the posted partials, then the block's first column
+    double pv = 0.0, p0 = 0.0;
+#pragma unroll
+    for (int w = 0; w < nw; ++w) {
+      pv += dots[w];
+      p0 += r0c[w];
+    }
+    const double kw = 0.5 * tau_prev * tau_prev * pv;
+    const double w0 = tau_prev * p0 - kw;          // v_i[0] = 1
     double part = 0.0;
-    const double vi0 = vi[0], wi0 = fma(-kw, vi0, wi[0]);
     for (int r = tid; r < m; r += NT) {
+      double wr = w0;
+      double vr = 1.0;
+      if (r > 0) {
+        double t = 0.0;
+#pragma unroll
+        for (int w = 0; w < nw; ++w) {
+          t += priv[w * nl + r];
+          priv[w * nl + r] = 0.0;
+        }
+        vr = vi[r] * sc_prev;
+        wr = fma(-kw, vr, tau_prev * t);
+      }
+      wb[r] = wr;
       const int idx = pk32(o + r, o);
-      const double vr = vi[r];
-      const double c = L[idx] - (vr * wi0 + fma(-kw, vr, wi[r]) * vi0);
+      const double c = L[idx] - (vr * w0 + wr);
       L[idx] = c;
       if (r == 0) d[o] = c;
       if (r >= 1) vn[r - 1] = c;
-      if (r == 1) s_alpha = c;
       if (r >= 2) part += c * c;
     }
     const double xn2 = block_sum1<nw>(part, red);
-    // (B)
-    double ti = 0.0;
+    // reflector o+1 from the updated column (every thread, same operands)
+    double ti = 0.0, sc = 0.0;
     if (next) {
-      const double alpha = s_alpha;
+      const double alpha = vn[0];
       double beta = alpha;
       if (xn2 > 0.0) {
         beta = -copysign(sqrt(alpha * alpha + xn2), alpha);
         ti = (beta - alpha) / beta;
-        const double sc = 1.0 / (alpha - beta);
-        for (int k = tid + 1; k < m - 1; k += NT) {
-          const double vk = vn[k] * sc;
-          vn[k] = vk;
-          ga[(int64_t)(i0 + o) * n + i0 + o + 1 + k] = vk;
-        }
-      } else {
-        for (int k = tid + 1; k < m - 1; k += NT) vn[k] = 0.0;
+        sc = 1.0 / (alpha - beta);
+        for (int k = tid + 1; k < m - 1; k += NT)
+          ga[(int64_t)(i0 + o) * n + i0 + o + 1 + k] = vn[k] * sc;
       }
       if (tid == 0) {
-        vn[0] = 1.0;
         e[o] = beta;
         tau[o] = ti;
       }
-    } else {
-      for (int k = tid; k < m; k += NT) vn[k] = 0.0;
     }
-    __syncthreads();
-    // (C) rank-2 update of the rest of the block, fused with A v_next
+    if (tid < nw) r0c[tid] = 0.0;     // read above, before the barrier; next used two columns on
+    // (C) rank-2 update of the rest of the block, fused with A v_{o+1}
     const int m1 = m - 1;
     {
       const int ntiles = tri_tiles(m1);
       double* pw = priv + warp * nl;
       const bool mv = next && ti != 0.0;
+      double dot = 0.0;
       for (int tl = warp; tl < ntiles; tl += nw) {
         int R, C;
         tri_tile(tl, R, C);
-        fused_tile(L, o + 1, m1, R * kTileRows, C << 5, vi + 1, wi + 1, kw, vn, pw, lane, mv);
+        fused_tile2(L, o + 1, m1, R * kTileRows, C << 5, vi + 1, sc_prev, wb + 1, vn, sc, pw,
+                    r0n + warp, lane, mv, dot);
       }
+      dot = warp_sum(dot);
+      if (lane == 0) dots[warp] = mv ? dot : 0.0;
     }
     __syncthreads();
     if (!next) break;
-    // (D) w_next = tau p (stored) and its correction kw = (tau/2)(tau p . v)
-    double pv = 0.0;
-    for (int k = tid; k < m1; k += NT) {
-      double t = 0.0;
-#pragma unroll
-      for (int w = 0; w < nw; ++w) {
-        t += priv[w * nl + k];
-        priv[w * nl + k] = 0.0;
-      }
-      t *= ti;
-      wn[k] = t;
-      pv += t * vn[k];
-    }
-    kw = 0.5 * ti * block_sum1<nw>(pv, red + 32);
+    tau_prev = ti;
+    sc_prev = sc;
     cur ^= 1;
   }
   if (tid == 0) {
@@ -586,10 +677,14 @@ __global__ void __launch_bounds__(NT) k_tridiag_smem(EigArgs g, const int32_t* l
   }
 }
 
+size_t tridiag_smem_bytes(int nl, int nt) {
+  return ((size_t)nl * (nl + 1) / 2 + (3 + nt / 32) * (size_t)nl + 32 + 32 + 64 + 8) * sizeof(double);
+}
+
 // Global-memory prefix of the same reduction for systems larger than the
 // shared-memory block: the first K = n - nloc reflectors are formed in place
 // on the lower triangle of the square matrix (L2 / HBM resident), with the
-// same four phases per column as the shared-memory kernel, so each column
+// four phases per column described above, so each column
 // reads and writes the trailing triangle once, in coalesced 8 x 32 tiles.
 // The last step (column K) applies reflector K-1 to the trailing block and
 // forms no reflector: the block from row/column K is then A^(K), which the
@@ -703,9 +798,6 @@ __global__ void __launch_bounds__(NT) k_tridiag_prefix(EigArgs g, int nloc) {
 
 size_t tridiag_prefix_bytes(int n, int nt) { return ((4 + (size_t)nt / 32) * n + 64) * sizeof(double); }
 
-size_t tridiag_smem_bytes(int nl, int nt) {
-  return ((size_t)nl * (nl + 1) / 2 + (4 + nt / 32) * (size_t)nl + 72) * sizeof(double);
-}
 
 // Largest trailing block the shared-memory kernel holds (227 KB per CTA).
 constexpr int kTridiagSmemMax = 228;
