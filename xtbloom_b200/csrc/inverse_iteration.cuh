@@ -71,7 +71,13 @@ __device__ __forceinline__ void inverse_iteration_block(const double* d, const d
       // the off-pivot element times the reciprocal pivot (within an ulp of
       // the quotient), and the reciprocal is reused as U1 unless the pivot
       // is replaced by +-tiny.
+      // The first forward elimination runs inside the factorisation: the
+      // start vector's elements are formed where the elimination reads them
+      // and y_k is final once step k has chosen its pivot (the same
+      // operations, in the same order, as a separate sweep).
+      const uint32_t hseed = (uint32_t)j * 7919u + seed;
       double diag = d[0] - x, sup = n > 1 ? e[0] : 0.0;
+      double yk = hash_unit(0u, hseed);
       for (int k = 0; k < n - 1; ++k) {
         const double ck = e[k];
         const double nd = d[k + 1] - x;
@@ -80,43 +86,56 @@ __device__ __forceinline__ void inverse_iteration_block(const double* d, const d
         const double u1 = keep ? diag : ck;
         const double r = __drcp_rn(u1);
         double l;
+        double yn = hash_unit((uint32_t)(k + 1), hseed);
         if (keep) {
           l = diag != 0.0 ? ck * r : 0.0;
           U2(k) = sup; U3(k) = 0.0; LM(k) = l;
           diag = nd - l * sup;
           sup = ns;
+          yn -= l * yk;
         } else {
           l = diag * r;
-          U2(k) = nd; U3(k) = ns; LM(k) = -l - 4.0;
+          const double lenc = -l - 4.0;   // the stored encoding; the sweeps decode -lenc - 4
+          U2(k) = nd; U3(k) = ns; LM(k) = lenc;
           diag = sup - l * nd;
           sup = -l * ns;
+          const double tmp = yk;
+          yk = yn;
+          yn = tmp - (-lenc - 4.0) * yk;
         }
         U1(k) = fabs(u1) < tiny ? __drcp_rn(u1 < 0.0 ? -tiny : tiny) : r;
+        Y(k) = yk;
+        yk = yn;
       }
+      Y(n - 1) = yk;
       {
         double u1 = diag;
         if (fabs(u1) < tiny) u1 = u1 < 0.0 ? -tiny : tiny;
         U1(n - 1) = 1.0 / u1;
       }
-      for (int k = 0; k < n; ++k) Y(k) = hash_unit((uint32_t)k, (uint32_t)j * 7919u + seed);
       const int iters = (j > lead) ? 3 : 2;
+      // scale: the normalisation of the previous sweep, applied where the
+      // next one reads y (the product is the value the scaled vector held)
+      double scale = 1.0;
       for (int it = 0; it < iters; ++it) {
-        // forward elimination with the recorded interchanges
-        double yk = Y(0);
-        for (int k = 0; k < n - 1; ++k) {
-          double yn = Y(k + 1);
-          const double lk = LM(k);
-          if (lk < -2.0) {
-            const double tmp = yk;
-            yk = yn;
-            yn = tmp - (-lk - 4.0) * yk;
-          } else {
-            yn -= lk * yk;
+        if (it > 0) {
+          // forward elimination with the recorded interchanges
+          double yk2 = Y(0) * scale;
+          for (int k = 0; k < n - 1; ++k) {
+            double yn = Y(k + 1) * scale;
+            const double lk = LM(k);
+            if (lk < -2.0) {
+              const double tmp = yk2;
+              yk2 = yn;
+              yn = tmp - (-lk - 4.0) * yk2;
+            } else {
+              yn -= lk * yk2;
+            }
+            Y(k) = yk2;
+            yk2 = yn;
           }
-          Y(k) = yk;
-          yk = yn;
+          Y(n - 1) = yk2;
         }
-        Y(n - 1) = yk;
         // back substitution
         double y2 = 0.0, y1 = Y(n - 1) * U1(n - 1);
         Y(n - 1) = y1;
@@ -145,17 +164,20 @@ __device__ __forceinline__ void inverse_iteration_block(const double* d, const d
           nrm = 0.0;
           for (int k = 0; k < n; ++k) nrm += Y(k) * Y(k);
         }
-        const double inv = 1.0 / sqrt(nrm);
-        for (int k = 0; k < n; ++k) Y(k) *= inv;
+        scale = 1.0 / sqrt(nrm);
       }
       // sign convention: largest component positive; publish row j of Z
+      // (normalised as it is read)
       int kmax = 0;
-      double amax = 0.0;
-      for (int k = 0; k < n; ++k)
-        if (fabs(Y(k)) > amax) { amax = fabs(Y(k)); kmax = k; }
-      const double sgn = Y(kmax) < 0.0 ? -1.0 : 1.0;
+      double amax = 0.0, vmax = 0.0;
+      for (int k = 0; k < n; ++k) {
+        const double v = Y(k) * scale;
+        if (fabs(v) > amax) { amax = fabs(v); kmax = k; vmax = v; }
+      }
+      (void)kmax;
+      const double sgn = vmax < 0.0 ? -1.0 : 1.0;
       double* y = Z + (int64_t)j * n;
-      for (int k = 0; k < n; ++k) y[k] = sgn * Y(k);
+      for (int k = 0; k < n; ++k) y[k] = sgn * (Y(k) * scale);
     }
   }
 }
