@@ -1498,13 +1498,25 @@ __global__ void __launch_bounds__(256) k_backtransform_dmma(EigArgs g, int mcap)
         for (int q = 0; q < 4; ++q) d[q][0] = d[q][1] = 0.0;
         const int jl = jb * 8 + gq;
         const double* z = Z + (int64_t)(j0 + jl) * n + i0 + 1;
-        for (int r0 = 0; r0 < L; r0 += 4) {
-          const int r = r0 + tq;
-          const double bz = (jl < mc && r < L) ? z[r] : 0.0;
+        // four K steps' loads of Z issued before their products (the
+        // products run in the same order as one step at a time)
+        for (int r0 = 0; r0 < L; r0 += 16) {
+          double bz[4];
 #pragma unroll
-          for (int q = 0; q < 4; ++q) {
-            const double av = r < L ? V[r * P + q * 8 + gq] : 0.0;
-            mma_f64(d[q], av, bz);
+          for (int u = 0; u < 4; ++u) {
+            const int r = r0 + 4 * u + tq;
+            bz[u] = (jl < mc && r < L) ? z[r] : 0.0;
+          }
+#pragma unroll
+          for (int u = 0; u < 4; ++u) {
+            const int r = r0 + 4 * u + tq;
+            if (r0 + 4 * u < L) {
+#pragma unroll
+              for (int q = 0; q < 4; ++q) {
+                const double av = r < L ? V[r * P + q * 8 + gq] : 0.0;
+                mma_f64(d[q], av, bz[u]);
+              }
+            }
           }
         }
 #pragma unroll
@@ -1527,6 +1539,14 @@ __global__ void __launch_bounds__(256) k_backtransform_dmma(EigArgs g, int mcap)
         const int jb = t / rb_count, rb = t - (t / rb_count) * rb_count;
         double d[2] = {0.0, 0.0};
         const int jl = jb * 8 + gq, rr = rb * 8 + gq;
+        // the two elements of Z this lane updates, loaded before the products
+        double* z = Z + (int64_t)(j0 + jl) * n + i0 + 1;
+        double zold[2];
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+          const int r = rb * 8 + 2 * tq + h;
+          zold[h] = (jl < mc && r < L) ? z[r] : 0.0;
+        }
 #pragma unroll
         for (int q0 = 0; q0 < WB; q0 += 4) {
           const double aw = jl < mc ? Wm[(q0 + tq) * mcap + jl] : 0.0;
@@ -1534,11 +1554,10 @@ __global__ void __launch_bounds__(256) k_backtransform_dmma(EigArgs g, int mcap)
           mma_f64(d, aw, bv);
         }
         if (jl < mc) {
-          double* z = Z + (int64_t)(j0 + jl) * n + i0 + 1;
 #pragma unroll
           for (int h = 0; h < 2; ++h) {
             const int r = rb * 8 + 2 * tq + h;
-            if (r < L) z[r] -= d[h];
+            if (r < L) z[r] = zold[h] - d[h];
           }
         }
       }
