@@ -78,10 +78,7 @@ __device__ __forceinline__ void inverse_iteration_block(const double* d, const d
       const uint32_t hseed = (uint32_t)j * 7919u + seed;
       double diag = d[0] - x, sup = n > 1 ? e[0] : 0.0;
       double yk = hash_unit(0u, hseed);
-      for (int k = 0; k < n - 1; ++k) {
-        const double ck = e[k];
-        const double nd = d[k + 1] - x;
-        const double ns = (k + 1 < n - 1) ? e[k + 1] : 0.0;
+      auto lustep = [&](double ck, double nd, double ns, int k) {
         const bool keep = fabs(diag) >= fabs(ck);
         const double u1 = keep ? diag : ck;
         const double r = __drcp_rn(u1);
@@ -106,6 +103,22 @@ __device__ __forceinline__ void inverse_iteration_block(const double* d, const d
         U1(k) = fabs(u1) < tiny ? __drcp_rn(u1 < 0.0 ? -tiny : tiny) : r;
         Y(k) = yk;
         yk = yn;
+      };
+      {
+        // the matrix entries of four steps are loaded before the steps run
+        int k = 0;
+        for (; k + 4 <= n - 1; k += 4) {
+          double cv[4], dv[4], sv[4];
+#pragma unroll
+          for (int u = 0; u < 4; ++u) {
+            cv[u] = e[k + u];
+            dv[u] = d[k + u + 1] - x;
+            sv[u] = (k + u + 1 < n - 1) ? e[k + u + 1] : 0.0;
+          }
+#pragma unroll
+          for (int u = 0; u < 4; ++u) lustep(cv[u], dv[u], sv[u], k + u);
+        }
+        for (; k < n - 1; ++k) lustep(e[k], d[k + 1] - x, (k + 1 < n - 1) ? e[k + 1] : 0.0, k);
       }
       Y(n - 1) = yk;
       {
@@ -119,11 +132,12 @@ __device__ __forceinline__ void inverse_iteration_block(const double* d, const d
       double scale = 1.0;
       for (int it = 0; it < iters; ++it) {
         if (it > 0) {
-          // forward elimination with the recorded interchanges
+          // forward elimination with the recorded interchanges; the inputs of
+          // four steps are loaded before the steps run (the sweep writes only
+          // elements it has passed, so the loads see the values they would)
           double yk2 = Y(0) * scale;
-          for (int k = 0; k < n - 1; ++k) {
-            double yn = Y(k + 1) * scale;
-            const double lk = LM(k);
+          auto fstep = [&](double ynext, double lk, int k) {
+            double yn = ynext * scale;
             if (lk < -2.0) {
               const double tmp = yk2;
               yk2 = yn;
@@ -133,7 +147,19 @@ __device__ __forceinline__ void inverse_iteration_block(const double* d, const d
             }
             Y(k) = yk2;
             yk2 = yn;
+          };
+          int k = 0;
+          for (; k + 4 <= n - 1; k += 4) {
+            double yv[4], lv[4];
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+              yv[u] = Y(k + 1 + u);
+              lv[u] = LM(k + u);
+            }
+#pragma unroll
+            for (int u = 0; u < 4; ++u) fstep(yv[u], lv[u], k + u);
           }
+          for (; k < n - 1; ++k) fstep(Y(k + 1), LM(k), k);
           Y(n - 1) = yk2;
         }
         // back substitution
@@ -146,12 +172,29 @@ __device__ __forceinline__ void inverse_iteration_block(const double* d, const d
           y1 = y0;
         }
         double nrm = y1 * y1 + (n >= 2 ? y2 * y2 : 0.0);
-        for (int k = n - 3; k >= 0; --k) {
-          const double y0 = (Y(k) - U2(k) * y1 - U3(k) * y2) * U1(k);
+        auto bstep = [&](double yv, double u1, double u2, double u3, int k) {
+          const double y0 = (yv - u2 * y1 - u3 * y2) * u1;
           Y(k) = y0;
           nrm += y0 * y0;
           y2 = y1;
           y1 = y0;
+        };
+        {
+          // back substitution, four steps' inputs loaded ahead as above
+          int k = n - 3;
+          for (; k >= 3; k -= 4) {
+            double yv[4], a1[4], a2[4], a3[4];
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+              yv[u] = Y(k - u);
+              a1[u] = U1(k - u);
+              a2[u] = U2(k - u);
+              a3[u] = U3(k - u);
+            }
+#pragma unroll
+            for (int u = 0; u < 4; ++u) bstep(yv[u], a1[u], a2[u], a3[u], k - u);
+          }
+          for (; k >= 0; --k) bstep(Y(k), U1(k), U2(k), U3(k), k);
         }
         // orthogonalise against the earlier members of the cluster
         if (j > lead) {
