@@ -481,21 +481,23 @@ __device__ __forceinline__ void tri_tile(int tl, int& R, int& C) {
 //   (C) every thread forms alpha, beta, tau and the scale redundantly; the
 //       8 x 32 tiles of the rest are updated with (v_i, w_i) and multiplied
 //       by v_{i+1}; the warps' partials of p and p.v are posted -> one barrier.
+// FULL: the caller guarantees that the tile lies strictly below the diagonal
+// with every row inside the block (C0 + 32 <= R0, R0 + kTileRows <= m); the
+// row, column and diagonal masks, which then select nothing, are compiled out.
+template <bool FULL>
 __device__ __forceinline__ void fused_tile2(double* L, int o, int m, int R0, int C0,
                                             const double* vi, double sci, const double* wi,
                                             const double* vn, double scn, double* pw, double* pw0,
                                             int lane, bool want_mv, double& dot) {
   const int cj = C0 + lane;
-  const bool cok = cj < m;
+  const bool cok = FULL || cj < m;
   const double vn_c = cok ? (cj == 0 ? 1.0 : vn[cj] * scn) : 0.0;
   const double vi_c = cok ? vi[cj] * sci : 0.0;
   const double wi_c = cok ? wi[cj] : 0.0;
   const int rl = R0 + (lane & (kTileRows - 1));
-  const bool rok = rl < m;
-  const double vi_r = rok ? vi[rl] * sci : 0.0;
-  const double wi_r = rok ? wi[rl] : 0.0;
-  const double vn_r = rok ? (rl == 0 ? 1.0 : vn[rl] * scn) : 0.0;
-  const int rows = min(kTileRows, m - R0);
+  const bool rok = FULL || rl < m;
+  const double vn_r = rok ? ((!FULL && rl == 0) ? 1.0 : vn[rl] * scn) : 0.0;
+  const int rows = FULL ? kTileRows : min(kTileRows, m - R0);
   const int dcol = cj - R0;
   double a[kTileRows];
   const int base0 = pk32(o + R0, o) + cj;
@@ -503,26 +505,33 @@ __device__ __forceinline__ void fused_tile2(double* L, int o, int m, int R0, int
     int base = base0;
 #pragma unroll
     for (int i = 0; i < kTileRows; ++i) {
-      const bool ok = i < rows && cok && dcol <= i;
+      const bool ok = FULL || (i < rows && cok && dcol <= i);
       a[i] = ok ? L[base] : 0.0;
       base += o + R0 + i + 1;
     }
   }
   double col = 0.0;
+  // The row values are warp-uniform: one broadcast shared-memory load each
+  // (a shuffle of a double is two shuffles, and the shuffles, not the
+  // arithmetic, bound this loop on large blocks).  Rows past m read in-bounds
+  // scratch that the select discards.
 #pragma unroll
   for (int i = 0; i < kTileRows; ++i) {
-    const double vr = __shfl_sync(0xffffffffu, vi_r, i);
-    const double wr = __shfl_sync(0xffffffffu, wi_r, i);
-    const double nr = __shfl_sync(0xffffffffu, vn_r, i);
-    const double u = a[i] - (vr * wi_c + wr * vi_c);
-    a[i] = dcol > i ? 0.0 : u;
-    if (dcol < i) col = fma(a[i], nr, col);
+    const bool ri = FULL || i < rows;
+    const double vr = ri ? vi[R0 + i] * sci : 0.0;
+    const double wr = ri ? wi[R0 + i] : 0.0;
+    const double nr = ri ? ((!FULL && R0 + i == 0) ? 1.0 : vn[R0 + i] * scn) : 0.0;
+    // contraction written out, so that the rounding does not depend on the
+    // compiler's choice of which product to fuse
+    const double u = a[i] - fma(vr, wi_c, wr * vi_c);
+    a[i] = (!FULL && dcol > i) ? 0.0 : u;
+    if (FULL || dcol < i) col = fma(a[i], nr, col);
   }
   {
     int base = base0;
 #pragma unroll
     for (int i = 0; i < kTileRows; ++i) {
-      const bool ok = i < rows && cok && dcol <= i;
+      const bool ok = FULL || (i < rows && cok && dcol <= i);
       if (ok) L[base] = a[i];
       base += o + R0 + i + 1;
     }
@@ -543,7 +552,7 @@ __device__ __forceinline__ void fused_tile2(double* L, int o, int m, int R0, int
 #pragma unroll
   for (int x = kTileRows; x < 32; x <<= 1) a[0] += __shfl_xor_sync(0xffffffffu, a[0], x);
   if (lane < kTileRows && rok) {
-    double* dst = rl == 0 ? pw0 : pw + rl;
+    double* dst = (!FULL && rl == 0) ? pw0 : pw + rl;
     *dst += a[0];
     dot = fma(a[0], vn_r, dot);
   }
@@ -656,8 +665,14 @@ __global__ void __launch_bounds__(NT, 512 / NT) k_tridiag_smem(EigArgs g, const 
       for (int tl = warp; tl < ntiles; tl += nw) {
         int R, C;
         tri_tile(tl, R, C);
-        fused_tile2(L, o + 1, m1, R * kTileRows, C << 5, vi + 1, sc_prev, wb + 1, vn, sc, pw,
-                    r0n + warp, lane, mv, dot);
+        // tiles strictly below the diagonal with every row in the block (most
+        // of a large block) skip the masks: the same operations, unmasked
+        if ((C << 5) + 32 <= R * kTileRows && (R + 1) * kTileRows <= m1)
+          fused_tile2<true>(L, o + 1, m1, R * kTileRows, C << 5, vi + 1, sc_prev, wb + 1, vn, sc, pw,
+                            r0n + warp, lane, mv, dot);
+        else
+          fused_tile2<false>(L, o + 1, m1, R * kTileRows, C << 5, vi + 1, sc_prev, wb + 1, vn, sc, pw,
+                             r0n + warp, lane, mv, dot);
       }
       dot = warp_sum(dot);
       if (lane == 0) dots[warp] = mv ? dot : 0.0;
