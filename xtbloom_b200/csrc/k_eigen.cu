@@ -466,11 +466,31 @@ __device__ __forceinline__ void tri_tile(int tl, int& R, int& C) {
 }
 
 
+// tri_tile as a table for blocks of up to 256 rows (tri_tiles(256) = 144
+// tiles): the shared-memory kernel looks a tile up with one warp-uniform
+// constant load instead of a square root and an integer division per tile.
+constexpr int kTileTableRows = 256;
+constexpr int kTileTableSize = 144;
+struct TileTable {
+  unsigned short rc[kTileTableSize];   // row block | column block << 8
+};
+constexpr TileTable make_tile_table() {
+  TileTable t{};
+  int tl = 0;
+  for (int R = 0; tl < kTileTableSize; ++R)
+    for (int C = 0; C <= R / kTileGroup && tl < kTileTableSize; ++C)
+      t.rc[tl++] = (unsigned short)(R | (C << 8));
+  return t;
+}
+__constant__ TileTable c_tile_table = make_tile_table();
+
 // Shared-memory kernel: the trailing nl x nl block (rows/columns i0..n-1,
 // i0 = max(0, n - nloc)) in packed lower storage in one CTA's shared memory,
 // two barriers per column.  The reflector of a column is kept unscaled (the
-// column's own values) and scaled by 1/(alpha - beta) where it is read, so no
-// pass has to wait for a scaled copy; the warps' partial products
+// column's own values) and scaled by 1/(alpha - beta) where its own column's
+// tiles read it, so no pass has to wait for a scaled copy; the next column's
+// first pass, which forms v_r for its row anyway, stores that scaled value in
+// place for the next column's tiles.  The warps' partial products
 // A v and their dot products with v are posted by the tile pass and summed by
 // the next column's first pass, where w = tau p - (tau/2)(tau p.v) v is formed.
 // Per column:
@@ -486,13 +506,13 @@ __device__ __forceinline__ void tri_tile(int tl, int& R, int& C) {
 // row, column and diagonal masks, which then select nothing, are compiled out.
 template <bool FULL>
 __device__ __forceinline__ void fused_tile2(double* L, int o, int m, int R0, int C0,
-                                            const double* vi, double sci, const double* wi,
+                                            const double* vi, const double* wi,
                                             const double* vn, double scn, double* pw, double* pw0,
                                             int lane, bool want_mv, double& dot) {
   const int cj = C0 + lane;
   const bool cok = FULL || cj < m;
   const double vn_c = cok ? (cj == 0 ? 1.0 : vn[cj] * scn) : 0.0;
-  const double vi_c = cok ? vi[cj] * sci : 0.0;
+  const double vi_c = cok ? vi[cj] : 0.0;
   const double wi_c = cok ? wi[cj] : 0.0;
   const int rl = R0 + (lane & (kTileRows - 1));
   const bool rok = FULL || rl < m;
@@ -518,7 +538,7 @@ __device__ __forceinline__ void fused_tile2(double* L, int o, int m, int R0, int
 #pragma unroll
   for (int i = 0; i < kTileRows; ++i) {
     const bool ri = FULL || i < rows;
-    const double vr = ri ? vi[R0 + i] * sci : 0.0;
+    const double vr = ri ? vi[R0 + i] : 0.0;
     const double wr = ri ? wi[R0 + i] : 0.0;
     const double nr = ri ? ((!FULL && R0 + i == 0) ? 1.0 : vn[R0 + i] * scn) : 0.0;
     // contraction written out, so that the rounding does not depend on the
@@ -600,7 +620,7 @@ __global__ void __launch_bounds__(NT, 512 / NT) k_tridiag_smem(EigArgs g, const 
   double sc_prev = 0.0, tau_prev = 0.0;
   for (int i = -1; i + 2 < nl; ++i) {
     const int o = i + 1, m = nl - o;
-    const double* vi = cur ? vb1 : vb0;
+    double* vi = cur ? vb1 : vb0;
     double* vn = cur ? vb0 : vb1;
     double* r0c = row0 + 32 * cur;
     double* r0n = row0 + 32 * (cur ^ 1);
@@ -626,6 +646,7 @@ __global__ void __launch_bounds__(NT, 512 / NT) k_tridiag_smem(EigArgs g, const 
           priv[w * nl + r] = 0.0;
         }
         vr = vi[r] * sc_prev;
+        vi[r] = vr;        // the tiles below read the scaled reflector
         wr = fma(-kw, vr, tau_prev * t);
       }
       wb[r] = wr;
@@ -663,15 +684,15 @@ __global__ void __launch_bounds__(NT, 512 / NT) k_tridiag_smem(EigArgs g, const 
       const bool mv = next && ti != 0.0;
       double dot = 0.0;
       for (int tl = warp; tl < ntiles; tl += nw) {
-        int R, C;
-        tri_tile(tl, R, C);
+        const unsigned rc = c_tile_table.rc[tl];
+        const int R = rc & 0xff, C = rc >> 8;
         // tiles strictly below the diagonal with every row in the block (most
         // of a large block) skip the masks: the same operations, unmasked
         if ((C << 5) + 32 <= R * kTileRows && (R + 1) * kTileRows <= m1)
-          fused_tile2<true>(L, o + 1, m1, R * kTileRows, C << 5, vi + 1, sc_prev, wb + 1, vn, sc, pw,
+          fused_tile2<true>(L, o + 1, m1, R * kTileRows, C << 5, vi + 1, wb + 1, vn, sc, pw,
                             r0n + warp, lane, mv, dot);
         else
-          fused_tile2<false>(L, o + 1, m1, R * kTileRows, C << 5, vi + 1, sc_prev, wb + 1, vn, sc, pw,
+          fused_tile2<false>(L, o + 1, m1, R * kTileRows, C << 5, vi + 1, wb + 1, vn, sc, pw,
                              r0n + warp, lane, mv, dot);
       }
       dot = warp_sum(dot);
@@ -816,6 +837,7 @@ size_t tridiag_prefix_bytes(int n, int nt) { return ((4 + (size_t)nt / 32) * n +
 
 // Largest trailing block the shared-memory kernel holds (227 KB per CTA).
 constexpr int kTridiagSmemMax = 228;
+static_assert(kTridiagSmemMax <= kTileTableRows, "the shared-memory kernel's tiles come from c_tile_table");
 
 void launch_tridiag_smem(const EigArgs& g, const int32_t* list, int count, int max_n, cudaStream_t stream) {
   if (count == 0) return;
