@@ -501,23 +501,29 @@ __constant__ TileTable c_tile_table = make_tile_table();
 //   (C) every thread forms alpha, beta, tau and the scale redundantly; the
 //       8 x 32 tiles of the rest are updated with (v_i, w_i) and multiplied
 //       by v_{i+1}; the warps' partials of p and p.v are posted -> one barrier.
-// FULL: the caller guarantees that the tile lies strictly below the diagonal
-// with every row inside the block (C0 + 32 <= R0, R0 + kTileRows <= m); the
-// row, column and diagonal masks, which then select nothing, are compiled out.
-template <bool FULL>
+// KIND (what the caller guarantees; the masks that then select nothing are
+// compiled out, the operations on the elements are the same):
+//   kTileFull  every row inside the block and the tile strictly below the
+//              diagonal (R0 + kTileRows <= m, C0 + 32 <= R0): no masks;
+//   kTileRowsIn every row inside the block: only the diagonal mask (an
+//              element on or below the diagonal has its column inside too);
+//   kTileEdge  the last row block: every mask.
+constexpr int kTileEdge = 0, kTileRowsIn = 1, kTileFull = 2;
+template <int KIND>
 __device__ __forceinline__ void fused_tile2(double* L, int o, int m, int R0, int C0,
                                             const double* vi, const double* wi,
                                             const double* vn, double scn, double* pw, double* pw0,
                                             int lane, bool want_mv, double& dot) {
   const int cj = C0 + lane;
+  constexpr bool FULL = KIND == kTileFull, RIN = KIND != kTileEdge;
   const bool cok = FULL || cj < m;
   const double vn_c = cok ? (cj == 0 ? 1.0 : vn[cj] * scn) : 0.0;
   const double vi_c = cok ? vi[cj] : 0.0;
   const double wi_c = cok ? wi[cj] : 0.0;
   const int rl = R0 + (lane & (kTileRows - 1));
-  const bool rok = FULL || rl < m;
+  const bool rok = RIN || rl < m;
   const double vn_r = rok ? ((!FULL && rl == 0) ? 1.0 : vn[rl] * scn) : 0.0;
-  const int rows = FULL ? kTileRows : min(kTileRows, m - R0);
+  const int rows = RIN ? kTileRows : min(kTileRows, m - R0);
   const int dcol = cj - R0;
   double a[kTileRows];
   const int base0 = pk32(o + R0, o) + cj;
@@ -525,7 +531,7 @@ __device__ __forceinline__ void fused_tile2(double* L, int o, int m, int R0, int
     int base = base0;
 #pragma unroll
     for (int i = 0; i < kTileRows; ++i) {
-      const bool ok = FULL || (i < rows && cok && dcol <= i);
+      const bool ok = FULL || (RIN ? dcol <= i : (i < rows && cok && dcol <= i));
       a[i] = ok ? L[base] : 0.0;
       base += o + R0 + i + 1;
     }
@@ -537,7 +543,7 @@ __device__ __forceinline__ void fused_tile2(double* L, int o, int m, int R0, int
   // scratch that the select discards.
 #pragma unroll
   for (int i = 0; i < kTileRows; ++i) {
-    const bool ri = FULL || i < rows;
+    const bool ri = RIN || i < rows;
     const double vr = ri ? vi[R0 + i] : 0.0;
     const double wr = ri ? wi[R0 + i] : 0.0;
     const double nr = ri ? ((!FULL && R0 + i == 0) ? 1.0 : vn[R0 + i] * scn) : 0.0;
@@ -551,7 +557,7 @@ __device__ __forceinline__ void fused_tile2(double* L, int o, int m, int R0, int
     int base = base0;
 #pragma unroll
     for (int i = 0; i < kTileRows; ++i) {
-      const bool ok = FULL || (i < rows && cok && dcol <= i);
+      const bool ok = FULL || (RIN ? dcol <= i : (i < rows && cok && dcol <= i));
       if (ok) L[base] = a[i];
       base += o + R0 + i + 1;
     }
@@ -587,6 +593,7 @@ template <int NT>
 __global__ void __launch_bounds__(NT, 512 / NT) k_tridiag_smem(EigArgs g, const int32_t* list, int nloc) {
   extern __shared__ double sm[];
   constexpr int nw = NT / 32;
+  static_assert(NT >= 256, "(A) gives each thread at most one row: blocks have at most 228 rows");
   const int s = list[blockIdx.x];
   if (g.only != nullptr && g.only[s] == 0) return;
   const int n = g.nao[s];
@@ -625,15 +632,27 @@ __global__ void __launch_bounds__(NT, 512 / NT) k_tridiag_smem(EigArgs g, const 
     double* r0c = row0 + 32 * cur;
     double* r0n = row0 + 32 * (cur ^ 1);
     const bool next = o + 3 <= nl;
+    const int m1 = m - 1;
+    const int ntiles = tri_tiles(m1);
+    // A thread without a row in (A) skips the sums that only (A) uses, and a
+    // warp without a tile that stores no reflector element skips the
+    // reflector: blocks only shrink, so such a thread stays idle to the end
+    // and its values are never read.
+    const bool has_row = tid < m;
+    const bool forms = has_row || warp < ntiles;
     // (A) w_i from the posted partials, then the block's first column
     double pv = 0.0, p0 = 0.0;
+    if (has_row) {
 #pragma unroll
-    for (int w = 0; w < nw; ++w) {
-      pv += dots[w];
-      p0 += r0c[w];
+      for (int w = 0; w < nw; ++w) {
+        pv += dots[w];
+        p0 += r0c[w];
+      }
     }
     const double kw = 0.5 * tau_prev * tau_prev * pv;
-    const double w0 = tau_prev * p0 - kw;          // v_i[0] = 1
+    // contractions in this kernel are written out (fma), so that the rounding
+    // does not depend on the compiler's choice
+    const double w0 = fma(tau_prev, p0, -kw);      // v_i[0] = 1
     double part = 0.0;
     for (int r = tid; r < m; r += NT) {
       double wr = w0;
@@ -651,20 +670,30 @@ __global__ void __launch_bounds__(NT, 512 / NT) k_tridiag_smem(EigArgs g, const 
       }
       wb[r] = wr;
       const int idx = pk32(o + r, o);
-      const double c = L[idx] - (vr * w0 + wr);
+      const double c = L[idx] - fma(vr, w0, wr);
       L[idx] = c;
       if (r == 0) d[o] = c;
       if (r >= 1) vn[r - 1] = c;
-      if (r >= 2) part += c * c;
+      if (r >= 2) part = fma(c, c, part);
     }
-    const double xn2 = block_sum1<nw>(part, red);
-    // reflector o+1 from the updated column (every thread, same operands)
+    // the column's norm (block_sum1, with the final sum only where it is used)
+    double xn2 = 0.0;
+    {
+      const double ws = warp * 32 < m ? warp_sum(part) : 0.0;
+      if (lane == 0) red[warp] = ws;
+      __syncthreads();
+      if (forms) {
+#pragma unroll
+        for (int w = 0; w < nw; ++w) xn2 += red[w];
+      }
+    }
+    // reflector o+1 from the updated column (every working thread, same operands)
     double ti = 0.0, sc = 0.0;
-    if (next) {
+    if (next && forms) {
       const double alpha = vn[0];
       double beta = alpha;
       if (xn2 > 0.0) {
-        beta = -copysign(sqrt(alpha * alpha + xn2), alpha);
+        beta = -copysign(sqrt(fma(alpha, alpha, xn2)), alpha);
         ti = (beta - alpha) / beta;
         sc = 1.0 / (alpha - beta);
         for (int k = tid + 1; k < m - 1; k += NT)
@@ -677,26 +706,29 @@ __global__ void __launch_bounds__(NT, 512 / NT) k_tridiag_smem(EigArgs g, const 
     }
     if (tid < nw) r0c[tid] = 0.0;     // read above, before the barrier; next used two columns on
     // (C) rank-2 update of the rest of the block, fused with A v_{o+1}
-    const int m1 = m - 1;
-    {
-      const int ntiles = tri_tiles(m1);
+    if (warp < ntiles) {
       double* pw = priv + warp * nl;
       const bool mv = next && ti != 0.0;
       double dot = 0.0;
       for (int tl = warp; tl < ntiles; tl += nw) {
         const unsigned rc = c_tile_table.rc[tl];
         const int R = rc & 0xff, C = rc >> 8;
-        // tiles strictly below the diagonal with every row in the block (most
-        // of a large block) skip the masks: the same operations, unmasked
-        if ((C << 5) + 32 <= R * kTileRows && (R + 1) * kTileRows <= m1)
-          fused_tile2<true>(L, o + 1, m1, R * kTileRows, C << 5, vi + 1, wb + 1, vn, sc, pw,
-                            r0n + warp, lane, mv, dot);
+        // most tiles of a large block lie strictly below the diagonal with
+        // every row inside it, and only the last row block needs row masks
+        if ((R + 1) * kTileRows > m1)
+          fused_tile2<kTileEdge>(L, o + 1, m1, R * kTileRows, C << 5, vi + 1, wb + 1, vn, sc, pw,
+                                 r0n + warp, lane, mv, dot);
+        else if ((C << 5) + 32 <= R * kTileRows)
+          fused_tile2<kTileFull>(L, o + 1, m1, R * kTileRows, C << 5, vi + 1, wb + 1, vn, sc, pw,
+                                 r0n + warp, lane, mv, dot);
         else
-          fused_tile2<false>(L, o + 1, m1, R * kTileRows, C << 5, vi + 1, wb + 1, vn, sc, pw,
-                             r0n + warp, lane, mv, dot);
+          fused_tile2<kTileRowsIn>(L, o + 1, m1, R * kTileRows, C << 5, vi + 1, wb + 1, vn, sc, pw,
+                                   r0n + warp, lane, mv, dot);
       }
       dot = warp_sum(dot);
       if (lane == 0) dots[warp] = mv ? dot : 0.0;
+    } else if (lane == 0) {
+      dots[warp] = 0.0;
     }
     __syncthreads();
     if (!next) break;
