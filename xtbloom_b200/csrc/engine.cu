@@ -298,13 +298,20 @@ struct Engine::Impl {
   static constexpr int kBucketStreams = 8;
   cudaStream_t bst[kBucketStreams] = {};
   cudaEvent_t bfork = nullptr, bjoin[kBucketStreams] = {};
+  // per bucket stream: a second stream for the WY T factors, which need only
+  // the reflectors and run beside the eigenvalues and the inverse iteration
+  cudaStream_t fst[kBucketStreams] = {};
+  cudaEvent_t ffork[kBucketStreams] = {}, wydone[kBucketStreams] = {};
   bool bstreams = false;
   bool ensure_bucket_streams() {
     if (bstreams) return true;
     if (cudaEventCreateWithFlags(&bfork, cudaEventDisableTiming) != cudaSuccess) return false;
     for (int i = 0; i < kBucketStreams; ++i)
       if (cudaStreamCreateWithFlags(&bst[i], cudaStreamNonBlocking) != cudaSuccess ||
-          cudaEventCreateWithFlags(&bjoin[i], cudaEventDisableTiming) != cudaSuccess)
+          cudaEventCreateWithFlags(&bjoin[i], cudaEventDisableTiming) != cudaSuccess ||
+          cudaStreamCreateWithFlags(&fst[i], cudaStreamNonBlocking) != cudaSuccess ||
+          cudaEventCreateWithFlags(&ffork[i], cudaEventDisableTiming) != cudaSuccess ||
+          cudaEventCreateWithFlags(&wydone[i], cudaEventDisableTiming) != cudaSuccess)
         return false;
     bstreams = true;
     return true;
@@ -489,6 +496,9 @@ Engine::~Engine() {
   for (int i = 0; i < Impl::kBucketStreams; ++i) {
     if (impl_->bst[i]) cudaStreamDestroy(impl_->bst[i]);
     if (impl_->bjoin[i]) cudaEventDestroy(impl_->bjoin[i]);
+    if (impl_->fst[i]) cudaStreamDestroy(impl_->fst[i]);
+    if (impl_->ffork[i]) cudaEventDestroy(impl_->ffork[i]);
+    if (impl_->wydone[i]) cudaEventDestroy(impl_->wydone[i]);
   }
   if (impl_->bfork) cudaEventDestroy(impl_->bfork);
   if (impl_->h_count) cudaFreeHost(impl_->h_count);
@@ -699,7 +709,7 @@ xtbloom_status_t build_topology(Engine::Impl& m, const HostBatch& hb, cudaStream
     mat_off[sy + 1] = mat_off[sy] + n * n;
     gam_off[sy + 1] = gam_off[sy] + k * k;
     vec_off[sy + 1] = vec_off[sy] + hb.nch[sy] * (g1 ? k : k + 9 * na);
-    scr_off[sy + 1] = scr_off[sy] + 128 * 5 * n;
+    scr_off[sy + 1] = scr_off[sy] + eig_scratch(n);
   }
   // largest systems first
   std::vector<int32_t> order(B);
@@ -762,7 +772,7 @@ xtbloom_status_t build_topology(Engine::Impl& m, const HostBatch& hb, cudaStream
       ch_nel_b[c] = 0.0;
       xm += n * n;
       xv += n;
-      xs += 128 * 5 * n;
+      xs += eig_scratch(n);
     }
   }
   m.nchan = NC;
@@ -1408,30 +1418,47 @@ xtbloom_status_t Engine::compute(const ComputeRequest& req, std::string& error) 
       launch_inverse_iteration(sub(bk), bk.count, bk.max_n,
                                mode != 0 ? bk.max_n : std::min(bk.max_m + 4, bk.max_n), ortol_rel, st);
     };
-    auto backtransform = [&](const Bucket& bk, cudaStream_t st) {
-      const EigArgs gb = sub(bk);
+    auto wy_cap = [&](const Bucket& bk) {
       const int want = mode != 0 ? bk.max_n : std::min(bk.max_m, bk.max_n);
       const long budget = 220L * 1024 / 8 - (long)bk.max_n * 33 - 32 * 33 - 8;
-      const int wcap = (int)std::min<long>(want, budget / 32);
+      return (int)std::min<long>(want, budget / 32);
+    };
+    // factored: the T factors were launched already (launch_wy_factor)
+    auto backtransform = [&](const Bucket& bk, cudaStream_t st, bool factored = false) {
+      const EigArgs gb = sub(bk);
+      const int want = mode != 0 ? bk.max_n : std::min(bk.max_m, bk.max_n);
+      const int wcap = wy_cap(bk);
       if (wcap >= 8) {
-        launch_backtransform_wy(gb, bk.count, bk.max_n, wcap, want, st);
+        launch_backtransform_wy(gb, bk.count, bk.max_n, wcap, want, st, factored);
       } else {
         // a block of reflectors no longer fits in shared memory: row chunks
         launch_backtransform_rows(gb, bk.count, bk.max_n, want, st);
       }
     };
-    if (bks.size() > 1 && !m.prof.on && m.ensure_bucket_streams()) {
+    if (!bks.empty() && !m.prof.on && m.ensure_bucket_streams()) {
       // Each bucket runs its whole chain on its own side stream, forked from
-      // and joined back into the call's stream (also inside graph capture).
+      // and joined back into the call's stream (also inside graph capture);
+      // its WY T factors run on a second stream from the tridiagonalisation
+      // on, beside the eigenvalues and the inverse iteration, and join before
+      // the back-transform.
       cudaEventRecord(m.bfork, s);
       const int ns = std::min<int>((int)bks.size(), Impl::kBucketStreams);
       for (int i = 0; i < ns; ++i) cudaStreamWaitEvent(m.bst[i], m.bfork, 0);
       for (size_t i = 0; i < bks.size(); ++i) {
-        cudaStream_t st = m.bst[i % Impl::kBucketStreams];
+        const int k = (int)(i % Impl::kBucketStreams);
+        cudaStream_t st = m.bst[k];
         tridiag(bks[i], st);
+        const bool fork = wy_cap(bks[i]) >= 8;
+        if (fork) {
+          cudaEventRecord(m.ffork[k], st);
+          cudaStreamWaitEvent(m.fst[k], m.ffork[k], 0);
+          launch_wy_factor(sub(bks[i]), bks[i].count, bks[i].max_n, m.fst[k]);
+          cudaEventRecord(m.wydone[k], m.fst[k]);
+        }
         eigvals(bks[i], st);
         invit(bks[i], st);
-        backtransform(bks[i], st);
+        if (fork) cudaStreamWaitEvent(st, m.wydone[k], 0);
+        backtransform(bks[i], st, fork);
       }
       for (int i = 0; i < ns; ++i) {
         cudaEventRecord(m.bjoin[i], m.bst[i]);

@@ -1382,7 +1382,7 @@ __global__ void __launch_bounds__(256) k_wy_factor(EigArgs g) {
       T[lane * P + j] = (lane <= j) ? t : 0.0;
       __syncwarp();
     }
-    double* out = g.scratch + g.scratch_off[s] + (int64_t)b * WB * WB;
+    double* out = g.scratch + g.scratch_off[s] + wy_t_offset(n) + (int64_t)b * WB * WB;
     for (int j = 0; j < WB; ++j) out[lane * WB + j] = T[lane * P + j];
   }
 }
@@ -1436,7 +1436,7 @@ __global__ void __launch_bounds__(256) k_backtransform_wy(EigArgs g, int wcap, i
   const int jbeg = blockIdx.x * per;
   const int m = min(mt - jbeg, per);
   const double* a = g.A + g.mat_off[s];
-  const double* tf = g.scratch + g.scratch_off[s];
+  const double* tf = g.scratch + g.scratch_off[s] + wy_t_offset(n);
   double* gZ = g.Z + g.mat_off[s] + (int64_t)jbeg * n;
   const int nr = n - 2;
   if (nr <= 0 || m <= 0) return;
@@ -1535,7 +1535,7 @@ __global__ void __launch_bounds__(256) k_backtransform_dmma(EigArgs g, int mcap)
   if (nr <= 0 || m <= 0) return;
   constexpr int P = WB + 1;
   const double* a = g.A + g.mat_off[s];
-  const double* tf = g.scratch + g.scratch_off[s];
+  const double* tf = g.scratch + g.scratch_off[s] + wy_t_offset(n);
   double* Z = g.Z + g.mat_off[s];
   double* V = sm;                        // n x P
   double* T = V + (size_t)n * P;         // WB x P
@@ -1639,15 +1639,19 @@ size_t backtransform_dmma_bytes(int n, int mcap) {
   return ((size_t)n * (WB + 1) + WB * (WB + 1) + 2 * (size_t)WB * mcap) * sizeof(double);
 }
 
+void launch_wy_factor(const EigArgs& g, int count, int max_n, cudaStream_t stream) {
+  if (count == 0) return;
+  allow_max_dynamic_smem(k_wy_factor);
+  const int nblk = std::max(1, (max_n - 2 + WB - 1) / WB);
+  k_wy_factor<<<dim3(nblk, count), 256, wy_factor_bytes(max_n), stream>>>(g);
+}
+
 void launch_backtransform_wy(const EigArgs& g, int count, int max_n, int max_m, int want_m,
-                             cudaStream_t stream) {
+                             cudaStream_t stream, bool factored) {
   if (count == 0) return;
   const size_t cap = allow_max_dynamic_smem(k_backtransform_wy<false>);
   const size_t cap_s = allow_max_dynamic_smem(k_backtransform_wy<true>);
-  const size_t cap_f = allow_max_dynamic_smem(k_wy_factor);
-  (void)cap_f;
-  const int nblk = std::max(1, (max_n - 2 + WB - 1) / WB);
-  k_wy_factor<<<dim3(nblk, count), 256, wy_factor_bytes(max_n), stream>>>(g);
+  if (!factored) launch_wy_factor(g, count, max_n, stream);
   // Few systems: split each system's vectors over CTAs, at least 8 vectors
   // each, and keep each CTA's slice in shared memory when it fits.
   const int sms = sm_count();
@@ -1756,7 +1760,7 @@ __global__ void __launch_bounds__(256) k_wy_factor_rows(EigArgs g) {
       T[lane * P + j] = (lane <= j) ? t : 0.0;
       __syncwarp();
     }
-    double* out = g.scratch + g.scratch_off[s] + (int64_t)b * WB * WB;
+    double* out = g.scratch + g.scratch_off[s] + wy_t_offset(n) + (int64_t)b * WB * WB;
     for (int j = 0; j < WB; ++j) out[lane * WB + j] = T[lane * P + j];
   }
 }
@@ -1777,7 +1781,7 @@ __global__ void __launch_bounds__(256) k_backtransform_rows(EigArgs g) {
   const int nr = n - 2;
   if (nr <= 0) return;
   const double* a = g.A + g.mat_off[s];
-  const double* tf = g.scratch + g.scratch_off[s];
+  const double* tf = g.scratch + g.scratch_off[s] + wy_t_offset(n);
   constexpr int P = WB + 1;
   double* Z = sm;                          // MC x n
   double* Vc = Z + (size_t)MC * n;         // kWyRows x P

@@ -168,8 +168,20 @@ void launch_eigvals(const EigArgs& g, int mode, double kt, int count, int max_n,
 void launch_inverse_iteration(const EigArgs& g, int count, int max_n, int want_m, double ortol_rel,
                               cudaStream_t stream);
 void launch_backtransform_rows(const EigArgs& g, int count, int max_n, int want_m, cudaStream_t stream);
+// Compact-WY back-transform.  factored: the T factors were formed already by
+// launch_wy_factor (which needs only the reflectors, so it can run beside the
+// eigenvalues and the inverse iteration); otherwise they are formed first.
+void launch_wy_factor(const EigArgs& g, int count, int max_n, cudaStream_t stream);
 void launch_backtransform_wy(const EigArgs& g, int count, int max_n, int max_m, int want_m,
-                             cudaStream_t stream);
+                             cudaStream_t stream, bool factored = false);
+// Per-channel scratch of the eigensolver, in doubles: the inverse
+// iteration's work arrays (5 n per thread of a 128-thread block), then the
+// T factors of the compact-WY blocks (32 x 32 per block of 32 reflectors)
+// at wy_t_offset(n), apart from them so that both can be live at once.
+__host__ __device__ inline int64_t wy_t_offset(int64_t n) { return 128 * 5 * n; }
+__host__ __device__ inline int64_t eig_scratch(int64_t n) {
+  return wy_t_offset(n) + ((n > 2 ? n - 2 : 0) + 31) / 32 * 32 * 32;
+}
 size_t backtransform_wy_bytes(int n, int m);
 void launch_lowdin_weights(const EigArgs& g, int32_t* status, int count, cudaStream_t stream);
 
