@@ -45,7 +45,7 @@ __device__ __forceinline__ void mma_f64(double* d, double a, double b) {
 // of 4) at either tile width, so both widths give identical results.
 template <bool TA, bool W, int TB>
 __device__ __forceinline__ void gemm_tile_f64(const GemmArgs& g, int s, int M, int N, int K, int ld,
-                                              int ti, int tj, bool mirror) {
+                                              int ti, int tj, bool mirror, unsigned char* smem) {
   constexpr int LPT = TB * GK / 256;     // elements of each operand chunk per thread
   constexpr int MT = TB / 16, NT = TB / 32;   // 8x8 products per warp and dimension
   constexpr int SP = TB + 4;
@@ -53,8 +53,10 @@ __device__ __forceinline__ void gemm_tile_f64(const GemmArgs& g, int s, int M, i
   const double* B = g.B + g.offB[s];
   double* C = g.C + g.offC[s];
   const double* w = W ? g.w + g.offW[s] : nullptr;
-  __shared__ double As[GK][SP];
-  __shared__ double Bs[GK][SP];
+  // two stages: chunk t is multiplied from one while chunk t+1 is stored
+  // into the other, so each chunk needs one barrier
+  double (*As)[GK][SP] = reinterpret_cast<double (*)[GK][SP]>(smem);   // [2][GK][SP]
+  double (*Bs)[GK][SP] = As + 2;                                       // [2][GK][SP]
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int wm = warp >> 2, wn = warp & 3;
   const int gq = lane >> 2, tq = lane & 3;
@@ -65,7 +67,8 @@ __device__ __forceinline__ void gemm_tile_f64(const GemmArgs& g, int s, int M, i
     for (int j = 0; j < NT; ++j) acc[i][j][0] = acc[i][j][1] = 0.0;
   const int i0 = ti * TB, j0 = tj * TB;
   // The next chunk's operands are loaded into registers while the current
-  // chunk is multiplied, so global latency overlaps the products.
+  // chunk is multiplied, so global latency overlaps the products; they go to
+  // the other shared-memory stage after the products.
   double ra[LPT], rb[LPT];
   auto fetch = [&](int k0) {
 #pragma unroll
@@ -88,30 +91,38 @@ __device__ __forceinline__ void gemm_tile_f64(const GemmArgs& g, int s, int M, i
       rb[q] = bv;
     }
   };
-  fetch(0);
-  for (int k0 = 0; k0 < K; k0 += GK) {
+  auto stage = [&](int st) {
 #pragma unroll
     for (int q = 0; q < LPT; ++q) {
       const int e = tid + q * 256;
-      if (TA) As[e / TB][e % TB] = ra[q];
-      else As[e % GK][e / GK] = ra[q];
-      Bs[e / TB][e % TB] = rb[q];
+      if (TA) As[st][e / TB][e % TB] = ra[q];
+      else As[st][e % GK][e / GK] = ra[q];
+      Bs[st][e / TB][e % TB] = rb[q];
     }
-    __syncthreads();
-    if (k0 + GK < K) fetch(k0 + GK);
+  };
+  fetch(0);
+  stage(0);
+  __syncthreads();
+  int st = 0;
+  for (int k0 = 0; k0 < K; k0 += GK) {
+    const bool more = k0 + GK < K;
+    if (more) fetch(k0 + GK);
 #pragma unroll
     for (int ks = 0; ks < GK; ks += 4) {
       double a[MT], b[NT];
 #pragma unroll
-      for (int i = 0; i < MT; ++i) a[i] = As[ks + tq][wm * (TB / 2) + i * 8 + gq];
+      for (int i = 0; i < MT; ++i) a[i] = As[st][ks + tq][wm * (TB / 2) + i * 8 + gq];
 #pragma unroll
-      for (int j = 0; j < NT; ++j) b[j] = Bs[ks + tq][wn * (TB / 4) + j * 8 + gq];
+      for (int j = 0; j < NT; ++j) b[j] = Bs[st][ks + tq][wn * (TB / 4) + j * 8 + gq];
 #pragma unroll
       for (int i = 0; i < MT; ++i)
 #pragma unroll
         for (int j = 0; j < NT; ++j) mma_f64(acc[i][j], a[i], b[j]);
     }
+    // every warp finished reading stage st ^ 1 before the previous barrier
+    if (more) stage(st ^ 1);
     __syncthreads();
+    st ^= 1;
   }
 #pragma unroll
   for (int i = 0; i < MT; ++i) {
@@ -154,14 +165,16 @@ __device__ __forceinline__ void mma_tf32(float* c, const uint32_t* a, const uint
 // Eight warps as 2 x 4, each 32 x 16 of the 64 x 64 tile (2 x 2 m16n8k8).
 template <bool TA, bool W>
 __device__ __forceinline__ void gemm_tile_tf32x3(const GemmArgs& g, int s, int M, int N, int K,
-                                                 int ld, int ti, int tj) {
+                                                 int ld, int ti, int tj, unsigned char* smem) {
   const double* A = g.A + g.offA[s];
   const double* B = g.B + g.offB[s];
   double* C = g.C + g.offC[s];
   const double* w = W ? g.w + g.offW[s] : nullptr;
   constexpr int AP = GK + 4, BP = GB + 8;   // conflict-free fragment reads
-  __shared__ uint32_t Ah[GB][AP], Al[GB][AP];
-  __shared__ uint32_t Bh[GK][BP], Bl[GK][BP];
+  uint32_t (*Ah)[AP] = reinterpret_cast<uint32_t (*)[AP]>(smem);   // [GB][AP]
+  uint32_t (*Al)[AP] = Ah + GB;                                      // [GB][AP]
+  uint32_t (*Bh)[BP] = reinterpret_cast<uint32_t (*)[BP]>(Al + GB);  // [GK][BP]
+  uint32_t (*Bl)[BP] = Bh + GK;                                      // [GK][BP]
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int gq = lane >> 2, tq = lane & 3;
   const int wm = warp >> 2, wn = warp & 3;
@@ -258,6 +271,11 @@ __device__ __forceinline__ void gemm_tile_tf32x3(const GemmArgs& g, int s, int M
 // ---------------------------------------------------------------------------
 template <bool TA, bool W, int TB>
 __global__ void __launch_bounds__(256, 3) k_gemm(GemmArgs g) {
+  // one buffer for whichever tile runs: the FP64 tile's two operand stages
+  // or the split tile's TF32 parts
+  constexpr int kF64Bytes = 2 * 2 * GK * (TB + 4) * 8;
+  constexpr int kTf32Bytes = (2 * GB * (GK + 4) + 2 * GK * (GB + 8)) * 4;
+  __shared__ __align__(16) unsigned char gsm[kF64Bytes > kTf32Bytes ? kF64Bytes : kTf32Bytes];
   const int s = g.list[blockIdx.y];
   if (g.only != nullptr && g.only[s] == 0) return;
   const int M = g.dm[s], N = g.dn[s], K = g.dk[s];
@@ -294,9 +312,9 @@ __global__ void __launch_bounds__(256, 3) k_gemm(GemmArgs g) {
   // 32-wide launch multiplies every system in FP64
   if (TB == GB && g.prec != nullptr && g.prec[g.prec_of != nullptr ? g.prec_of[s] : s] == 0) {
     if (g.umma) return;   // formed by k_gemm_umma
-    gemm_tile_tf32x3<TA, W>(g, s, M, N, K, ld, ti, tj);
+    gemm_tile_tf32x3<TA, W>(g, s, M, N, K, ld, ti, tj, gsm);
   } else
-    gemm_tile_f64<TA, W, TB>(g, s, M, N, K, ld, ti, tj, mirror);
+    gemm_tile_f64<TA, W, TB>(g, s, M, N, K, ld, ti, tj, mirror, gsm);
 }
 
 template <int TB>
