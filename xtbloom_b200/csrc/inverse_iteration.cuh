@@ -31,6 +31,10 @@ __device__ __forceinline__ double hash_unit(uint32_t a, uint32_t b) {
 // ((a*n + k) * LD + t)) so that every sequential sweep over k is a coalesced
 // access.  Every scratch element is written before it is read.  seed varies
 // the start vectors.
+// The sweeps load the inputs of kAhead steps before running them, so that
+// several scratch loads of a thread are in flight at once (the sweeps are
+// bound by their latency).
+constexpr int kAhead = 8;
 template <int LD>
 __device__ __forceinline__ void inverse_iteration_block(const double* d, const double* e,
                                                         const double* ev, int n, int m, double* Z,
@@ -105,18 +109,18 @@ __device__ __forceinline__ void inverse_iteration_block(const double* d, const d
         yk = yn;
       };
       {
-        // the matrix entries of four steps are loaded before the steps run
+        // the matrix entries of kAhead steps are loaded before the steps run
         int k = 0;
-        for (; k + 4 <= n - 1; k += 4) {
-          double cv[4], dv[4], sv[4];
+        for (; k + kAhead <= n - 1; k += kAhead) {
+          double cv[kAhead], dv[kAhead], sv[kAhead];
 #pragma unroll
-          for (int u = 0; u < 4; ++u) {
+          for (int u = 0; u < kAhead; ++u) {
             cv[u] = e[k + u];
             dv[u] = d[k + u + 1] - x;
             sv[u] = (k + u + 1 < n - 1) ? e[k + u + 1] : 0.0;
           }
 #pragma unroll
-          for (int u = 0; u < 4; ++u) lustep(cv[u], dv[u], sv[u], k + u);
+          for (int u = 0; u < kAhead; ++u) lustep(cv[u], dv[u], sv[u], k + u);
         }
         for (; k < n - 1; ++k) lustep(e[k], d[k + 1] - x, (k + 1 < n - 1) ? e[k + 1] : 0.0, k);
       }
@@ -133,7 +137,7 @@ __device__ __forceinline__ void inverse_iteration_block(const double* d, const d
       for (int it = 0; it < iters; ++it) {
         if (it > 0) {
           // forward elimination with the recorded interchanges; the inputs of
-          // four steps are loaded before the steps run (the sweep writes only
+          // kAhead steps are loaded before the steps run (the sweep writes only
           // elements it has passed, so the loads see the values they would)
           double yk2 = Y(0) * scale;
           auto fstep = [&](double ynext, double lk, int k) {
@@ -149,15 +153,15 @@ __device__ __forceinline__ void inverse_iteration_block(const double* d, const d
             yk2 = yn;
           };
           int k = 0;
-          for (; k + 4 <= n - 1; k += 4) {
-            double yv[4], lv[4];
+          for (; k + kAhead <= n - 1; k += kAhead) {
+            double yv[kAhead], lv[kAhead];
 #pragma unroll
-            for (int u = 0; u < 4; ++u) {
+            for (int u = 0; u < kAhead; ++u) {
               yv[u] = Y(k + 1 + u);
               lv[u] = LM(k + u);
             }
 #pragma unroll
-            for (int u = 0; u < 4; ++u) fstep(yv[u], lv[u], k + u);
+            for (int u = 0; u < kAhead; ++u) fstep(yv[u], lv[u], k + u);
           }
           for (; k < n - 1; ++k) fstep(Y(k + 1), LM(k), k);
           Y(n - 1) = yk2;
@@ -180,19 +184,19 @@ __device__ __forceinline__ void inverse_iteration_block(const double* d, const d
           y1 = y0;
         };
         {
-          // back substitution, four steps' inputs loaded ahead as above
+          // back substitution, kAhead steps' inputs loaded ahead as above
           int k = n - 3;
-          for (; k >= 3; k -= 4) {
-            double yv[4], a1[4], a2[4], a3[4];
+          for (; k >= kAhead - 1; k -= kAhead) {
+            double yv[kAhead], a1[kAhead], a2[kAhead], a3[kAhead];
 #pragma unroll
-            for (int u = 0; u < 4; ++u) {
+            for (int u = 0; u < kAhead; ++u) {
               yv[u] = Y(k - u);
               a1[u] = U1(k - u);
               a2[u] = U2(k - u);
               a3[u] = U3(k - u);
             }
 #pragma unroll
-            for (int u = 0; u < 4; ++u) bstep(yv[u], a1[u], a2[u], a3[u], k - u);
+            for (int u = 0; u < kAhead; ++u) bstep(yv[u], a1[u], a2[u], a3[u], k - u);
           }
           for (; k >= 0; --k) bstep(Y(k), U1(k), U2(k), U3(k), k);
         }
@@ -202,7 +206,20 @@ __device__ __forceinline__ void inverse_iteration_block(const double* d, const d
             const double* zq = Z + (int64_t)q * n;
             double dot = 0.0;
             for (int k = 0; k < n; ++k) dot += Y(k) * zq[k];
-            for (int k = 0; k < n; ++k) Y(k) -= dot * zq[k];
+            // kAhead elements loaded before they are stored (the compiler
+            // cannot tell the scratch from Z, so it would not reorder them)
+            int k = 0;
+            for (; k + kAhead <= n; k += kAhead) {
+              double yv[kAhead], zv[kAhead];
+#pragma unroll
+              for (int u = 0; u < kAhead; ++u) {
+                yv[u] = Y(k + u);
+                zv[u] = zq[k + u];
+              }
+#pragma unroll
+              for (int u = 0; u < kAhead; ++u) Y(k + u) = yv[u] - dot * zv[u];
+            }
+            for (; k < n; ++k) Y(k) -= dot * zq[k];
           }
           nrm = 0.0;
           for (int k = 0; k < n; ++k) nrm += Y(k) * Y(k);
@@ -220,7 +237,15 @@ __device__ __forceinline__ void inverse_iteration_block(const double* d, const d
       (void)kmax;
       const double sgn = vmax < 0.0 ? -1.0 : 1.0;
       double* y = Z + (int64_t)j * n;
-      for (int k = 0; k < n; ++k) y[k] = sgn * (Y(k) * scale);
+      int k = 0;
+      for (; k + kAhead <= n; k += kAhead) {   // loads ahead of the stores, as above
+        double yv[kAhead];
+#pragma unroll
+        for (int u = 0; u < kAhead; ++u) yv[u] = Y(k + u);
+#pragma unroll
+        for (int u = 0; u < kAhead; ++u) y[k + u] = sgn * (yv[u] * scale);
+      }
+      for (; k < n; ++k) y[k] = sgn * (Y(k) * scale);
     }
   }
 }
