@@ -436,30 +436,35 @@ __global__ void __launch_bounds__(256) k_atm(ForceArgs f, int parts) {
       const int zk = t.Z[gk];
       const double cik = C6[(int64_t)i * na + k], cjk = C6[(int64_t)j * na + k];
       const double r0ik = d4_r0(t, zi, zk), r0jk = d4_r0(t, zj, zk);
+      // one reciprocal for every power of r = sqrt(r2ij r2ik r2jk), and
+      // (r0 / r)^(16/3) as (r0 / r)^5 cbrt(r0 / r)
       const double r2p = r2ij * r2ik * r2jk;
-      const double r1p = sqrt(r2p);
-      const double r3p = r2p * r1p;
-      const double r5p = r3p * r2p;
-      const double ratio = r0ij * r0ik * r0jk / r1p;
-      const double rpow = pow(ratio, 16.0 / 3.0);
+      const double ir1 = 1.0 / sqrt(r2p);
+      const double ir2 = ir1 * ir1;
+      const double ir3 = ir2 * ir1;
+      const double ir5 = ir3 * ir2;
+      const double ratio = r0ij * r0ik * r0jk * ir1;
+      const double rat2 = ratio * ratio;
+      const double rpow = rat2 * rat2 * ratio * cbrt(ratio);
       const double damp = 1.0 / (1.0 + 6.0 * rpow);
-      const double ang = 0.375 * (r2ij + r2jk - r2ik) * (r2ij - r2jk + r2ik) * (-r2ij + r2jk + r2ik) / r5p +
-                         1.0 / r3p;
+      const double ang = 0.375 * (r2ij + r2jk - r2ik) * (r2ij - r2jk + r2ik) * (-r2ij + r2jk + r2ik) * ir5 +
+                         ir3;
       const double prod = cij * cik * cjk;
       const double c9 = -t.m.d4_s9 * sqrt(fabs(prod));
       eatm -= ang * damp * c9;
       if (!grad || !(cij > 0.0) || !(cik > 0.0) || !(cjk > 0.0)) continue;
       const double ddmp = -2.0 * 16.0 * rpow * damp * damp;
-      auto dg = [&](double tt, double o1, double o2) {
+      // itt = 1 / tt from the reciprocal of the product: 1/r2ij = r2ik r2jk / r2p
+      auto dg = [&](double tt, double o1, double o2, double itt) {
         const double dang = -0.375 *
                             (tt * tt * tt + tt * tt * (o1 + o2) + tt * (3.0 * o1 * o1 + 2.0 * o1 * o2 + 3.0 * o2 * o2) -
-                             5.0 * (o1 - o2) * (o1 - o2) * (o1 + o2)) / r5p;
-        return c9 * (-dang * damp + ang * ddmp) / tt;
+                             5.0 * (o1 - o2) * (o1 - o2) * (o1 + o2)) * ir5;
+        return c9 * (-dang * damp + ang * ddmp) * itt;
       };
       // vij = R_j - R_i as in the reference's pair cache (first = j, second = i)
-      const double sij = dg(r2ij, r2jk, r2ik);
-      const double sik = dg(r2ik, r2jk, r2ij);
-      const double sjk = dg(r2jk, r2ik, r2ij);
+      const double sij = dg(r2ij, r2jk, r2ik, r2ik * r2jk * ir2);
+      const double sik = dg(r2ik, r2jk, r2ij, r2ij * r2jk * ir2);
+      const double sjk = dg(r2jk, r2ik, r2ij, r2ij * r2ik * ir2);
       for (int c = 0; c < 3; ++c) {
         const double gij = sij * vij[c], gik = sik * vik[c], gjk = sjk * vjk[c];
         g_i[c] -= gij + gik;
@@ -469,9 +474,12 @@ __global__ void __launch_bounds__(256) k_atm(ForceArgs f, int parts) {
       const double de = ang * damp * c9;
       const double cik_i = D[(int64_t)i * na + k], cik_k = D[(int64_t)k * na + i];
       const double cjk_j = D[(int64_t)j * na + k], cjk_k = D[(int64_t)k * na + j];
-      a_i -= 0.5 * de * (cij_i / cij + cik_i / cik);
-      a_j -= 0.5 * de * (cij_j / cij + cjk_j / cjk);
-      fix_add(&acn4[k], -0.5 * de * (cik_k / cik + cjk_k / cjk));
+      // 1/cij, 1/cik, 1/cjk from one reciprocal of their product (all > 0 here)
+      const double iprod = 1.0 / prod;
+      const double icij = cik * cjk * iprod, icik = cij * cjk * iprod, icjk = cij * cik * iprod;
+      a_i -= 0.5 * de * (cij_i * icij + cik_i * icik);
+      a_j -= 0.5 * de * (cij_j * icij + cjk_j * icjk);
+      fix_add(&acn4[k], -0.5 * de * (cik_k * icik + cjk_k * icjk));
     }
     if (grad) {
 #pragma unroll
