@@ -161,6 +161,77 @@ __device__ __forceinline__ void cart_pair_acc(const int eb[3], const int ek[3], 
   }
 }
 
+// Primitive-pair factors of one shell pair at separation v (independent of
+// the Cartesian components): 1/(a_k + a_b), the screening exponent and, for
+// the pairs that pass the screen, exp(-est) and sqrt(1/(a_k + a_b)).  Index
+// ik * npb + ib.  cart_pair_acc_pp reads them instead of recomputing them
+// for every component pair; the values and the order of every product are
+// those of cart_pair_acc.
+constexpr int kPrimPairs = 36;   // shells with at most 6 primitives
+struct PrimPairs {
+  double inv[kPrimPairs], est[kPrimPairs], e[kPrimPairs], sinv[kPrimPairs];
+};
+__device__ __forceinline__ void prim_pairs(const double* ab, int npb, const double* ak, int npk,
+                                           const double v[3], PrimPairs& pp) {
+  // the contraction cart_pair_acc's r^2 compiles to, written out
+  const double r2 = fma(v[2], v[2], fma(v[0], v[0], v[1] * v[1]));
+  for (int ik = 0; ik < npk; ++ik) {
+    const double aK = ak[ik];
+    for (int ib = 0; ib < npb; ++ib) {
+      const double aB = ab[ib];
+      const int q = ik * npb + ib;
+      const double inv = 1.0 / (aK + aB);
+      const double est = aK * aB * r2 * inv;
+      pp.inv[q] = inv;
+      pp.est[q] = est;
+      if (est > kIntegralCutoff) continue;
+      pp.e[q] = exp(-est);
+      pp.sinv[q] = sqrt(inv);
+    }
+  }
+}
+
+template <bool GRAD>
+__device__ __forceinline__ void cart_pair_acc_pp(const int eb[3], const int ek[3], const double* ab,
+                                                 const double* cb, int npb, const double* ak,
+                                                 const double* ck, int npk, const double v[3],
+                                                 double w, const PrimPairs& pp, double out[10],
+                                                 double dout[3][10]) {
+  for (int ik = 0; ik < npk; ++ik) {
+    const double aK = ak[ik];
+    for (int ib = 0; ib < npb; ++ib) {
+      const double aB = ab[ib];
+      const int q = ik * npb + ib;
+      const double inv = pp.inv[q];
+      if (pp.est[q] > kIntegralCutoff) continue;
+      const double pref = w * pp.e[q] * kSqrtPi3 * inv * pp.sinv[q] * ck[ik] * cb[ib];
+      const double inv2p = 0.5 * inv;
+      double O[3][3], G[3][3];
+#pragma unroll
+      for (int c = 0; c < 3; ++c)
+        axis_factors<GRAD>(-v[c] * aB * inv, v[c] * aK * inv, inv2p, aK, ek[c], eb[c], O[c], G[c]);
+      out[0] += pref * O[0][0] * O[1][0] * O[2][0];
+      if (GRAD) {
+        dout[0][0] += pref * G[0][0] * O[1][0] * O[2][0];
+        dout[1][0] += pref * O[0][0] * G[1][0] * O[2][0];
+        dout[2][0] += pref * O[0][0] * O[1][0] * G[2][0];
+      }
+#pragma unroll
+      for (int m = 0; m < 9; ++m) {
+        int p[3];
+        moment_powers(m, p);
+        const double ox = O[0][p[0]], oy = O[1][p[1]], oz = O[2][p[2]];
+        out[1 + m] += pref * ox * oy * oz;
+        if (GRAD) {
+          dout[0][1 + m] += pref * G[0][p[0]] * oy * oz;
+          dout[1][1 + m] += pref * ox * G[1][p[1]] * oz;
+          dout[2][1 + m] += pref * ox * oy * G[2][p[2]];
+        }
+      }
+    }
+  }
+}
+
 __device__ __forceinline__ void make_traceless(double* m /* 6 raw: xx xy yy xz yz zz */) {
   const double tr = 0.5 * (m[0] + m[2] + m[5]);
   m[0] = 1.5 * m[0] - tr;
@@ -193,6 +264,37 @@ __device__ __forceinline__ void sph_pair(int lb, int mb, int lk, int mk, const d
       int ek[3];
       cart_exponents(lk, tk.c[j], ek);
       cart_pair_acc<GRAD>(eb, ek, ab, cb, npb, ak, ck, npk, v, tb.w[i] * tk.w[j], out, dout);
+    }
+  }
+  make_traceless(out + 4);
+  if (GRAD) {
+    make_traceless(dout[0] + 4);
+    make_traceless(dout[1] + 4);
+    make_traceless(dout[2] + 4);
+  }
+}
+
+// sph_pair with the primitive-pair factors of prim_pairs.
+template <bool GRAD>
+__device__ __forceinline__ void sph_pair_pp(int lb, int mb, int lk, int mk, const double* ab,
+                                            const double* cb, int npb, const double* ak,
+                                            const double* ck, int npk, const double v[3],
+                                            const PrimPairs& pp, double out[10],
+                                            double dout[3][10]) {
+#pragma unroll
+  for (int i = 0; i < 10; ++i) {
+    out[i] = 0.0;
+    if (GRAD) { dout[0][i] = 0.0; dout[1][i] = 0.0; dout[2][i] = 0.0; }
+  }
+  const SphTerms tb = sph_terms(lb, mb);
+  const SphTerms tk = sph_terms(lk, mk);
+  for (int i = 0; i < tb.n; ++i) {
+    int eb[3];
+    cart_exponents(lb, tb.c[i], eb);
+    for (int j = 0; j < tk.n; ++j) {
+      int ek[3];
+      cart_exponents(lk, tk.c[j], ek);
+      cart_pair_acc_pp<GRAD>(eb, ek, ab, cb, npb, ak, ck, npk, v, tb.w[i] * tk.w[j], pp, out, dout);
     }
   }
   make_traceless(out + 4);

@@ -74,6 +74,11 @@ __global__ void __launch_bounds__(128) k_force_pairs(ForceArgs f) {
       const double dspat = ps * (t.sh_shpoly[bs] * p2 + t.sh_shpoly[ks] * p1) * rr / (2.0 * r);
       const double fac = avg * spat;
       double bw = 0.0;
+      // the primitive-pair factors of this shell pair, shared by its 2l+1 x
+      // 2l'+1 function pairs (shells with more primitives recompute them)
+      const bool cached = npk * npb <= kPrimPairs;
+      PrimPairs pp;
+      if (cached) prim_pairs(ab, npb, ak, npk, v, pp);
       for (int ib = 0; ib < 2 * lb + 1; ++ib) {
         const int64_t row = t.sh_ao[bs] + ib;
         for (int ik = 0; ik < 2 * lk + 1; ++ik) {
@@ -81,7 +86,10 @@ __global__ void __launch_bounds__(128) k_force_pairs(ForceArgs f) {
           const double Pv = P[row * n + col];
           const double Wv = W[row * n + col];
           double val[10], dv[3][10];
-          sph_pair<true>(lb, ib, lk, ik, ab, cb, npb, ak, ck, npk, v, val, dv);
+          if (cached)
+            sph_pair_pp<true>(lb, ib, lk, ik, ab, cb, npb, ak, ck, npk, v, pp, val, dv);
+          else
+            sph_pair<true>(lb, ib, lk, ik, ab, cb, npb, ak, ck, npk, v, val, dv);
           const double S = val[0];
           bw += Pv * S;
           double sA = 2.0 * (Pv * fac - Wv) - Pv * (vb + vk);
