@@ -388,7 +388,7 @@ XTBLOOM_API xtbloom_status_t xtbloom_b200_context_set_execution(xtbloom_context_
  * so n is limited to 256 (INVALID_ARGUMENT beyond, before anything runs);
  * nothing in it has to start at zero.  Calls that overlap on one device race
  * on that array: serialise them.  The first call on each device looks the
- * array up (and may load the module): make it before any stream capture.
+ * array up (and may load the module), so it belongs in the caller's set-up.
  */
 XTBLOOM_API xtbloom_status_t xtbloom_b200_tridiag_eigenvectors_static(
     const double* diagonal, const double* offdiagonal, const double* eigenvalues, int32_t n,

@@ -19,8 +19,8 @@
 //     overwrite each other's work vectors.  Serialise them on one stream or
 //     with events.
 //   * The first call on each device resolves the scratch address
-//     (cudaGetSymbolAddress, which can load the module); make that first call
-//     before any stream capture begins.
+//     (cudaGetSymbolAddress, which can load the module), so it belongs in
+//     the caller's set-up.
 #include <cuda_runtime.h>
 
 #include <mutex>
