@@ -1412,7 +1412,8 @@ xtbloom_status_t Engine::compute(const ComputeRequest& req, std::string& error) 
         launch_tridiag_smem(gb, gb.list, bk.count, bk.max_n, st);
     };
     auto eigvals = [&](const Bucket& bk, cudaStream_t st) {
-      launch_eigvals(sub(bk), mode, kt, bk.count, bk.max_n, st);
+      // levels_needed: ceil(max(nel_a, nel_b)) + 8 = bk.max_m + 4
+      launch_eigvals(sub(bk), mode, kt, bk.count, bk.max_n, bk.max_m + 4, st);
     };
     auto invit = [&](const Bucket& bk, cudaStream_t st) {
       launch_inverse_iteration(sub(bk), bk.count, bk.max_n,

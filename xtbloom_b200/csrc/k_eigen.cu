@@ -1075,7 +1075,8 @@ __device__ void warp_fermi(const double* eps, int n, double nel, double kt, doub
 }
 
 __device__ void bisect_range(const double* d, const double* e2, int n, double glo, double ghi,
-                             double pivmin, int j0, int j1, double unscale, int tpe_max, double* ev);
+                             double pivmin, int j0, int j1, double unscale, int tpe_max,
+                             int tpe_block, double* ev);
 
 // Number of eigenvalues the SCC needs: the occupied levels and eight above
 // them (mode 0); all of them for the overlap (mode 1) and for an SCC
@@ -1146,8 +1147,12 @@ __global__ void __launch_bounds__(256) k_eigvals_part(EigArgs g, int mode, int p
   double* e2 = sm + n;
   double* red = sm + 2 * n;
   const ScaledTridiag t = load_scaled_tridiag(g, o, n, d, e2, red);
-  bisect_range(d, e2, n, t.glo, t.ghi, t.pivmin, j0, j1, t.unscale, 32, g.eig + o);
+  bisect_range(d, e2, n, t.glo, t.ghi, t.pivmin, j0, j1, t.unscale, 32, (int)blockDim.x, g.eig + o);
 }
+
+// The block size k_tridiag_eigvals chooses its threads per eigenvalue for
+// (bisect_range's tpe_block), whatever block it is launched with.
+constexpr int kEigvalsTpeBlock = 256;
 
 // mode 0: SCC (occupations, needed vectors); mode 1: all vectors, no
 // occupations; mode 2: SCC occupations from the whole spectrum.
@@ -1175,7 +1180,7 @@ __global__ void __launch_bounds__(256) k_tridiag_eigvals(EigArgs g, int mode, do
   if (have) {
     for (int j = tid; j < nk; j += bs) ev[j] = g.eig[o + j];
   } else {
-    bisect_range(d, e2, n, t.glo, t.ghi, t.pivmin, 0, nk, t.unscale, tpe_max, ev);
+    bisect_range(d, e2, n, t.glo, t.ghi, t.pivmin, 0, nk, t.unscale, tpe_max, kEigvalsTpeBlock, ev);
   }
   __syncthreads();
   if (mode == 1) {
@@ -1199,7 +1204,7 @@ __global__ void __launch_bounds__(256) k_tridiag_eigvals(EigArgs g, int mode, do
     }
     __syncthreads();
     if (!need_more) break;
-    bisect_range(d, e2, n, t.glo, t.ghi, t.pivmin, nk, n, t.unscale, 8, ev);
+    bisect_range(d, e2, n, t.glo, t.ghi, t.pivmin, nk, n, t.unscale, 8, kEigvalsTpeBlock, ev);
     nk = n;
     __syncthreads();
   }
@@ -1218,16 +1223,20 @@ __global__ void __launch_bounds__(256) k_tridiag_eigvals(EigArgs g, int mode, do
 }
 
 // Eigenvalues j0..j1-1 (ascending) of the scaled symmetric tridiagonal (d, e2)
-// by multisection.  A group of tpe threads (a power of two, as many as the
-// block has to spare, at most tpe_max <= 32) shares one eigenvalue: each thread evaluates
-// four interleaved Sturm sequences (sturm4), so a round cuts the interval into
-// 4 tpe + 1 parts.  Results are written unscaled (times `unscale`).
+// by multisection.  A group of tpe threads (a power of two, as many as a
+// block of tpe_block threads has to spare, at most tpe_max <= 32) shares one
+// eigenvalue: each thread evaluates four interleaved Sturm sequences
+// (sturm4), so a round cuts the interval into 4 tpe + 1 parts.  tpe fixes
+// every eigenvalue's sequence of brackets; the block's threads take the
+// eigenvalues in turn, so the results do not depend on the actual block
+// size.  Results are written unscaled (times `unscale`).
 __device__ void bisect_range(const double* d, const double* e2, int n, double glo, double ghi,
-                             double pivmin, int j0, int j1, double unscale, int tpe_max, double* ev) {
+                             double pivmin, int j0, int j1, double unscale, int tpe_max,
+                             int tpe_block, double* ev) {
   const int cnt = j1 - j0;
   if (cnt <= 0) return;
   int tpe = 1;
-  while (tpe < tpe_max && cnt * tpe * 2 <= (int)blockDim.x) tpe *= 2;
+  while (tpe < tpe_max && cnt * tpe * 2 <= tpe_block) tpe *= 2;
   const int r = threadIdx.x & (tpe - 1);
   const int lane = threadIdx.x & 31;
   const unsigned gmask = (tpe == 32 ? 0xffffffffu : ((1u << tpe) - 1u)) << (lane & ~(tpe - 1));
@@ -1915,17 +1924,22 @@ int sm_count() {
   return n;
 }
 
-void launch_eigvals(const EigArgs& g, int mode, double kt, int count, int max_n, cudaStream_t stream) {
+void launch_eigvals(const EigArgs& g, int mode, double kt, int count, int max_n, int max_levels,
+                    cudaStream_t stream) {
   if (count == 0) return;
   const int kNumSMs = sm_count();
   const size_t sm = (5 * (size_t)max_n + 40) * sizeof(double);
   const size_t cap = allow_max_dynamic_smem(k_tridiag_eigvals);
   (void)cap;
   // Enough systems to fill the GPU: one CTA each, one thread per eigenvalue
-  // (fewest Sturm sequences in total).  Few systems: spread each system's
+  // (fewest Sturm sequences in total), and in the SCC (mode 0) no more
+  // threads than the bucket's needed levels (at least the two Fermi warps),
+  // so that more systems share an SM.  Few systems: spread each system's
   // eigenvalues over several CTAs, up to a warp per eigenvalue (fewest rounds).
   if (count >= kNumSMs) {
-    k_tridiag_eigvals<<<count, 256, sm, stream>>>(g, mode, kt, 0, 1);
+    int threads = kEigvalsTpeBlock;
+    if (mode == 0) threads = std::max(64, std::min(kEigvalsTpeBlock, (std::min(max_levels, max_n) + 31) / 32 * 32));
+    k_tridiag_eigvals<<<count, threads, sm, stream>>>(g, mode, kt, 0, 1);
     return;
   }
   // Sturm steps are issue-bound: 128-thread parts (a warp per scheduler,

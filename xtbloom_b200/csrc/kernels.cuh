@@ -164,7 +164,10 @@ int tridiag_reg_max_n();
 void launch_tridiag_reg(const EigArgs& g, const int32_t* list, int count, int max_n, cudaStream_t stream);
 size_t tridiag_smem_bytes(int nl, int nt);
 int sm_count();   // multiprocessors of the current device (cached)
-void launch_eigvals(const EigArgs& g, int mode, double kt, int count, int max_n, cudaStream_t stream);
+// max_levels: the most eigenvalues a system of the launch needs in the SCC
+// (mode 0): its occupied levels and eight above them.
+void launch_eigvals(const EigArgs& g, int mode, double kt, int count, int max_n, int max_levels,
+                    cudaStream_t stream);
 void launch_inverse_iteration(const EigArgs& g, int count, int max_n, int want_m, double ortol_rel,
                               cudaStream_t stream);
 void launch_backtransform_rows(const EigArgs& g, int count, int max_n, int want_m, cudaStream_t stream);
