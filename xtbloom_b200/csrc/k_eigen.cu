@@ -516,9 +516,11 @@ __constant__ TileTable c_tile_table = make_tile_table();
 //       sit in a separate double-buffered array, because every thread reads
 //       them), w_r, the update of the block's first column with (v_i, w_i),
 //       the column's norm -> one barrier;
-//   (C) every thread forms alpha, beta, tau and the scale redundantly; the
-//       8 x 32 tiles of the rest are updated with (v_i, w_i) and multiplied
-//       by v_{i+1}; the warps' partials of p and p.v are posted -> one barrier.
+//   (C) every working thread (one with a row in (A), or in a warp with
+//       tiles) forms alpha, beta, tau and the scale redundantly; the 8 x 32
+//       tiles of the rest (indices from c_tile_table, dealt round-robin to
+//       the warps) are updated with (v_i, w_i) and multiplied by v_{i+1};
+//       the warps' partials of p and p.v are posted -> one barrier.
 // KIND (what the caller guarantees; the masks that then select nothing are
 // compiled out, the operations on the elements are the same):
 //   kTileFull  every row inside the block and the tile strictly below the
